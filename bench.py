@@ -1,0 +1,345 @@
+#!/usr/bin/env python
+"""Throughput of the Mixture-of-Grids force-and-step path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2|c1] [--impl ours|reference]
+
+Default workload (one GPU): the plain MOG step of the colliding-disk set,
+N = 1,048,576 particles, k = 240 grids of 16^3, G = 100, dt = 1e-5,
+damping 0.999 (seeded synthetic particles: two exponential disks with scale
+radius 8 and sech^2 height 0.5, centres 40 apart, relative speed 5).
+
+One JSON line is printed by rank 0.  ``value`` is particle-steps/s with
+particles resident in HBM (device time of K steps measured with CUDA events,
+L2 flushed between steps); ``e2e`` is the same metric through the public
+``Simulation.step`` call with the particles copied from pinned host memory
+and back every step.  Under torchrun (N > 1) every rank advances its own
+independent simulation of the same size (replicas; the step has no
+cross-GPU exchange in this mode) and the time is the maximum over ranks.
+
+``--impl reference`` times the reference's own shader code on the host cores
+(the GLSL compute shaders compiled as C++ by oracle/, OpenMP over all
+threads) on a bounded sample of the same workload; without that build it
+falls back to the C/NumPy restatement in oracle/.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "particle-steps/s at fixed RMS force error vs FP64 direct sum: learned k=32 vs plain k=240"
+UNIT = "particle-steps/s"
+
+WORKLOADS = {
+    "c2": dict(desc="plain MOG k=240 g=16, two colliding exponential disks, N=1,048,576",
+               n=1 << 20, k=240, g=16, L=100.0, G=100.0, dt=1e-5, damping=0.999, ic="disks",
+               seed=1),
+    "c1": dict(desc="plain MOG k=16 g=16, uniform cube, N=65,536",
+               n=1 << 16, k=16, g=16, L=100.0, G=100.0, dt=1e-5, damping=0.999, ic="uniform",
+               seed=0),
+}
+
+CLOCK_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+
+def phase_bytes(w: dict) -> dict:
+    """Algorithmic bytes per launch of each kernel.
+
+    deposit: position read (16 N) + one 4-byte cell update per (particle,
+    grid) (4 N k) + mass-grid write (4 k g^3); solve: mass read + 3 force
+    components written (16 k g^3); update: position and velocity read and
+    written (64 N) + one 12-byte force read per (particle, grid) (12 N k).
+    The whole step uses B = 64 N + 16 N k + 20 k g^3 (the deposit's
+    position read is counted once, inside the 64 N).
+    """
+    n, k, g3 = w["n"], w["k"], w["g"] ** 3
+    return {"deposit": 16 * n + 4 * n * k + 4 * k * g3,
+            "solve": 16 * k * g3,
+            "update": 64 * n + 12 * n * k,
+            "step": 64 * n + 16 * n * k + 20 * k * g3}
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def profiled_traffic(kernel: str, workload: str):
+    """DRAM bytes per launch from a committed ncu summary, if one exists."""
+    p = ROOT / "profiles" / f"traffic_{kernel}_{workload}.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("dram_bytes_per_launch:"):
+            return float(line.split(":", 1)[1])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={CLOCK_FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        return False
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_particles(w: dict, sim, seed_offset: int = 0):
+    from mog_solver_b200 import ics
+
+    n, L = w["n"], w["L"]
+    if w["ic"] == "disks":
+        return ics.two_disks(n, L, seed=w["seed"] + seed_offset, g_eff=sim.effective_g())
+    return ics.uniform_cube(n, L, seed=w["seed"] + seed_offset)
+
+
+def cpu_baseline(w: dict, budget_s: float = 20.0, steps: int | None = None) -> dict:
+    """Time the reference's CPU path on a bounded sample of the workload."""
+    import oracle.baseline as ob
+
+    return ob.time_reference(w, budget_s=budget_s, steps=steps)
+
+
+def run_reference(args, w: dict) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    res = cpu_baseline(w, budget_s=max(30.0, 3.0 * (args.steps + args.warmup)),
+                       steps=args.steps + args.warmup)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": res["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": {"workload": w["desc"], "n": w["n"], "k": w["k"], "g": w["g"],
+                   "sample_particles": res["sample_n"]},
+        "cpu_baseline": {"value": res["value"], "unit": UNIT, "cores": res["cores"],
+                         "kind": res["kind"], "sample": res["sample"]},
+        "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, w: dict) -> None:
+    import ctypes
+
+    import torch
+    import torch.distributed as dist
+
+    from mog_solver_b200 import Simulation, _lib
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+
+    cfg = {"n_grids": w["k"], "grid_size": w["g"], "world_size": w["L"], "num_particles": w["n"],
+           "G": w["G"], "dt": w["dt"], "damping": w["damping"], "solver": "fft", "seed": 0,
+           "index_mode": args.index_mode}
+    sim = Simulation(cfg, device=dev)
+    pos, vel = make_particles(w, sim, seed_offset=rank)
+    sim.set_particles(pos, vel)
+    n = sim.n_particles
+    lib = _lib.lib()
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    phase = (ctypes.c_float * 3)()
+    dt_eff = float(w["dt"])
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    torch.cuda.synchronize()  # particles were uploaded on the default stream
+
+    with torch.cuda.stream(stream):
+        h = sim.handle
+        sptr = ctypes.c_void_p(stream.cuda_stream)
+        for _ in range(args.warmup):
+            _lib.check(lib.mog_step(h, sim.pos.data_ptr(), sim.vel.data_ptr(), n, dt_eff, sptr),
+                       "warmup")
+        stream.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        step_ms, phases = [], []
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as clocks:
+            for _ in range(args.steps):
+                flush.zero_()  # evict L2 between timed steps
+                ev0.record(stream)
+                _lib.check(lib.mog_step_profiled(h, sim.pos.data_ptr(), sim.vel.data_ptr(), n,
+                                                 dt_eff, phase, sptr), "timed step")
+                ev1.record(stream)
+                ev1.synchronize()
+                step_ms.append(ev0.elapsed_time(ev1))
+                phases.append(list(phase))
+        torch.cuda.synchronize()
+        barrier()
+        sim.check()
+
+        # end to end through the public API, host buffers every step
+        host_pos = torch.empty((n, 4), dtype=torch.float32).pin_memory()
+        host_vel = torch.empty((n, 4), dtype=torch.float32).pin_memory()
+        host_pos.copy_(sim.pos)
+        host_vel.copy_(sim.vel)
+        torch.cuda.synchronize()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e2e_ms = []
+        for _ in range(args.steps):
+            flush.zero_()
+            e0.record(stream)
+            sim.pos.copy_(host_pos, non_blocking=True)
+            sim.vel.copy_(host_vel, non_blocking=True)
+            sim.step()
+            host_pos.copy_(sim.pos, non_blocking=True)
+            host_vel.copy_(sim.vel, non_blocking=True)
+            e1.record(stream)
+            e1.synchronize()
+            e2e_ms.append(e0.elapsed_time(e1))
+        barrier()
+
+    tot = torch.tensor([sum(step_ms), sum(e2e_ms)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(tot, op=dist.ReduceOp.MAX)
+    total_ms, total_e2e = float(tot[0]), float(tot[1])
+    value = n * world * args.steps / (total_ms / 1e3)
+    e2e = n * world * args.steps / (total_e2e / 1e3)
+    ph = np.array(phases)
+    mean_ph = ph.mean(axis=0)
+    names = ["deposit", "solve", "update"]
+    dom = int(np.argmax(mean_ph))
+    pb = phase_bytes(w)
+    peaks = measured_peaks()
+    achieved = pb[names[dom]] / (mean_ph[dom] / 1e3) / 1e9
+    step_gbs = pb["step"] / (float(np.mean(step_ms)) / 1e3) / 1e9
+    clk = clocks.summary()
+
+    if rank == 0:
+        base = None
+        if world == 1 and not args.no_cpu_baseline:
+            r = cpu_baseline(w)
+            base = {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": r["kind"],
+                    "sample": r["sample"]}
+        launches = 3 if w["g"] <= 16 else 10
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded two-disk set)"
+            if w["ic"] == "disks" else "synthetic (seeded uniform cube)",
+            "config": {"workload": w["desc"] + " (plain path; learned k=32 not in this line)",
+                       "n": w["n"], "k": w["k"], "g": w["g"], "G": w["G"], "dt": w["dt"],
+                       "damping": w["damping"], "index_mode": args.index_mode,
+                       "mass_mode": "u64 fixed point", "parallelism":
+                       "single GPU" if world == 1 else f"{world} independent replicas",
+                       "l2": "flushed between timed steps (256 MiB write)"},
+            "phase_ms": {nm: float(v) for nm, v in zip(names, mean_ph)},
+            "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved,
+                         "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
+                         "algorithmic_bytes": pb[names[dom]],
+                         "traffic": profiled_traffic(names[dom], args.workload),
+                         "step_achieved": step_gbs, "step_frac": step_gbs / peaks["hbm_gbs"]},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 2 * 16 * n,
+                    "d2h_bytes_per_step": 2 * 16 * n, "ms_per_step": total_e2e / args.steps},
+            "gpu_launches": launches * args.steps,
+            "clocks": clk,
+        }
+        if base is not None:
+            line["cpu_baseline"] = base
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--index-mode", default="fast", choices=["fast", "exact"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    w = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        run_reference(args, w)
+    else:
+        run_ours(args, w)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,184 @@
+/*
+ * mog.h — C ABI of the B200 (sm_100a) Mixture-of-Grids force-and-step library.
+ *
+ * The reference (tbmo/mog-solver) runs one particle-mesh gravity step as a
+ * sequence of GLSL compute dispatches issued from Python through moderngl
+ * (main.py:592-669).  Its state lives in GL buffers owned by the
+ * `Simulation` object.  This header is the drop-in boundary that replaces
+ * that pipeline: the caller owns the particle buffers (device memory,
+ * 16-byte float4 records exactly like the reference's std430 `vec4`
+ * SSBOs), the library owns the grids, spectra, tables and graphs.
+ *
+ * Conventions
+ *  - Every pointer named pos4 / vel4 / acc4 is device memory holding n
+ *    float4 records (x, y, z, w); pos.w is the particle mass, vel.w is 0
+ *    (update.glsl:88-89).
+ *  - `stream` is a cudaStream_t passed as void* (0 = legacy default stream).
+ *    All work is stream ordered; no entry point synchronises the host
+ *    except mog_create, mog_get_status, mog_step_profiled and
+ *    mog_diagnostics.
+ *  - Every entry point returns MOG_OK (0) or an error code; the text of the
+ *    last error on the calling thread is available from mog_last_error().
+ */
+#ifndef MOG_H
+#define MOG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes --------------------------------------------------- */
+#define MOG_OK              0
+#define MOG_ERR_CONFIG      1  /* invalid configuration value             */
+#define MOG_ERR_CUDA        2  /* a CUDA runtime call failed              */
+#define MOG_ERR_OVERFLOW    3  /* fixed-point mass total left u64 range   */
+#define MOG_ERR_NONFINITE   4  /* a particle position became NaN/Inf      */
+#define MOG_ERR_TIMEOUT     5  /* a bounded device wait gave up           */
+#define MOG_ERR_ARG         6  /* bad pointer / size argument             */
+#define MOG_ERR_UNSUPPORTED 7  /* combination not built (e.g. g > 64)     */
+
+/* ---- enumerations ----------------------------------------------------- */
+/* solver switch, config.yaml `solver: fft|convolution` (main.py:125-126)  */
+#define MOG_SOLVER_FFT          0
+#define MOG_SOLVER_CONVOLUTION  1
+/* mass fixed point: u64 with scale 2^scale_bits (deterministic, exact),  */
+/* or the reference's uint32(m*1000) truncation (mass.glsl:52-54)          */
+#define MOG_MASS_U64_FIXED      0
+#define MOG_MASS_U32_X1000      1
+/* cell-index arithmetic: FAST = floor((R^T c)/h + (L/2-off)/h) mod g with */
+/* a pre-scaled matrix and fused multiply-adds; EXACT = the shader's own   */
+/* op sequence (mass.glsl:42-50) with IEEE division and no contraction     */
+#define MOG_INDEX_FAST          0
+#define MOG_INDEX_EXACT         1
+/* spectral transform precision                                             */
+#define MOG_DFT_FFT32           0  /* FP32 radix-2 FFT in shared memory      */
+#define MOG_DFT_TC_BF16X3       1  /* DFT stages on tcgen05, bf16 hi+lo x3   */
+
+/* device status flag bits returned by mog_get_status */
+#define MOG_FLAG_NONFINITE  1u
+#define MOG_FLAG_OVERFLOW   2u
+#define MOG_FLAG_TIMEOUT    4u
+#define MOG_FLAG_BADMASS    8u
+
+/*
+ * Configuration.  Field names follow config.yaml (config.yaml:2-18) and
+ * the reference's parse (main.py:115-126); the last block holds the keys
+ * this library adds.
+ */
+typedef struct mog_config {
+    int32_t n_grids;        /* k  (config `n_grids`,  main.py:115)          */
+    int32_t grid_size;      /* g  (config `grid_size`, main.py:116); 2..64, power of 2 */
+    float   world_size;     /* L  (config `world_size`, main.py:117)        */
+    float   G;              /* config `G` (main.py:120)                     */
+    float   dt;             /* config `dt` (main.py:121)                    */
+    float   damping;        /* config `damping`, default 1.0 (main.py:667)  */
+    int32_t solver;         /* MOG_SOLVER_*                                 */
+    int32_t mass_mode;      /* MOG_MASS_*                                   */
+    int32_t scale_bits;     /* u64 mode: q = trunc(m * 2^scale_bits), 0..100 */
+    int32_t index_mode;     /* MOG_INDEX_*                                  */
+    int32_t dft_prec;       /* MOG_DFT_*                                    */
+    int32_t reserved0;
+    int64_t num_particles;  /* capacity: largest n passed to the step calls */
+} mog_config;
+
+typedef struct mog_handle mog_handle;
+
+/* Fill a config with the reference's in-code defaults (main.py:179-189). */
+int mog_config_default(mog_config* cfg);
+
+/*
+ * Create a solver.  rot12 is k x 12 floats, off4 is k x 4 floats, both in
+ * host memory, packed exactly as the reference's compute_transforms
+ * (main.py:157-172): rotations[i][4j..4j+2] = row j of the rotation
+ * matrix M_i, offsets[i][0..2] = offset of grid i.  Replaces
+ * Simulation.__init__ buffer/texture/shader set-up (main.py:191-248).
+ */
+int mog_create(const mog_config* cfg, const float* rot12, const float* off4,
+               mog_handle** out);
+
+/* Release every device resource of the handle. */
+int mog_destroy(mog_handle* h);
+
+/*
+ * One step: deposit -> spectral solve -> gather/rotate/average ->
+ * leapfrog with damping, in place on pos4/vel4.  Replaces
+ * Simulation.step / step_fft (main.py:592-672).  dt_eff is the step's
+ * deltaTime = dt * timescale (main.py:662); negative values run backwards.
+ */
+int mog_step(mog_handle* h, float* pos4, float* vel4, int64_t n,
+             float dt_eff, void* stream);
+
+/*
+ * n_steps steps replayed from a CUDA graph captured once per
+ * (pos4, vel4, n, dt_eff) combination.  Same result as n_steps calls of
+ * mog_step (the frame loop of main.py:674-676, without rendering).
+ */
+int mog_step_n(mog_handle* h, float* pos4, float* vel4, int64_t n,
+               float dt_eff, int32_t n_steps, void* stream);
+
+/*
+ * Ensemble-averaged force at every particle (the avgForce of
+ * update.glsl:81) without moving anything: acc4[p] = (Fx, Fy, Fz, 0).
+ * Used for accuracy measurements and by the learned correction.
+ */
+int mog_forces(mog_handle* h, const float* pos4, float* acc4, int64_t n,
+               void* stream);
+
+/*
+ * Stage entry points (parity testing and custom pipelines).
+ *
+ * mog_deposit: mass.glsl:27-55 into a caller buffer of k*g^3 cells
+ *   (uint64 in MOG_MASS_U64_FIXED mode, uint32 in MOG_MASS_U32_X1000 mode).
+ *   The buffer is zeroed first (main.py:558-562).
+ * mog_solve: complex.glsl + fft_batched.glsl + fourier.glsl + greens.glsl
+ *   + pack.glsl from a caller mass grid to a caller force grid of k*g^3
+ *   float4 (fx, fy, fz, |f|) in each grid's own frame (the reference's
+ *   gradient texture layout, pack.glsl:23-29).
+ * mog_update: update.glsl:53-89 from a caller force grid in that same
+ *   layout.
+ */
+int mog_deposit(mog_handle* h, const float* pos4, int64_t n, void* mass_out,
+                void* stream);
+int mog_solve(mog_handle* h, const void* mass_in, float* force4_out,
+              void* stream);
+int mog_update(mog_handle* h, float* pos4, float* vel4, int64_t n,
+               const float* force4_in, float dt_eff, void* stream);
+
+/*
+ * mog_step with CUDA events recorded on `stream` between its kernels;
+ * phase_ms[0..2] receive the device time of the deposit, the solve and the
+ * gather/update.  Synchronises the stream (measurement only).
+ */
+int mog_step_profiled(mog_handle* h, float* pos4, float* vel4, int64_t n,
+                      float dt_eff, float* phase_ms, void* stream);
+
+/*
+ * Reads (and clears) the device status word: OR of MOG_FLAG_* bits raised
+ * since the last call.  Synchronises the handle's work on `stream`.
+ */
+int mog_get_status(mog_handle* h, uint32_t* flags, void* stream);
+
+/*
+ * FP64 diagnostics of a particle set: out[0..2] = total momentum
+ * sum(m v), out[3] = kinetic energy sum(m |v|^2 / 2), out[4] = total
+ * mass, out[5..7] = centre of mass.  No counterpart in the reference,
+ * which prints nothing but its configuration (main.py:147-155).
+ */
+int mog_diagnostics(mog_handle* h, const float* pos4, const float* vel4,
+                    int64_t n, double* out8, void* stream);
+
+/* Human-readable text for a status code, and the calling thread's last
+ * error message. */
+const char* mog_strerror(int code);
+const char* mog_last_error(void);
+
+/* Library version string. */
+const char* mog_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MOG_H */

@@ -1,0 +1,136 @@
+"""ctypes bindings for libmog.so (the C ABI declared in include/mog.h).
+
+The library is loaded from this package directory.  There is no fallback:
+if it is missing or fails to load, every call raises ``MogLibraryError``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "libmog.so"
+
+# status codes (include/mog.h)
+MOG_OK = 0
+MOG_ERR_CONFIG = 1
+MOG_ERR_CUDA = 2
+MOG_ERR_OVERFLOW = 3
+MOG_ERR_NONFINITE = 4
+MOG_ERR_TIMEOUT = 5
+MOG_ERR_ARG = 6
+MOG_ERR_UNSUPPORTED = 7
+
+SOLVER_FFT = 0
+SOLVER_CONVOLUTION = 1
+MASS_U64_FIXED = 0
+MASS_U32_X1000 = 1
+INDEX_FAST = 0
+INDEX_EXACT = 1
+DFT_FFT32 = 0
+DFT_TC_BF16X3 = 1
+
+FLAG_NONFINITE = 1
+FLAG_OVERFLOW = 2
+FLAG_TIMEOUT = 4
+FLAG_BADMASS = 8
+
+# Every symbol include/mog.h declares.
+EXPORTS = (
+    "mog_config_default", "mog_create", "mog_destroy", "mog_step", "mog_step_n",
+    "mog_step_profiled", "mog_forces", "mog_deposit", "mog_solve", "mog_update", "mog_get_status",
+    "mog_diagnostics", "mog_strerror", "mog_last_error", "mog_version",
+)
+
+
+class MogLibraryError(RuntimeError):
+    """libmog.so is missing or could not be loaded."""
+
+
+class MogError(RuntimeError):
+    """A libmog call returned a non-zero status."""
+
+    def __init__(self, code: int, where: str, detail: str):
+        self.code = code
+        super().__init__(f"{where}: {detail} (status {code})")
+
+
+class MogConfigC(ctypes.Structure):
+    _fields_ = [
+        ("n_grids", ctypes.c_int32),
+        ("grid_size", ctypes.c_int32),
+        ("world_size", ctypes.c_float),
+        ("G", ctypes.c_float),
+        ("dt", ctypes.c_float),
+        ("damping", ctypes.c_float),
+        ("solver", ctypes.c_int32),
+        ("mass_mode", ctypes.c_int32),
+        ("scale_bits", ctypes.c_int32),
+        ("index_mode", ctypes.c_int32),
+        ("dft_prec", ctypes.c_int32),
+        ("reserved0", ctypes.c_int32),
+        ("num_particles", ctypes.c_int64),
+    ]
+
+
+_lib = None
+
+
+def _declare(lib: ctypes.CDLL) -> None:
+    P = ctypes.c_void_p
+    I64 = ctypes.c_int64
+    F = ctypes.c_float
+    I = ctypes.c_int
+    lib.mog_config_default.argtypes = [ctypes.POINTER(MogConfigC)]
+    lib.mog_create.argtypes = [ctypes.POINTER(MogConfigC), P, P, ctypes.POINTER(P)]
+    lib.mog_destroy.argtypes = [P]
+    lib.mog_step.argtypes = [P, P, P, I64, F, P]
+    lib.mog_step_n.argtypes = [P, P, P, I64, F, ctypes.c_int32, P]
+    lib.mog_step_profiled.argtypes = [P, P, P, I64, F, ctypes.POINTER(ctypes.c_float), P]
+    lib.mog_forces.argtypes = [P, P, P, I64, P]
+    lib.mog_deposit.argtypes = [P, P, I64, P, P]
+    lib.mog_solve.argtypes = [P, P, P, P]
+    lib.mog_update.argtypes = [P, P, P, I64, P, F, P]
+    lib.mog_get_status.argtypes = [P, ctypes.POINTER(ctypes.c_uint32), P]
+    lib.mog_diagnostics.argtypes = [P, P, P, I64, ctypes.POINTER(ctypes.c_double), P]
+    lib.mog_strerror.argtypes = [I]
+    lib.mog_strerror.restype = ctypes.c_char_p
+    lib.mog_last_error.argtypes = []
+    lib.mog_last_error.restype = ctypes.c_char_p
+    lib.mog_version.argtypes = []
+    lib.mog_version.restype = ctypes.c_char_p
+    for name in EXPORTS:
+        if name not in ("mog_strerror", "mog_last_error", "mog_version"):
+            getattr(lib, name).restype = ctypes.c_int
+
+
+def lib() -> ctypes.CDLL:
+    """Load libmog.so (once).  Raises MogLibraryError if it is not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = Path(os.environ.get("MOG_LIBRARY", LIB_PATH))
+    if not path.exists():
+        raise MogLibraryError(
+            f"{path} is not built; run `python -m mog_solver_b200.build` (CUDA is required, "
+            "there is no CPU fallback)")
+    try:
+        handle = ctypes.CDLL(str(path))
+    except OSError as exc:  # pragma: no cover - depends on the environment
+        raise MogLibraryError(f"cannot load {path}: {exc}") from exc
+    _declare(handle)
+    _lib = handle
+    return handle
+
+
+def check(code: int, where: str) -> None:
+    if code != MOG_OK:
+        detail = lib().mog_last_error().decode() or lib().mog_strerror(code).decode()
+        raise MogError(code, where, detail)
+
+
+def default_config() -> MogConfigC:
+    c = MogConfigC()
+    check(lib().mog_config_default(ctypes.byref(c)), "mog_config_default")
+    return c

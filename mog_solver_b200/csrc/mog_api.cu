@@ -1,0 +1,583 @@
+// mog_api.cu — the C ABI of include/mog.h.
+//
+// Replaces the reference's Simulation set-up and step orchestration
+// (main.py:108-248 for buffers, textures, shaders and transforms;
+// main.py:558-672 for clear_mass / step_fft / step).  The reference issues
+// a host upload of zeros plus about 65 dispatches with a memory barrier
+// after each (g = 16); one step here is three kernels on the caller's
+// stream (deposit, spectral solve, gather + update), and mog_step_n
+// replays a captured CUDA graph of that step.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/mog.h"
+#include "mog_internal.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+int cuda_fail(cudaError_t err, const char* where) {
+    std::string m = std::string(where) + ": " + cudaGetErrorName(err) + " (" +
+                    cudaGetErrorString(err) + ")";
+    return fail(MOG_ERR_CUDA, m);
+}
+
+#define MOG_CUDA(call, where)                          \
+    do {                                               \
+        cudaError_t err__ = (call);                    \
+        if (err__ != cudaSuccess) return cuda_fail(err__, where); \
+    } while (0)
+
+}  // namespace
+
+namespace mog {
+
+int num_sms() {
+    static int cached[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return 148;
+    if (cached[dev] == 0) {
+        int v = 0;
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0)
+            v = 148;
+        cached[dev] = v;
+    }
+    return cached[dev];
+}
+
+namespace {
+
+__global__ void check_total_kernel(Ensemble e) {
+    if (e.mass_mode == 0 && e.mass_total) {
+        if (*e.mass_total >= 18446744073709551616.0) atomicOr(e.flags, 2u);
+        *e.mass_total = 0.0;
+    }
+}
+
+// FP64 reductions: per-block partial sums, then a fixed-order final sum, so
+// the result does not depend on scheduling.
+__global__ void __launch_bounds__(256) diag_partial_kernel(const float4* __restrict__ pos,
+                                                           const float4* __restrict__ vel,
+                                                           int64_t n, double* __restrict__ partial) {
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+         p += (int64_t)gridDim.x * blockDim.x) {
+        const float4 P = pos[p];
+        const float4 V = vel[p];
+        const double m = P.w, vx = V.x, vy = V.y, vz = V.z;
+        acc[0] += m * vx;
+        acc[1] += m * vy;
+        acc[2] += m * vz;
+        acc[3] += 0.5 * m * (vx * vx + vy * vy + vz * vz);
+        acc[4] += m;
+        acc[5] += m * (double)P.x;
+        acc[6] += m * (double)P.y;
+        acc[7] += m * (double)P.z;
+    }
+    __shared__ double red[8][256];
+    for (int q = 0; q < 8; ++q) red[q][threadIdx.x] = acc[q];
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w)
+            for (int q = 0; q < 8; ++q) red[q][threadIdx.x] += red[q][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x < 8) partial[blockIdx.x * 8 + threadIdx.x] = red[threadIdx.x][0];
+}
+
+__global__ void diag_final_kernel(const double* __restrict__ partial, int nblocks,
+                                  double* __restrict__ out8) {
+    if (threadIdx.x != 0) return;
+    double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int b = 0; b < nblocks; ++b)
+        for (int q = 0; q < 8; ++q) s[q] += partial[b * 8 + q];
+    for (int q = 0; q < 5; ++q) out8[q] = s[q];
+    const double m = s[4];
+    for (int q = 0; q < 3; ++q) out8[5 + q] = m != 0.0 ? s[5 + q] / m : 0.0;
+}
+
+}  // namespace
+
+cudaError_t launch_diagnostics(const float4* pos, const float4* vel, int64_t n, double* partial,
+                               int nblocks, double* out8, cudaStream_t s) {
+    diag_partial_kernel<<<nblocks, 256, 0, s>>>(pos, vel, n, partial);
+    diag_final_kernel<<<1, 32, 0, s>>>(partial, nblocks, out8);
+    return cudaGetLastError();
+}
+
+}  // namespace mog
+
+struct GraphEntry {
+    float* pos = nullptr;
+    float* vel = nullptr;
+    int64_t n = 0;
+    float dt = 0.f;
+    cudaGraphExec_t exec = nullptr;
+};
+
+struct mog_handle {
+    mog_config cfg{};
+    int device = 0;
+    mog::Ensemble e;
+    mog::DepositShape dshape;
+    mog::UpdateShape ushape;
+    float* d_rot12 = nullptr;
+    float* d_off4 = nullptr;
+    mog::FastXf* d_fast = nullptr;
+    float* d_green = nullptr;
+    float* d_ktab = nullptr;
+    float4* d_conv = nullptr;
+    unsigned* d_flags = nullptr;
+    double* d_total = nullptr;
+    void* d_mass = nullptr;      // k g^3 (u64 or u32)
+    float4* d_force = nullptr;   // k g^3 world-frame forces
+    float4* d_force2 = nullptr;  // stage-update staging (lazy)
+    void* d_scratch = nullptr;   // spectral scratch (g >= 32)
+    double* d_diag = nullptr;    // diagnostics partials + result
+    std::vector<GraphEntry> graphs;
+};
+
+namespace {
+
+constexpr int kDiagBlocks = 296;
+
+bool is_pow2(int v) { return v > 0 && (v & (v - 1)) == 0; }
+
+int validate(const mog_config& c) {
+    if (c.n_grids <= 0) return fail(MOG_ERR_CONFIG, "n_grids must be positive");
+    if (c.n_grids > 4096) return fail(MOG_ERR_CONFIG, "n_grids must be <= 4096");
+    if (!is_pow2(c.grid_size) || c.grid_size < 2 || c.grid_size > 64)
+        return fail(MOG_ERR_CONFIG, "grid_size must be a power of two in [2, 64]");
+    if (!(std::isfinite(c.world_size) && c.world_size > 0.f))
+        return fail(MOG_ERR_CONFIG, "world_size must be finite and positive");
+    if (!std::isfinite(c.G)) return fail(MOG_ERR_CONFIG, "G must be finite");
+    if (!std::isfinite(c.dt)) return fail(MOG_ERR_CONFIG, "dt must be finite");
+    if (!std::isfinite(c.damping)) return fail(MOG_ERR_CONFIG, "damping must be finite");
+    if (c.solver != MOG_SOLVER_FFT && c.solver != MOG_SOLVER_CONVOLUTION)
+        return fail(MOG_ERR_CONFIG, "solver must be fft (0) or convolution (1)");
+    if (c.solver == MOG_SOLVER_CONVOLUTION && c.grid_size > 32)
+        return fail(MOG_ERR_UNSUPPORTED, "convolution solver supports grid_size <= 32");
+    if (c.mass_mode != MOG_MASS_U64_FIXED && c.mass_mode != MOG_MASS_U32_X1000)
+        return fail(MOG_ERR_CONFIG, "mass_mode must be 0 (u64 fixed) or 1 (u32 x1000)");
+    if (c.scale_bits < 0 || c.scale_bits > 100)
+        return fail(MOG_ERR_CONFIG, "scale_bits must be in [0, 100]");
+    if (c.index_mode != MOG_INDEX_FAST && c.index_mode != MOG_INDEX_EXACT)
+        return fail(MOG_ERR_CONFIG, "index_mode must be 0 (fast) or 1 (exact)");
+    if (c.dft_prec != MOG_DFT_FFT32 && c.dft_prec != MOG_DFT_TC_BF16X3)
+        return fail(MOG_ERR_CONFIG, "dft_prec must be 0 (fp32 fft) or 1 (tensor-core bf16x3)");
+    if (c.num_particles < 0) return fail(MOG_ERR_CONFIG, "num_particles must be >= 0");
+    return MOG_OK;
+}
+
+// Real-space kernel of init_greens_kernel (main.py:250-278), FP64 then f4,
+// same operation order so the table matches the reference's bit for bit.
+std::vector<float> conv_kernel_table(int g, double voxel) {
+    std::vector<float> k((size_t)g * g * g * 4, 0.f);
+    const double pi = 3.141592653589793;
+    for (int iz = 0; iz < g; ++iz)
+        for (int iy = 0; iy < g; ++iy)
+            for (int ix = 0; ix < g; ++ix) {
+                const int dx = ix <= g / 2 ? ix : ix - g;
+                const int dy = iy <= g / 2 ? iy : iy - g;
+                const int dz = iz <= g / 2 ? iz : iz - g;
+                const double rx = dx * voxel, ry = dy * voxel, rz = dz * voxel;
+                const double r2 = rx * rx + ry * ry + rz * rz;
+                const double r = std::sqrt(r2);
+                if (r > 1e-10) {
+                    const double f = 1.0 / (4.0 * pi * r2 * r);
+                    float* o = &k[(((size_t)iz * g + iy) * g + ix) * 4];
+                    o[0] = (float)(rx * f);
+                    o[1] = (float)(ry * f);
+                    o[2] = (float)(rz * f);
+                }
+            }
+    return k;
+}
+
+int set_device(mog_handle* h) {
+    int cur = -1;
+    MOG_CUDA(cudaGetDevice(&cur), "cudaGetDevice");
+    if (cur != h->device) MOG_CUDA(cudaSetDevice(h->device), "cudaSetDevice");
+    return MOG_OK;
+}
+
+int check_particles(mog_handle* h, const void* pos, const void* vel, int64_t n, bool need_vel) {
+    if (n < 0) return fail(MOG_ERR_ARG, "n must be >= 0");
+    if (n > 0 && !pos) return fail(MOG_ERR_ARG, "pos4 is null");
+    if (n > 0 && need_vel && !vel) return fail(MOG_ERR_ARG, "vel4 is null");
+    if (((uintptr_t)pos & 15) || ((uintptr_t)vel & 15))
+        return fail(MOG_ERR_ARG, "pos4/vel4 must be 16-byte aligned");
+    if (h->cfg.num_particles > 0 && n > h->cfg.num_particles)
+        return fail(MOG_ERR_ARG, "n exceeds the handle's num_particles capacity");
+    return MOG_OK;
+}
+
+// The three kernels of one step (or of a force evaluation when acc != null).
+int run_pipeline(mog_handle* h, float4* pos, float4* vel, int64_t n, float dt, float4* acc,
+                 cudaStream_t s) {
+    const mog::Ensemble& e = h->e;
+    cudaError_t err = mog::launch_deposit(e, pos, n, h->d_mass, h->dshape, s);
+    if (err != cudaSuccess) return cuda_fail(err, "deposit");
+    if (h->cfg.solver == MOG_SOLVER_FFT)
+        err = mog::launch_spectral(e, h->d_mass, h->d_force, true, true, h->d_scratch, s);
+    else
+        err = mog::launch_convolution(e, h->d_mass, h->d_force, true, true, s);
+    if (err != cudaSuccess) return cuda_fail(err, "solve");
+    err = mog::launch_update(e, pos, vel, n, h->d_force, dt, h->cfg.damping, acc, h->ushape, s);
+    if (err != cudaSuccess) return cuda_fail(err, "update");
+    return MOG_OK;
+}
+
+size_t mass_bytes(const mog_handle* h) {
+    return (size_t)h->e.cells() * (h->cfg.mass_mode == MOG_MASS_U64_FIXED ? 8 : 4);
+}
+
+void release(mog_handle* h) {
+    for (auto& g : h->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    h->graphs.clear();
+    void* ptrs[] = {h->d_rot12, h->d_off4, h->d_fast, h->d_green, h->d_ktab, h->d_conv,
+                    h->d_flags, h->d_total, h->d_mass, h->d_force, h->d_force2, h->d_scratch,
+                    h->d_diag};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+}
+
+}  // namespace
+
+extern "C" {
+
+int mog_config_default(mog_config* c) {
+    if (!c) return fail(MOG_ERR_ARG, "cfg is null");
+    std::memset(c, 0, sizeof(*c));
+    // main.py:179-189 (no config.yaml) and main.py:667 (damping default)
+    c->n_grids = 16;
+    c->grid_size = 16;
+    c->world_size = 100.0f;
+    c->G = 1.0f;
+    c->dt = 0.00001f;
+    c->damping = 1.0f;
+    c->solver = MOG_SOLVER_FFT;
+    c->mass_mode = MOG_MASS_U64_FIXED;
+    c->scale_bits = 32;
+    c->index_mode = MOG_INDEX_FAST;
+    c->dft_prec = MOG_DFT_FFT32;
+    c->num_particles = 100000;
+    return MOG_OK;
+}
+
+int mog_create(const mog_config* cfg, const float* rot12, const float* off4, mog_handle** out) {
+    if (!cfg || !rot12 || !off4 || !out) return fail(MOG_ERR_ARG, "null argument to mog_create");
+    *out = nullptr;
+    int rc = validate(*cfg);
+    if (rc) return rc;
+    if (cfg->dft_prec == MOG_DFT_TC_BF16X3)
+        return fail(MOG_ERR_UNSUPPORTED, "tensor-core DFT precision is not built in this library");
+    for (int i = 0; i < cfg->n_grids * 12; ++i)
+        if (!std::isfinite(rot12[i])) return fail(MOG_ERR_CONFIG, "rotation entries must be finite");
+    for (int i = 0; i < cfg->n_grids * 4; ++i)
+        if (!std::isfinite(off4[i])) return fail(MOG_ERR_CONFIG, "offset entries must be finite");
+
+    mog_handle* h = new mog_handle();
+    h->cfg = *cfg;
+    cudaGetDevice(&h->device);
+    const int k = cfg->n_grids, g = cfg->grid_size;
+    int lg = 0;
+    while ((1 << lg) < g) ++lg;
+    mog::Ensemble& e = h->e;
+    e.k = k;
+    e.g = g;
+    e.lg = lg;
+    e.mass_mode = cfg->mass_mode;
+    e.index_mode = cfg->index_mode;
+    e.world = cfg->world_size;
+    // voxel = world / grid in double, passed to the shaders as a float
+    // uniform (main.py:118, mass.glsl:17)
+    e.voxel = (float)((double)cfg->world_size / (double)g);
+    e.G = cfg->G;
+    e.scale = std::ldexp(1.0f, cfg->scale_bits);
+    e.inv_scale = std::ldexp(1.0f, -cfg->scale_bits);
+
+    // FAST-mode rows: t_r = sum_j (M[j][r] / h) c_j + (L/2 - off_r) / h
+    std::vector<mog::FastXf> fast(k);
+    const double hv = (double)e.voxel;
+    const double half_l = (double)(cfg->world_size * 0.5f);
+    for (int i = 0; i < k; ++i) {
+        const float* R = rot12 + 12 * i;
+        float* rows = reinterpret_cast<float*>(&fast[i]);
+        for (int r = 0; r < 3; ++r) {
+            for (int j = 0; j < 3; ++j) rows[4 * r + j] = (float)((double)R[4 * j + r] / hv);
+            rows[4 * r + 3] = (float)((half_l - (double)off4[4 * i + r]) / hv);
+        }
+    }
+    const size_t cells = (size_t)e.cells();
+    const size_t g3 = (size_t)g * g * g;
+    auto fail_free = [&](cudaError_t err, const char* where) {
+        release(h);
+        delete h;
+        return cuda_fail(err, where);
+    };
+#define ALLOC(ptr, bytes)                                                     \
+    do {                                                                      \
+        cudaError_t err__ = cudaMalloc((void**)&(ptr), (bytes));              \
+        if (err__ != cudaSuccess) return fail_free(err__, "cudaMalloc " #ptr); \
+    } while (0)
+    ALLOC(h->d_rot12, sizeof(float) * 12 * k);
+    ALLOC(h->d_off4, sizeof(float) * 4 * k);
+    ALLOC(h->d_fast, sizeof(mog::FastXf) * k);
+    ALLOC(h->d_green, sizeof(float) * g3);
+    ALLOC(h->d_ktab, sizeof(float) * g);
+    ALLOC(h->d_conv, sizeof(float4) * g3);
+    ALLOC(h->d_flags, sizeof(unsigned) * 4);
+    ALLOC(h->d_total, sizeof(double) * 2);
+    ALLOC(h->d_mass, cells * (cfg->mass_mode == MOG_MASS_U64_FIXED ? 8 : 4));
+    ALLOC(h->d_force, sizeof(float4) * cells);
+    ALLOC(h->d_diag, sizeof(double) * (kDiagBlocks * 8 + 8));
+    const size_t scratch = mog::spectral_scratch_bytes(e);
+    if (scratch) ALLOC(h->d_scratch, scratch);
+#undef ALLOC
+    cudaError_t err;
+    std::vector<float> convk = conv_kernel_table(g, hv);
+    if ((err = cudaMemcpy(h->d_rot12, rot12, sizeof(float) * 12 * k, cudaMemcpyHostToDevice)) ||
+        (err = cudaMemcpy(h->d_off4, off4, sizeof(float) * 4 * k, cudaMemcpyHostToDevice)) ||
+        (err = cudaMemcpy(h->d_fast, fast.data(), sizeof(mog::FastXf) * k, cudaMemcpyHostToDevice)) ||
+        (err = cudaMemcpy(h->d_conv, convk.data(), sizeof(float) * convk.size(), cudaMemcpyHostToDevice)) ||
+        (err = cudaMemset(h->d_flags, 0, sizeof(unsigned) * 4)) ||
+        (err = cudaMemset(h->d_total, 0, sizeof(double) * 2)) ||
+        (err = cudaMemset(h->d_mass, 0, mass_bytes(h))))
+        return fail_free(err, "mog_create upload");
+    e.rot12 = h->d_rot12;
+    e.off4 = h->d_off4;
+    e.fast = h->d_fast;
+    e.green = h->d_green;
+    e.ktab = h->d_ktab;
+    e.conv_kernel = h->d_conv;
+    e.flags = h->d_flags;
+    e.mass_total = h->d_total;
+    if ((err = mog::launch_build_tables(g, cfg->world_size, cfg->G, h->d_green, h->d_ktab, 0)) ||
+        (err = cudaDeviceSynchronize()))
+        return fail_free(err, "Green's table build");
+    *out = h;
+    return MOG_OK;
+}
+
+int mog_destroy(mog_handle* h) {
+    if (!h) return MOG_OK;
+    set_device(h);
+    release(h);
+    delete h;
+    return MOG_OK;
+}
+
+int mog_step(mog_handle* h, float* pos4, float* vel4, int64_t n, float dt_eff, void* stream) {
+    if (!h) return fail(MOG_ERR_ARG, "handle is null");
+    int rc = check_particles(h, pos4, vel4, n, true);
+    if (rc) return rc;
+    if (!std::isfinite(dt_eff)) return fail(MOG_ERR_ARG, "dt_eff must be finite");
+    if ((rc = set_device(h))) return rc;
+    return run_pipeline(h, reinterpret_cast<float4*>(pos4), reinterpret_cast<float4*>(vel4), n,
+                        dt_eff, nullptr, static_cast<cudaStream_t>(stream));
+}
+
+int mog_step_n(mog_handle* h, float* pos4, float* vel4, int64_t n, float dt_eff, int32_t n_steps,
+               void* stream) {
+    if (!h) return fail(MOG_ERR_ARG, "handle is null");
+    int rc = check_particles(h, pos4, vel4, n, true);
+    if (rc) return rc;
+    if (n_steps < 0) return fail(MOG_ERR_ARG, "n_steps must be >= 0");
+    if (!std::isfinite(dt_eff)) return fail(MOG_ERR_ARG, "dt_eff must be finite");
+    if ((rc = set_device(h))) return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (n_steps == 0 || n == 0) return MOG_OK;
+    // The legacy default stream cannot be captured: run the steps directly.
+    if (s == nullptr || s == cudaStreamLegacy) {
+        for (int i = 0; i < n_steps; ++i)
+            if ((rc = run_pipeline(h, reinterpret_cast<float4*>(pos4),
+                                   reinterpret_cast<float4*>(vel4), n, dt_eff, nullptr, s)))
+                return rc;
+        return MOG_OK;
+    }
+    GraphEntry* ge = nullptr;
+    for (auto& g : h->graphs)
+        if (g.pos == pos4 && g.vel == vel4 && g.n == n && g.dt == dt_eff) ge = &g;
+    if (!ge) {
+        cudaGraph_t graph = nullptr;
+        MOG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
+        rc = run_pipeline(h, reinterpret_cast<float4*>(pos4), reinterpret_cast<float4*>(vel4), n,
+                          dt_eff, nullptr, s);
+        cudaError_t end = cudaStreamEndCapture(s, &graph);
+        if (rc) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        if (end != cudaSuccess) return cuda_fail(end, "end capture");
+        GraphEntry entry;
+        entry.pos = pos4;
+        entry.vel = vel4;
+        entry.n = n;
+        entry.dt = dt_eff;
+        cudaError_t err = cudaGraphInstantiate(&entry.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (err != cudaSuccess) return cuda_fail(err, "graph instantiate");
+        if (h->graphs.size() >= 8) {
+            cudaGraphExecDestroy(h->graphs.front().exec);
+            h->graphs.erase(h->graphs.begin());
+        }
+        h->graphs.push_back(entry);
+        ge = &h->graphs.back();
+    }
+    for (int i = 0; i < n_steps; ++i) MOG_CUDA(cudaGraphLaunch(ge->exec, s), "graph launch");
+    return MOG_OK;
+}
+
+int mog_step_profiled(mog_handle* h, float* pos4, float* vel4, int64_t n, float dt_eff,
+                      float* phase_ms, void* stream) {
+    if (!h || !phase_ms) return fail(MOG_ERR_ARG, "null argument");
+    int rc = check_particles(h, pos4, vel4, n, true);
+    if (rc) return rc;
+    if (!std::isfinite(dt_eff)) return fail(MOG_ERR_ARG, "dt_eff must be finite");
+    if ((rc = set_device(h))) return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaEvent_t ev[4];
+    for (auto& e : ev) MOG_CUDA(cudaEventCreate(&e), "event create");
+    const mog::Ensemble& e = h->e;
+    float4* pos = reinterpret_cast<float4*>(pos4);
+    float4* vel = reinterpret_cast<float4*>(vel4);
+    cudaError_t err = cudaEventRecord(ev[0], s);
+    if (!err) err = mog::launch_deposit(e, pos, n, h->d_mass, h->dshape, s);
+    if (!err) err = cudaEventRecord(ev[1], s);
+    if (!err)
+        err = h->cfg.solver == MOG_SOLVER_FFT
+                  ? mog::launch_spectral(e, h->d_mass, h->d_force, true, true, h->d_scratch, s)
+                  : mog::launch_convolution(e, h->d_mass, h->d_force, true, true, s);
+    if (!err) err = cudaEventRecord(ev[2], s);
+    if (!err) err = mog::launch_update(e, pos, vel, n, h->d_force, dt_eff, h->cfg.damping, nullptr, h->ushape, s);
+    if (!err) err = cudaEventRecord(ev[3], s);
+    if (!err) err = cudaEventSynchronize(ev[3]);
+    for (int i = 0; i < 3 && !err; ++i) err = cudaEventElapsedTime(&phase_ms[i], ev[i], ev[i + 1]);
+    for (auto& x : ev) cudaEventDestroy(x);
+    if (err) return cuda_fail(err, "profiled step");
+    return MOG_OK;
+}
+
+int mog_forces(mog_handle* h, const float* pos4, float* acc4, int64_t n, void* stream) {
+    if (!h) return fail(MOG_ERR_ARG, "handle is null");
+    int rc = check_particles(h, pos4, acc4, n, true);
+    if (rc) return rc;
+    if ((rc = set_device(h))) return rc;
+    return run_pipeline(h, const_cast<float4*>(reinterpret_cast<const float4*>(pos4)), nullptr, n,
+                        0.f, reinterpret_cast<float4*>(acc4), static_cast<cudaStream_t>(stream));
+}
+
+int mog_deposit(mog_handle* h, const float* pos4, int64_t n, void* mass_out, void* stream) {
+    if (!h) return fail(MOG_ERR_ARG, "handle is null");
+    int rc = check_particles(h, pos4, nullptr, n, false);
+    if (rc) return rc;
+    if (!mass_out) return fail(MOG_ERR_ARG, "mass_out is null");
+    if ((rc = set_device(h))) return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    MOG_CUDA(cudaMemsetAsync(mass_out, 0, mass_bytes(h), s), "clear mass");
+    cudaError_t err =
+        mog::launch_deposit(h->e, reinterpret_cast<const float4*>(pos4), n, mass_out, h->dshape, s);
+    if (err != cudaSuccess) return cuda_fail(err, "deposit");
+    mog::check_total_kernel<<<1, 1, 0, s>>>(h->e);
+    MOG_CUDA(cudaGetLastError(), "check total");
+    return MOG_OK;
+}
+
+int mog_solve(mog_handle* h, const void* mass_in, float* force4_out, void* stream) {
+    if (!h) return fail(MOG_ERR_ARG, "handle is null");
+    if (!mass_in || !force4_out) return fail(MOG_ERR_ARG, "null buffer");
+    if ((uintptr_t)force4_out & 15) return fail(MOG_ERR_ARG, "force4_out must be 16-byte aligned");
+    int rc = set_device(h);
+    if (rc) return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaError_t err;
+    if (h->cfg.solver == MOG_SOLVER_FFT)
+        err = mog::launch_spectral(h->e, const_cast<void*>(mass_in),
+                                   reinterpret_cast<float4*>(force4_out), false, false,
+                                   h->d_scratch, s);
+    else
+        err = mog::launch_convolution(h->e, const_cast<void*>(mass_in),
+                                      reinterpret_cast<float4*>(force4_out), false, false, s);
+    if (err != cudaSuccess) return cuda_fail(err, "solve");
+    return MOG_OK;
+}
+
+int mog_update(mog_handle* h, float* pos4, float* vel4, int64_t n, const float* force4_in,
+               float dt_eff, void* stream) {
+    if (!h) return fail(MOG_ERR_ARG, "handle is null");
+    int rc = check_particles(h, pos4, vel4, n, true);
+    if (rc) return rc;
+    if (!force4_in) return fail(MOG_ERR_ARG, "force4_in is null");
+    if ((rc = set_device(h))) return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (!h->d_force2) MOG_CUDA(cudaMalloc((void**)&h->d_force2, sizeof(float4) * h->e.cells()), "cudaMalloc force2");
+    cudaError_t err = mog::launch_prerotate(h->e, reinterpret_cast<const float4*>(force4_in), h->d_force2, s);
+    if (err != cudaSuccess) return cuda_fail(err, "prerotate");
+    err = mog::launch_update(h->e, reinterpret_cast<float4*>(pos4), reinterpret_cast<float4*>(vel4), n,
+                             h->d_force2, dt_eff, h->cfg.damping, nullptr, h->ushape, s);
+    if (err != cudaSuccess) return cuda_fail(err, "update");
+    return MOG_OK;
+}
+
+int mog_get_status(mog_handle* h, uint32_t* flags, void* stream) {
+    if (!h || !flags) return fail(MOG_ERR_ARG, "null argument");
+    int rc = set_device(h);
+    if (rc) return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    unsigned v = 0;
+    MOG_CUDA(cudaMemcpyAsync(&v, h->d_flags, sizeof(unsigned), cudaMemcpyDeviceToHost, s), "read flags");
+    MOG_CUDA(cudaMemsetAsync(h->d_flags, 0, sizeof(unsigned), s), "clear flags");
+    MOG_CUDA(cudaStreamSynchronize(s), "sync");
+    *flags = v;
+    return MOG_OK;
+}
+
+int mog_diagnostics(mog_handle* h, const float* pos4, const float* vel4, int64_t n, double* out8,
+                    void* stream) {
+    if (!h || !out8) return fail(MOG_ERR_ARG, "null argument");
+    int rc = check_particles(h, pos4, vel4, n, true);
+    if (rc) return rc;
+    if ((rc = set_device(h))) return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    double* res = h->d_diag + kDiagBlocks * 8;
+    cudaError_t err = mog::launch_diagnostics(reinterpret_cast<const float4*>(pos4),
+                                              reinterpret_cast<const float4*>(vel4), n, h->d_diag,
+                                              kDiagBlocks, res, s);
+    if (err != cudaSuccess) return cuda_fail(err, "diagnostics");
+    MOG_CUDA(cudaMemcpyAsync(out8, res, 8 * sizeof(double), cudaMemcpyDeviceToHost, s), "read diagnostics");
+    MOG_CUDA(cudaStreamSynchronize(s), "sync");
+    return MOG_OK;
+}
+
+const char* mog_strerror(int code) {
+    switch (code) {
+        case MOG_OK: return "ok";
+        case MOG_ERR_CONFIG: return "invalid configuration";
+        case MOG_ERR_CUDA: return "CUDA error";
+        case MOG_ERR_OVERFLOW: return "fixed-point mass overflow";
+        case MOG_ERR_NONFINITE: return "non-finite particle state";
+        case MOG_ERR_TIMEOUT: return "bounded device wait timed out";
+        case MOG_ERR_ARG: return "invalid argument";
+        case MOG_ERR_UNSUPPORTED: return "unsupported configuration";
+        default: return "unknown status";
+    }
+}
+
+const char* mog_last_error(void) { return g_last_error.c_str(); }
+
+const char* mog_version(void) { return "mog-b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

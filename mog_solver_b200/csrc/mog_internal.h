@@ -1,0 +1,95 @@
+// mog_internal.h — host-side launcher interface between the C ABI layer
+// (mog_api.cu) and the kernel translation units.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "mog_device.cuh"
+
+namespace mog {
+
+// Everything about one grid ensemble that the kernels read.  All pointers
+// are device memory owned by the handle.
+struct Ensemble {
+    int k = 0;             // number of grids
+    int g = 0;             // cells per axis (power of two)
+    int lg = 0;            // log2 g
+    int mass_mode = 0;     // MOG_MASS_*
+    int index_mode = 0;    // MOG_INDEX_*
+    float world = 0.f;     // L
+    float voxel = 0.f;     // h
+    float G = 0.f;
+    float scale = 0.f;     // 2^scale_bits (u64 mode)
+    float inv_scale = 0.f; // 2^-scale_bits
+    const float* rot12 = nullptr;   // k x 12 (reference packing)
+    const float* off4 = nullptr;    // k x 4
+    const FastXf* fast = nullptr;   // k FAST-mode rows
+    const float* green = nullptr;   // g^3 Green's factors -2 pi G / k^2 (0 when k^2 <= 1e-4)
+    const float* ktab = nullptr;    // g wave numbers 2 pi shift(i) / L
+    const float4* conv_kernel = nullptr;  // g^3 real-space kernel r/(4 pi r^3) (main.py:250-278)
+    unsigned* flags = nullptr;      // device status word
+    double* mass_total = nullptr;   // running sum of q for the overflow check
+
+    __host__ __device__ int64_t cells() const { return (int64_t)k << (3 * lg); }
+    __host__ __device__ IndexParams index_params() const {
+        IndexParams ip;
+        ip.half_l = world * 0.5f;
+        ip.world = world;
+        ip.voxel = voxel;
+        ip.lg = lg;
+        return ip;
+    }
+};
+
+// Launch-shape knobs (chosen by the autotuner or by defaults).
+struct DepositShape {
+    int threads = 512;
+    int grids_per_cta = 0;  // 0 = default for (g, mass mode)
+    int chunks = 0;         // particle chunks; 0 = derived from n
+    int aggregate = 1;      // warp-aggregate equal-mass adds
+};
+struct UpdateShape {
+    int threads = 1024;
+    int staged = -1;        // -1 auto, 0 global gathers, 1 smem-staged grids
+    int ctas = 0;           // staged kernel CTAs; 0 = one per SM
+};
+
+int num_sms();
+
+// mass grid (u64 or u32 per mode) <- particles.  Zeroes nothing: the
+// caller provides a zeroed grid.
+cudaError_t launch_deposit(const Ensemble& e, const float4* pos, int64_t n, void* mass,
+                           const DepositShape& shape, cudaStream_t s);
+
+// force grid (float4 per cell) <- mass grid.  world_frame: rotate each
+// cell's force by M_i and store (x, y, z, 0) — what the production gather
+// reads; otherwise store (fx, fy, fz, |f|) in the grid's own frame (the
+// reference's gradient texture).  zero_mass clears the input for the next
+// step.  scratch: device memory of spectral_scratch_bytes(e) bytes.
+cudaError_t launch_spectral(const Ensemble& e, void* mass, float4* force, bool world_frame,
+                            bool zero_mass, void* scratch, cudaStream_t s);
+size_t spectral_scratch_bytes(const Ensemble& e);
+
+cudaError_t launch_convolution(const Ensemble& e, void* mass, float4* force, bool world_frame,
+                               bool zero_mass, cudaStream_t s);
+
+// Rotate a grid-frame force grid into the world frame (stage entry point).
+cudaError_t launch_prerotate(const Ensemble& e, const float4* force_grid, float4* force_world,
+                             cudaStream_t s);
+
+// Gather + average + (optionally) leapfrog.  When acc_out is non-null the
+// averaged force is written there and pos/vel are left untouched.
+cudaError_t launch_update(const Ensemble& e, float4* pos, float4* vel, int64_t n,
+                          const float4* force_world, float dt, float damping,
+                          float4* acc_out, const UpdateShape& shape, cudaStream_t s);
+
+// Green's-function and wave-number tables (FP64 arithmetic on the device).
+cudaError_t launch_build_tables(int g, float world, float G, float* green, float* ktab,
+                                cudaStream_t s);
+
+// FP64 momentum / energy / mass / centre-of-mass reduction.
+cudaError_t launch_diagnostics(const float4* pos, const float4* vel, int64_t n, double* partial,
+                               int nblocks, double* out8, cudaStream_t s);
+
+}  // namespace mog

@@ -1,0 +1,323 @@
+// update.cu — K3: force gather over all k grids, ensemble average and the
+// damped leapfrog update.
+//
+// Replaces update.glsl:53-89 (one thread per particle, k image loads and
+// k 3x3 transposed-rotation products).  Two changes make it cheap:
+//  * the spectral epilogue already stored every grid's force rotated back
+//    into the world frame (M_i F_i(cell), the very product update.glsl:77
+//    forms, with the same FP32 operations), so a (particle, grid) touch is
+//    one cell index + one float4 load + three adds;
+//  * for large particle counts each CTA stages grid i's whole force field
+//    (g^3 float4, 64 KB at g = 16) in shared memory with one bulk async
+//    copy (cp.async.bulk + mbarrier), three stages deep, and every
+//    particle the CTA owns gathers from shared memory.  The per-particle
+//    state (centred position, running force) stays in registers across all
+//    k grids, so HBM sees each particle once for reading and once for
+//    writing.
+// The force accumulates grid by grid in index order, like the shader's
+// loop, so the result is bit-identical to a sequential FP32 evaluation.
+#include <algorithm>
+
+#include "mog_internal.h"
+
+namespace mog {
+
+namespace {
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_fence_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes,
+                                         uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: gives up after ~2^31 SM cycles (about a second) and
+// reports false; the caller then abandons the launch with MOG_FLAG_TIMEOUT.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity)) {
+        if (clock64() - t0 > (1ll << 31)) return false;
+    }
+    return true;
+}
+
+// Shared epilogue: average, then update.glsl:81-89 with IEEE ops.
+template <bool ACC_OUT>
+__device__ __forceinline__ void finish_particle(int64_t p, float4 P, float ax, float ay, float az,
+                                                float4* __restrict__ pos, float4* __restrict__ vel,
+                                                float4* __restrict__ acc_out, float kf, float dt,
+                                                float damp, float world, unsigned& bad) {
+    ax = __fdiv_rn(ax, kf);
+    ay = __fdiv_rn(ay, kf);
+    az = __fdiv_rn(az, kf);
+    if (ACC_OUT) {
+        acc_out[p] = make_float4(ax, ay, az, 0.f);
+        return;
+    }
+    const float4 V = vel[p];
+    float vx = __fsub_rn(V.x, __fmul_rn(ax, dt));
+    float vy = __fsub_rn(V.y, __fmul_rn(ay, dt));
+    float vz = __fsub_rn(V.z, __fmul_rn(az, dt));
+    vx = __fmul_rn(vx, damp);
+    vy = __fmul_rn(vy, damp);
+    vz = __fmul_rn(vz, damp);
+    float px = glsl_mod(__fadd_rn(P.x, __fmul_rn(vx, dt)), world);
+    float py = glsl_mod(__fadd_rn(P.y, __fmul_rn(vy, dt)), world);
+    float pz = glsl_mod(__fadd_rn(P.z, __fmul_rn(vz, dt)), world);
+    if (!(isfinite(px) && isfinite(py) && isfinite(pz))) bad |= 1u;
+    pos[p] = make_float4(px, py, pz, P.w);
+    vel[p] = make_float4(vx, vy, vz, 0.f);
+}
+
+__device__ __forceinline__ uint32_t cell_of(int idx_mode, const float* xf, float cx, float cy,
+                                            float cz, const IndexParams& ip) {
+    if (idx_mode == 0) {
+        const float4* r = reinterpret_cast<const float4*>(xf);
+        return cell_fast(r[0], r[1], r[2], cx, cy, cz, ip.lg);
+    }
+    return cell_exact(xf, xf + 12, cx, cy, cz, ip);
+}
+
+// Staged gather.  Launch: one CTA per SM (smem-bound), `threads` threads,
+// each thread owning up to PPT particles p = lo + tid + j * threads.
+template <int IDX, int PPT, bool ACC_OUT>
+__global__ void __launch_bounds__(512, 1)
+    update_staged_kernel(float4* __restrict__ pos, float4* __restrict__ vel, int64_t n,
+                         int64_t per_cta, const float4* __restrict__ W, Ensemble e, float dt,
+                         float damp, float4* __restrict__ acc_out, int nstage) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int G3 = 1 << (3 * e.lg);
+    const unsigned grid_bytes = (unsigned)G3 * 16u;
+    float4* stage = reinterpret_cast<float4*>(smem);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + (size_t)nstage * grid_bytes);
+    float* xf = reinterpret_cast<float*>(full + 8);
+    __shared__ int abort_flag;
+
+    const int tid = threadIdx.x;
+    const int T = blockDim.x;
+    if (tid == 0) {
+        abort_flag = 0;
+        for (int s = 0; s < nstage; ++s) mbar_init(full + s, 1);
+        mbar_fence_init();
+    }
+    for (int i = tid; i < e.k * 16; i += T) {
+        const int j = i >> 4, w = i & 15;
+        float v;
+        if (IDX == 0)
+            v = (w < 12) ? reinterpret_cast<const float*>(e.fast + j)[w] : 0.f;
+        else
+            v = (w < 12) ? e.rot12[j * 12 + w] : e.off4[j * 4 + (w - 12)];
+        xf[i] = v;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        for (int s = 0; s < nstage && s < e.k; ++s) {
+            mbar_expect_tx(full + s, grid_bytes);
+            bulk_g2s(stage + (size_t)s * G3, W + (size_t)s * G3, grid_bytes, full + s);
+        }
+    }
+
+    const IndexParams ip = e.index_params();
+    const int64_t lo = (int64_t)blockIdx.x * per_cta;
+    const int64_t hi = min(n, lo + per_cta);
+    float cx[PPT], cy[PPT], cz[PPT], ax[PPT], ay[PPT], az[PPT];
+#pragma unroll
+    for (int j = 0; j < PPT; ++j) {
+        const int64_t p = lo + tid + (int64_t)j * T;
+        float4 P = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (p < hi) P = pos[p];
+        cx[j] = __fsub_rn(P.x, ip.half_l);
+        cy[j] = __fsub_rn(P.y, ip.half_l);
+        cz[j] = __fsub_rn(P.z, ip.half_l);
+        ax[j] = ay[j] = az[j] = 0.f;
+    }
+    // number of particle slots of this thread that are in range
+    const int64_t mine = hi - lo - tid;
+    const int64_t slots = (mine + T - 1) / T;
+    const int cnt = mine <= 0 ? 0 : (int)(slots < PPT ? slots : PPT);
+
+    int i_abort = -1;
+    for (int i = 0; i < e.k; ++i) {
+        const int s = i % nstage;
+        const unsigned parity = (unsigned)((i / nstage) & 1);
+        if (!mbar_wait_bounded(full + s, parity)) abort_flag = 1;
+        const float4* F = stage + (size_t)s * G3;
+        const float* x = xf + i * 16;
+#pragma unroll
+        for (int j = 0; j < PPT; ++j) {
+            if (j < cnt) {
+                const uint32_t c = cell_of(IDX, x, cx[j], cy[j], cz[j], ip);
+                const float4 f = F[c];
+                ax[j] = __fadd_rn(ax[j], f.x);
+                ay[j] = __fadd_rn(ay[j], f.y);
+                az[j] = __fadd_rn(az[j], f.z);
+            }
+        }
+        __syncthreads();
+        if (abort_flag) {
+            i_abort = i;
+            break;
+        }
+        if (tid == 0 && i + nstage < e.k) {
+            mbar_expect_tx(full + s, grid_bytes);
+            bulk_g2s(stage + (size_t)s * G3, W + (size_t)(i + nstage) * G3, grid_bytes, full + s);
+        }
+    }
+    if (i_abort >= 0) {
+        // Copies for grids i_abort .. i_abort + nstage - 1 may still be in
+        // flight: let them land (bounded as well) before the CTA's shared
+        // memory is released, then report and leave.
+        if (tid == 0) {
+            atomicOr(e.flags, 4u);
+            for (int j = i_abort; j < i_abort + nstage && j < e.k; ++j)
+                (void)mbar_wait_bounded(full + (j % nstage), (unsigned)((j / nstage) & 1));
+        }
+        return;
+    }
+
+    unsigned bad = 0;
+    const float kf = (float)e.k;
+#pragma unroll
+    for (int j = 0; j < PPT; ++j) {
+        if (j < cnt) {
+            const int64_t p = lo + tid + (int64_t)j * T;
+            const float4 P = pos[p];
+            finish_particle<ACC_OUT>(p, P, ax[j], ay[j], az[j], pos, vel, acc_out, kf, dt, damp,
+                                     e.world, bad);
+        }
+    }
+    if (bad) raise_flags(e.flags, bad);
+}
+
+// Direct gather from L2: one thread per particle, any g.
+template <int IDX, bool ACC_OUT>
+__global__ void __launch_bounds__(256) update_direct_kernel(float4* __restrict__ pos,
+                                                            float4* __restrict__ vel, int64_t n,
+                                                            const float4* __restrict__ W,
+                                                            Ensemble e, float dt, float damp,
+                                                            float4* __restrict__ acc_out) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const IndexParams ip = e.index_params();
+    const float4 P = pos[p];
+    const float cx = __fsub_rn(P.x, ip.half_l);
+    const float cy = __fsub_rn(P.y, ip.half_l);
+    const float cz = __fsub_rn(P.z, ip.half_l);
+    const int G3 = 1 << (3 * e.lg);
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    for (int i = 0; i < e.k; ++i) {
+        uint32_t c;
+        if (IDX == 0) {
+            const FastXf f = e.fast[i];
+            c = cell_fast(f.row[0], f.row[1], f.row[2], cx, cy, cz, ip.lg);
+        } else {
+            c = cell_exact(e.rot12 + 12 * i, e.off4 + 4 * i, cx, cy, cz, ip);
+        }
+        const float4 f = __ldg(W + (size_t)i * G3 + c);
+        ax = __fadd_rn(ax, f.x);
+        ay = __fadd_rn(ay, f.y);
+        az = __fadd_rn(az, f.z);
+    }
+    unsigned bad = 0;
+    finish_particle<ACC_OUT>(p, P, ax, ay, az, pos, vel, acc_out, (float)e.k, dt, damp, e.world,
+                             bad);
+    if (bad) raise_flags(e.flags, bad);
+}
+
+template <int IDX, int PPT, bool ACC>
+cudaError_t launch_staged(const Ensemble& e, float4* pos, float4* vel, int64_t n,
+                          const float4* W, float dt, float damp, float4* acc, int ctas,
+                          int threads, int nstage, size_t smem, cudaStream_t s) {
+    auto kern = update_staged_kernel<IDX, PPT, ACC>;
+    cudaError_t err =
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return err;
+    const int64_t per_cta = (n + ctas - 1) / ctas;
+    kern<<<ctas, threads, smem, s>>>(pos, vel, n, per_cta, W, e, dt, damp, acc, nstage);
+    return cudaGetLastError();
+}
+
+template <int IDX, bool ACC>
+cudaError_t update_mode(const Ensemble& e, float4* pos, float4* vel, int64_t n, const float4* W,
+                        float dt, float damp, float4* acc, const UpdateShape& sh, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    const size_t grid_bytes = (size_t)16 << (3 * e.lg);
+    const int sms = num_sms();
+    const int threads = 512;
+    const int nstage = 3;
+    const size_t smem = nstage * grid_bytes + 8 * sizeof(uint64_t) + (size_t)e.k * 16 * sizeof(float);
+    bool staged;
+    if (sh.staged >= 0)
+        staged = sh.staged != 0;
+    else
+        staged = e.g <= 16 && n >= (int64_t)sms * threads * 2 && smem <= 220 * 1024;
+    if (staged && smem > 220 * 1024) staged = false;
+    if (!staged) {
+        const int64_t blocks = (n + 255) / 256;
+        update_direct_kernel<IDX, ACC><<<(unsigned)blocks, 256, 0, s>>>(pos, vel, n, W, e, dt,
+                                                                         damp, acc);
+        return cudaGetLastError();
+    }
+    // Enough CTAs that PPT (particles per thread) stays within the template.
+    int ctas = sh.ctas > 0 ? sh.ctas : sms;
+    const int64_t per_thread = (n + (int64_t)ctas * threads - 1) / ((int64_t)ctas * threads);
+    if (per_thread > 16) ctas = (int)((n + 16LL * threads - 1) / (16LL * threads));
+    const int64_t ppt = (n + (int64_t)ctas * threads - 1) / ((int64_t)ctas * threads);
+    if (ppt <= 4)
+        return launch_staged<IDX, 4, ACC>(e, pos, vel, n, W, dt, damp, acc, ctas, threads, nstage,
+                                          smem, s);
+    if (ppt <= 8)
+        return launch_staged<IDX, 8, ACC>(e, pos, vel, n, W, dt, damp, acc, ctas, threads, nstage,
+                                          smem, s);
+    if (ppt <= 12)
+        return launch_staged<IDX, 12, ACC>(e, pos, vel, n, W, dt, damp, acc, ctas, threads, nstage,
+                                           smem, s);
+    if (ppt <= 14)
+        return launch_staged<IDX, 14, ACC>(e, pos, vel, n, W, dt, damp, acc, ctas, threads, nstage,
+                                           smem, s);
+    return launch_staged<IDX, 16, ACC>(e, pos, vel, n, W, dt, damp, acc, ctas, threads, nstage,
+                                       smem, s);
+}
+
+}  // namespace
+
+cudaError_t launch_update(const Ensemble& e, float4* pos, float4* vel, int64_t n,
+                          const float4* force_world, float dt, float damping, float4* acc_out,
+                          const UpdateShape& shape, cudaStream_t s) {
+    if (acc_out) {
+        return e.index_mode == 0
+                   ? update_mode<0, true>(e, pos, vel, n, force_world, dt, damping, acc_out, shape, s)
+                   : update_mode<1, true>(e, pos, vel, n, force_world, dt, damping, acc_out, shape, s);
+    }
+    return e.index_mode == 0
+               ? update_mode<0, false>(e, pos, vel, n, force_world, dt, damping, nullptr, shape, s)
+               : update_mode<1, false>(e, pos, vel, n, force_world, dt, damping, nullptr, shape, s);
+}
+
+}  // namespace mog

@@ -1,0 +1,129 @@
+"""Seeded synthetic particle sets (host-side numpy, float32 (N, 4) records).
+
+The reference initialises particles with a GPU Perlin/fBm rejection sampler
+(init_particles.glsl, driven from main.py:280-310) or an unseeded two-galaxy
+numpy routine (main.py:312-357).  The benchmark workloads of this library
+use their own seeded distributions instead:
+
+* ``uniform_cube``    positions U[0, L)^3, zero velocity;
+* ``two_disks``       two exponential disks (scale radius R_d, sech^2 scale
+                      height z0) with circular velocities from the enclosed
+                      mass, centres ``sep`` apart along x, approaching with
+                      relative speed ``v_rel``;
+* ``plummer``         a Plummer sphere of scale radius a, at rest;
+* ``clumps``          a Gaussian mixture (log-uniform widths) plus a uniform
+                      background fraction.
+
+Every record is (x, y, z, m) for positions and (vx, vy, vz, 0) for
+velocities, the std430 vec4 layout of the reference's buffers
+(main.py:192-193, update.glsl:3-4).  Masses are ``total_mass / N``.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def _records(xyz: np.ndarray, m: float, vel: np.ndarray | None = None):
+    n = xyz.shape[0]
+    pos = np.empty((n, 4), dtype=np.float32)
+    pos[:, :3] = xyz
+    pos[:, 3] = np.float32(m)
+    v = np.zeros((n, 4), dtype=np.float32)
+    if vel is not None:
+        v[:, :3] = vel
+    return pos, v
+
+
+def wrap(xyz: np.ndarray, world: float) -> np.ndarray:
+    return np.mod(xyz, world).astype(np.float32)
+
+
+def uniform_cube(n: int, world: float = 100.0, seed: int = 0, total_mass: float = 1.0):
+    rng = np.random.default_rng(seed)
+    xyz = rng.uniform(0.0, world, (n, 3)).astype(np.float32)
+    xyz = np.minimum(xyz, np.nextafter(np.float32(world), np.float32(0)))
+    return _records(xyz, total_mass / n if n else 0.0)
+
+
+def _exp_disk(rng, n: int, r_d: float, z0: float, r_max: float):
+    # Surface density ~ exp(-R/R_d): R ~ Gamma(2, R_d); truncated at r_max.
+    r = rng.gamma(2.0, r_d, size=n)
+    bad = r > r_max
+    while bad.any():
+        r[bad] = rng.gamma(2.0, r_d, size=int(bad.sum()))
+        bad = r > r_max
+    phi = rng.uniform(0.0, 2 * np.pi, n)
+    # sech^2(z/z0) profile: CDF (1 + tanh(z/z0)) / 2
+    u = rng.uniform(1e-7, 1 - 1e-7, n)
+    z = z0 * np.arctanh(2 * u - 1)
+    z = np.clip(z, -10 * z0, 10 * z0)
+    return r, phi, z
+
+
+def two_disks(n: int, world: float = 100.0, seed: int = 1, r_d: float = 8.0, z0: float = 0.5,
+              sep: float = 40.0, v_rel: float = 5.0, g_eff: float = 1.0, total_mass: float = 1.0,
+              r_max: float = 18.0):
+    """Two colliding exponential disks.
+
+    ``g_eff`` is the gravitational constant in the units of the solver's
+    acceleration (for the reference's normalisation: G * h^3 / 2, see
+    ``Simulation.effective_g``); circular speeds are sqrt(g_eff M(<R) / R)
+    with M(<R) the disk mass inside cylindrical radius R.
+    """
+    rng = np.random.default_rng(seed)
+    n_a = n // 2
+    n_b = n - n_a
+    c = world / 2.0
+    centres = [np.array([c - sep / 2, c, c]), np.array([c + sep / 2, c, c])]
+    bulk = [np.array([v_rel / 2, 0.0, 0.0]), np.array([-v_rel / 2, 0.0, 0.0])]
+    # disk normals: the second disk is tilted 30 degrees about x
+    t = np.radians(30.0)
+    frames = [np.eye(3), np.array([[1, 0, 0], [0, np.cos(t), -np.sin(t)], [0, np.sin(t), np.cos(t)]])]
+    m_disk = [total_mass * n_a / n, total_mass * n_b / n]
+    xs, vs = [], []
+    for count, centre, vb, frame, md in zip((n_a, n_b), centres, bulk, frames, m_disk):
+        r, phi, z = _exp_disk(rng, count, r_d, z0, r_max)
+        order = np.argsort(r)
+        enclosed = np.empty(count)
+        enclosed[order] = (np.arange(count) + 1) * (md / count)
+        vc = np.sqrt(g_eff * enclosed / np.maximum(r, 1e-3))
+        local = np.stack([r * np.cos(phi), r * np.sin(phi), z], axis=1)
+        lv = np.stack([-vc * np.sin(phi), vc * np.cos(phi), np.zeros(count)], axis=1)
+        xs.append(local @ frame.T + centre)
+        vs.append(lv @ frame.T + vb)
+    xyz = wrap(np.concatenate(xs), world)
+    vel = np.concatenate(vs).astype(np.float32)
+    return _records(xyz, total_mass / n, vel)
+
+
+def plummer(n: int, world: float = 100.0, seed: int = 0, a: float = 5.0,
+            total_mass: float = 1.0, r_max: float | None = None):
+    rng = np.random.default_rng(seed)
+    r_max = world * 0.45 if r_max is None else r_max
+    out = np.empty((0, 3))
+    while out.shape[0] < n:
+        m = n - out.shape[0]
+        u = rng.uniform(1e-9, 1.0, m)
+        r = a / np.sqrt(u ** (-2.0 / 3.0) - 1.0)
+        d = rng.normal(size=(m, 3))
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        pts = d * r[:, None]
+        out = np.concatenate([out, pts[r <= r_max]])
+    xyz = wrap(out[:n] + world / 2.0, world)
+    return _records(xyz, total_mass / n)
+
+
+def clumps(n: int, world: float = 100.0, seed: int = 100, n_clumps: int = 20,
+           sigma_range: tuple[float, float] = (1.0, 8.0), background: float = 0.1,
+           total_mass: float = 1.0):
+    rng = np.random.default_rng(seed)
+    n_bg = int(round(background * n))
+    n_cl = n - n_bg
+    centres = rng.uniform(0.15 * world, 0.85 * world, (n_clumps, 3))
+    sig = np.exp(rng.uniform(np.log(sigma_range[0]), np.log(sigma_range[1]), n_clumps))
+    which = rng.integers(0, n_clumps, n_cl)
+    pts = centres[which] + rng.normal(size=(n_cl, 3)) * sig[which, None]
+    bg = rng.uniform(0.0, world, (n_bg, 3))
+    xyz = wrap(np.concatenate([pts, bg]), world)
+    xyz = xyz[rng.permutation(n)]
+    return _records(xyz, total_mass / n)
