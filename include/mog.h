@@ -56,6 +56,14 @@ extern "C" {
 #define MOG_DFT_FFT32           0  /* FP32 radix-2 FFT in shared memory      */
 #define MOG_DFT_TC_BF16X3       1  /* DFT stages on tcgen05, bf16 hi+lo x3   */
 
+/* compatibility flags (mog_config.compat_flags) */
+/* Reproduce the reference's texture aliasing in run_fft_3d_batched        */
+/* (main.py:564-590, 638-646): when 3 (log2 g + 1) is odd (g = 4, 16, 64)  */
+/* the z inverse transform reuses the texture holding the finished x       */
+/* result, so pack.glsl reads the z-gradient as the x force.  Off by       */
+/* default: the library computes the gradient the shaders intend.          */
+#define MOG_COMPAT_FFT_TEXTURE_ALIAS 1
+
 /* device status flag bits returned by mog_get_status */
 #define MOG_FLAG_NONFINITE  1u
 #define MOG_FLAG_OVERFLOW   2u
@@ -79,11 +87,27 @@ typedef struct mog_config {
     int32_t scale_bits;     /* u64 mode: q = trunc(m * 2^scale_bits), 0..100 */
     int32_t index_mode;     /* MOG_INDEX_*                                  */
     int32_t dft_prec;       /* MOG_DFT_*                                    */
-    int32_t reserved0;
+    int32_t compat_flags;   /* MOG_COMPAT_* bits                            */
     int64_t num_particles;  /* capacity: largest n passed to the step calls */
 } mog_config;
 
 typedef struct mog_handle mog_handle;
+
+/*
+ * Launch-shape knobs: the interface of the project's autotuner
+ * (mog_solver_b200/autotune.py).  No counterpart in the reference, whose
+ * dispatch shapes are fixed in main.py:596-668.  Zero means "library
+ * default" for every field except update_staged (-1 = automatic).
+ */
+typedef struct mog_tuning {
+    int32_t deposit_threads;        /* threads per deposit CTA, 64..1024, multiple of 32 */
+    int32_t deposit_grids_per_cta;  /* grids per CTA histogram; -1 = global atomics        */
+    int32_t deposit_chunks;         /* particle chunks per grid group                       */
+    int32_t deposit_ppt;            /* particles per thread in the deposit: 1, 2 or 4       */
+    int32_t update_staged;          /* -1 auto, 0 gathers from L2, 1 shared-memory staged    */
+    int32_t update_ctas;            /* CTAs of the staged gather (0 = one per SM)            */
+    int32_t reserved[2];
+} mog_tuning;
 
 /* Fill a config with the reference's in-code defaults (main.py:179-189). */
 int mog_config_default(mog_config* cfg);
@@ -153,6 +177,10 @@ int mog_update(mog_handle* h, float* pos4, float* vel4, int64_t n,
  */
 int mog_step_profiled(mog_handle* h, float* pos4, float* vel4, int64_t n,
                       float dt_eff, float* phase_ms, void* stream);
+
+/* Read / replace the handle's launch shapes (drops cached CUDA graphs). */
+int mog_get_tuning(const mog_handle* h, mog_tuning* out);
+int mog_set_tuning(mog_handle* h, const mog_tuning* t);
 
 /*
  * Reads (and clears) the device status word: OR of MOG_FLAG_* bits raised

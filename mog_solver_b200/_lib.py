@@ -31,6 +31,8 @@ INDEX_EXACT = 1
 DFT_FFT32 = 0
 DFT_TC_BF16X3 = 1
 
+COMPAT_FFT_TEXTURE_ALIAS = 1
+
 FLAG_NONFINITE = 1
 FLAG_OVERFLOW = 2
 FLAG_TIMEOUT = 4
@@ -40,7 +42,8 @@ FLAG_BADMASS = 8
 EXPORTS = (
     "mog_config_default", "mog_create", "mog_destroy", "mog_step", "mog_step_n",
     "mog_step_profiled", "mog_forces", "mog_deposit", "mog_solve", "mog_update", "mog_get_status",
-    "mog_diagnostics", "mog_strerror", "mog_last_error", "mog_version",
+    "mog_get_tuning", "mog_set_tuning", "mog_diagnostics", "mog_strerror", "mog_last_error",
+    "mog_version",
 )
 
 
@@ -69,8 +72,20 @@ class MogConfigC(ctypes.Structure):
         ("scale_bits", ctypes.c_int32),
         ("index_mode", ctypes.c_int32),
         ("dft_prec", ctypes.c_int32),
-        ("reserved0", ctypes.c_int32),
+        ("compat_flags", ctypes.c_int32),
         ("num_particles", ctypes.c_int64),
+    ]
+
+
+class MogTuningC(ctypes.Structure):
+    _fields_ = [
+        ("deposit_threads", ctypes.c_int32),
+        ("deposit_grids_per_cta", ctypes.c_int32),
+        ("deposit_chunks", ctypes.c_int32),
+        ("deposit_ppt", ctypes.c_int32),
+        ("update_staged", ctypes.c_int32),
+        ("update_ctas", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 2),
     ]
 
 
@@ -92,6 +107,8 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.mog_deposit.argtypes = [P, P, I64, P, P]
     lib.mog_solve.argtypes = [P, P, P, P]
     lib.mog_update.argtypes = [P, P, P, I64, P, F, P]
+    lib.mog_get_tuning.argtypes = [P, ctypes.POINTER(MogTuningC)]
+    lib.mog_set_tuning.argtypes = [P, ctypes.POINTER(MogTuningC)]
     lib.mog_get_status.argtypes = [P, ctypes.POINTER(ctypes.c_uint32), P]
     lib.mog_diagnostics.argtypes = [P, P, P, I64, ctypes.POINTER(ctypes.c_double), P]
     lib.mog_strerror.argtypes = [I]

@@ -18,7 +18,9 @@ so FFT is what such a config actually executed.
 Keys this library adds: ``seed`` (transform sampler seed), ``mass_mode``
 (``u64`` | ``u32x1000``), ``scale_bits`` (u64 fixed-point scale, ``None`` =
 chosen from the total mass), ``index_mode`` (``fast`` | ``exact``),
-``dft_precision`` (``fp32`` | ``bf16x3``).
+``dft_precision`` (``fp32`` | ``bf16x3``), ``reference_texture_aliasing``
+(reproduce the reference's x <- z force aliasing at g = 4, 16, 64; see
+include/mog.h MOG_COMPAT_FFT_TEXTURE_ALIAS).
 """
 from __future__ import annotations
 
@@ -76,6 +78,7 @@ class MogConfig:
     scale_bits: int | None = None
     index_mode: str = "fast"
     dft_precision: str = "fp32"
+    reference_texture_aliasing: bool = False
 
     @property
     def voxel_size(self) -> float:
@@ -110,6 +113,7 @@ class MogConfig:
             scale_bits=None if cfg.get("scale_bits") is None else int(cfg["scale_bits"]),
             index_mode=str(cfg.get("index_mode", "fast")),
             dft_precision=str(cfg.get("dft_precision", "fp32")),
+            reference_texture_aliasing=bool(cfg.get("reference_texture_aliasing", False)),
         )
         out.validate()
         return out

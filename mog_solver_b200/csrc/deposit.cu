@@ -6,14 +6,10 @@
 //
 // Design: a CTA owns `gpc` grids (or one slab of one grid when g^3 cells do
 // not fit shared memory) and a chunk of particles.  It accumulates a
-// private fixed-point histogram in shared memory with 32/64-bit shared
+// private fixed-point histogram in shared memory with 32-bit shared
 // atomics, then flushes the non-zero cells to the global grid with one
 // global atomic each.  Integer addition is associative, so the result is
-// bit-identical whatever the schedule.  When all particles of a warp carry
-// the same quantised mass (the equal-mass case of every benchmark
-// configuration) lanes that hit the same cell are merged with
-// __match_any_sync and a single add of popc * q, which removes the
-// shared-atomic serialisation in dense regions.
+// bit-identical whatever the schedule.
 #include <algorithm>
 
 #include "mog_internal.h"
@@ -37,26 +33,70 @@ struct Quant<unsigned> {
     }
 };
 
-constexpr uint32_t kNoCell = 0xffffffffu;
+// Shared histograms are 32-bit words: 64-bit shared atomics are several
+// times slower on this part, and 32-bit adds to one address from many
+// lanes are merged by the hardware.  MODE 0 (u32 x1000 grids): one word
+// per cell, wrapping mod 2^32 like the reference's uint atomicAdd.
+// MODE 1 (u64 fixed point): a low and a high word per cell; q is split into
+// halves, the low add returns the previous value so its carry is counted
+// exactly once, and the cell's 64-bit value is (hi << 32) + lo.  Equal
+// power-of-two masses have an all-zero low half and cost one add.
+template <int MODE>
+struct SmemHist;
+template <>
+struct SmemHist<0> {
+    using Acc = unsigned;
+    static constexpr int kWords = 1;
+    static __device__ __forceinline__ void add(unsigned* lo, unsigned*, uint32_t c, Acc q) {
+        atomicAdd(lo + c, q);
+    }
+    static __device__ __forceinline__ Acc read(const unsigned* lo, const unsigned*, uint32_t c) {
+        return lo[c];
+    }
+};
+template <>
+struct SmemHist<1> {
+    using Acc = unsigned long long;
+    static constexpr int kWords = 2;
+    static __device__ __forceinline__ void add(unsigned* lo, unsigned* hi, uint32_t c, Acc q) {
+        const unsigned ql = (unsigned)q;
+        unsigned qh = (unsigned)(q >> 32);
+        if (ql) {
+            const unsigned old = atomicAdd(lo + c, ql);
+            qh += (old > ~ql) ? 1u : 0u;  // old + ql wrapped past 2^32
+        }
+        if (qh) atomicAdd(hi + c, qh);
+    }
+    static __device__ __forceinline__ Acc read(const unsigned* lo, const unsigned* hi, uint32_t c) {
+        return ((Acc)hi[c] << 32) | lo[c];
+    }
+};
 
 // Shared-memory histogram deposit.  blockIdx.x: particle chunk; blockIdx.y:
 // group of `gpc` grids; blockIdx.z: slab of (1 << slab_lg) consecutive
-// cells of each grid (slab_lg == 3*lg means the whole grid).
-template <typename Acc, int IDX, bool AGG>
+// cells of each grid (slab_lg == 3*lg means the whole grid).  Each thread
+// carries PPT particles through the grid loop, so the grid's cell-index
+// rows are loaded once per PPT particles and the PPT index computations
+// and shared adds overlap.
+template <int MODE, int IDX, int PPT>
 __global__ void __launch_bounds__(1024) deposit_smem_kernel(const float4* __restrict__ pos,
                                                             int64_t n, int64_t chunk,
                                                             Ensemble e, int gpc, int slab_lg,
-                                                            Acc* __restrict__ mass) {
+                                                            typename SmemHist<MODE>::Acc* __restrict__ mass) {
+    using H = SmemHist<MODE>;
+    using Acc = typename H::Acc;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lg = e.lg;
     const uint32_t slab_cells = 1u << slab_lg;
     const uint32_t slab_lo = (uint32_t)blockIdx.z << slab_lg;
     const int g0 = blockIdx.y * gpc;
     const int ng = min(gpc, e.k - g0);
+    const uint32_t words = (uint32_t)ng * slab_cells;
 
-    // shared layout: [transforms: gpc * 16 floats][histogram: gpc * slab_cells]
+    // shared layout: [transforms: gpc * 16 floats][lo words][hi words]
     float* xf = reinterpret_cast<float*>(smem_raw);
-    Acc* hist = reinterpret_cast<Acc*>(smem_raw + (size_t)gpc * 16 * sizeof(float));
+    unsigned* lo_w = reinterpret_cast<unsigned*>(smem_raw + (size_t)gpc * 16 * sizeof(float));
+    unsigned* hi_w = lo_w + (size_t)gpc * slab_cells;
 
     for (int i = threadIdx.x; i < ng * 16; i += blockDim.x) {
         const int j = i >> 4, w = i & 15;
@@ -68,67 +108,73 @@ __global__ void __launch_bounds__(1024) deposit_smem_kernel(const float4* __rest
         }
         xf[i] = v;
     }
-    for (uint32_t i = threadIdx.x; i < (uint32_t)ng * slab_cells; i += blockDim.x) hist[i] = 0;
+    for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) {
+        lo_w[i] = 0u;
+        if (H::kWords == 2) hi_w[i] = 0u;
+    }
     __syncthreads();
 
     const IndexParams ip = e.index_params();
     const int64_t lo = (int64_t)blockIdx.x * chunk;
     const int64_t hi = min(n, lo + chunk);
-    const int lane = threadIdx.x & 31;
+    const int T = blockDim.x;
     unsigned bad = 0;
     double qsum = 0.0;
 
-    for (int64_t base = lo; base < hi; base += blockDim.x) {
-        const int64_t p = base + threadIdx.x;
-        const bool valid = p < hi;
-        float4 P = valid ? __ldg(pos + p) : make_float4(0.f, 0.f, 0.f, 0.f);
-        Acc q = valid ? Quant<Acc>::q(P.w, e.scale, bad) : Acc(0);
-        qsum += (double)q;
-        const float cx = __fsub_rn(P.x, ip.half_l);
-        const float cy = __fsub_rn(P.y, ip.half_l);
-        const float cz = __fsub_rn(P.z, ip.half_l);
-
-        bool uni = false;
-        Acc q0 = q;
-        if (AGG) {
-            const unsigned vmask = __ballot_sync(kFull, valid);
-            q0 = __shfl_sync(kFull, q, vmask ? __ffs(vmask) - 1 : 0);
-            uni = __all_sync(kFull, !valid || q == q0);
+    for (int64_t base = lo; base < hi; base += (int64_t)T * PPT) {
+        float cx[PPT], cy[PPT], cz[PPT];
+        Acc q[PPT];
+        bool valid[PPT];
+#pragma unroll
+        for (int u = 0; u < PPT; ++u) {
+            const int64_t p = base + threadIdx.x + (int64_t)u * T;
+            valid[u] = p < hi;
+            const float4 P = valid[u] ? __ldg(pos + p) : make_float4(0.f, 0.f, 0.f, 0.f);
+            unsigned b = 0;
+            if (MODE == 1)
+                q[u] = valid[u] ? quantize_u64(P.w, e.scale, b) : 0ull;
+            else
+                q[u] = valid[u] ? quantize_u32(P.w, b) : 0u;
+            bad |= b;
+            qsum += (double)q[u];
+            cx[u] = __fsub_rn(P.x, ip.half_l);
+            cy[u] = __fsub_rn(P.y, ip.half_l);
+            cz[u] = __fsub_rn(P.z, ip.half_l);
         }
-#pragma unroll 2
         for (int j = 0; j < ng; ++j) {
-            uint32_t cell;
+            unsigned* lw = lo_w + (size_t)j * slab_cells;
+            unsigned* hw = hi_w + (size_t)j * slab_cells;
             if (IDX == 0) {
                 const float4* r = reinterpret_cast<const float4*>(xf + j * 16);
-                cell = cell_fast(r[0], r[1], r[2], cx, cy, cz, lg);
+                const float4 r0 = r[0], r1 = r[1], r2 = r[2];
+#pragma unroll
+                for (int u = 0; u < PPT; ++u) {
+                    const uint32_t local = cell_fast(r0, r1, r2, cx[u], cy[u], cz[u], lg) - slab_lo;
+                    if (valid[u] && local < slab_cells) H::add(lw, hw, local, q[u]);
+                }
             } else {
-                cell = cell_exact(xf + j * 16, xf + j * 16 + 12, cx, cy, cz, ip);
-            }
-            uint32_t local = cell - slab_lo;
-            const bool hit = valid && local < slab_cells;
-            Acc* h = hist + (size_t)j * slab_cells;
-            if (AGG && uni) {
-                const uint32_t key = hit ? local : kNoCell;
-                const unsigned m = __match_any_sync(kFull, key);
-                if (hit && lane == __ffs(m) - 1) atomicAdd(h + local, q0 * (Acc)__popc(m));
-            } else if (hit) {
-                atomicAdd(h + local, q);
+#pragma unroll
+                for (int u = 0; u < PPT; ++u) {
+                    const uint32_t local =
+                        cell_exact(xf + j * 16, xf + j * 16 + 12, cx[u], cy[u], cz[u], ip) - slab_lo;
+                    if (valid[u] && local < slab_cells) H::add(lw, hw, local, q[u]);
+                }
             }
         }
     }
 
     // Overflow bookkeeping: every grid receives every particle's q, so the
     // total of one grid bounds every cell; the first grid group counts it.
-    if (blockIdx.y == 0 && blockIdx.z == 0 && sizeof(Acc) == 8) {
+    if (MODE == 1 && blockIdx.y == 0 && blockIdx.z == 0) {
         for (int o = 16; o > 0; o >>= 1) qsum += __shfl_xor_sync(kFull, qsum, o);
-        if (lane == 0 && qsum != 0.0) atomicAdd(e.mass_total, qsum);
+        if ((threadIdx.x & 31) == 0 && qsum != 0.0) atomicAdd(e.mass_total, qsum);
     }
     if (bad) raise_flags(e.flags, bad);
     __syncthreads();
 
     const size_t gcells = (size_t)1 << (3 * lg);
-    for (uint32_t i = threadIdx.x; i < (uint32_t)ng * slab_cells; i += blockDim.x) {
-        const Acc v = hist[i];
+    for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) {
+        const Acc v = H::read(lo_w, hi_w, i);
         if (v) {
             const uint32_t j = i >> slab_lg, c = i & (slab_cells - 1);
             atomicAdd(mass + (size_t)(g0 + j) * gcells + slab_lo + c, v);
@@ -171,13 +217,17 @@ __global__ void __launch_bounds__(256) deposit_global_kernel(const float4* __res
 
 }  // namespace
 
-template <typename Acc, int IDX>
-static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, int64_t n, Acc* mass,
+template <int MODE, int IDX>
+static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, int64_t n, void* mass_v,
                                  const DepositShape& sh, cudaStream_t s) {
+    using H = SmemHist<MODE>;
+    using Acc = typename H::Acc;
+    Acc* mass = static_cast<Acc*>(mass_v);
     if (n <= 0) return cudaSuccess;
     const int cells_lg = 3 * e.lg;
-    const size_t grid_bytes = sizeof(Acc) << cells_lg;
-    const size_t budget = 100 * 1024;  // two CTAs per SM
+    const size_t word_bytes = 4 * H::kWords;
+    const size_t grid_bytes = word_bytes << cells_lg;
+    const size_t budget = 200 * 1024;  // one CTA of up to 1024 threads per SM
     if (sh.grids_per_cta < 0) {
         const int threads = 256;
         const int64_t blocks = (n + threads - 1) / threads;
@@ -186,19 +236,14 @@ static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, int64_t n
     }
     int gpc = sh.grids_per_cta;
     int slab_lg = cells_lg;
-    if (gpc == 0) {
-        if (grid_bytes <= budget) {
-            gpc = (int)std::min<size_t>((size_t)e.k, budget / grid_bytes);
-        } else {
-            gpc = 1;
-            while (((size_t)sizeof(Acc) << slab_lg) > 128 * 1024) --slab_lg;
-        }
-    } else if (grid_bytes * gpc > 200 * 1024) {
+    if (gpc == 0) gpc = (int)std::max<size_t>(1, std::min<size_t>((size_t)e.k, budget / grid_bytes));
+    if (grid_bytes * gpc > budget) {
         gpc = 1;
-        while (((size_t)sizeof(Acc) << slab_lg) > 128 * 1024) --slab_lg;
+        while ((word_bytes << slab_lg) > 128 * 1024) --slab_lg;
     }
     gpc = std::max(1, std::min(gpc, e.k));
-    const size_t smem = (size_t)gpc * 16 * sizeof(float) + ((size_t)gpc * sizeof(Acc) << slab_lg);
+    const size_t smem = (size_t)gpc * 16 * sizeof(float) + ((size_t)gpc * word_bytes << slab_lg);
+    const int ppt = sh.ppt == 1 || sh.ppt == 2 || sh.ppt == 4 ? sh.ppt : 2;
     auto launch = [&](auto kern) -> cudaError_t {
         cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                (int)smem);
@@ -207,31 +252,30 @@ static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, int64_t n
         const int slabs = 1 << (cells_lg - slab_lg);
         int chunks = sh.chunks;
         if (chunks <= 0) {
+            // a few waves of CTAs; each extra chunk costs one histogram flush
             const int per_sm = smem > 110 * 1024 ? 1 : 2;
-            const int64_t target = (int64_t)num_sms() * per_sm * 4;
+            const int64_t target = (int64_t)num_sms() * per_sm * 8;
             int64_t c = (target + (int64_t)groups * slabs - 1) / ((int64_t)groups * slabs);
-            const int64_t max_c = (n + 2047) / 2048;
-            chunks = (int)std::max<int64_t>(1, std::min<int64_t>(c, max_c));
+            const int64_t max_c = (n + 4095) / 4096;
+            chunks = (int)std::max<int64_t>(1, std::min<int64_t>(std::max<int64_t>(c, 32), max_c));
         }
         const int64_t chunk = (n + chunks - 1) / chunks;
         dim3 grid(chunks, groups, slabs);
         kern<<<grid, sh.threads, smem, s>>>(pos, n, chunk, e, gpc, slab_lg, mass);
         return cudaGetLastError();
     };
-    if (sh.aggregate) return launch(deposit_smem_kernel<Acc, IDX, true>);
-    return launch(deposit_smem_kernel<Acc, IDX, false>);
+    if (ppt == 1) return launch(deposit_smem_kernel<MODE, IDX, 1>);
+    if (ppt == 4) return launch(deposit_smem_kernel<MODE, IDX, 4>);
+    return launch(deposit_smem_kernel<MODE, IDX, 2>);
 }
 
 cudaError_t launch_deposit(const Ensemble& e, const float4* pos, int64_t n, void* mass,
                            const DepositShape& shape, cudaStream_t s) {
-    if (e.mass_mode == 0) {
-        auto* m = static_cast<unsigned long long*>(mass);
-        return e.index_mode == 0 ? deposit_typed<unsigned long long, 0>(e, pos, n, m, shape, s)
-                                 : deposit_typed<unsigned long long, 1>(e, pos, n, m, shape, s);
-    }
-    auto* m = static_cast<unsigned*>(mass);
-    return e.index_mode == 0 ? deposit_typed<unsigned, 0>(e, pos, n, m, shape, s)
-                             : deposit_typed<unsigned, 1>(e, pos, n, m, shape, s);
+    if (e.mass_mode == 0)
+        return e.index_mode == 0 ? deposit_typed<1, 0>(e, pos, n, mass, shape, s)
+                                 : deposit_typed<1, 1>(e, pos, n, mass, shape, s);
+    return e.index_mode == 0 ? deposit_typed<0, 0>(e, pos, n, mass, shape, s)
+                             : deposit_typed<0, 1>(e, pos, n, mass, shape, s);
 }
 
 }  // namespace mog

@@ -177,6 +177,8 @@ int validate(const mog_config& c) {
     if (c.dft_prec != MOG_DFT_FFT32 && c.dft_prec != MOG_DFT_TC_BF16X3)
         return fail(MOG_ERR_CONFIG, "dft_prec must be 0 (fp32 fft) or 1 (tensor-core bf16x3)");
     if (c.num_particles < 0) return fail(MOG_ERR_CONFIG, "num_particles must be >= 0");
+    if (c.compat_flags & ~MOG_COMPAT_FFT_TEXTURE_ALIAS)
+        return fail(MOG_ERR_CONFIG, "unknown compat_flags bits");
     return MOG_OK;
 }
 
@@ -308,6 +310,9 @@ int mog_create(const mog_config* cfg, const float* rot12, const float* off4, mog
     e.G = cfg->G;
     e.scale = std::ldexp(1.0f, cfg->scale_bits);
     e.inv_scale = std::ldexp(1.0f, -cfg->scale_bits);
+    // the reference's ping-pong leaves the result in its scratch texture
+    // after an odd number of passes, 3 (log2 g + 1)
+    e.alias_xz = (cfg->compat_flags & MOG_COMPAT_FFT_TEXTURE_ALIAS) && ((3 * (lg + 1)) & 1) ? 1 : 0;
 
     // FAST-mode rows: t_r = sum_j (M[j][r] / h) c_j + (L/2 - off_r) / h
     std::vector<mog::FastXf> fast(k);
@@ -529,6 +534,39 @@ int mog_update(mog_handle* h, float* pos4, float* vel4, int64_t n, const float* 
     err = mog::launch_update(h->e, reinterpret_cast<float4*>(pos4), reinterpret_cast<float4*>(vel4), n,
                              h->d_force2, dt_eff, h->cfg.damping, nullptr, h->ushape, s);
     if (err != cudaSuccess) return cuda_fail(err, "update");
+    return MOG_OK;
+}
+
+int mog_get_tuning(const mog_handle* h, mog_tuning* out) {
+    if (!h || !out) return fail(MOG_ERR_ARG, "null argument");
+    std::memset(out, 0, sizeof(*out));
+    out->deposit_threads = h->dshape.threads;
+    out->deposit_grids_per_cta = h->dshape.grids_per_cta;
+    out->deposit_chunks = h->dshape.chunks;
+    out->deposit_ppt = h->dshape.ppt;
+    out->update_staged = h->ushape.staged;
+    out->update_ctas = h->ushape.ctas;
+    return MOG_OK;
+}
+
+int mog_set_tuning(mog_handle* h, const mog_tuning* t) {
+    if (!h || !t) return fail(MOG_ERR_ARG, "null argument");
+    if (t->deposit_threads && (t->deposit_threads < 64 || t->deposit_threads > 1024 ||
+                               t->deposit_threads % 32))
+        return fail(MOG_ERR_ARG, "deposit_threads must be a multiple of 32 in [64, 1024]");
+    if (t->deposit_grids_per_cta < -1 || t->deposit_chunks < 0 || t->update_ctas < 0 ||
+        t->update_staged < -1 || t->update_staged > 1 ||
+        (t->deposit_ppt != 0 && t->deposit_ppt != 1 && t->deposit_ppt != 2 && t->deposit_ppt != 4))
+        return fail(MOG_ERR_ARG, "tuning value out of range");
+    h->dshape.threads = t->deposit_threads ? t->deposit_threads : 1024;
+    h->dshape.grids_per_cta = t->deposit_grids_per_cta;
+    h->dshape.chunks = t->deposit_chunks;
+    h->dshape.ppt = t->deposit_ppt ? t->deposit_ppt : 2;
+    h->ushape.staged = t->update_staged;
+    h->ushape.ctas = t->update_ctas;
+    for (auto& g : h->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    h->graphs.clear();
     return MOG_OK;
 }
 

@@ -17,6 +17,7 @@ struct Ensemble {
     int lg = 0;            // log2 g
     int mass_mode = 0;     // MOG_MASS_*
     int index_mode = 0;    // MOG_INDEX_*
+    int alias_xz = 0;      // reproduce the reference's x <- z force aliasing
     float world = 0.f;     // L
     float voxel = 0.f;     // h
     float G = 0.f;
@@ -44,10 +45,10 @@ struct Ensemble {
 
 // Launch-shape knobs (chosen by the autotuner or by defaults).
 struct DepositShape {
-    int threads = 512;
-    int grids_per_cta = 0;  // 0 = default for (g, mass mode)
+    int threads = 1024;
+    int grids_per_cta = 0;  // 0 = default for (g, mass mode); -1 = global atomics
     int chunks = 0;         // particle chunks; 0 = derived from n
-    int aggregate = 1;      // warp-aggregate equal-mass adds
+    int ppt = 2;            // particles per thread carried through the grid loop
 };
 struct UpdateShape {
     int threads = 1024;

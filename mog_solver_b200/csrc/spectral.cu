@@ -212,7 +212,8 @@ __global__ void __launch_bounds__(G * G, (G == 16 ? 2 : 1))
         float4* fa = force + (size_t)ga * G3 + row;
 #pragma unroll
         for (int x = 0; x < G; ++x)
-            fa[x] = make_out(WORLD, R, r[x].x * invn, r[x].y * invn, r2[x].x * invn);
+            fa[x] = make_out(WORLD, R, (e.alias_xz ? r2[x].x : r[x].x) * invn, r[x].y * invn,
+                             r2[x].x * invn);
         if (hasb) {
 #pragma unroll
             for (int x = 0; x < G; ++x) r[x] = S2[(z * G + y) * P + x];
@@ -224,7 +225,8 @@ __global__ void __launch_bounds__(G * G, (G == 16 ? 2 : 1))
             float4* fb = force + (size_t)gb * G3 + row;
 #pragma unroll
             for (int x = 0; x < G; ++x)
-                fb[x] = make_out(WORLD, R, r[x].x * invn, r[x].y * invn, r2[x].y * invn);
+                fb[x] = make_out(WORLD, R, (e.alias_xz ? r2[x].y : r[x].x) * invn, r[x].y * invn,
+                                 r2[x].y * invn);
         }
     }
 }
@@ -339,12 +341,14 @@ __global__ void __launch_bounds__(256) mp_store_kernel(const float2* __restrict_
     float R[12];
     if (WORLD)
         for (int q = 0; q < 12; ++q) R[q] = __ldg(e.rot12 + 12 * ga + q);
-    force[(size_t)ga * G3 + c] = make_out(WORLD, R, a.x * invn, a.y * invn, z.x * invn);
+    force[(size_t)ga * G3 + c] =
+        make_out(WORLD, R, (e.alias_xz ? z.x : a.x) * invn, a.y * invn, z.x * invn);
     if (gb < e.k) {
         const float2 b = Z3[idx];
         if (WORLD)
             for (int q = 0; q < 12; ++q) R[q] = __ldg(e.rot12 + 12 * gb + q);
-        force[(size_t)gb * G3 + c] = make_out(WORLD, R, b.x * invn, b.y * invn, z.y * invn);
+        force[(size_t)gb * G3 + c] =
+            make_out(WORLD, R, (e.alias_xz ? z.y : b.x) * invn, b.y * invn, z.y * invn);
     }
 }
 

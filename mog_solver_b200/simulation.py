@@ -82,6 +82,7 @@ class Simulation:
         self.vel = torch.zeros((n, 4), dtype=torch.float32, device=self.device)
         self._handle = None
         self._handle_bits = None
+        self._auto_bits = None
         self.steps_taken = 0
 
     # ------------------------------------------------------------------
@@ -121,15 +122,26 @@ class Simulation:
         cc.scale_bits = scale_bits
         cc.index_mode = _INDEX[c.index_mode]
         cc.dft_prec = _DFT[c.dft_precision]
+        cc.compat_flags = _lib.COMPAT_FFT_TEXTURE_ALIAS if c.reference_texture_aliasing else 0
         cc.num_particles = max(self.n_particles, c.num_particles)
         return cc
 
     def _scale_bits(self) -> int:
+        """Configured scale, else one chosen from the total mass (computed once
+        per particle set, so steps never synchronise the host)."""
         if self.cfg.scale_bits is not None:
             return self.cfg.scale_bits
-        torch = _torch()
-        total = float(self.pos[:, 3].to(torch.float64).sum().item()) if self.n_particles else 1.0
-        return auto_scale_bits(total)
+        if self._auto_bits is None:
+            torch = _torch()
+            total = float(self.pos[:, 3].to(torch.float64).sum().item()) if self.n_particles else 1.0
+            self._auto_bits = auto_scale_bits(total)
+        return self._auto_bits
+
+    @property
+    def scale_bits(self) -> int:
+        """u64 fixed-point scale 2^bits of the current handle (0 in u32 mode)."""
+        self.handle
+        return self._handle_bits
 
     @property
     def handle(self):
@@ -179,7 +191,7 @@ class Simulation:
             self.close()
         self.pos = p
         self.vel = v
-        self.close()  # the fixed-point scale depends on the masses
+        self._auto_bits = None  # the fixed-point scale depends on the masses
 
     def init_particles(self, kind: str = "uniform", seed: int = 0, **kw) -> None:
         from . import ics

@@ -171,8 +171,18 @@ def fft3_f32(re, im, direction: int):
     return re, im
 
 
-def forces_grid_f32(mass_u32: np.ndarray, G: float, world: float) -> np.ndarray:
-    """Shader chain in FP32 from a u32 x1000 mass grid -> (k, g, g, g, 4)."""
+def texture_aliasing(g: int) -> bool:
+    """True when run_fft_3d_batched's 3 (log2 g + 1) passes are odd, so the z
+    inverse transform overwrites the x result (main.py:564-590, 638-646)."""
+    return (3 * (int(np.log2(g)) + 1)) % 2 == 1
+
+
+def forces_grid_f32(mass_u32: np.ndarray, G: float, world: float,
+                    aliasing: bool = True) -> np.ndarray:
+    """Shader chain in FP32 from a u32 x1000 mass grid -> (k, g, g, g, 4).
+
+    With ``aliasing`` (the reference's behaviour) the x component is the
+    z-gradient wherever ``texture_aliasing(g)``."""
     g = mass_u32.shape[-1]
     re = (mass_u32.astype(np.float32) / np.float32(1000.0)).astype(np.float32)  # complex.glsl:23
     im = np.zeros_like(re)
@@ -195,6 +205,8 @@ def forces_grid_f32(mass_u32: np.ndarray, G: float, world: float) -> np.ndarray:
         gi = (pr * kk).astype(np.float32)
         rr, _ = fft3_f32(gr, gi, -1)
         out[..., comp] = rr * scale
+    if aliasing and texture_aliasing(g):
+        out[..., 0] = out[..., 2]
     f = out[..., :3]
     out[..., 3] = np.sqrt((f[..., 0] * f[..., 0] + f[..., 1] * f[..., 1]) + f[..., 2] * f[..., 2])
     return out

@@ -1,0 +1,222 @@
+// ref_harness.cpp — runs the reference's GLSL compute shaders (translated
+// to C++ by ref_build.py into _ref/gen/*.inc) on the CPU, dispatch by
+// dispatch, exactly in the order and with the bindings and uniforms of
+// Simulation.step_fft (main.py:592-669) and run_fft_3d_batched
+// (main.py:564-590), including its texture ping-pong.  TEST / BASELINE
+// INFRASTRUCTURE ONLY.  Invocations of one dispatch run in parallel with
+// OpenMP (they are independent except for the atomics of mass.glsl); each
+// dispatch completes before the next starts (the memory_barrier calls).
+#include <omp.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "glsl_compat.hpp"
+#include "mass.inc"
+#include "complex.inc"
+#include "fft_batched.inc"
+#include "fourier.inc"
+#include "greens.inc"
+#include "pack.inc"
+#include "update.inc"
+
+namespace glsl {
+thread_local uvec3 gl_GlobalInvocationID;
+}
+
+using namespace glsl;
+
+namespace {
+
+static_assert(sizeof(vec4) == 16, "vec4 must alias a float4 record");
+
+template <class F>
+void dispatch(int gx, int gy, int gz, int lx, int ly, int lz, F fn) {
+    const long X = (long)gx * lx, Y = (long)gy * ly, Z = (long)gz * lz;
+    const long total = X * Y * Z;
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < total; ++i) {
+        gl_GlobalInvocationID = uvec3{(uint)(i % X), (uint)((i / X) % Y), (uint)(i / (X * Y))};
+        fn();
+    }
+}
+
+struct Textures {
+    int k = -1, g = -1;
+    image3D ca, cb, gx, gy, gz, grad;
+    void ensure(int kk, int gg) {
+        if (kk == k && gg == g) return;
+        k = kk;
+        g = gg;
+        for (image3D* t : {&ca, &cb, &gx, &gy, &gz}) t->allocate(g, g, g * k, 2);
+        grad.allocate(g, g, g * k, 4);
+    }
+};
+Textures T;
+
+int grid_dispatch(int g) { return std::max(1, g / 8); }
+
+// run_fft_3d_batched: 3 axes x (log2 g + 1) passes, swapping textures
+// after every pass; returns the texture written last.
+image3D* run_fft(image3D* src, image3D* dst, bool forward, int gs, int ng) {
+    namespace S = fft_batched_glsl;
+    const int num_stages = (int)std::log2((double)gs);
+    S::direction = forward ? 1 : -1;
+    S::gridSize = gs;
+    S::nGrids = ng;
+    image3D* cs = src;
+    image3D* cd = dst;
+    for (int axis = 0; axis < 3; ++axis) {
+        S::axis = axis;
+        for (int stage = 0; stage < num_stages + 1; ++stage) {
+            S::stage = stage;
+            S::inputTexture.p = cs;
+            S::outputTexture.p = cd;
+            dispatch(grid_dispatch(gs), grid_dispatch(gs), ng, 8, 8, 1, [] { S::main(); });
+            std::swap(cs, cd);
+        }
+    }
+    return cs;
+}
+
+void do_mass(float* pos4, int n, const float* off4, const float* rot12, int k, int g,
+             float world, float voxel, uint* mass) {
+    namespace S = mass_glsl;
+    const int cells = k * g * g * g;
+    std::memset(mass, 0, sizeof(uint) * cells);  // clear_mass (main.py:558-562)
+    S::positions.data = reinterpret_cast<vec4*>(pos4);
+    S::positions.n = n;
+    S::mass_grid.data = mass;
+    S::mass_grid.n = cells;
+    S::offsets.data = reinterpret_cast<vec4*>(const_cast<float*>(off4));
+    S::offsets.n = k;
+    S::rotations.data = reinterpret_cast<vec4*>(const_cast<float*>(rot12));
+    S::rotations.n = 3 * k;
+    S::gridSize = g;
+    S::nGrids = k;
+    S::voxelSize = voxel;
+    S::worldSize = world;
+    dispatch((n + 255) / 256, 1, 1, 256, 1, 1, [] { S::main(); });
+}
+
+void do_solve(uint* mass, int k, int g, float world, float Gc) {
+    const int cells = k * g * g * g;
+    T.ensure(k, g);
+    const int d = grid_dispatch(g);
+    {
+        namespace S = complex_glsl;
+        S::mass_grid.data = mass;
+        S::mass_grid.n = cells;
+        S::complexTexture.p = &T.ca;
+        S::gridSize = g;
+        S::nGrids = k;
+        dispatch(d, d, g * k, 8, 8, 1, [] { S::main(); });
+    }
+    image3D* spec = run_fft(&T.ca, &T.cb, true, g, k);
+    {
+        namespace S = fourier_glsl;
+        S::spectrumTex.p = spec;
+        S::gridSize = g;
+        S::nGrids = k;
+        dispatch(d, d, g * k, 8, 8, 1, [] { S::main(); });
+    }
+    {
+        namespace S = greens_glsl;
+        S::inputTexture.p = spec;
+        S::outGradX.p = &T.gx;
+        S::outGradY.p = &T.gy;
+        S::outGradZ.p = &T.gz;
+        S::gridSize = g;
+        S::nGrids = k;
+        S::G = Gc;
+        S::worldSize = world;
+        dispatch(d, d, g * k, 8, 8, 1, [] { S::main(); });
+    }
+    image3D* rx = run_fft(&T.gx, &T.cb, false, g, k);
+    image3D* ry = run_fft(&T.gy, &T.ca, false, g, k);
+    image3D* rz = run_fft(&T.gz, &T.cb, false, g, k);
+    {
+        namespace S = pack_glsl;
+        S::realGradX.p = rx;
+        S::realGradY.p = ry;
+        S::realGradZ.p = rz;
+        S::finalForce.p = &T.grad;
+        S::gridSize = g;
+        S::nGrids = k;
+        dispatch(d, d, g * k, 8, 8, 1, [] { S::main(); });
+    }
+}
+
+void do_update(float* pos4, float* vel4, int n, const float* off4, const float* rot12, int k,
+               int g, float world, float voxel, float dt, float damping) {
+    namespace S = update_glsl;
+    S::positions.data = reinterpret_cast<vec4*>(pos4);
+    S::positions.n = n;
+    S::velocities.data = reinterpret_cast<vec4*>(vel4);
+    S::velocities.n = n;
+    S::offsets.data = reinterpret_cast<vec4*>(const_cast<float*>(off4));
+    S::offsets.n = k;
+    S::rotations.data = reinterpret_cast<vec4*>(const_cast<float*>(rot12));
+    S::rotations.n = 3 * k;
+    S::gradientTexture.p = &T.grad;
+    S::deltaTime = dt;
+    S::gridSize = g;
+    S::nGrids = k;
+    S::worldSize = world;
+    S::voxelSize = voxel;
+    S::damping = damping;
+    dispatch((n + 255) / 256, 1, 1, 256, 1, 1, [] { S::main(); });
+}
+
+}  // namespace
+
+extern "C" {
+
+__attribute__((visibility("default"))) int ref_threads(int nthreads) {
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+    return omp_get_max_threads();
+}
+
+// mass.glsl into mass_out (k g^3 uint32).
+__attribute__((visibility("default"))) void ref_deposit(float* pos4, int n, const float* off4,
+                                                        const float* rot12, int k, int g,
+                                                        float world, float voxel,
+                                                        uint32_t* mass_out) {
+    do_mass(pos4, n, off4, rot12, k, g, world, voxel, mass_out);
+}
+
+// complex .. pack from a uint32 mass grid; grad_out: k g^3 x 4 floats
+// (the gradient texture, [z][y][x] with z = grid * g + local z).
+__attribute__((visibility("default"))) void ref_solve(uint32_t* mass, int k, int g, float world,
+                                                      float Gc, float* grad_out) {
+    do_solve(mass, k, g, world, Gc);
+    std::memcpy(grad_out, T.grad.texels.data(), sizeof(float) * T.grad.texels.size());
+}
+
+// update.glsl from a caller gradient texture.
+__attribute__((visibility("default"))) void ref_update(float* pos4, float* vel4, int n,
+                                                       const float* off4, const float* rot12,
+                                                       int k, int g, float world, float voxel,
+                                                       float dt, float damping,
+                                                       const float* grad_in) {
+    T.ensure(k, g);
+    std::memcpy(T.grad.texels.data(), grad_in, sizeof(float) * T.grad.texels.size());
+    do_update(pos4, vel4, n, off4, rot12, k, g, world, voxel, dt, damping);
+}
+
+// One whole step_fft.  mass_scratch: k g^3 uint32 (contents on return:
+// this step's mass grid).
+__attribute__((visibility("default"))) void ref_step(float* pos4, float* vel4, int n,
+                                                     const float* off4, const float* rot12, int k,
+                                                     int g, float world, float voxel, float Gc,
+                                                     float dt, float damping,
+                                                     uint32_t* mass_scratch) {
+    do_mass(pos4, n, off4, rot12, k, g, world, voxel, mass_scratch);
+    do_solve(mass_scratch, k, g, world, Gc);
+    do_update(pos4, vel4, n, off4, rot12, k, g, world, voxel, dt, damping);
+}
+
+}  // extern "C"

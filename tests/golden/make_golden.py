@@ -1,0 +1,137 @@
+"""Generate the golden fixtures in tests/golden from the reference itself.
+
+Run in a container that has the reference checkout (default /root/reference,
+or $MOG_REFERENCE) and the built oracle/_ref (python -m oracle.ref_build):
+
+    python tests/golden/make_golden.py
+
+* transforms.npz   — Simulation.compute_transforms (main.py:157-172) with
+                     the reference's own RandomSE3Sampler (main.py:9-62),
+                     seeded; main.py is imported with its GL modules stubbed.
+* greens_kernel.npz — Simulation.init_greens_kernel (main.py:250-278).
+* shaders_g{8,16}.npz — the reference's compute shaders (compiled as C++ by
+                     oracle/_ref) on small seeded particle sets: the mass
+                     grid of mass.glsl, the gradient texture of the
+                     complex..pack chain, and the particles after one
+                     update.glsl pass (and after one whole step_fft).
+
+The fixtures are committed so the tests never need the reference.
+"""
+from __future__ import annotations
+
+import os
+import sys
+import types
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parent.parent
+sys.path.insert(0, str(ROOT))
+REF = Path(os.environ.get("MOG_REFERENCE", "/root/reference"))
+
+
+def import_reference_main():
+    """main.py with moderngl / moderngl_window replaced by empty modules."""
+    mgl = types.ModuleType("moderngl")
+    mglw = types.ModuleType("moderngl_window")
+    mglw.WindowConfig = object
+    sys.modules.setdefault("moderngl", mgl)
+    sys.modules.setdefault("moderngl_window", mglw)
+    sys.path.insert(0, str(REF))
+    import main as ref_main  # noqa: E402
+
+    return ref_main
+
+
+class _FakeBuffer:
+    def __init__(self, data):
+        self.data = data
+
+
+class _FakeCtx:
+    def buffer(self, data):
+        return _FakeBuffer(data)
+
+
+def transforms(ref_main):
+    cases = [(16, 16, 100.0, 0), (3, 8, 100.0, 1), (240, 16, 100.0, 1), (32, 32, 2000.0, 7)]
+    out = {}
+    for k, g, L, seed in cases:
+        orig = ref_main.RandomSE3Sampler
+
+        def seeded(*a, _seed=seed, _orig=orig, **kw):
+            kw["seed"] = _seed
+            return _orig(*a, **kw)
+
+        ref_main.RandomSE3Sampler = seeded
+        try:
+            fake = types.SimpleNamespace(n_grids=k, grid_size=g, world_size=L)
+            off, rot = ref_main.Simulation.compute_transforms(fake)
+        finally:
+            ref_main.RandomSE3Sampler = orig
+        key = f"k{k}_g{g}_L{int(L)}_s{seed}"
+        out[f"{key}_offsets"] = off
+        out[f"{key}_rotations"] = rot
+    np.savez_compressed(HERE / "transforms.npz", **out)
+
+
+def greens_kernel(ref_main):
+    out = {}
+    for g, L in [(8, 100.0), (16, 100.0)]:
+        fake = types.SimpleNamespace(grid_size=g, voxel_size=L / g, ctx=_FakeCtx())
+        import contextlib
+        import io
+
+        with contextlib.redirect_stdout(io.StringIO()):
+            ref_main.Simulation.init_greens_kernel(fake)
+        k = np.frombuffer(fake.green_kernel_buf.data, dtype=np.float32).reshape(g, g, g, 4)
+        out[f"g{g}"] = k
+    np.savez_compressed(HERE / "greens_kernel.npz", **out)
+
+
+def shaders():
+    from oracle import ref_harness as rh
+
+    assert rh.available(), "build oracle/_ref first (python -m oracle.ref_build)"
+    T = np.load(HERE / "transforms.npz")
+    for g, k, n in [(8, 3, 1500), (16, 3, 1000)]:
+        L, G, dt, damping = 100.0, 10.0, 1e-3, 0.999
+        key = "k3_g8_L100_s1" if g == 8 else None
+        rng = np.random.default_rng(100 + g)
+        if key is None:
+            from mog_solver_b200.transforms import compute_transforms
+
+            off, rot = compute_transforms(k, g, L, seed=5)
+        else:
+            off, rot = T[f"{key}_offsets"], T[f"{key}_rotations"]
+        pos = np.zeros((n, 4), dtype=np.float32)
+        half = n // 2
+        pos[:half, :3] = rng.normal(L / 2, L / 10, (half, 3))
+        pos[half:, :3] = rng.uniform(0, L, (n - half, 3))
+        pos[:, :3] = np.mod(pos[:, :3], np.float32(L)).astype(np.float32)
+        pos[:, 3] = rng.choice(np.array([1.0, 0.5, 2.0], dtype=np.float32), n)
+        vel = np.zeros_like(pos)
+        vel[:, :3] = rng.normal(0, 2, (n, 3))
+        mass = rh.deposit(pos, off, rot, g, L)
+        grad = rh.solve(mass, L, G)
+        p1, v1 = rh.update(pos, vel, off, rot, grad, g, L, dt, damping)
+        p2, v2, m2 = rh.step(pos, vel, off, rot, g, L, G, dt, damping)
+        assert np.array_equal(m2, mass) and np.array_equal(p2, p1) and np.array_equal(v2, v1)
+        np.savez_compressed(HERE / f"shaders_g{g}.npz", pos=pos, vel=vel, offsets=off,
+                            rotations=rot, mass=mass, grad=grad, pos1=p1, vel1=v1,
+                            params=np.array([L, G, dt, damping], dtype=np.float64))
+
+
+def main():
+    ref_main = import_reference_main()
+    transforms(ref_main)
+    greens_kernel(ref_main)
+    shaders()
+    for f in sorted(HERE.glob("*.npz")):
+        print(f.name, f.stat().st_size)
+
+
+if __name__ == "__main__":
+    main()

@@ -72,7 +72,7 @@ def test_deposit_bit_exact(mass_mode, index_mode, n, k, g, equal_mass):
     got = sim.mass_grid().cpu().numpy()
     mm = oracle.MASS_U64 if mass_mode == "u64" else oracle.MASS_U32
     im = oracle.INDEX_FAST if index_mode == "fast" else oracle.INDEX_EXACT
-    bits = sim._handle_bits or 0
+    bits = sim.scale_bits
     ref = oracle.deposit(pos, sim.rotations, sim.offsets, g, L, mm, bits, im)
     got = got.view(np.uint64 if mm == oracle.MASS_U64 else np.uint32)
     assert got.shape == ref.shape
@@ -122,7 +122,7 @@ def test_solve_matches_fp64(mass_mode, k, g):
     F = sim.solve_grid(m).cpu().numpy()
     mm = m.cpu().numpy()
     if mass_mode == "u64":
-        rho = mm.view(np.uint64).astype(np.float64) * 2.0 ** -sim._handle_bits
+        rho = mm.view(np.uint64).astype(np.float64) * 2.0 ** -sim.scale_bits
     else:
         rho = mm.view(np.uint32).astype(np.float64) / 1000.0
     ref = pl.forces_grid_fp64(rho, G, L)
@@ -142,8 +142,8 @@ def test_forces_match_fp64_pipeline(index_mode):
     acc = sim.forces().cpu().numpy()[:, :3]
     im = oracle.INDEX_FAST if index_mode == "fast" else oracle.INDEX_EXACT
     mass = oracle.deposit(pos, sim.rotations, sim.offsets, g, L, oracle.MASS_U64,
-                          sim._handle_bits, im)
-    rho = mass.astype(np.float64) * 2.0 ** -sim._handle_bits
+                          sim.scale_bits, im)
+    rho = mass.astype(np.float64) * 2.0 ** -sim.scale_bits
     fgrid = pl.forces_grid_fp64(rho, G, L)
     cells = oracle.cells(pos, sim.rotations, sim.offsets, g, L, im)
     ref = pl.gather_fp64(cells, fgrid, sim.rotations)
@@ -197,7 +197,7 @@ def test_ten_steps_track_fp64_pipeline():
     pos, vel = particles(n, L, seed=0, clustered=False)
     vel[:] = 0
     sim.set_particles(pos, vel)
-    bits = sim._handle_bits
+    bits = sim.scale_bits
     p, v = pos.astype(np.float64), vel.astype(np.float64)
     for _ in range(10):
         p32 = p.astype(np.float32)
@@ -220,7 +220,7 @@ def test_convolution_solver_matches_fp64():
     sim.set_particles(pos, vel)
     m = sim.mass_grid()
     F = sim.solve_grid(m).cpu().numpy()[..., :3]
-    rho = m.cpu().numpy().view(np.uint64).astype(np.float64) * 2.0 ** -sim._handle_bits
+    rho = m.cpu().numpy().view(np.uint64).astype(np.float64) * 2.0 ** -sim.scale_bits
     h = L / g
     sh = pl.shift(g)
     d = sh * h
