@@ -106,7 +106,8 @@ typedef struct mog_tuning {
     int32_t deposit_ppt;            /* particles per thread in the deposit: 1, 2 or 4       */
     int32_t update_staged;          /* -1 auto, 0 gathers from L2, 1 shared-memory staged    */
     int32_t update_ctas;            /* CTAs of the staged gather (0 = one per SM)            */
-    int32_t reserved[2];
+    int32_t sort_every;             /* spatial re-ordering period in steps; 0 = never, -1 = default (1) */
+    int32_t update_direct_ppt;      /* particles per thread of the L2-gather update: 1, 2, 4 */
 } mog_tuning;
 
 /* Fill a config with the reference's in-code defaults (main.py:179-189). */
@@ -172,7 +173,8 @@ int mog_update(mog_handle* h, float* pos4, float* vel4, int64_t n,
 
 /*
  * mog_step with CUDA events recorded on `stream` between its kernels;
- * phase_ms[0..2] receive the device time of the deposit, the solve and the
+ * phase_ms[0..3] receive the device time of the spatial ordering (0 when
+ * this step does not re-order), the deposit, the solve and the
  * gather/update.  Synchronises the stream (measurement only).
  */
 int mog_step_profiled(mog_handle* h, float* pos4, float* vel4, int64_t n,
@@ -196,6 +198,19 @@ int mog_get_status(mog_handle* h, uint32_t* flags, void* stream);
  */
 int mog_diagnostics(mog_handle* h, const float* pos4, const float* vel4,
                     int64_t n, double* out8, void* stream);
+
+/*
+ * FP64 direct-sum judge of force accuracy (no counterpart in the
+ * reference).  For each of nt target records (device float4, w ignored)
+ * sums over ns source records (device float4, w = mass):
+ *     out3[t] = g_eff * sum_j m_j d / (|d|^2 + soft^2)^(3/2),
+ * d = target - source wrapped to the minimum image of a periodic box of
+ * side `world`.  With g_eff = G h^3 / 2 this is the Newtonian field in the
+ * solver's units (greens.glsl:40, pack.glsl:21).  out3: device, nt x 3
+ * doubles.  Deterministic (fixed-order reduction); synchronous-free.
+ */
+int mog_direct_sum(const float* targets4, int64_t nt, const float* sources4, int64_t ns,
+                   double world, double g_eff, double soft, double* out3, void* stream);
 
 /* Human-readable text for a status code, and the calling thread's last
  * error message. */

@@ -42,8 +42,8 @@ FLAG_BADMASS = 8
 EXPORTS = (
     "mog_config_default", "mog_create", "mog_destroy", "mog_step", "mog_step_n",
     "mog_step_profiled", "mog_forces", "mog_deposit", "mog_solve", "mog_update", "mog_get_status",
-    "mog_get_tuning", "mog_set_tuning", "mog_diagnostics", "mog_strerror", "mog_last_error",
-    "mog_version",
+    "mog_get_tuning", "mog_set_tuning", "mog_diagnostics", "mog_direct_sum", "mog_strerror",
+    "mog_last_error", "mog_version",
 )
 
 
@@ -85,7 +85,8 @@ class MogTuningC(ctypes.Structure):
         ("deposit_ppt", ctypes.c_int32),
         ("update_staged", ctypes.c_int32),
         ("update_ctas", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 2),
+        ("sort_every", ctypes.c_int32),
+        ("update_direct_ppt", ctypes.c_int32),
     ]
 
 
@@ -111,6 +112,8 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.mog_set_tuning.argtypes = [P, ctypes.POINTER(MogTuningC)]
     lib.mog_get_status.argtypes = [P, ctypes.POINTER(ctypes.c_uint32), P]
     lib.mog_diagnostics.argtypes = [P, P, P, I64, ctypes.POINTER(ctypes.c_double), P]
+    D = ctypes.c_double
+    lib.mog_direct_sum.argtypes = [P, I64, P, I64, D, D, D, P, P]
     lib.mog_strerror.argtypes = [I]
     lib.mog_strerror.restype = ctypes.c_char_p
     lib.mog_last_error.argtypes = []

@@ -19,7 +19,8 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 OUT = PKG / "libmog.so"
-SOURCES = ["mog_api.cu", "deposit.cu", "spectral.cu", "update.cu", "convolution.cu"]
+SOURCES = ["mog_api.cu", "deposit.cu", "spectral.cu", "update.cu", "convolution.cu",
+           "diagnostics.cu", "sort.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

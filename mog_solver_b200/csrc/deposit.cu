@@ -80,6 +80,7 @@ struct SmemHist<1> {
 // and shared adds overlap.
 template <int MODE, int IDX, int PPT>
 __global__ void __launch_bounds__(1024) deposit_smem_kernel(const float4* __restrict__ pos,
+                                                            const int* __restrict__ perm,
                                                             int64_t n, int64_t chunk,
                                                             Ensemble e, int gpc, int slab_lg,
                                                             typename SmemHist<MODE>::Acc* __restrict__ mass) {
@@ -127,9 +128,12 @@ __global__ void __launch_bounds__(1024) deposit_smem_kernel(const float4* __rest
         bool valid[PPT];
 #pragma unroll
         for (int u = 0; u < PPT; ++u) {
-            const int64_t p = base + threadIdx.x + (int64_t)u * T;
-            valid[u] = p < hi;
-            const float4 P = valid[u] ? __ldg(pos + p) : make_float4(0.f, 0.f, 0.f, 0.f);
+            // each thread takes PPT consecutive slots: with a spatial
+            // ordering they are neighbours and mostly share cells
+            const int64_t slot = base + (int64_t)threadIdx.x * PPT + u;
+            valid[u] = slot < hi;
+            float4 P = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (valid[u]) P = __ldg(pos + (perm ? (int64_t)__ldg(perm + slot) : slot));
             unsigned b = 0;
             if (MODE == 1)
                 q[u] = valid[u] ? quantize_u64(P.w, e.scale, b) : 0ull;
@@ -144,22 +148,37 @@ __global__ void __launch_bounds__(1024) deposit_smem_kernel(const float4* __rest
         for (int j = 0; j < ng; ++j) {
             unsigned* lw = lo_w + (size_t)j * slab_cells;
             unsigned* hw = hi_w + (size_t)j * slab_cells;
+            uint32_t key[PPT];
             if (IDX == 0) {
                 const float4* r = reinterpret_cast<const float4*>(xf + j * 16);
                 const float4 r0 = r[0], r1 = r[1], r2 = r[2];
 #pragma unroll
                 for (int u = 0; u < PPT; ++u) {
                     const uint32_t local = cell_fast(r0, r1, r2, cx[u], cy[u], cz[u], lg) - slab_lo;
-                    if (valid[u] && local < slab_cells) H::add(lw, hw, local, q[u]);
+                    key[u] = (valid[u] && local < slab_cells) ? local : 0xffffffffu;
                 }
             } else {
 #pragma unroll
                 for (int u = 0; u < PPT; ++u) {
                     const uint32_t local =
                         cell_exact(xf + j * 16, xf + j * 16 + 12, cx[u], cy[u], cz[u], ip) - slab_lo;
-                    if (valid[u] && local < slab_cells) H::add(lw, hw, local, q[u]);
+                    key[u] = (valid[u] && local < slab_cells) ? local : 0xffffffffu;
                 }
             }
+            // merge runs of equal cells before touching shared memory
+            uint32_t cur = key[0];
+            Acc acc = q[0];
+#pragma unroll
+            for (int u = 1; u < PPT; ++u) {
+                if (key[u] == cur) {
+                    acc += q[u];
+                } else {
+                    if (cur != 0xffffffffu) H::add(lw, hw, cur, acc);
+                    cur = key[u];
+                    acc = q[u];
+                }
+            }
+            if (cur != 0xffffffffu) H::add(lw, hw, cur, acc);
         }
     }
 
@@ -218,8 +237,8 @@ __global__ void __launch_bounds__(256) deposit_global_kernel(const float4* __res
 }  // namespace
 
 template <int MODE, int IDX>
-static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, int64_t n, void* mass_v,
-                                 const DepositShape& sh, cudaStream_t s) {
+static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, const int* perm, int64_t n,
+                                 void* mass_v, const DepositShape& sh, cudaStream_t s) {
     using H = SmemHist<MODE>;
     using Acc = typename H::Acc;
     Acc* mass = static_cast<Acc*>(mass_v);
@@ -243,7 +262,7 @@ static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, int64_t n
     }
     gpc = std::max(1, std::min(gpc, e.k));
     const size_t smem = (size_t)gpc * 16 * sizeof(float) + ((size_t)gpc * word_bytes << slab_lg);
-    const int ppt = sh.ppt == 1 || sh.ppt == 2 || sh.ppt == 4 ? sh.ppt : 2;
+    const int ppt = sh.ppt == 1 || sh.ppt == 2 || sh.ppt == 4 ? sh.ppt : 4;
     auto launch = [&](auto kern) -> cudaError_t {
         cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                (int)smem);
@@ -261,7 +280,7 @@ static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, int64_t n
         }
         const int64_t chunk = (n + chunks - 1) / chunks;
         dim3 grid(chunks, groups, slabs);
-        kern<<<grid, sh.threads, smem, s>>>(pos, n, chunk, e, gpc, slab_lg, mass);
+        kern<<<grid, sh.threads, smem, s>>>(pos, perm, n, chunk, e, gpc, slab_lg, mass);
         return cudaGetLastError();
     };
     if (ppt == 1) return launch(deposit_smem_kernel<MODE, IDX, 1>);
@@ -269,13 +288,13 @@ static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, int64_t n
     return launch(deposit_smem_kernel<MODE, IDX, 2>);
 }
 
-cudaError_t launch_deposit(const Ensemble& e, const float4* pos, int64_t n, void* mass,
-                           const DepositShape& shape, cudaStream_t s) {
+cudaError_t launch_deposit(const Ensemble& e, const float4* pos, const int* perm, int64_t n,
+                           void* mass, const DepositShape& shape, cudaStream_t s) {
     if (e.mass_mode == 0)
-        return e.index_mode == 0 ? deposit_typed<1, 0>(e, pos, n, mass, shape, s)
-                                 : deposit_typed<1, 1>(e, pos, n, mass, shape, s);
-    return e.index_mode == 0 ? deposit_typed<0, 0>(e, pos, n, mass, shape, s)
-                             : deposit_typed<0, 1>(e, pos, n, mass, shape, s);
+        return e.index_mode == 0 ? deposit_typed<1, 0>(e, pos, perm, n, mass, shape, s)
+                                 : deposit_typed<1, 1>(e, pos, perm, n, mass, shape, s);
+    return e.index_mode == 0 ? deposit_typed<0, 0>(e, pos, perm, n, mass, shape, s)
+                             : deposit_typed<0, 1>(e, pos, perm, n, mass, shape, s);
 }
 
 }  // namespace mog

@@ -123,6 +123,7 @@ struct GraphEntry {
     float* vel = nullptr;
     int64_t n = 0;
     float dt = 0.f;
+    bool sorts = false;       // whether the captured step re-orders the particles
     cudaGraphExec_t exec = nullptr;
 };
 
@@ -145,6 +146,12 @@ struct mog_handle {
     float4* d_force2 = nullptr;  // stage-update staging (lazy)
     void* d_scratch = nullptr;   // spectral scratch (g >= 32)
     double* d_diag = nullptr;    // diagnostics partials + result
+    int* d_perm = nullptr;       // spatial order of the particles (slot -> particle)
+    void* d_sort = nullptr;      // counting-sort scratch
+    int64_t perm_cap = 0;        // capacity of d_perm
+    int64_t perm_n = -1;         // n the permutation was built for
+    int sort_every = 1;          // re-order every this many steps (0 = never)
+    uint64_t step_count = 0;     // steps issued (decides when to re-order)
     std::vector<GraphEntry> graphs;
 };
 
@@ -225,18 +232,49 @@ int check_particles(mog_handle* h, const void* pos, const void* vel, int64_t n, 
     return MOG_OK;
 }
 
-// The three kernels of one step (or of a force evaluation when acc != null).
+// Whether the next step re-orders the particles (a permutation of [0, n)
+// must exist for this n before any kernel reads it).
+bool wants_sort(const mog_handle* h, int64_t n) {
+    if (h->sort_every <= 0 || n <= 0) return false;
+    return h->perm_n != n || h->step_count % (uint64_t)h->sort_every == 0;
+}
+
+// Launch the spatial ordering if `sort`; returns the permutation to use.
+int order_particles(mog_handle* h, const float4* pos, int64_t n, bool sort, cudaStream_t s,
+                    const int** perm) {
+    *perm = nullptr;
+    if (h->sort_every <= 0 || n <= 0) return MOG_OK;
+    if (sort) {
+        if (n > h->perm_cap) {
+            if (h->d_perm) cudaFree(h->d_perm);
+            h->d_perm = nullptr;
+            MOG_CUDA(cudaMalloc((void**)&h->d_perm, sizeof(int) * n), "cudaMalloc perm");
+            h->perm_cap = n;
+        }
+        if (!h->d_sort) MOG_CUDA(cudaMalloc(&h->d_sort, mog::sort_scratch_bytes()), "cudaMalloc sort");
+        cudaError_t err = mog::launch_sort(pos, n, h->e.world, h->d_sort, h->d_perm, s);
+        if (err != cudaSuccess) return cuda_fail(err, "spatial order");
+        h->perm_n = n;
+    }
+    if (h->perm_n == n) *perm = h->d_perm;
+    return MOG_OK;
+}
+
+// The kernels of one step (or of a force evaluation when acc != null).
 int run_pipeline(mog_handle* h, float4* pos, float4* vel, int64_t n, float dt, float4* acc,
-                 cudaStream_t s) {
+                 cudaStream_t s, bool sort) {
     const mog::Ensemble& e = h->e;
-    cudaError_t err = mog::launch_deposit(e, pos, n, h->d_mass, h->dshape, s);
+    const int* perm = nullptr;
+    int rc = order_particles(h, pos, n, sort, s, &perm);
+    if (rc) return rc;
+    cudaError_t err = mog::launch_deposit(e, pos, perm, n, h->d_mass, h->dshape, s);
     if (err != cudaSuccess) return cuda_fail(err, "deposit");
     if (h->cfg.solver == MOG_SOLVER_FFT)
         err = mog::launch_spectral(e, h->d_mass, h->d_force, true, true, h->d_scratch, s);
     else
         err = mog::launch_convolution(e, h->d_mass, h->d_force, true, true, s);
     if (err != cudaSuccess) return cuda_fail(err, "solve");
-    err = mog::launch_update(e, pos, vel, n, h->d_force, dt, h->cfg.damping, acc, h->ushape, s);
+    err = mog::launch_update(e, pos, vel, perm, n, h->d_force, dt, h->cfg.damping, acc, h->ushape, s);
     if (err != cudaSuccess) return cuda_fail(err, "update");
     return MOG_OK;
 }
@@ -251,7 +289,7 @@ void release(mog_handle* h) {
     h->graphs.clear();
     void* ptrs[] = {h->d_rot12, h->d_off4, h->d_fast, h->d_green, h->d_ktab, h->d_conv,
                     h->d_flags, h->d_total, h->d_mass, h->d_force, h->d_force2, h->d_scratch,
-                    h->d_diag};
+                    h->d_diag, h->d_perm, h->d_sort};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }
@@ -391,8 +429,10 @@ int mog_step(mog_handle* h, float* pos4, float* vel4, int64_t n, float dt_eff, v
     if (rc) return rc;
     if (!std::isfinite(dt_eff)) return fail(MOG_ERR_ARG, "dt_eff must be finite");
     if ((rc = set_device(h))) return rc;
-    return run_pipeline(h, reinterpret_cast<float4*>(pos4), reinterpret_cast<float4*>(vel4), n,
-                        dt_eff, nullptr, static_cast<cudaStream_t>(stream));
+    rc = run_pipeline(h, reinterpret_cast<float4*>(pos4), reinterpret_cast<float4*>(vel4), n,
+                      dt_eff, nullptr, static_cast<cudaStream_t>(stream), wants_sort(h, n));
+    if (!rc) ++h->step_count;
+    return rc;
 }
 
 int mog_step_n(mog_handle* h, float* pos4, float* vel4, int64_t n, float dt_eff, int32_t n_steps,
@@ -407,42 +447,53 @@ int mog_step_n(mog_handle* h, float* pos4, float* vel4, int64_t n, float dt_eff,
     if (n_steps == 0 || n == 0) return MOG_OK;
     // The legacy default stream cannot be captured: run the steps directly.
     if (s == nullptr || s == cudaStreamLegacy) {
-        for (int i = 0; i < n_steps; ++i)
+        for (int i = 0; i < n_steps; ++i) {
             if ((rc = run_pipeline(h, reinterpret_cast<float4*>(pos4),
-                                   reinterpret_cast<float4*>(vel4), n, dt_eff, nullptr, s)))
+                                   reinterpret_cast<float4*>(vel4), n, dt_eff, nullptr, s,
+                                   wants_sort(h, n))))
                 return rc;
+            ++h->step_count;
+        }
         return MOG_OK;
     }
-    GraphEntry* ge = nullptr;
-    for (auto& g : h->graphs)
-        if (g.pos == pos4 && g.vel == vel4 && g.n == n && g.dt == dt_eff) ge = &g;
-    if (!ge) {
-        cudaGraph_t graph = nullptr;
-        MOG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
-        rc = run_pipeline(h, reinterpret_cast<float4*>(pos4), reinterpret_cast<float4*>(vel4), n,
-                          dt_eff, nullptr, s);
-        cudaError_t end = cudaStreamEndCapture(s, &graph);
-        if (rc) {
-            if (graph) cudaGraphDestroy(graph);
-            return rc;
+    for (int i = 0; i < n_steps; ++i) {
+        // Two graphs per particle set: with and without the re-ordering.
+        const bool sorts = wants_sort(h, n);
+        if (h->perm_n != n && h->sort_every > 0 && !sorts) return fail(MOG_ERR_ARG, "internal: no order");
+        GraphEntry* ge = nullptr;
+        for (auto& g : h->graphs)
+            if (g.pos == pos4 && g.vel == vel4 && g.n == n && g.dt == dt_eff && g.sorts == sorts)
+                ge = &g;
+        if (!ge) {
+            cudaGraph_t graph = nullptr;
+            MOG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
+            rc = run_pipeline(h, reinterpret_cast<float4*>(pos4), reinterpret_cast<float4*>(vel4), n,
+                              dt_eff, nullptr, s, sorts);
+            cudaError_t end = cudaStreamEndCapture(s, &graph);
+            if (rc) {
+                if (graph) cudaGraphDestroy(graph);
+                return rc;
+            }
+            if (end != cudaSuccess) return cuda_fail(end, "end capture");
+            GraphEntry entry;
+            entry.pos = pos4;
+            entry.vel = vel4;
+            entry.n = n;
+            entry.dt = dt_eff;
+            entry.sorts = sorts;
+            cudaError_t err = cudaGraphInstantiate(&entry.exec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (err != cudaSuccess) return cuda_fail(err, "graph instantiate");
+            if (h->graphs.size() >= 8) {
+                cudaGraphExecDestroy(h->graphs.front().exec);
+                h->graphs.erase(h->graphs.begin());
+            }
+            h->graphs.push_back(entry);
+            ge = &h->graphs.back();
         }
-        if (end != cudaSuccess) return cuda_fail(end, "end capture");
-        GraphEntry entry;
-        entry.pos = pos4;
-        entry.vel = vel4;
-        entry.n = n;
-        entry.dt = dt_eff;
-        cudaError_t err = cudaGraphInstantiate(&entry.exec, graph, 0);
-        cudaGraphDestroy(graph);
-        if (err != cudaSuccess) return cuda_fail(err, "graph instantiate");
-        if (h->graphs.size() >= 8) {
-            cudaGraphExecDestroy(h->graphs.front().exec);
-            h->graphs.erase(h->graphs.begin());
-        }
-        h->graphs.push_back(entry);
-        ge = &h->graphs.back();
+        MOG_CUDA(cudaGraphLaunch(ge->exec, s), "graph launch");
+        ++h->step_count;
     }
-    for (int i = 0; i < n_steps; ++i) MOG_CUDA(cudaGraphLaunch(ge->exec, s), "graph launch");
     return MOG_OK;
 }
 
@@ -454,25 +505,37 @@ int mog_step_profiled(mog_handle* h, float* pos4, float* vel4, int64_t n, float 
     if (!std::isfinite(dt_eff)) return fail(MOG_ERR_ARG, "dt_eff must be finite");
     if ((rc = set_device(h))) return rc;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    cudaEvent_t ev[4];
+    cudaEvent_t ev[5];
     for (auto& e : ev) MOG_CUDA(cudaEventCreate(&e), "event create");
     const mog::Ensemble& e = h->e;
     float4* pos = reinterpret_cast<float4*>(pos4);
     float4* vel = reinterpret_cast<float4*>(vel4);
+    const int* perm = nullptr;
     cudaError_t err = cudaEventRecord(ev[0], s);
-    if (!err) err = mog::launch_deposit(e, pos, n, h->d_mass, h->dshape, s);
+    if (!err) {
+        rc = order_particles(h, pos, n, wants_sort(h, n), s, &perm);
+        if (rc) {
+            for (auto& x : ev) cudaEventDestroy(x);
+            return rc;
+        }
+    }
     if (!err) err = cudaEventRecord(ev[1], s);
+    if (!err) err = mog::launch_deposit(e, pos, perm, n, h->d_mass, h->dshape, s);
+    if (!err) err = cudaEventRecord(ev[2], s);
     if (!err)
         err = h->cfg.solver == MOG_SOLVER_FFT
                   ? mog::launch_spectral(e, h->d_mass, h->d_force, true, true, h->d_scratch, s)
                   : mog::launch_convolution(e, h->d_mass, h->d_force, true, true, s);
-    if (!err) err = cudaEventRecord(ev[2], s);
-    if (!err) err = mog::launch_update(e, pos, vel, n, h->d_force, dt_eff, h->cfg.damping, nullptr, h->ushape, s);
     if (!err) err = cudaEventRecord(ev[3], s);
-    if (!err) err = cudaEventSynchronize(ev[3]);
-    for (int i = 0; i < 3 && !err; ++i) err = cudaEventElapsedTime(&phase_ms[i], ev[i], ev[i + 1]);
+    if (!err)
+        err = mog::launch_update(e, pos, vel, perm, n, h->d_force, dt_eff, h->cfg.damping, nullptr,
+                                 h->ushape, s);
+    if (!err) err = cudaEventRecord(ev[4], s);
+    if (!err) err = cudaEventSynchronize(ev[4]);
+    for (int i = 0; i < 4 && !err; ++i) err = cudaEventElapsedTime(&phase_ms[i], ev[i], ev[i + 1]);
     for (auto& x : ev) cudaEventDestroy(x);
     if (err) return cuda_fail(err, "profiled step");
+    ++h->step_count;
     return MOG_OK;
 }
 
@@ -482,7 +545,8 @@ int mog_forces(mog_handle* h, const float* pos4, float* acc4, int64_t n, void* s
     if (rc) return rc;
     if ((rc = set_device(h))) return rc;
     return run_pipeline(h, const_cast<float4*>(reinterpret_cast<const float4*>(pos4)), nullptr, n,
-                        0.f, reinterpret_cast<float4*>(acc4), static_cast<cudaStream_t>(stream));
+                        0.f, reinterpret_cast<float4*>(acc4), static_cast<cudaStream_t>(stream),
+                        h->sort_every > 0);
 }
 
 int mog_deposit(mog_handle* h, const float* pos4, int64_t n, void* mass_out, void* stream) {
@@ -493,8 +557,11 @@ int mog_deposit(mog_handle* h, const float* pos4, int64_t n, void* mass_out, voi
     if ((rc = set_device(h))) return rc;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     MOG_CUDA(cudaMemsetAsync(mass_out, 0, mass_bytes(h), s), "clear mass");
-    cudaError_t err =
-        mog::launch_deposit(h->e, reinterpret_cast<const float4*>(pos4), n, mass_out, h->dshape, s);
+    const int* perm = nullptr;
+    if ((rc = order_particles(h, reinterpret_cast<const float4*>(pos4), n, h->sort_every > 0, s, &perm)))
+        return rc;
+    cudaError_t err = mog::launch_deposit(h->e, reinterpret_cast<const float4*>(pos4), perm, n,
+                                          mass_out, h->dshape, s);
     if (err != cudaSuccess) return cuda_fail(err, "deposit");
     mog::check_total_kernel<<<1, 1, 0, s>>>(h->e);
     MOG_CUDA(cudaGetLastError(), "check total");
@@ -531,8 +598,11 @@ int mog_update(mog_handle* h, float* pos4, float* vel4, int64_t n, const float* 
     if (!h->d_force2) MOG_CUDA(cudaMalloc((void**)&h->d_force2, sizeof(float4) * h->e.cells()), "cudaMalloc force2");
     cudaError_t err = mog::launch_prerotate(h->e, reinterpret_cast<const float4*>(force4_in), h->d_force2, s);
     if (err != cudaSuccess) return cuda_fail(err, "prerotate");
-    err = mog::launch_update(h->e, reinterpret_cast<float4*>(pos4), reinterpret_cast<float4*>(vel4), n,
-                             h->d_force2, dt_eff, h->cfg.damping, nullptr, h->ushape, s);
+    const int* perm = nullptr;
+    if ((rc = order_particles(h, reinterpret_cast<const float4*>(pos4), n, h->sort_every > 0, s, &perm)))
+        return rc;
+    err = mog::launch_update(h->e, reinterpret_cast<float4*>(pos4), reinterpret_cast<float4*>(vel4),
+                             perm, n, h->d_force2, dt_eff, h->cfg.damping, nullptr, h->ushape, s);
     if (err != cudaSuccess) return cuda_fail(err, "update");
     return MOG_OK;
 }
@@ -546,6 +616,8 @@ int mog_get_tuning(const mog_handle* h, mog_tuning* out) {
     out->deposit_ppt = h->dshape.ppt;
     out->update_staged = h->ushape.staged;
     out->update_ctas = h->ushape.ctas;
+    out->sort_every = h->sort_every;
+    out->update_direct_ppt = h->ushape.direct_ppt;
     return MOG_OK;
 }
 
@@ -556,7 +628,10 @@ int mog_set_tuning(mog_handle* h, const mog_tuning* t) {
         return fail(MOG_ERR_ARG, "deposit_threads must be a multiple of 32 in [64, 1024]");
     if (t->deposit_grids_per_cta < -1 || t->deposit_chunks < 0 || t->update_ctas < 0 ||
         t->update_staged < -1 || t->update_staged > 1 ||
-        (t->deposit_ppt != 0 && t->deposit_ppt != 1 && t->deposit_ppt != 2 && t->deposit_ppt != 4))
+        (t->deposit_ppt != 0 && t->deposit_ppt != 1 && t->deposit_ppt != 2 && t->deposit_ppt != 4) ||
+        t->sort_every < -1 ||
+        (t->update_direct_ppt != 0 && t->update_direct_ppt != 1 && t->update_direct_ppt != 2 &&
+         t->update_direct_ppt != 4))
         return fail(MOG_ERR_ARG, "tuning value out of range");
     h->dshape.threads = t->deposit_threads ? t->deposit_threads : 1024;
     h->dshape.grids_per_cta = t->deposit_grids_per_cta;
@@ -564,6 +639,8 @@ int mog_set_tuning(mog_handle* h, const mog_tuning* t) {
     h->dshape.ppt = t->deposit_ppt ? t->deposit_ppt : 2;
     h->ushape.staged = t->update_staged;
     h->ushape.ctas = t->update_ctas;
+    h->ushape.direct_ppt = t->update_direct_ppt ? t->update_direct_ppt : 4;
+    h->sort_every = t->sort_every < 0 ? 1 : t->sort_every;
     for (auto& g : h->graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);
     h->graphs.clear();
@@ -597,6 +674,25 @@ int mog_diagnostics(mog_handle* h, const float* pos4, const float* vel4, int64_t
     if (err != cudaSuccess) return cuda_fail(err, "diagnostics");
     MOG_CUDA(cudaMemcpyAsync(out8, res, 8 * sizeof(double), cudaMemcpyDeviceToHost, s), "read diagnostics");
     MOG_CUDA(cudaStreamSynchronize(s), "sync");
+    return MOG_OK;
+}
+
+int mog_direct_sum(const float* targets4, int64_t nt, const float* sources4, int64_t ns,
+                   double world, double g_eff, double soft, double* out3, void* stream) {
+    if (nt < 0 || ns < 0) return fail(MOG_ERR_ARG, "negative size");
+    if ((nt && (!targets4 || !out3)) || (ns && !sources4)) return fail(MOG_ERR_ARG, "null buffer");
+    if (!(world > 0.0) || !std::isfinite(g_eff) || !(soft >= 0.0))
+        return fail(MOG_ERR_ARG, "world must be positive, g_eff finite, soft >= 0");
+    if (nt == 0) return MOG_OK;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int chunks = (int)std::max<int64_t>(1, std::min<int64_t>(32, (ns + 8191) / 8192));
+    double* partial = nullptr;
+    MOG_CUDA(cudaMallocAsync((void**)&partial, sizeof(double) * 3 * nt * chunks, s), "alloc partial");
+    cudaError_t err = mog::launch_direct_sum(reinterpret_cast<const float4*>(targets4), nt,
+                                             reinterpret_cast<const float4*>(sources4), ns, world,
+                                             g_eff, soft, partial, chunks, out3, s);
+    cudaFreeAsync(partial, s);
+    if (err != cudaSuccess) return cuda_fail(err, "direct sum");
     return MOG_OK;
 }
 

@@ -48,20 +48,22 @@ struct DepositShape {
     int threads = 1024;
     int grids_per_cta = 0;  // 0 = default for (g, mass mode); -1 = global atomics
     int chunks = 0;         // particle chunks; 0 = derived from n
-    int ppt = 2;            // particles per thread carried through the grid loop
+    int ppt = 4;            // particles per thread carried through the grid loop
 };
 struct UpdateShape {
-    int threads = 1024;
+    int threads = 512;
     int staged = -1;        // -1 auto, 0 global gathers, 1 smem-staged grids
     int ctas = 0;           // staged kernel CTAs; 0 = one per SM
+    int direct_ppt = 4;     // particles per thread of the direct gather
 };
 
 int num_sms();
 
 // mass grid (u64 or u32 per mode) <- particles.  Zeroes nothing: the
 // caller provides a zeroed grid.
-cudaError_t launch_deposit(const Ensemble& e, const float4* pos, int64_t n, void* mass,
-                           const DepositShape& shape, cudaStream_t s);
+// perm (nullable): slot s processes particle perm[s].
+cudaError_t launch_deposit(const Ensemble& e, const float4* pos, const int* perm, int64_t n,
+                           void* mass, const DepositShape& shape, cudaStream_t s);
 
 // force grid (float4 per cell) <- mass grid.  world_frame: rotate each
 // cell's force by M_i and store (x, y, z, 0) — what the production gather
@@ -81,9 +83,15 @@ cudaError_t launch_prerotate(const Ensemble& e, const float4* force_grid, float4
 
 // Gather + average + (optionally) leapfrog.  When acc_out is non-null the
 // averaged force is written there and pos/vel are left untouched.
-cudaError_t launch_update(const Ensemble& e, float4* pos, float4* vel, int64_t n,
-                          const float4* force_world, float dt, float damping,
+cudaError_t launch_update(const Ensemble& e, float4* pos, float4* vel, const int* perm,
+                          int64_t n, const float4* force_world, float dt, float damping,
                           float4* acc_out, const UpdateShape& shape, cudaStream_t s);
+
+// Spatial ordering: perm <- particles sorted by the Morton index of their
+// 32^3 world cell.  scratch: sort_scratch_bytes() bytes.
+size_t sort_scratch_bytes();
+cudaError_t launch_sort(const float4* pos, int64_t n, float world, void* scratch, int* perm,
+                        cudaStream_t s);
 
 // Green's-function and wave-number tables (FP64 arithmetic on the device).
 cudaError_t launch_build_tables(int g, float world, float G, float* green, float* ktab,
@@ -92,5 +100,11 @@ cudaError_t launch_build_tables(int g, float world, float G, float* green, float
 // FP64 momentum / energy / mass / centre-of-mass reduction.
 cudaError_t launch_diagnostics(const float4* pos, const float4* vel, int64_t n, double* partial,
                                int nblocks, double* out8, cudaStream_t s);
+
+// FP64 direct-sum judge: out3[t] = g_eff * sum_j m_j d / (|d|^2 + soft^2)^1.5
+// over minimum-image separations.  partial: chunks * nt * 3 doubles.
+cudaError_t launch_direct_sum(const float4* targets, int64_t nt, const float4* sources, int64_t ns,
+                              double world, double g_eff, double soft, double* partial, int chunks,
+                              double* out3, cudaStream_t s);
 
 }  // namespace mog

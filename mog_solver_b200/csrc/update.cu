@@ -104,13 +104,21 @@ __device__ __forceinline__ uint32_t cell_of(int idx_mode, const float* xf, float
     return cell_exact(xf, xf + 12, cx, cy, cz, ip);
 }
 
-// Staged gather.  Launch: one CTA per SM (smem-bound), `threads` threads,
-// each thread owning up to PPT particles p = lo + tid + j * threads.
+__device__ __forceinline__ int64_t particle_of(const int* __restrict__ perm, int64_t slot) {
+    return perm ? (int64_t)__ldg(perm + slot) : slot;
+}
+
+// Staged gather.  Launch: one CTA per SM (shared-memory bound).  The CTA
+// owns slots [lo, hi); thread t owns `ppt` consecutive slots starting at
+// lo + t * ppt, so that with a spatial ordering its particles are
+// neighbours: when a particle falls in the same cell as the previous one
+// the shared-memory load is reused.
 template <int IDX, int PPT, bool ACC_OUT>
 __global__ void __launch_bounds__(512, 1)
-    update_staged_kernel(float4* __restrict__ pos, float4* __restrict__ vel, int64_t n,
-                         int64_t per_cta, const float4* __restrict__ W, Ensemble e, float dt,
-                         float damp, float4* __restrict__ acc_out, int nstage) {
+    update_staged_kernel(float4* __restrict__ pos, float4* __restrict__ vel,
+                         const int* __restrict__ perm, int64_t n, int64_t per_cta,
+                         const float4* __restrict__ W, Ensemble e, float dt, float damp,
+                         float4* __restrict__ acc_out, int nstage) {
     extern __shared__ __align__(128) unsigned char smem[];
     const int G3 = 1 << (3 * e.lg);
     const unsigned grid_bytes = (unsigned)G3 * 16u;
@@ -146,21 +154,20 @@ __global__ void __launch_bounds__(512, 1)
     const IndexParams ip = e.index_params();
     const int64_t lo = (int64_t)blockIdx.x * per_cta;
     const int64_t hi = min(n, lo + per_cta);
+    const int ppt = (int)((per_cta + T - 1) / T);
+    const int64_t first = lo + (int64_t)tid * ppt;
+    const int64_t mine = hi - first;
+    const int cnt = mine <= 0 ? 0 : (int)(mine < ppt ? mine : ppt);
     float cx[PPT], cy[PPT], cz[PPT], ax[PPT], ay[PPT], az[PPT];
 #pragma unroll
     for (int j = 0; j < PPT; ++j) {
-        const int64_t p = lo + tid + (int64_t)j * T;
         float4 P = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (p < hi) P = pos[p];
+        if (j < cnt) P = pos[particle_of(perm, first + j)];
         cx[j] = __fsub_rn(P.x, ip.half_l);
         cy[j] = __fsub_rn(P.y, ip.half_l);
         cz[j] = __fsub_rn(P.z, ip.half_l);
         ax[j] = ay[j] = az[j] = 0.f;
     }
-    // number of particle slots of this thread that are in range
-    const int64_t mine = hi - lo - tid;
-    const int64_t slots = (mine + T - 1) / T;
-    const int cnt = mine <= 0 ? 0 : (int)(slots < PPT ? slots : PPT);
 
     int i_abort = -1;
     for (int i = 0; i < e.k; ++i) {
@@ -169,11 +176,14 @@ __global__ void __launch_bounds__(512, 1)
         if (!mbar_wait_bounded(full + s, parity)) abort_flag = 1;
         const float4* F = stage + (size_t)s * G3;
         const float* x = xf + i * 16;
+        uint32_t prev = 0xffffffffu;
+        float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
         for (int j = 0; j < PPT; ++j) {
             if (j < cnt) {
                 const uint32_t c = cell_of(IDX, x, cx[j], cy[j], cz[j], ip);
-                const float4 f = F[c];
+                if (c != prev) f = F[c];
+                prev = c;
                 ax[j] = __fadd_rn(ax[j], f.x);
                 ay[j] = __fadd_rn(ay[j], f.y);
                 az[j] = __fadd_rn(az[j], f.z);
@@ -206,7 +216,7 @@ __global__ void __launch_bounds__(512, 1)
 #pragma unroll
     for (int j = 0; j < PPT; ++j) {
         if (j < cnt) {
-            const int64_t p = lo + tid + (int64_t)j * T;
+            const int64_t p = particle_of(perm, first + j);
             const float4 P = pos[p];
             finish_particle<ACC_OUT>(p, P, ax[j], ay[j], az[j], pos, vel, acc_out, kf, dt, damp,
                                      e.world, bad);
@@ -215,43 +225,67 @@ __global__ void __launch_bounds__(512, 1)
     if (bad) raise_flags(e.flags, bad);
 }
 
-// Direct gather from L2: one thread per particle, any g.
-template <int IDX, bool ACC_OUT>
+// Direct gather from L1/L2, any g: each thread owns DPPT consecutive slots
+// and reuses a force value when consecutive particles share a cell.
+template <int IDX, int DPPT, bool ACC_OUT>
 __global__ void __launch_bounds__(256) update_direct_kernel(float4* __restrict__ pos,
-                                                            float4* __restrict__ vel, int64_t n,
+                                                            float4* __restrict__ vel,
+                                                            const int* __restrict__ perm,
+                                                            int64_t n,
                                                             const float4* __restrict__ W,
                                                             Ensemble e, float dt, float damp,
                                                             float4* __restrict__ acc_out) {
-    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
+    const int64_t first = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * DPPT;
+    if (first >= n) return;
+    const int cnt = (int)(n - first < DPPT ? n - first : DPPT);
     const IndexParams ip = e.index_params();
-    const float4 P = pos[p];
-    const float cx = __fsub_rn(P.x, ip.half_l);
-    const float cy = __fsub_rn(P.y, ip.half_l);
-    const float cz = __fsub_rn(P.z, ip.half_l);
+    float cx[DPPT], cy[DPPT], cz[DPPT], ax[DPPT], ay[DPPT], az[DPPT];
+#pragma unroll
+    for (int j = 0; j < DPPT; ++j) {
+        float4 P = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (j < cnt) P = pos[particle_of(perm, first + j)];
+        cx[j] = __fsub_rn(P.x, ip.half_l);
+        cy[j] = __fsub_rn(P.y, ip.half_l);
+        cz[j] = __fsub_rn(P.z, ip.half_l);
+        ax[j] = ay[j] = az[j] = 0.f;
+    }
     const int G3 = 1 << (3 * e.lg);
-    float ax = 0.f, ay = 0.f, az = 0.f;
     for (int i = 0; i < e.k; ++i) {
-        uint32_t c;
-        if (IDX == 0) {
-            const FastXf f = e.fast[i];
-            c = cell_fast(f.row[0], f.row[1], f.row[2], cx, cy, cz, ip.lg);
-        } else {
-            c = cell_exact(e.rot12 + 12 * i, e.off4 + 4 * i, cx, cy, cz, ip);
+        const float4* F = W + (size_t)i * G3;
+        uint32_t prev = 0xffffffffu;
+        float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int j = 0; j < DPPT; ++j) {
+            if (j < cnt) {
+                uint32_t c;
+                if (IDX == 0) {
+                    const FastXf x = e.fast[i];
+                    c = cell_fast(x.row[0], x.row[1], x.row[2], cx[j], cy[j], cz[j], ip.lg);
+                } else {
+                    c = cell_exact(e.rot12 + 12 * i, e.off4 + 4 * i, cx[j], cy[j], cz[j], ip);
+                }
+                if (c != prev) f = __ldg(F + c);
+                prev = c;
+                ax[j] = __fadd_rn(ax[j], f.x);
+                ay[j] = __fadd_rn(ay[j], f.y);
+                az[j] = __fadd_rn(az[j], f.z);
+            }
         }
-        const float4 f = __ldg(W + (size_t)i * G3 + c);
-        ax = __fadd_rn(ax, f.x);
-        ay = __fadd_rn(ay, f.y);
-        az = __fadd_rn(az, f.z);
     }
     unsigned bad = 0;
-    finish_particle<ACC_OUT>(p, P, ax, ay, az, pos, vel, acc_out, (float)e.k, dt, damp, e.world,
-                             bad);
+#pragma unroll
+    for (int j = 0; j < DPPT; ++j) {
+        if (j < cnt) {
+            const int64_t p = particle_of(perm, first + j);
+            finish_particle<ACC_OUT>(p, pos[p], ax[j], ay[j], az[j], pos, vel, acc_out,
+                                     (float)e.k, dt, damp, e.world, bad);
+        }
+    }
     if (bad) raise_flags(e.flags, bad);
 }
 
 template <int IDX, int PPT, bool ACC>
-cudaError_t launch_staged(const Ensemble& e, float4* pos, float4* vel, int64_t n,
+cudaError_t launch_staged(const Ensemble& e, float4* pos, float4* vel, const int* perm, int64_t n,
                           const float4* W, float dt, float damp, float4* acc, int ctas,
                           int threads, int nstage, size_t smem, cudaStream_t s) {
     auto kern = update_staged_kernel<IDX, PPT, ACC>;
@@ -259,13 +293,14 @@ cudaError_t launch_staged(const Ensemble& e, float4* pos, float4* vel, int64_t n
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess) return err;
     const int64_t per_cta = (n + ctas - 1) / ctas;
-    kern<<<ctas, threads, smem, s>>>(pos, vel, n, per_cta, W, e, dt, damp, acc, nstage);
+    kern<<<ctas, threads, smem, s>>>(pos, vel, perm, n, per_cta, W, e, dt, damp, acc, nstage);
     return cudaGetLastError();
 }
 
 template <int IDX, bool ACC>
-cudaError_t update_mode(const Ensemble& e, float4* pos, float4* vel, int64_t n, const float4* W,
-                        float dt, float damp, float4* acc, const UpdateShape& sh, cudaStream_t s) {
+cudaError_t update_mode(const Ensemble& e, float4* pos, float4* vel, const int* perm, int64_t n,
+                        const float4* W, float dt, float damp, float4* acc, const UpdateShape& sh,
+                        cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
     const size_t grid_bytes = (size_t)16 << (3 * e.lg);
     const int sms = num_sms();
@@ -279,45 +314,55 @@ cudaError_t update_mode(const Ensemble& e, float4* pos, float4* vel, int64_t n, 
         staged = e.g <= 16 && n >= (int64_t)sms * threads * 2 && smem <= 220 * 1024;
     if (staged && smem > 220 * 1024) staged = false;
     if (!staged) {
-        const int64_t blocks = (n + 255) / 256;
-        update_direct_kernel<IDX, ACC><<<(unsigned)blocks, 256, 0, s>>>(pos, vel, n, W, e, dt,
-                                                                         damp, acc);
+        const int dppt = sh.direct_ppt == 1 ? 1 : (sh.direct_ppt == 2 ? 2 : 4);
+        const int64_t threads_needed = (n + dppt - 1) / dppt;
+        const unsigned blocks = (unsigned)((threads_needed + 255) / 256);
+        if (dppt == 1)
+            update_direct_kernel<IDX, 1, ACC><<<blocks, 256, 0, s>>>(pos, vel, perm, n, W, e, dt,
+                                                                     damp, acc);
+        else if (dppt == 2)
+            update_direct_kernel<IDX, 2, ACC><<<blocks, 256, 0, s>>>(pos, vel, perm, n, W, e, dt,
+                                                                     damp, acc);
+        else
+            update_direct_kernel<IDX, 4, ACC><<<blocks, 256, 0, s>>>(pos, vel, perm, n, W, e, dt,
+                                                                     damp, acc);
         return cudaGetLastError();
     }
-    // Enough CTAs that PPT (particles per thread) stays within the template.
+    // Enough CTAs that the particles per thread stay within the template.
     int ctas = sh.ctas > 0 ? sh.ctas : sms;
     const int64_t per_thread = (n + (int64_t)ctas * threads - 1) / ((int64_t)ctas * threads);
     if (per_thread > 16) ctas = (int)((n + 16LL * threads - 1) / (16LL * threads));
     const int64_t ppt = (n + (int64_t)ctas * threads - 1) / ((int64_t)ctas * threads);
     if (ppt <= 4)
-        return launch_staged<IDX, 4, ACC>(e, pos, vel, n, W, dt, damp, acc, ctas, threads, nstage,
-                                          smem, s);
+        return launch_staged<IDX, 4, ACC>(e, pos, vel, perm, n, W, dt, damp, acc, ctas, threads,
+                                          nstage, smem, s);
     if (ppt <= 8)
-        return launch_staged<IDX, 8, ACC>(e, pos, vel, n, W, dt, damp, acc, ctas, threads, nstage,
-                                          smem, s);
+        return launch_staged<IDX, 8, ACC>(e, pos, vel, perm, n, W, dt, damp, acc, ctas, threads,
+                                          nstage, smem, s);
     if (ppt <= 12)
-        return launch_staged<IDX, 12, ACC>(e, pos, vel, n, W, dt, damp, acc, ctas, threads, nstage,
-                                           smem, s);
+        return launch_staged<IDX, 12, ACC>(e, pos, vel, perm, n, W, dt, damp, acc, ctas, threads,
+                                           nstage, smem, s);
     if (ppt <= 14)
-        return launch_staged<IDX, 14, ACC>(e, pos, vel, n, W, dt, damp, acc, ctas, threads, nstage,
-                                           smem, s);
-    return launch_staged<IDX, 16, ACC>(e, pos, vel, n, W, dt, damp, acc, ctas, threads, nstage,
-                                       smem, s);
+        return launch_staged<IDX, 14, ACC>(e, pos, vel, perm, n, W, dt, damp, acc, ctas, threads,
+                                           nstage, smem, s);
+    return launch_staged<IDX, 16, ACC>(e, pos, vel, perm, n, W, dt, damp, acc, ctas, threads,
+                                       nstage, smem, s);
 }
 
 }  // namespace
 
-cudaError_t launch_update(const Ensemble& e, float4* pos, float4* vel, int64_t n,
+cudaError_t launch_update(const Ensemble& e, float4* pos, float4* vel, const int* perm, int64_t n,
                           const float4* force_world, float dt, float damping, float4* acc_out,
                           const UpdateShape& shape, cudaStream_t s) {
-    if (acc_out) {
-        return e.index_mode == 0
-                   ? update_mode<0, true>(e, pos, vel, n, force_world, dt, damping, acc_out, shape, s)
-                   : update_mode<1, true>(e, pos, vel, n, force_world, dt, damping, acc_out, shape, s);
-    }
-    return e.index_mode == 0
-               ? update_mode<0, false>(e, pos, vel, n, force_world, dt, damping, nullptr, shape, s)
-               : update_mode<1, false>(e, pos, vel, n, force_world, dt, damping, nullptr, shape, s);
+    if (acc_out)
+        return e.index_mode == 0 ? update_mode<0, true>(e, pos, vel, perm, n, force_world, dt,
+                                                        damping, acc_out, shape, s)
+                                 : update_mode<1, true>(e, pos, vel, perm, n, force_world, dt,
+                                                        damping, acc_out, shape, s);
+    return e.index_mode == 0 ? update_mode<0, false>(e, pos, vel, perm, n, force_world, dt, damping,
+                                                     nullptr, shape, s)
+                             : update_mode<1, false>(e, pos, vel, perm, n, force_world, dt, damping,
+                                                     nullptr, shape, s);
 }
 
 }  // namespace mog
