@@ -106,8 +106,10 @@ typedef struct mog_tuning {
     int32_t deposit_ppt;            /* particles per thread in the deposit: 1, 2 or 4       */
     int32_t update_staged;          /* -1 auto, 0 gathers from L2, 1 shared-memory staged    */
     int32_t update_ctas;            /* CTAs of the staged gather (0 = one per SM)            */
-    int32_t sort_every;             /* spatial re-ordering period in steps; 0 = never, -1 = default (1) */
+    int32_t sort_every;             /* spatial re-ordering period in steps; 0 = never (default) */
     int32_t update_direct_ppt;      /* particles per thread of the L2-gather update: 1, 2, 4 */
+    int32_t deposit_aggregate;      /* warp-merge runs of equal cells: -1 auto, 0 off, 1 on  */
+    int32_t reserved;
 } mog_tuning;
 
 /* Fill a config with the reference's in-code defaults (main.py:179-189). */

@@ -87,6 +87,8 @@ class MogTuningC(ctypes.Structure):
         ("update_ctas", ctypes.c_int32),
         ("sort_every", ctypes.c_int32),
         ("update_direct_ppt", ctypes.c_int32),
+        ("deposit_aggregate", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
     ]
 
 

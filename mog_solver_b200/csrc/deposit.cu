@@ -77,8 +77,10 @@ struct SmemHist<1> {
 // cells of each grid (slab_lg == 3*lg means the whole grid).  Each thread
 // carries PPT particles through the grid loop, so the grid's cell-index
 // rows are loaded once per PPT particles and the PPT index computations
-// and shared adds overlap.
-template <int MODE, int IDX, int PPT>
+// and shared adds overlap.  With AGG (used when the particles come in
+// spatial order) the lanes of a warp merge runs of equal cells with a
+// ballot of run heads, so a run costs one shared add.
+template <int MODE, int IDX, int PPT, bool AGG>
 __global__ void __launch_bounds__(1024) deposit_smem_kernel(const float4* __restrict__ pos,
                                                             const int* __restrict__ perm,
                                                             int64_t n, int64_t chunk,
@@ -122,15 +124,16 @@ __global__ void __launch_bounds__(1024) deposit_smem_kernel(const float4* __rest
     unsigned bad = 0;
     double qsum = 0.0;
 
+    const int lane = threadIdx.x & 31;
     for (int64_t base = lo; base < hi; base += (int64_t)T * PPT) {
         float cx[PPT], cy[PPT], cz[PPT];
         Acc q[PPT];
         bool valid[PPT];
 #pragma unroll
         for (int u = 0; u < PPT; ++u) {
-            // each thread takes PPT consecutive slots: with a spatial
-            // ordering they are neighbours and mostly share cells
-            const int64_t slot = base + (int64_t)threadIdx.x * PPT + u;
+            // the 32 lanes of a warp take 32 consecutive slots, so with a
+            // spatial ordering they are neighbours and share cells
+            const int64_t slot = base + (int64_t)u * T + threadIdx.x;
             valid[u] = slot < hi;
             float4 P = make_float4(0.f, 0.f, 0.f, 0.f);
             if (valid[u]) P = __ldg(pos + (perm ? (int64_t)__ldg(perm + slot) : slot));
@@ -145,40 +148,56 @@ __global__ void __launch_bounds__(1024) deposit_smem_kernel(const float4* __rest
             cy[u] = __fsub_rn(P.y, ip.half_l);
             cz[u] = __fsub_rn(P.z, ip.half_l);
         }
+        // equal masses across the warp (checked once per batch) let a run
+        // of lanes on one cell add q * (run length) without a scan
+        bool uni[PPT];
+        if (AGG) {
+#pragma unroll
+            for (int u = 0; u < PPT; ++u) {
+                const unsigned vm = __ballot_sync(kFull, valid[u]);
+                const Acc q0 = __shfl_sync(kFull, q[u], vm ? __ffs(vm) - 1 : 0);
+                uni[u] = __all_sync(kFull, !valid[u] || q[u] == q0);
+            }
+        }
         for (int j = 0; j < ng; ++j) {
             unsigned* lw = lo_w + (size_t)j * slab_cells;
             unsigned* hw = hi_w + (size_t)j * slab_cells;
-            uint32_t key[PPT];
+            const float4* r = reinterpret_cast<const float4*>(xf + j * 16);
+            float4 r0, r1, r2;
             if (IDX == 0) {
-                const float4* r = reinterpret_cast<const float4*>(xf + j * 16);
-                const float4 r0 = r[0], r1 = r[1], r2 = r[2];
-#pragma unroll
-                for (int u = 0; u < PPT; ++u) {
-                    const uint32_t local = cell_fast(r0, r1, r2, cx[u], cy[u], cz[u], lg) - slab_lo;
-                    key[u] = (valid[u] && local < slab_cells) ? local : 0xffffffffu;
-                }
-            } else {
-#pragma unroll
-                for (int u = 0; u < PPT; ++u) {
-                    const uint32_t local =
-                        cell_exact(xf + j * 16, xf + j * 16 + 12, cx[u], cy[u], cz[u], ip) - slab_lo;
-                    key[u] = (valid[u] && local < slab_cells) ? local : 0xffffffffu;
-                }
+                r0 = r[0];
+                r1 = r[1];
+                r2 = r[2];
             }
-            // merge runs of equal cells before touching shared memory
-            uint32_t cur = key[0];
-            Acc acc = q[0];
 #pragma unroll
-            for (int u = 1; u < PPT; ++u) {
-                if (key[u] == cur) {
-                    acc += q[u];
+            for (int u = 0; u < PPT; ++u) {
+                uint32_t local;
+                if (IDX == 0)
+                    local = cell_fast(r0, r1, r2, cx[u], cy[u], cz[u], lg) - slab_lo;
+                else
+                    local = cell_exact(xf + j * 16, xf + j * 16 + 12, cx[u], cy[u], cz[u], ip) - slab_lo;
+                const uint32_t key = (valid[u] && local < slab_cells) ? local : 0xffffffffu;
+                if (!AGG) {
+                    if (key != 0xffffffffu) H::add(lw, hw, key, q[u]);
+                    continue;
+                }
+                // warp-segmented merge of runs of equal keys (sorted input)
+                const uint32_t prev = __shfl_up_sync(kFull, key, 1);
+                const unsigned heads = __ballot_sync(kFull, lane == 0 || key != prev);
+                const int start = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));
+                const bool tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
+                Acc v = q[u];
+                if (uni[u]) {
+                    v = q[u] * (Acc)(lane - start + 1);
                 } else {
-                    if (cur != 0xffffffffu) H::add(lw, hw, cur, acc);
-                    cur = key[u];
-                    acc = q[u];
+#pragma unroll
+                    for (int d = 1; d < 32; d <<= 1) {
+                        const Acc o = __shfl_up_sync(kFull, v, d);
+                        if (lane - d >= start) v += o;
+                    }
                 }
+                if (tail && key != 0xffffffffu) H::add(lw, hw, key, v);
             }
-            if (cur != 0xffffffffu) H::add(lw, hw, cur, acc);
         }
     }
 
@@ -263,6 +282,7 @@ static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, const int
     gpc = std::max(1, std::min(gpc, e.k));
     const size_t smem = (size_t)gpc * 16 * sizeof(float) + ((size_t)gpc * word_bytes << slab_lg);
     const int ppt = sh.ppt == 1 || sh.ppt == 2 || sh.ppt == 4 ? sh.ppt : 4;
+    const bool agg = sh.aggregate < 0 ? perm != nullptr : sh.aggregate != 0;
     auto launch = [&](auto kern) -> cudaError_t {
         cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                (int)smem);
@@ -283,9 +303,14 @@ static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, const int
         kern<<<grid, sh.threads, smem, s>>>(pos, perm, n, chunk, e, gpc, slab_lg, mass);
         return cudaGetLastError();
     };
-    if (ppt == 1) return launch(deposit_smem_kernel<MODE, IDX, 1>);
-    if (ppt == 4) return launch(deposit_smem_kernel<MODE, IDX, 4>);
-    return launch(deposit_smem_kernel<MODE, IDX, 2>);
+    if (agg) {
+        if (ppt == 1) return launch(deposit_smem_kernel<MODE, IDX, 1, true>);
+        if (ppt == 4) return launch(deposit_smem_kernel<MODE, IDX, 4, true>);
+        return launch(deposit_smem_kernel<MODE, IDX, 2, true>);
+    }
+    if (ppt == 1) return launch(deposit_smem_kernel<MODE, IDX, 1, false>);
+    if (ppt == 4) return launch(deposit_smem_kernel<MODE, IDX, 4, false>);
+    return launch(deposit_smem_kernel<MODE, IDX, 2, false>);
 }
 
 cudaError_t launch_deposit(const Ensemble& e, const float4* pos, const int* perm, int64_t n,

@@ -150,7 +150,7 @@ struct mog_handle {
     void* d_sort = nullptr;      // counting-sort scratch
     int64_t perm_cap = 0;        // capacity of d_perm
     int64_t perm_n = -1;         // n the permutation was built for
-    int sort_every = 1;          // re-order every this many steps (0 = never)
+    int sort_every = 0;          // re-order every this many steps (0 = never)
     uint64_t step_count = 0;     // steps issued (decides when to re-order)
     std::vector<GraphEntry> graphs;
 };
@@ -246,12 +246,15 @@ int order_particles(mog_handle* h, const float4* pos, int64_t n, bool sort, cuda
     if (h->sort_every <= 0 || n <= 0) return MOG_OK;
     if (sort) {
         if (n > h->perm_cap) {
+            cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+            cudaStreamIsCapturing(s, &cs);
+            if (cs != cudaStreamCaptureStatusNone)
+                return fail(MOG_ERR_ARG, "n exceeds num_particles inside a captured step");
             if (h->d_perm) cudaFree(h->d_perm);
             h->d_perm = nullptr;
             MOG_CUDA(cudaMalloc((void**)&h->d_perm, sizeof(int) * n), "cudaMalloc perm");
             h->perm_cap = n;
         }
-        if (!h->d_sort) MOG_CUDA(cudaMalloc(&h->d_sort, mog::sort_scratch_bytes()), "cudaMalloc sort");
         cudaError_t err = mog::launch_sort(pos, n, h->e.world, h->d_sort, h->d_perm, s);
         if (err != cudaSuccess) return cuda_fail(err, "spatial order");
         h->perm_n = n;
@@ -389,6 +392,13 @@ int mog_create(const mog_config* cfg, const float* rot12, const float* off4, mog
     ALLOC(h->d_diag, sizeof(double) * (kDiagBlocks * 8 + 8));
     const size_t scratch = mog::spectral_scratch_bytes(e);
     if (scratch) ALLOC(h->d_scratch, scratch);
+    // spatial-order buffers for the declared capacity (no allocation may
+    // happen later inside a captured step)
+    if (cfg->num_particles > 0) {
+        ALLOC(h->d_perm, sizeof(int) * cfg->num_particles);
+        h->perm_cap = cfg->num_particles;
+    }
+    ALLOC(h->d_sort, mog::sort_scratch_bytes());
 #undef ALLOC
     cudaError_t err;
     std::vector<float> convk = conv_kernel_table(g, hv);
@@ -617,6 +627,7 @@ int mog_get_tuning(const mog_handle* h, mog_tuning* out) {
     out->update_staged = h->ushape.staged;
     out->update_ctas = h->ushape.ctas;
     out->sort_every = h->sort_every;
+    out->deposit_aggregate = h->dshape.aggregate;
     out->update_direct_ppt = h->ushape.direct_ppt;
     return MOG_OK;
 }
@@ -629,7 +640,7 @@ int mog_set_tuning(mog_handle* h, const mog_tuning* t) {
     if (t->deposit_grids_per_cta < -1 || t->deposit_chunks < 0 || t->update_ctas < 0 ||
         t->update_staged < -1 || t->update_staged > 1 ||
         (t->deposit_ppt != 0 && t->deposit_ppt != 1 && t->deposit_ppt != 2 && t->deposit_ppt != 4) ||
-        t->sort_every < -1 ||
+        t->sort_every < -1 || t->deposit_aggregate < -1 || t->deposit_aggregate > 1 ||
         (t->update_direct_ppt != 0 && t->update_direct_ppt != 1 && t->update_direct_ppt != 2 &&
          t->update_direct_ppt != 4))
         return fail(MOG_ERR_ARG, "tuning value out of range");
@@ -641,6 +652,7 @@ int mog_set_tuning(mog_handle* h, const mog_tuning* t) {
     h->ushape.ctas = t->update_ctas;
     h->ushape.direct_ppt = t->update_direct_ppt ? t->update_direct_ppt : 4;
     h->sort_every = t->sort_every < 0 ? 1 : t->sort_every;
+    h->dshape.aggregate = t->deposit_aggregate;
     for (auto& g : h->graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);
     h->graphs.clear();

@@ -49,6 +49,7 @@ struct DepositShape {
     int grids_per_cta = 0;  // 0 = default for (g, mass mode); -1 = global atomics
     int chunks = 0;         // particle chunks; 0 = derived from n
     int ppt = 4;            // particles per thread carried through the grid loop
+    int aggregate = -1;     // warp-merge runs of equal cells: -1 auto (when ordered), 0, 1
 };
 struct UpdateShape {
     int threads = 512;

@@ -109,10 +109,10 @@ __device__ __forceinline__ int64_t particle_of(const int* __restrict__ perm, int
 }
 
 // Staged gather.  Launch: one CTA per SM (shared-memory bound).  The CTA
-// owns slots [lo, hi); thread t owns `ppt` consecutive slots starting at
-// lo + t * ppt, so that with a spatial ordering its particles are
-// neighbours: when a particle falls in the same cell as the previous one
-// the shared-memory load is reused.
+// owns slots [lo, hi); thread t owns slots lo + t + j * blockDim, so the
+// 32 lanes of a warp always hold consecutive slots: with a spatial
+// ordering they fall in the same few cells and their shared-memory loads
+// broadcast instead of conflicting.
 template <int IDX, int PPT, bool ACC_OUT>
 __global__ void __launch_bounds__(512, 1)
     update_staged_kernel(float4* __restrict__ pos, float4* __restrict__ vel,
@@ -154,15 +154,15 @@ __global__ void __launch_bounds__(512, 1)
     const IndexParams ip = e.index_params();
     const int64_t lo = (int64_t)blockIdx.x * per_cta;
     const int64_t hi = min(n, lo + per_cta);
-    const int ppt = (int)((per_cta + T - 1) / T);
-    const int64_t first = lo + (int64_t)tid * ppt;
+    const int64_t first = lo + tid;
     const int64_t mine = hi - first;
-    const int cnt = mine <= 0 ? 0 : (int)(mine < ppt ? mine : ppt);
+    const int64_t slots = (mine + T - 1) / T;
+    const int cnt = mine <= 0 ? 0 : (int)(slots < PPT ? slots : PPT);
     float cx[PPT], cy[PPT], cz[PPT], ax[PPT], ay[PPT], az[PPT];
 #pragma unroll
     for (int j = 0; j < PPT; ++j) {
         float4 P = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (j < cnt) P = pos[particle_of(perm, first + j)];
+        if (j < cnt) P = pos[particle_of(perm, first + (int64_t)j * T)];
         cx[j] = __fsub_rn(P.x, ip.half_l);
         cy[j] = __fsub_rn(P.y, ip.half_l);
         cz[j] = __fsub_rn(P.z, ip.half_l);
@@ -176,14 +176,11 @@ __global__ void __launch_bounds__(512, 1)
         if (!mbar_wait_bounded(full + s, parity)) abort_flag = 1;
         const float4* F = stage + (size_t)s * G3;
         const float* x = xf + i * 16;
-        uint32_t prev = 0xffffffffu;
-        float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
         for (int j = 0; j < PPT; ++j) {
             if (j < cnt) {
                 const uint32_t c = cell_of(IDX, x, cx[j], cy[j], cz[j], ip);
-                if (c != prev) f = F[c];
-                prev = c;
+                const float4 f = F[c];
                 ax[j] = __fadd_rn(ax[j], f.x);
                 ay[j] = __fadd_rn(ay[j], f.y);
                 az[j] = __fadd_rn(az[j], f.z);
@@ -216,7 +213,7 @@ __global__ void __launch_bounds__(512, 1)
 #pragma unroll
     for (int j = 0; j < PPT; ++j) {
         if (j < cnt) {
-            const int64_t p = particle_of(perm, first + j);
+            const int64_t p = particle_of(perm, first + (int64_t)j * T);
             const float4 P = pos[p];
             finish_particle<ACC_OUT>(p, P, ax[j], ay[j], az[j], pos, vel, acc_out, kf, dt, damp,
                                      e.world, bad);

@@ -159,6 +159,12 @@ class Simulation:
                        "mog_create")
         self._handle = h
         self._handle_bits = bits
+        if getattr(self, "_tuning", None):
+            t = _lib.MogTuningC()
+            _lib.check(lib.mog_get_tuning(h, ctypes.byref(t)), "mog_get_tuning")
+            for k, v in self._tuning.items():
+                setattr(t, k, int(v))
+            _lib.check(lib.mog_set_tuning(h, ctypes.byref(t)), "mog_set_tuning")
         return h
 
     def close(self) -> None:
@@ -172,6 +178,24 @@ class Simulation:
             self.close()
         except Exception:
             pass
+
+    def tuning(self) -> dict[str, int]:
+        """Current launch shapes of the handle (mog_get_tuning)."""
+        t = _lib.MogTuningC()
+        _lib.check(_lib.lib().mog_get_tuning(self.handle, ctypes.byref(t)), "mog_get_tuning")
+        return {name: getattr(t, name) for name, _ in t._fields_ if name != "reserved"}
+
+    def tune(self, **shapes: int) -> None:
+        """Set launch shapes (mog_set_tuning); results never depend on them."""
+        t = _lib.MogTuningC()
+        lib = _lib.lib()
+        _lib.check(lib.mog_get_tuning(self.handle, ctypes.byref(t)), "mog_get_tuning")
+        for k, v in shapes.items():
+            if k not in {name for name, _ in t._fields_}:
+                raise KeyError(f"unknown tuning field {k!r}")
+            setattr(t, k, int(v))
+        _lib.check(lib.mog_set_tuning(self.handle, ctypes.byref(t)), "mog_set_tuning")
+        self._tuning = dict(shapes)
 
     # ------------------------------------------------------------------
     def set_particles(self, pos, vel=None) -> None:

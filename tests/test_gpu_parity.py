@@ -58,12 +58,24 @@ SHAPES = [(1, 1, 8), (7, 3, 16), (257, 16, 16), (65536, 16, 16), (5000, 5, 32), 
           (4096, 3, 64)]
 
 
+# launch shapes that take different code paths; none may change a bit
+DEPOSIT_TUNINGS = {
+    "sorted+merged": dict(sort_every=1, deposit_aggregate=-1),
+    "unsorted": dict(sort_every=0, deposit_aggregate=0),
+    "sorted+plain": dict(sort_every=1, deposit_aggregate=0, deposit_ppt=1),
+    "unsorted+merged": dict(sort_every=0, deposit_aggregate=1, deposit_ppt=2),
+    "global": dict(sort_every=0, deposit_grids_per_cta=-1),
+}
+
+
 @pytest.mark.parametrize("mass_mode,index_mode", MODES)
 @pytest.mark.parametrize("n,k,g", SHAPES)
 @pytest.mark.parametrize("equal_mass", [True, False])
-def test_deposit_bit_exact(mass_mode, index_mode, n, k, g, equal_mass):
+@pytest.mark.parametrize("tuning", ["sorted+merged", "unsorted"])
+def test_deposit_bit_exact(mass_mode, index_mode, n, k, g, equal_mass, tuning):
     L = 100.0
     sim = make_sim(k=k, g=g, L=L, n=n, mass_mode=mass_mode, index_mode=index_mode, seed=n + k)
+    sim.tune(**DEPOSIT_TUNINGS[tuning])
     mass = None
     if mass_mode == "u32x1000":
         mass = 1.0 if equal_mass else np.random.default_rng(1).uniform(0.5, 3.0, n).astype(np.float32)
@@ -80,6 +92,23 @@ def test_deposit_bit_exact(mass_mode, index_mode, n, k, g, equal_mass):
     assert sim.status() == 0
 
 
+@pytest.mark.parametrize("tuning", sorted(DEPOSIT_TUNINGS))
+@pytest.mark.parametrize("mass_mode", ["u64", "u32x1000"])
+def test_deposit_tunings_bit_exact(tuning, mass_mode):
+    n, k, g, L = 100000, 12, 16, 100.0
+    sim = make_sim(k=k, g=g, L=L, n=n, mass_mode=mass_mode)
+    sim.tune(**DEPOSIT_TUNINGS[tuning])
+    mass = 1.0 if mass_mode == "u32x1000" else None
+    for equal in (True, False):
+        m = mass if (mass is None or equal) else np.random.default_rng(2).uniform(0.5, 2, n)
+        pos, vel = particles(n, L, seed=6, equal_mass=equal, mass=m)
+        sim.set_particles(pos, vel)
+        got = sim.mass_grid().cpu().numpy()
+        mm = oracle.MASS_U64 if mass_mode == "u64" else oracle.MASS_U32
+        ref = oracle.deposit(pos, sim.rotations, sim.offsets, g, L, mm, sim.scale_bits)
+        assert np.array_equal(got.view(ref.dtype), ref)
+
+
 def test_deposit_repeat_is_identical():
     sim = make_sim(k=32, g=16, n=200000)
     pos, vel = particles(200000, seed=3)
@@ -89,13 +118,23 @@ def test_deposit_repeat_is_identical():
     assert np.array_equal(a, b)
 
 
+UPDATE_TUNINGS = {
+    "auto": dict(),
+    "unsorted": dict(sort_every=0),
+    "direct4": dict(update_staged=0, update_direct_ppt=4),
+    "direct1-unsorted": dict(update_staged=0, update_direct_ppt=1, sort_every=0),
+}
+
+
 @pytest.mark.parametrize("index_mode", ["fast", "exact"])
 @pytest.mark.parametrize("n,k,g", [(1, 1, 8), (1000, 3, 16), (200000, 24, 16), (3000, 4, 32),
                                    (160000, 8, 8), (1 << 20, 4, 16)])
-def test_update_bit_exact(index_mode, n, k, g):
+@pytest.mark.parametrize("tuning", sorted(UPDATE_TUNINGS))
+def test_update_bit_exact(index_mode, n, k, g, tuning):
     """update.glsl from one force grid: GPU (direct or staged) == C oracle."""
     L = 100.0
     sim = make_sim(k=k, g=g, L=L, n=n, index_mode=index_mode, dt=3e-3, damping=0.97)
+    sim.tune(**UPDATE_TUNINGS[tuning])
     pos, vel = particles(n, L, seed=11)
     sim.set_particles(pos, vel)
     rng = np.random.default_rng(5)
