@@ -257,7 +257,8 @@ __global__ void __launch_bounds__(256) deposit_global_kernel(const float4* __res
 
 template <int MODE, int IDX>
 static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, const int* perm, int64_t n,
-                                 void* mass_v, const DepositShape& sh, cudaStream_t s) {
+                                 bool ordered, void* mass_v, const DepositShape& sh,
+                                 cudaStream_t s) {
     using H = SmemHist<MODE>;
     using Acc = typename H::Acc;
     Acc* mass = static_cast<Acc*>(mass_v);
@@ -282,7 +283,7 @@ static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, const int
     gpc = std::max(1, std::min(gpc, e.k));
     const size_t smem = (size_t)gpc * 16 * sizeof(float) + ((size_t)gpc * word_bytes << slab_lg);
     const int ppt = sh.ppt == 1 || sh.ppt == 2 || sh.ppt == 4 ? sh.ppt : 4;
-    const bool agg = sh.aggregate < 0 ? perm != nullptr : sh.aggregate != 0;
+    const bool agg = sh.aggregate < 0 ? ordered : sh.aggregate != 0;
     auto launch = [&](auto kern) -> cudaError_t {
         cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                (int)smem);
@@ -314,12 +315,12 @@ static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, const int
 }
 
 cudaError_t launch_deposit(const Ensemble& e, const float4* pos, const int* perm, int64_t n,
-                           void* mass, const DepositShape& shape, cudaStream_t s) {
+                           bool ordered, void* mass, const DepositShape& shape, cudaStream_t s) {
     if (e.mass_mode == 0)
-        return e.index_mode == 0 ? deposit_typed<1, 0>(e, pos, perm, n, mass, shape, s)
-                                 : deposit_typed<1, 1>(e, pos, perm, n, mass, shape, s);
-    return e.index_mode == 0 ? deposit_typed<0, 0>(e, pos, perm, n, mass, shape, s)
-                             : deposit_typed<0, 1>(e, pos, perm, n, mass, shape, s);
+        return e.index_mode == 0 ? deposit_typed<1, 0>(e, pos, perm, n, ordered, mass, shape, s)
+                                 : deposit_typed<1, 1>(e, pos, perm, n, ordered, mass, shape, s);
+    return e.index_mode == 0 ? deposit_typed<0, 0>(e, pos, perm, n, ordered, mass, shape, s)
+                             : deposit_typed<0, 1>(e, pos, perm, n, ordered, mass, shape, s);
 }
 
 }  // namespace mog

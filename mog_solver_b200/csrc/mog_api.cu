@@ -147,6 +147,7 @@ struct mog_handle {
     void* d_scratch = nullptr;   // spectral scratch (g >= 32)
     double* d_diag = nullptr;    // diagnostics partials + result
     int* d_perm = nullptr;       // spatial order of the particles (slot -> particle)
+    float4* d_pos_s = nullptr;   // positions in spatial order (refreshed every step)
     void* d_sort = nullptr;      // counting-sort scratch
     int64_t perm_cap = 0;        // capacity of d_perm
     int64_t perm_n = -1;         // n the permutation was built for
@@ -239,27 +240,37 @@ bool wants_sort(const mog_handle* h, int64_t n) {
     return h->perm_n != n || h->step_count % (uint64_t)h->sort_every == 0;
 }
 
-// Launch the spatial ordering if `sort`; returns the permutation to use.
+// Spatial ordering.  When ordering is on, (re)build the permutation if
+// `sort`, then gather the positions into spatial order (every step: they
+// move); *perm and *pos_s are what the kernels read, or null when off.
 int order_particles(mog_handle* h, const float4* pos, int64_t n, bool sort, cudaStream_t s,
-                    const int** perm) {
+                    const int** perm, const float4** pos_s) {
     *perm = nullptr;
+    *pos_s = nullptr;
     if (h->sort_every <= 0 || n <= 0) return MOG_OK;
-    if (sort) {
-        if (n > h->perm_cap) {
-            cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-            cudaStreamIsCapturing(s, &cs);
-            if (cs != cudaStreamCaptureStatusNone)
-                return fail(MOG_ERR_ARG, "n exceeds num_particles inside a captured step");
-            if (h->d_perm) cudaFree(h->d_perm);
-            h->d_perm = nullptr;
-            MOG_CUDA(cudaMalloc((void**)&h->d_perm, sizeof(int) * n), "cudaMalloc perm");
-            h->perm_cap = n;
-        }
+    if (n > h->perm_cap) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        cudaStreamIsCapturing(s, &cs);
+        if (cs != cudaStreamCaptureStatusNone)
+            return fail(MOG_ERR_ARG, "n exceeds num_particles inside a captured step");
+        if (h->d_perm) cudaFree(h->d_perm);
+        if (h->d_pos_s) cudaFree(h->d_pos_s);
+        h->d_perm = nullptr;
+        h->d_pos_s = nullptr;
+        h->perm_n = -1;
+        MOG_CUDA(cudaMalloc((void**)&h->d_perm, sizeof(int) * n), "cudaMalloc perm");
+        MOG_CUDA(cudaMalloc((void**)&h->d_pos_s, sizeof(float4) * n), "cudaMalloc sorted positions");
+        h->perm_cap = n;
+    }
+    if (sort || h->perm_n != n) {
         cudaError_t err = mog::launch_sort(pos, n, h->e.world, h->d_sort, h->d_perm, s);
         if (err != cudaSuccess) return cuda_fail(err, "spatial order");
         h->perm_n = n;
     }
-    if (h->perm_n == n) *perm = h->d_perm;
+    cudaError_t err = mog::launch_gather_sorted(pos, h->d_perm, n, h->d_pos_s, s);
+    if (err != cudaSuccess) return cuda_fail(err, "gather sorted positions");
+    *perm = h->d_perm;
+    *pos_s = h->d_pos_s;
     return MOG_OK;
 }
 
@@ -268,16 +279,19 @@ int run_pipeline(mog_handle* h, float4* pos, float4* vel, int64_t n, float dt, f
                  cudaStream_t s, bool sort) {
     const mog::Ensemble& e = h->e;
     const int* perm = nullptr;
-    int rc = order_particles(h, pos, n, sort, s, &perm);
+    const float4* pos_s = nullptr;
+    int rc = order_particles(h, pos, n, sort, s, &perm, &pos_s);
     if (rc) return rc;
-    cudaError_t err = mog::launch_deposit(e, pos, perm, n, h->d_mass, h->dshape, s);
+    cudaError_t err = pos_s ? mog::launch_deposit(e, pos_s, nullptr, n, true, h->d_mass, h->dshape, s)
+                            : mog::launch_deposit(e, pos, nullptr, n, false, h->d_mass, h->dshape, s);
     if (err != cudaSuccess) return cuda_fail(err, "deposit");
     if (h->cfg.solver == MOG_SOLVER_FFT)
         err = mog::launch_spectral(e, h->d_mass, h->d_force, true, true, h->d_scratch, s);
     else
         err = mog::launch_convolution(e, h->d_mass, h->d_force, true, true, s);
     if (err != cudaSuccess) return cuda_fail(err, "solve");
-    err = mog::launch_update(e, pos, vel, perm, n, h->d_force, dt, h->cfg.damping, acc, h->ushape, s);
+    err = mog::launch_update(e, pos, vel, pos_s, perm, n, h->d_force, dt, h->cfg.damping, acc,
+                             h->ushape, s);
     if (err != cudaSuccess) return cuda_fail(err, "update");
     return MOG_OK;
 }
@@ -292,7 +306,7 @@ void release(mog_handle* h) {
     h->graphs.clear();
     void* ptrs[] = {h->d_rot12, h->d_off4, h->d_fast, h->d_green, h->d_ktab, h->d_conv,
                     h->d_flags, h->d_total, h->d_mass, h->d_force, h->d_force2, h->d_scratch,
-                    h->d_diag, h->d_perm, h->d_sort};
+                    h->d_diag, h->d_perm, h->d_sort, h->d_pos_s};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }
@@ -396,6 +410,7 @@ int mog_create(const mog_config* cfg, const float* rot12, const float* off4, mog
     // happen later inside a captured step)
     if (cfg->num_particles > 0) {
         ALLOC(h->d_perm, sizeof(int) * cfg->num_particles);
+        ALLOC(h->d_pos_s, sizeof(float4) * cfg->num_particles);
         h->perm_cap = cfg->num_particles;
     }
     ALLOC(h->d_sort, mog::sort_scratch_bytes());
@@ -521,16 +536,19 @@ int mog_step_profiled(mog_handle* h, float* pos4, float* vel4, int64_t n, float 
     float4* pos = reinterpret_cast<float4*>(pos4);
     float4* vel = reinterpret_cast<float4*>(vel4);
     const int* perm = nullptr;
+    const float4* pos_s = nullptr;
     cudaError_t err = cudaEventRecord(ev[0], s);
     if (!err) {
-        rc = order_particles(h, pos, n, wants_sort(h, n), s, &perm);
+        rc = order_particles(h, pos, n, wants_sort(h, n), s, &perm, &pos_s);
         if (rc) {
             for (auto& x : ev) cudaEventDestroy(x);
             return rc;
         }
     }
     if (!err) err = cudaEventRecord(ev[1], s);
-    if (!err) err = mog::launch_deposit(e, pos, perm, n, h->d_mass, h->dshape, s);
+    if (!err)
+        err = pos_s ? mog::launch_deposit(e, pos_s, nullptr, n, true, h->d_mass, h->dshape, s)
+                    : mog::launch_deposit(e, pos, nullptr, n, false, h->d_mass, h->dshape, s);
     if (!err) err = cudaEventRecord(ev[2], s);
     if (!err)
         err = h->cfg.solver == MOG_SOLVER_FFT
@@ -538,8 +556,8 @@ int mog_step_profiled(mog_handle* h, float* pos4, float* vel4, int64_t n, float 
                   : mog::launch_convolution(e, h->d_mass, h->d_force, true, true, s);
     if (!err) err = cudaEventRecord(ev[3], s);
     if (!err)
-        err = mog::launch_update(e, pos, vel, perm, n, h->d_force, dt_eff, h->cfg.damping, nullptr,
-                                 h->ushape, s);
+        err = mog::launch_update(e, pos, vel, pos_s, perm, n, h->d_force, dt_eff, h->cfg.damping,
+                                 nullptr, h->ushape, s);
     if (!err) err = cudaEventRecord(ev[4], s);
     if (!err) err = cudaEventSynchronize(ev[4]);
     for (int i = 0; i < 4 && !err; ++i) err = cudaEventElapsedTime(&phase_ms[i], ev[i], ev[i + 1]);
@@ -568,10 +586,14 @@ int mog_deposit(mog_handle* h, const float* pos4, int64_t n, void* mass_out, voi
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     MOG_CUDA(cudaMemsetAsync(mass_out, 0, mass_bytes(h), s), "clear mass");
     const int* perm = nullptr;
-    if ((rc = order_particles(h, reinterpret_cast<const float4*>(pos4), n, h->sort_every > 0, s, &perm)))
+    const float4* pos_s = nullptr;
+    if ((rc = order_particles(h, reinterpret_cast<const float4*>(pos4), n, h->sort_every > 0, s,
+                              &perm, &pos_s)))
         return rc;
-    cudaError_t err = mog::launch_deposit(h->e, reinterpret_cast<const float4*>(pos4), perm, n,
-                                          mass_out, h->dshape, s);
+    cudaError_t err =
+        pos_s ? mog::launch_deposit(h->e, pos_s, nullptr, n, true, mass_out, h->dshape, s)
+              : mog::launch_deposit(h->e, reinterpret_cast<const float4*>(pos4), nullptr, n, false,
+                                    mass_out, h->dshape, s);
     if (err != cudaSuccess) return cuda_fail(err, "deposit");
     mog::check_total_kernel<<<1, 1, 0, s>>>(h->e);
     MOG_CUDA(cudaGetLastError(), "check total");
@@ -609,10 +631,12 @@ int mog_update(mog_handle* h, float* pos4, float* vel4, int64_t n, const float* 
     cudaError_t err = mog::launch_prerotate(h->e, reinterpret_cast<const float4*>(force4_in), h->d_force2, s);
     if (err != cudaSuccess) return cuda_fail(err, "prerotate");
     const int* perm = nullptr;
-    if ((rc = order_particles(h, reinterpret_cast<const float4*>(pos4), n, h->sort_every > 0, s, &perm)))
+    const float4* pos_s = nullptr;
+    if ((rc = order_particles(h, reinterpret_cast<const float4*>(pos4), n, h->sort_every > 0, s,
+                              &perm, &pos_s)))
         return rc;
     err = mog::launch_update(h->e, reinterpret_cast<float4*>(pos4), reinterpret_cast<float4*>(vel4),
-                             perm, n, h->d_force2, dt_eff, h->cfg.damping, nullptr, h->ushape, s);
+                             pos_s, perm, n, h->d_force2, dt_eff, h->cfg.damping, nullptr, h->ushape, s);
     if (err != cudaSuccess) return cuda_fail(err, "update");
     return MOG_OK;
 }
@@ -651,7 +675,7 @@ int mog_set_tuning(mog_handle* h, const mog_tuning* t) {
     h->ushape.staged = t->update_staged;
     h->ushape.ctas = t->update_ctas;
     h->ushape.direct_ppt = t->update_direct_ppt ? t->update_direct_ppt : 4;
-    h->sort_every = t->sort_every < 0 ? 1 : t->sort_every;
+    h->sort_every = t->sort_every < 0 ? 0 : t->sort_every;
     h->dshape.aggregate = t->deposit_aggregate;
     for (auto& g : h->graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);

@@ -62,9 +62,11 @@ int num_sms();
 
 // mass grid (u64 or u32 per mode) <- particles.  Zeroes nothing: the
 // caller provides a zeroed grid.
-// perm (nullable): slot s processes particle perm[s].
+// perm (nullable): slot s processes particle perm[s].  ordered: the
+// particles arrive in spatial order (pos already permuted, or perm set), so
+// warp merging of equal cells pays off.
 cudaError_t launch_deposit(const Ensemble& e, const float4* pos, const int* perm, int64_t n,
-                           void* mass, const DepositShape& shape, cudaStream_t s);
+                           bool ordered, void* mass, const DepositShape& shape, cudaStream_t s);
 
 // force grid (float4 per cell) <- mass grid.  world_frame: rotate each
 // cell's force by M_i and store (x, y, z, 0) — what the production gather
@@ -84,13 +86,20 @@ cudaError_t launch_prerotate(const Ensemble& e, const float4* force_grid, float4
 
 // Gather + average + (optionally) leapfrog.  When acc_out is non-null the
 // averaged force is written there and pos/vel are left untouched.
-cudaError_t launch_update(const Ensemble& e, float4* pos, float4* vel, const int* perm,
-                          int64_t n, const float4* force_world, float dt, float damping,
-                          float4* acc_out, const UpdateShape& shape, cudaStream_t s);
+// pos_sorted (nullable): pos[perm[s]] for every slot s, from which the
+// cells are computed; the caller's pos/vel are read and written once per
+// particle through perm.
+cudaError_t launch_update(const Ensemble& e, float4* pos, float4* vel, const float4* pos_sorted,
+                          const int* perm, int64_t n, const float4* force_world, float dt,
+                          float damping, float4* acc_out, const UpdateShape& shape, cudaStream_t s);
 
 // Spatial ordering: perm <- particles sorted by the Morton index of their
 // 32^3 world cell.  scratch: sort_scratch_bytes() bytes.
 size_t sort_scratch_bytes();
+// out[s] = pos[perm[s]]: the positions in spatial order, read coalesced by
+// the deposit and the gather.
+cudaError_t launch_gather_sorted(const float4* pos, const int* perm, int64_t n, float4* out,
+                                 cudaStream_t s);
 cudaError_t launch_sort(const float4* pos, int64_t n, float world, void* scratch, int* perm,
                         cudaStream_t s);
 

@@ -105,7 +105,21 @@ __global__ void __launch_bounds__(256) sort_scatter_kernel(const float4* __restr
     }
 }
 
+__global__ void __launch_bounds__(256) gather_sorted_kernel(const float4* __restrict__ pos,
+                                                            const int* __restrict__ perm,
+                                                            int64_t n, float4* __restrict__ out) {
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < n) out[s] = pos[__ldg(perm + s)];
+}
+
 }  // namespace
+
+cudaError_t launch_gather_sorted(const float4* pos, const int* perm, int64_t n, float4* out,
+                                 cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    gather_sorted_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(pos, perm, n, out);
+    return cudaGetLastError();
+}
 
 size_t sort_scratch_bytes() { return 2 * (size_t)kBins * sizeof(unsigned); }
 

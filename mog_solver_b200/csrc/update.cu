@@ -108,24 +108,85 @@ __device__ __forceinline__ int64_t particle_of(const int* __restrict__ perm, int
     return perm ? (int64_t)__ldg(perm + slot) : slot;
 }
 
+// Copy grid i's force field (or the z-slabs of it that the CTA's particles
+// can reach) into a stage.  t_z = a . c + b is affine in the centred
+// position, so over the CTA's bounding box of c it is extremal at the
+// corners; every particle's z cell lies in [floor(min t_z), floor(max t_z)]
+// (a 0.01-cell margin covers the rounding of either index mode).
+__device__ __forceinline__ void issue_grid(int i, int s, const float4* __restrict__ W,
+                                           float4* stage, uint64_t* full, int lg,
+                                           const float* box, bool sparse, const float* xf,
+                                           int idx_mode, const IndexParams& ip) {
+    const int g = 1 << lg;
+    const int G3 = 1 << (3 * lg);
+    const unsigned slab = (unsigned)g * g;  // float4 per z-slab
+    const float4* src = W + (size_t)i * G3;
+    float4* dst = stage + (size_t)s * G3;
+    int z0 = 0, nz = g;
+    if (sparse) {
+        float a0, a1, a2, b, inv = 1.0f;
+        const float* x = xf + i * 16;
+        if (idx_mode == 0) {
+            a0 = x[8];
+            a1 = x[9];
+            a2 = x[10];
+            b = x[11];
+        } else {  // rotated_z = R[2] c.x + R[6] c.y + R[10] c.z, t_z = (rotated_z + L/2 - off_z) / h
+            a0 = x[2];
+            a1 = x[6];
+            a2 = x[10];
+            b = ip.half_l - x[14];
+            inv = 1.0f / ip.voxel;
+        }
+        float tmin = 3.0e38f, tmax = -3.0e38f;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const float cx = box[(q & 1) ? 3 : 0], cy = box[(q & 2) ? 4 : 1], cz = box[(q & 4) ? 5 : 2];
+            const float t = (a0 * cx + a1 * cy + a2 * cz + b) * inv;
+            tmin = fminf(tmin, t);
+            tmax = fmaxf(tmax, t);
+        }
+        if (isfinite(tmin) && isfinite(tmax) && tmax - tmin < (float)(g - 2)) {
+            const int zlo = __float2int_rd(tmin - 0.01f);
+            const int zhi = __float2int_rd(tmax + 0.01f);
+            nz = zhi - zlo + 1;
+            z0 = zlo & (g - 1);
+        }
+    }
+    if (nz >= g) {
+        mbar_expect_tx(full + s, (unsigned)G3 * 16u);
+        bulk_g2s(dst, src, (unsigned)G3 * 16u, full + s);
+        return;
+    }
+    mbar_expect_tx(full + s, (unsigned)nz * slab * 16u);
+    const int first = min(nz, g - z0);
+    bulk_g2s(dst + (size_t)z0 * slab, src + (size_t)z0 * slab, (unsigned)first * slab * 16u, full + s);
+    if (nz > first)
+        bulk_g2s(dst, src, (unsigned)(nz - first) * slab * 16u, full + s);
+}
+
 // Staged gather.  Launch: one CTA per SM (shared-memory bound).  The CTA
 // owns slots [lo, hi); thread t owns slots lo + t + j * blockDim, so the
 // 32 lanes of a warp always hold consecutive slots: with a spatial
 // ordering they fall in the same few cells and their shared-memory loads
-// broadcast instead of conflicting.
+// broadcast instead of conflicting, and the CTA's particles occupy a small
+// box, so only the z-slabs of each grid that the box reaches are staged.
 template <int IDX, int PPT, bool ACC_OUT>
 __global__ void __launch_bounds__(512, 1)
     update_staged_kernel(float4* __restrict__ pos, float4* __restrict__ vel,
-                         const int* __restrict__ perm, int64_t n, int64_t per_cta,
-                         const float4* __restrict__ W, Ensemble e, float dt, float damp,
-                         float4* __restrict__ acc_out, int nstage) {
+                         const float4* __restrict__ pos_s, const int* __restrict__ perm,
+                         int64_t n, int64_t per_cta, const float4* __restrict__ W, Ensemble e,
+                         float dt, float damp, float4* __restrict__ acc_out, int nstage,
+                         int sparse) {
     extern __shared__ __align__(128) unsigned char smem[];
     const int G3 = 1 << (3 * e.lg);
-    const unsigned grid_bytes = (unsigned)G3 * 16u;
+    const size_t grid_bytes = (size_t)G3 * 16u;
     float4* stage = reinterpret_cast<float4*>(smem);
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + (size_t)nstage * grid_bytes);
     float* xf = reinterpret_cast<float*>(full + 8);
     __shared__ int abort_flag;
+    __shared__ float box[6];        // min c.xyz, max c.xyz of the CTA's particles
+    __shared__ float wbox[16][6];   // per-warp partial boxes
 
     const int tid = threadIdx.x;
     const int T = blockDim.x;
@@ -143,13 +204,6 @@ __global__ void __launch_bounds__(512, 1)
             v = (w < 12) ? e.rot12[j * 12 + w] : e.off4[j * 4 + (w - 12)];
         xf[i] = v;
     }
-    __syncthreads();
-    if (tid == 0) {
-        for (int s = 0; s < nstage && s < e.k; ++s) {
-            mbar_expect_tx(full + s, grid_bytes);
-            bulk_g2s(stage + (size_t)s * G3, W + (size_t)s * G3, grid_bytes, full + s);
-        }
-    }
 
     const IndexParams ip = e.index_params();
     const int64_t lo = (int64_t)blockIdx.x * per_cta;
@@ -159,14 +213,54 @@ __global__ void __launch_bounds__(512, 1)
     const int64_t slots = (mine + T - 1) / T;
     const int cnt = mine <= 0 ? 0 : (int)(slots < PPT ? slots : PPT);
     float cx[PPT], cy[PPT], cz[PPT], ax[PPT], ay[PPT], az[PPT];
+    float bmin[3] = {3.0e38f, 3.0e38f, 3.0e38f}, bmax[3] = {-3.0e38f, -3.0e38f, -3.0e38f};
 #pragma unroll
     for (int j = 0; j < PPT; ++j) {
         float4 P = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (j < cnt) P = pos[particle_of(perm, first + (int64_t)j * T)];
+        if (j < cnt) {
+            const int64_t slot = first + (int64_t)j * T;
+            P = pos_s ? pos_s[slot] : pos[particle_of(perm, slot)];
+        }
         cx[j] = __fsub_rn(P.x, ip.half_l);
         cy[j] = __fsub_rn(P.y, ip.half_l);
         cz[j] = __fsub_rn(P.z, ip.half_l);
         ax[j] = ay[j] = az[j] = 0.f;
+        if (j < cnt) {
+            bmin[0] = fminf(bmin[0], cx[j]);
+            bmin[1] = fminf(bmin[1], cy[j]);
+            bmin[2] = fminf(bmin[2], cz[j]);
+            bmax[0] = fmaxf(bmax[0], cx[j]);
+            bmax[1] = fmaxf(bmax[1], cy[j]);
+            bmax[2] = fmaxf(bmax[2], cz[j]);
+        }
+    }
+    if (sparse) {
+        for (int o = 16; o > 0; o >>= 1)
+            for (int a = 0; a < 3; ++a) {
+                bmin[a] = fminf(bmin[a], __shfl_xor_sync(kFull, bmin[a], o));
+                bmax[a] = fmaxf(bmax[a], __shfl_xor_sync(kFull, bmax[a], o));
+            }
+        if ((tid & 31) == 0)
+            for (int a = 0; a < 3; ++a) {
+                wbox[tid >> 5][a] = bmin[a];
+                wbox[tid >> 5][3 + a] = bmax[a];
+            }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        if (sparse) {
+            for (int a = 0; a < 3; ++a) {
+                float mn = 3.0e38f, mx = -3.0e38f;
+                for (int w = 0; w < (T >> 5); ++w) {
+                    mn = fminf(mn, wbox[w][a]);
+                    mx = fmaxf(mx, wbox[w][3 + a]);
+                }
+                box[a] = mn;
+                box[3 + a] = mx;
+            }
+        }
+        for (int s = 0; s < nstage && s < e.k; ++s)
+            issue_grid(s, s, W, stage, full, e.lg, box, sparse && box[0] <= box[3], xf, IDX, ip);
     }
 
     int i_abort = -1;
@@ -191,10 +285,9 @@ __global__ void __launch_bounds__(512, 1)
             i_abort = i;
             break;
         }
-        if (tid == 0 && i + nstage < e.k) {
-            mbar_expect_tx(full + s, grid_bytes);
-            bulk_g2s(stage + (size_t)s * G3, W + (size_t)(i + nstage) * G3, grid_bytes, full + s);
-        }
+        if (tid == 0 && i + nstage < e.k)
+            issue_grid(i + nstage, s, W, stage, full, e.lg, box, sparse && box[0] <= box[3], xf, IDX,
+                       ip);
     }
     if (i_abort >= 0) {
         // Copies for grids i_abort .. i_abort + nstage - 1 may still be in
@@ -213,8 +306,9 @@ __global__ void __launch_bounds__(512, 1)
 #pragma unroll
     for (int j = 0; j < PPT; ++j) {
         if (j < cnt) {
-            const int64_t p = particle_of(perm, first + (int64_t)j * T);
-            const float4 P = pos[p];
+            const int64_t slot = first + (int64_t)j * T;
+            const int64_t p = particle_of(perm, slot);
+            const float4 P = pos_s ? pos_s[slot] : pos[p];
             finish_particle<ACC_OUT>(p, P, ax[j], ay[j], az[j], pos, vel, acc_out, kf, dt, damp,
                                      e.world, bad);
         }
@@ -227,6 +321,7 @@ __global__ void __launch_bounds__(512, 1)
 template <int IDX, int DPPT, bool ACC_OUT>
 __global__ void __launch_bounds__(256) update_direct_kernel(float4* __restrict__ pos,
                                                             float4* __restrict__ vel,
+                                                            const float4* __restrict__ pos_s,
                                                             const int* __restrict__ perm,
                                                             int64_t n,
                                                             const float4* __restrict__ W,
@@ -240,7 +335,7 @@ __global__ void __launch_bounds__(256) update_direct_kernel(float4* __restrict__
 #pragma unroll
     for (int j = 0; j < DPPT; ++j) {
         float4 P = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (j < cnt) P = pos[particle_of(perm, first + j)];
+        if (j < cnt) P = pos_s ? pos_s[first + j] : pos[particle_of(perm, first + j)];
         cx[j] = __fsub_rn(P.x, ip.half_l);
         cy[j] = __fsub_rn(P.y, ip.half_l);
         cz[j] = __fsub_rn(P.z, ip.half_l);
@@ -274,7 +369,7 @@ __global__ void __launch_bounds__(256) update_direct_kernel(float4* __restrict__
     for (int j = 0; j < DPPT; ++j) {
         if (j < cnt) {
             const int64_t p = particle_of(perm, first + j);
-            finish_particle<ACC_OUT>(p, pos[p], ax[j], ay[j], az[j], pos, vel, acc_out,
+            finish_particle<ACC_OUT>(p, pos_s ? pos_s[first + j] : pos[p], ax[j], ay[j], az[j], pos, vel, acc_out,
                                      (float)e.k, dt, damp, e.world, bad);
         }
     }
@@ -282,22 +377,24 @@ __global__ void __launch_bounds__(256) update_direct_kernel(float4* __restrict__
 }
 
 template <int IDX, int PPT, bool ACC>
-cudaError_t launch_staged(const Ensemble& e, float4* pos, float4* vel, const int* perm, int64_t n,
-                          const float4* W, float dt, float damp, float4* acc, int ctas,
-                          int threads, int nstage, size_t smem, cudaStream_t s) {
+cudaError_t launch_staged(const Ensemble& e, float4* pos, float4* vel, const float4* pos_s,
+                          const int* perm, int64_t n, const float4* W, float dt, float damp,
+                          float4* acc, int ctas, int threads, int nstage, size_t smem,
+                          int sparse, cudaStream_t s) {
     auto kern = update_staged_kernel<IDX, PPT, ACC>;
     cudaError_t err =
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess) return err;
     const int64_t per_cta = (n + ctas - 1) / ctas;
-    kern<<<ctas, threads, smem, s>>>(pos, vel, perm, n, per_cta, W, e, dt, damp, acc, nstage);
+    kern<<<ctas, threads, smem, s>>>(pos, vel, pos_s, perm, n, per_cta, W, e, dt, damp, acc, nstage,
+                                     sparse);
     return cudaGetLastError();
 }
 
 template <int IDX, bool ACC>
-cudaError_t update_mode(const Ensemble& e, float4* pos, float4* vel, const int* perm, int64_t n,
-                        const float4* W, float dt, float damp, float4* acc, const UpdateShape& sh,
-                        cudaStream_t s) {
+cudaError_t update_mode(const Ensemble& e, float4* pos, float4* vel, const float4* pos_s,
+                        const int* perm, int64_t n, const float4* W, float dt, float damp,
+                        float4* acc, const UpdateShape& sh, cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
     const size_t grid_bytes = (size_t)16 << (3 * e.lg);
     const int sms = num_sms();
@@ -315,51 +412,53 @@ cudaError_t update_mode(const Ensemble& e, float4* pos, float4* vel, const int* 
         const int64_t threads_needed = (n + dppt - 1) / dppt;
         const unsigned blocks = (unsigned)((threads_needed + 255) / 256);
         if (dppt == 1)
-            update_direct_kernel<IDX, 1, ACC><<<blocks, 256, 0, s>>>(pos, vel, perm, n, W, e, dt,
+            update_direct_kernel<IDX, 1, ACC><<<blocks, 256, 0, s>>>(pos, vel, pos_s, perm, n, W, e, dt,
                                                                      damp, acc);
         else if (dppt == 2)
-            update_direct_kernel<IDX, 2, ACC><<<blocks, 256, 0, s>>>(pos, vel, perm, n, W, e, dt,
+            update_direct_kernel<IDX, 2, ACC><<<blocks, 256, 0, s>>>(pos, vel, pos_s, perm, n, W, e, dt,
                                                                      damp, acc);
         else
-            update_direct_kernel<IDX, 4, ACC><<<blocks, 256, 0, s>>>(pos, vel, perm, n, W, e, dt,
+            update_direct_kernel<IDX, 4, ACC><<<blocks, 256, 0, s>>>(pos, vel, pos_s, perm, n, W, e, dt,
                                                                      damp, acc);
         return cudaGetLastError();
     }
+    // Sparse staging only pays when the CTAs' particles are spatially compact.
+    const int sparse = (pos_s || perm) ? 1 : 0;
     // Enough CTAs that the particles per thread stay within the template.
     int ctas = sh.ctas > 0 ? sh.ctas : sms;
     const int64_t per_thread = (n + (int64_t)ctas * threads - 1) / ((int64_t)ctas * threads);
     if (per_thread > 16) ctas = (int)((n + 16LL * threads - 1) / (16LL * threads));
     const int64_t ppt = (n + (int64_t)ctas * threads - 1) / ((int64_t)ctas * threads);
     if (ppt <= 4)
-        return launch_staged<IDX, 4, ACC>(e, pos, vel, perm, n, W, dt, damp, acc, ctas, threads,
-                                          nstage, smem, s);
+        return launch_staged<IDX, 4, ACC>(e, pos, vel, pos_s, perm, n, W, dt, damp, acc, ctas,
+                                              threads, nstage, smem, sparse, s);
     if (ppt <= 8)
-        return launch_staged<IDX, 8, ACC>(e, pos, vel, perm, n, W, dt, damp, acc, ctas, threads,
-                                          nstage, smem, s);
+        return launch_staged<IDX, 8, ACC>(e, pos, vel, pos_s, perm, n, W, dt, damp, acc, ctas,
+                                              threads, nstage, smem, sparse, s);
     if (ppt <= 12)
-        return launch_staged<IDX, 12, ACC>(e, pos, vel, perm, n, W, dt, damp, acc, ctas, threads,
-                                           nstage, smem, s);
+        return launch_staged<IDX, 12, ACC>(e, pos, vel, pos_s, perm, n, W, dt, damp, acc, ctas,
+                                              threads, nstage, smem, sparse, s);
     if (ppt <= 14)
-        return launch_staged<IDX, 14, ACC>(e, pos, vel, perm, n, W, dt, damp, acc, ctas, threads,
-                                           nstage, smem, s);
-    return launch_staged<IDX, 16, ACC>(e, pos, vel, perm, n, W, dt, damp, acc, ctas, threads,
-                                       nstage, smem, s);
+        return launch_staged<IDX, 14, ACC>(e, pos, vel, pos_s, perm, n, W, dt, damp, acc, ctas,
+                                              threads, nstage, smem, sparse, s);
+    return launch_staged<IDX, 16, ACC>(e, pos, vel, pos_s, perm, n, W, dt, damp, acc, ctas,
+                                              threads, nstage, smem, sparse, s);
 }
 
 }  // namespace
 
-cudaError_t launch_update(const Ensemble& e, float4* pos, float4* vel, const int* perm, int64_t n,
-                          const float4* force_world, float dt, float damping, float4* acc_out,
-                          const UpdateShape& shape, cudaStream_t s) {
+cudaError_t launch_update(const Ensemble& e, float4* pos, float4* vel, const float4* pos_s,
+                          const int* perm, int64_t n, const float4* force_world, float dt,
+                          float damping, float4* acc_out, const UpdateShape& shape, cudaStream_t s) {
     if (acc_out)
-        return e.index_mode == 0 ? update_mode<0, true>(e, pos, vel, perm, n, force_world, dt,
-                                                        damping, acc_out, shape, s)
-                                 : update_mode<1, true>(e, pos, vel, perm, n, force_world, dt,
-                                                        damping, acc_out, shape, s);
-    return e.index_mode == 0 ? update_mode<0, false>(e, pos, vel, perm, n, force_world, dt, damping,
-                                                     nullptr, shape, s)
-                             : update_mode<1, false>(e, pos, vel, perm, n, force_world, dt, damping,
-                                                     nullptr, shape, s);
+        return e.index_mode == 0 ? update_mode<0, true>(e, pos, vel, pos_s, perm, n, force_world,
+                                                        dt, damping, acc_out, shape, s)
+                                 : update_mode<1, true>(e, pos, vel, pos_s, perm, n, force_world,
+                                                        dt, damping, acc_out, shape, s);
+    return e.index_mode == 0 ? update_mode<0, false>(e, pos, vel, pos_s, perm, n, force_world, dt,
+                                                     damping, nullptr, shape, s)
+                             : update_mode<1, false>(e, pos, vel, pos_s, perm, n, force_world, dt,
+                                                     damping, nullptr, shape, s);
 }
 
 }  // namespace mog
