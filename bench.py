@@ -57,7 +57,8 @@ CLOCK_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.a
 def phase_bytes(w: dict) -> dict:
     """Algorithmic bytes per launch of each kernel.
 
-    deposit: position read (16 N) + one 4-byte cell update per (particle,
+    order (when enabled): the spatial permutation and sorted copy of the
+    positions (16 N); deposit: position read (16 N) + one 4-byte cell update per (particle,
     grid) (4 N k) + mass-grid write (4 k g^3); solve: mass read + 3 force
     components written (16 k g^3); update: position and velocity read and
     written (64 N) + one 12-byte force read per (particle, grid) (12 N k).
@@ -65,7 +66,8 @@ def phase_bytes(w: dict) -> dict:
     position read is counted once, inside the 64 N).
     """
     n, k, g3 = w["n"], w["k"], w["g"] ** 3
-    return {"deposit": 16 * n + 4 * n * k + 4 * k * g3,
+    return {"order": 16 * n,
+            "deposit": 16 * n + 4 * n * k + 4 * k * g3,
             "solve": 16 * k * g3,
             "update": 64 * n + 12 * n * k,
             "step": 64 * n + 16 * n * k + 20 * k * g3}
@@ -209,7 +211,7 @@ def run_ours(args, w: dict) -> None:
     lib = _lib.lib()
     stream = torch.cuda.Stream(device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    phase = (ctypes.c_float * 3)()
+    phase = (ctypes.c_float * 4)()
     dt_eff = float(w["dt"])
 
     def barrier():
@@ -275,7 +277,7 @@ def run_ours(args, w: dict) -> None:
     e2e = n * world * args.steps / (total_e2e / 1e3)
     ph = np.array(phases)
     mean_ph = ph.mean(axis=0)
-    names = ["deposit", "solve", "update"]
+    names = ["order", "deposit", "solve", "update"]
     dom = int(np.argmax(mean_ph))
     pb = phase_bytes(w)
     peaks = measured_peaks()

@@ -214,6 +214,51 @@ int mog_diagnostics(mog_handle* h, const float* pos4, const float* vel4,
 int mog_direct_sum(const float* targets4, int64_t nt, const float* sources4, int64_t ns,
                    double world, double g_eff, double soft, double* out3, void* stream);
 
+/*
+ * Learned correction of a cheap ensemble (no counterpart in the reference,
+ * whose force is always the plain k-grid average, update.glsl:67-81).
+ * A model is a 12 -> 64 -> 64 -> 3 GELU network predicting, from per-particle
+ * statistics of the handle's ensemble, the residual to a larger ensemble.
+ *   params: MOG_MODEL_PARAMS floats, W1[64][12] b1[64] W2[64][64] b2[64]
+ *           W3[3][64] b3[3] (FP32 master copy; inference runs in BF16).
+ *   norm:   MOG_MODEL_NORM floats, mu[12] inv_sigma[12] force_scale
+ *           rho_ref out_scale pad — features are (f - mu) * inv_sigma with
+ *           forces divided by force_scale and densities by rho_ref; the
+ *           predicted residual is y * out_scale.
+ */
+#define MOG_MODEL_PARAMS 5187
+#define MOG_MODEL_NORM 28
+typedef struct mog_model mog_model;
+int mog_model_create(mog_model** out);
+int mog_model_destroy(mog_model* m);
+/* Upload parameters and normalisation (host memory); resets Adam state. */
+int mog_model_set(mog_model* m, const float* params, const float* norm);
+/* Download parameters and normalisation to host memory (synchronises). */
+int mog_model_get(const mog_model* m, float* params, float* norm);
+/*
+ * One Adam step (lr; betas 0.9, 0.999) on the mean squared error of the
+ * `batch` samples idx[0..batch) of feat16 (device, rows of 16 floats, the
+ * first 12 used) against target4 (device, rows of 4 floats, 3 used).
+ * Optional outputs: *loss_out (host; synchronises) and grad_out (device,
+ * MOG_MODEL_PARAMS floats).  lr = 0 computes the gradient only.
+ */
+int mog_model_train_step(mog_model* m, const float* feat16, const float* target4,
+                         const int* idx, int32_t batch, float lr, float* loss_out,
+                         float* grad_out, void* stream);
+/*
+ * Deposit + solve with the handle's ensemble, then per-particle features:
+ * mean4_out (device n float4, the plain ensemble force) and feat16_out
+ * (device n x 16 floats, standardised with m's norm).
+ */
+int mog_features(mog_handle* h, const mog_model* m, const float* pos4, int64_t n,
+                 float* mean4_out, float* feat16_out, void* stream);
+/* Corrected force (plain ensemble force + predicted residual) at every
+ * particle, and one damped leapfrog step with it (update.glsl:83-89). */
+int mog_learned_forces(mog_handle* h, const mog_model* m, const float* pos4, float* acc4,
+                       int64_t n, void* stream);
+int mog_learned_step(mog_handle* h, const mog_model* m, float* pos4, float* vel4, int64_t n,
+                     float dt_eff, void* stream);
+
 /* Human-readable text for a status code, and the calling thread's last
  * error message. */
 const char* mog_strerror(int code);

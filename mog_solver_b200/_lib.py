@@ -33,6 +33,9 @@ DFT_TC_BF16X3 = 1
 
 COMPAT_FFT_TEXTURE_ALIAS = 1
 
+MODEL_PARAMS = 5187
+MODEL_NORM = 28
+
 FLAG_NONFINITE = 1
 FLAG_OVERFLOW = 2
 FLAG_TIMEOUT = 4
@@ -42,8 +45,10 @@ FLAG_BADMASS = 8
 EXPORTS = (
     "mog_config_default", "mog_create", "mog_destroy", "mog_step", "mog_step_n",
     "mog_step_profiled", "mog_forces", "mog_deposit", "mog_solve", "mog_update", "mog_get_status",
-    "mog_get_tuning", "mog_set_tuning", "mog_diagnostics", "mog_direct_sum", "mog_strerror",
-    "mog_last_error", "mog_version",
+    "mog_get_tuning", "mog_set_tuning", "mog_diagnostics", "mog_direct_sum",
+    "mog_model_create", "mog_model_destroy", "mog_model_set", "mog_model_get",
+    "mog_model_train_step", "mog_features", "mog_learned_forces", "mog_learned_step",
+    "mog_strerror", "mog_last_error", "mog_version",
 )
 
 
@@ -116,6 +121,15 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.mog_diagnostics.argtypes = [P, P, P, I64, ctypes.POINTER(ctypes.c_double), P]
     D = ctypes.c_double
     lib.mog_direct_sum.argtypes = [P, I64, P, I64, D, D, D, P, P]
+    FP = ctypes.POINTER(ctypes.c_float)
+    lib.mog_model_create.argtypes = [ctypes.POINTER(P)]
+    lib.mog_model_destroy.argtypes = [P]
+    lib.mog_model_set.argtypes = [P, P, P]
+    lib.mog_model_get.argtypes = [P, P, P]
+    lib.mog_model_train_step.argtypes = [P, P, P, P, ctypes.c_int32, F, FP, P, P]
+    lib.mog_features.argtypes = [P, P, P, I64, P, P, P]
+    lib.mog_learned_forces.argtypes = [P, P, P, P, I64, P]
+    lib.mog_learned_step.argtypes = [P, P, P, P, I64, F, P]
     lib.mog_strerror.argtypes = [I]
     lib.mog_strerror.restype = ctypes.c_char_p
     lib.mog_last_error.argtypes = []

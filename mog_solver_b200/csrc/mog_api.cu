@@ -127,6 +127,20 @@ struct GraphEntry {
     cudaGraphExec_t exec = nullptr;
 };
 
+struct mog_model {
+    int device = 0;
+    float* d_params = nullptr;
+    float* d_m = nullptr;
+    float* d_v = nullptr;
+    float* d_grad = nullptr;
+    void* d_frags = nullptr;
+    float* d_partial = nullptr;
+    float* d_loss = nullptr;
+    int partial_ctas = 0;
+    int step = 0;
+    mog::ModelNorm norm{};
+};
+
 struct mog_handle {
     mog_config cfg{};
     int device = 0;
@@ -148,6 +162,10 @@ struct mog_handle {
     double* d_diag = nullptr;    // diagnostics partials + result
     int* d_perm = nullptr;       // spatial order of the particles (slot -> particle)
     float4* d_pos_s = nullptr;   // positions in spatial order (refreshed every step)
+    float4* d_mean = nullptr;    // learned path: plain ensemble force
+    float* d_feat = nullptr;     // learned path: features (n x 16)
+    float4* d_acc = nullptr;     // learned path: corrected force
+    int64_t learn_cap = 0;
     void* d_sort = nullptr;      // counting-sort scratch
     int64_t perm_cap = 0;        // capacity of d_perm
     int64_t perm_n = -1;         // n the permutation was built for
@@ -306,7 +324,8 @@ void release(mog_handle* h) {
     h->graphs.clear();
     void* ptrs[] = {h->d_rot12, h->d_off4, h->d_fast, h->d_green, h->d_ktab, h->d_conv,
                     h->d_flags, h->d_total, h->d_mass, h->d_force, h->d_force2, h->d_scratch,
-                    h->d_diag, h->d_perm, h->d_sort, h->d_pos_s};
+                    h->d_diag, h->d_perm, h->d_sort, h->d_pos_s, h->d_mean, h->d_feat,
+                    h->d_acc};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }
@@ -749,5 +768,195 @@ const char* mog_strerror(int code) {
 const char* mog_last_error(void) { return g_last_error.c_str(); }
 
 const char* mog_version(void) { return "mog-b200 0.1 (sm_100a)"; }
+
+}  // extern "C"
+
+// ---- learned correction ---------------------------------------------------
+
+static int learn_buffers(mog_handle* h, int64_t n, cudaStream_t s) {
+    if (n <= h->learn_cap) return MOG_OK;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(s, &cs);
+    if (cs != cudaStreamCaptureStatusNone)
+        return fail(MOG_ERR_ARG, "learned-path buffers must exist before stream capture");
+    cudaFree(h->d_mean);
+    cudaFree(h->d_feat);
+    cudaFree(h->d_acc);
+    h->d_mean = nullptr;
+    h->d_feat = nullptr;
+    h->d_acc = nullptr;
+    h->learn_cap = 0;
+    MOG_CUDA(cudaMalloc((void**)&h->d_mean, sizeof(float4) * n), "cudaMalloc mean");
+    MOG_CUDA(cudaMalloc((void**)&h->d_feat, sizeof(float) * 16 * n), "cudaMalloc features");
+    MOG_CUDA(cudaMalloc((void**)&h->d_acc, sizeof(float4) * n), "cudaMalloc acc");
+    h->learn_cap = n;
+    return MOG_OK;
+}
+
+// deposit + solve (mass grid kept for the density feature) + features
+static int run_features(mog_handle* h, const mog_model* m, const float4* pos, int64_t n,
+                        float4* mean, float* feat, cudaStream_t s) {
+    const mog::Ensemble& e = h->e;
+    cudaError_t err = mog::launch_deposit(e, pos, nullptr, n, false, h->d_mass, h->dshape, s);
+    if (err != cudaSuccess) return cuda_fail(err, "deposit");
+    if (h->cfg.solver == MOG_SOLVER_FFT)
+        err = mog::launch_spectral(e, h->d_mass, h->d_force, true, false, h->d_scratch, s);
+    else
+        err = mog::launch_convolution(e, h->d_mass, h->d_force, true, false, s);
+    if (err != cudaSuccess) return cuda_fail(err, "solve");
+    err = mog::launch_features(e, pos, n, h->d_force, h->d_mass, m->norm, mean, feat, s);
+    if (err != cudaSuccess) return cuda_fail(err, "features");
+    MOG_CUDA(cudaMemsetAsync(h->d_mass, 0, mass_bytes(h), s), "clear mass");
+    if (e.mass_mode == 0 && e.mass_total) MOG_CUDA(cudaMemsetAsync(e.mass_total, 0, sizeof(double), s), "clear total");
+    return MOG_OK;
+}
+
+extern "C" {
+
+int mog_model_create(mog_model** out) {
+    if (!out) return fail(MOG_ERR_ARG, "null argument");
+    *out = nullptr;
+    mog_model* m = new mog_model();
+    cudaGetDevice(&m->device);
+    const size_t pb = sizeof(float) * mog::mlp_param_count();
+    cudaError_t err;
+    if ((err = cudaMalloc((void**)&m->d_params, pb)) || (err = cudaMalloc((void**)&m->d_m, pb)) ||
+        (err = cudaMalloc((void**)&m->d_v, pb)) || (err = cudaMalloc((void**)&m->d_grad, pb)) ||
+        (err = cudaMalloc(&m->d_frags, mog::mlp_fragment_bytes())) ||
+        (err = cudaMemset(m->d_params, 0, pb)) || (err = cudaMemset(m->d_m, 0, pb)) ||
+        (err = cudaMemset(m->d_v, 0, pb))) {
+        mog_model_destroy(m);
+        return cuda_fail(err, "mog_model_create");
+    }
+    for (int j = 0; j < mog::kModelIn; ++j) m->norm.inv_sigma[j] = 1.f;
+    m->norm.force_scale = m->norm.rho_ref = m->norm.out_scale = 1.f;
+    *out = m;
+    return MOG_OK;
+}
+
+int mog_model_destroy(mog_model* m) {
+    if (!m) return MOG_OK;
+    void* ptrs[] = {m->d_params, m->d_m, m->d_v, m->d_grad, m->d_frags, m->d_partial, m->d_loss};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    delete m;
+    return MOG_OK;
+}
+
+int mog_model_set(mog_model* m, const float* params, const float* norm) {
+    if (!m || !params || !norm) return fail(MOG_ERR_ARG, "null argument");
+    for (int i = 0; i < MOG_MODEL_NORM; ++i)
+        if (!std::isfinite(norm[i])) return fail(MOG_ERR_ARG, "norm must be finite");
+    if (!(norm[24] > 0.f) || !(norm[25] > 0.f))
+        return fail(MOG_ERR_ARG, "force_scale and rho_ref must be positive");
+    const size_t pb = sizeof(float) * mog::mlp_param_count();
+    MOG_CUDA(cudaMemcpy(m->d_params, params, pb, cudaMemcpyHostToDevice), "upload params");
+    MOG_CUDA(cudaMemset(m->d_m, 0, pb), "reset adam");
+    MOG_CUDA(cudaMemset(m->d_v, 0, pb), "reset adam");
+    std::memcpy(&m->norm, norm, sizeof(mog::ModelNorm));
+    m->step = 0;
+    MOG_CUDA(mog::launch_pack_fragments(m->d_params, m->d_frags, 0), "pack fragments");
+    MOG_CUDA(cudaDeviceSynchronize(), "sync");
+    return MOG_OK;
+}
+
+int mog_model_get(const mog_model* m, float* params, float* norm) {
+    if (!m || !params || !norm) return fail(MOG_ERR_ARG, "null argument");
+    MOG_CUDA(cudaDeviceSynchronize(), "sync");
+    MOG_CUDA(cudaMemcpy(params, m->d_params, sizeof(float) * mog::mlp_param_count(),
+                        cudaMemcpyDeviceToHost), "download params");
+    std::memcpy(norm, &m->norm, sizeof(mog::ModelNorm));
+    return MOG_OK;
+}
+
+int mog_model_train_step(mog_model* m, const float* feat16, const float* target4, const int* idx,
+                         int32_t batch, float lr, float* loss_out, float* grad_out, void* stream) {
+    if (!m || !feat16 || !target4 || !idx) return fail(MOG_ERR_ARG, "null argument");
+    if (batch <= 0) return fail(MOG_ERR_ARG, "batch must be positive");
+    if (!std::isfinite(lr) || lr < 0.f) return fail(MOG_ERR_ARG, "lr must be finite and >= 0");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int ctas = (batch + 127) / 128;
+    if (ctas > m->partial_ctas) {
+        MOG_CUDA(cudaStreamSynchronize(s), "sync");
+        cudaFree(m->d_partial);
+        cudaFree(m->d_loss);
+        m->d_partial = nullptr;
+        m->d_loss = nullptr;
+        MOG_CUDA(cudaMalloc((void**)&m->d_partial, sizeof(float) * mog::mlp_param_count() * ctas), "partials");
+        MOG_CUDA(cudaMalloc((void**)&m->d_loss, sizeof(float) * ctas), "loss partials");
+        m->partial_ctas = ctas;
+    }
+    if (lr > 0.f) ++m->step;
+    cudaError_t err = mog::launch_mlp_train_step(feat16, target4, idx, batch, m->d_params,
+                                                 m->d_partial, m->d_loss, m->d_grad, m->d_m,
+                                                 m->d_v, lr, m->step, s);
+    if (err != cudaSuccess) return cuda_fail(err, "train step");
+    if (lr > 0.f) {
+        err = mog::launch_pack_fragments(m->d_params, m->d_frags, s);
+        if (err != cudaSuccess) return cuda_fail(err, "pack fragments");
+    }
+    if (grad_out)
+        MOG_CUDA(cudaMemcpyAsync(grad_out, m->d_grad, sizeof(float) * mog::mlp_param_count(),
+                                 cudaMemcpyDeviceToDevice, s), "copy grad");
+    if (loss_out) {
+        std::vector<float> l(ctas);
+        MOG_CUDA(cudaMemcpyAsync(l.data(), m->d_loss, sizeof(float) * ctas, cudaMemcpyDeviceToHost, s),
+                 "read loss");
+        MOG_CUDA(cudaStreamSynchronize(s), "sync");
+        double tot = 0;
+        for (float v : l) tot += v;
+        *loss_out = (float)(tot / batch);
+    }
+    return MOG_OK;
+}
+
+int mog_features(mog_handle* h, const mog_model* m, const float* pos4, int64_t n, float* mean4_out,
+                 float* feat16_out, void* stream) {
+    if (!h || !m) return fail(MOG_ERR_ARG, "null argument");
+    int rc = check_particles(h, pos4, mean4_out, n, true);
+    if (rc) return rc;
+    if (n > 0 && !feat16_out) return fail(MOG_ERR_ARG, "feat16_out is null");
+    if ((rc = set_device(h))) return rc;
+    return run_features(h, m, reinterpret_cast<const float4*>(pos4), n,
+                        reinterpret_cast<float4*>(mean4_out), feat16_out,
+                        static_cast<cudaStream_t>(stream));
+}
+
+int mog_learned_forces(mog_handle* h, const mog_model* m, const float* pos4, float* acc4, int64_t n,
+                       void* stream) {
+    if (!h || !m) return fail(MOG_ERR_ARG, "null argument");
+    int rc = check_particles(h, pos4, acc4, n, true);
+    if (rc) return rc;
+    if ((rc = set_device(h))) return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if ((rc = learn_buffers(h, n, s))) return rc;
+    if ((rc = run_features(h, m, reinterpret_cast<const float4*>(pos4), n, h->d_mean, h->d_feat, s)))
+        return rc;
+    cudaError_t err = mog::launch_mlp_infer(h->d_feat, n, m->d_frags, m->d_params, h->d_mean,
+                                            m->norm.out_scale, reinterpret_cast<float4*>(acc4), s);
+    if (err != cudaSuccess) return cuda_fail(err, "mlp inference");
+    return MOG_OK;
+}
+
+int mog_learned_step(mog_handle* h, const mog_model* m, float* pos4, float* vel4, int64_t n,
+                     float dt_eff, void* stream) {
+    if (!h || !m) return fail(MOG_ERR_ARG, "null argument");
+    int rc = check_particles(h, pos4, vel4, n, true);
+    if (rc) return rc;
+    if (!std::isfinite(dt_eff)) return fail(MOG_ERR_ARG, "dt_eff must be finite");
+    if ((rc = set_device(h))) return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if ((rc = learn_buffers(h, n, s))) return rc;
+    if ((rc = run_features(h, m, reinterpret_cast<const float4*>(pos4), n, h->d_mean, h->d_feat, s)))
+        return rc;
+    cudaError_t err = mog::launch_mlp_infer(h->d_feat, n, m->d_frags, m->d_params, h->d_mean,
+                                            m->norm.out_scale, h->d_acc, s);
+    if (err != cudaSuccess) return cuda_fail(err, "mlp inference");
+    err = mog::launch_apply_force(reinterpret_cast<float4*>(pos4), reinterpret_cast<float4*>(vel4), n,
+                                  h->d_acc, dt_eff, h->cfg.damping, h->e.world, h->d_flags, s);
+    if (err != cudaSuccess) return cuda_fail(err, "apply force");
+    ++h->step_count;
+    return MOG_OK;
+}
 
 }  // extern "C"

@@ -117,4 +117,33 @@ cudaError_t launch_direct_sum(const float4* targets, int64_t nt, const float4* s
                               double world, double g_eff, double soft, double* partial, int chunks,
                               double* out3, cudaStream_t s);
 
+// ---- learned correction (learned.cu) ------------------------------------
+constexpr int kModelIn = 12;
+// Per-model normalisation: x = (f - mu) / sigma, out = y * out_scale.
+struct ModelNorm {
+    float mu[kModelIn];
+    float inv_sigma[kModelIn];
+    float force_scale;   // s: forces enter the features as F / s
+    float rho_ref;       // mean cell mass (total mass / g^3)
+    float out_scale;     // residual = y * out_scale
+    float pad;
+};
+
+
+int mlp_param_count();
+size_t mlp_fragment_bytes();
+size_t mlp_train_smem();
+cudaError_t launch_features(const Ensemble& e, const float4* pos, int64_t n, const float4* W,
+                            const void* mass, const ModelNorm& norm, float4* mean, float* feat,
+                            cudaStream_t s);
+cudaError_t launch_pack_fragments(const float* params, void* frags, cudaStream_t s);
+cudaError_t launch_mlp_infer(const float* feat, int64_t n, const void* frags, const float* params,
+                             const float4* mean, float out_scale, float4* acc, cudaStream_t s);
+cudaError_t launch_mlp_train_step(const float* feat, const float* target, const int* idx,
+                                  int batch, float* params, float* partial, float* loss_partial,
+                                  float* grad, float* m, float* v, float lr, int t,
+                                  cudaStream_t s);
+cudaError_t launch_apply_force(float4* pos, float4* vel, int64_t n, const float4* acc, float dt,
+                               float damp, float world, unsigned* flags, cudaStream_t s);
+
 }  // namespace mog
