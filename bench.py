@@ -207,6 +207,13 @@ def run_ours(args, w: dict) -> None:
     sim = Simulation(cfg, device=dev)
     pos, vel = make_particles(w, sim, seed_offset=rank)
     sim.set_particles(pos, vel)
+    tuning = json.loads(args.tuning) if args.tuning else {}
+    if tuning:
+        sim.tune(**tuning)
+    if args.autotune:
+        from mog_solver_b200.autotune import autotune
+
+        tuning = autotune(sim, cache=None)["tuning"]
     n = sim.n_particles
     lib = _lib.lib()
     stream = torch.cuda.Stream(device=dev)
@@ -303,7 +310,8 @@ def run_ours(args, w: dict) -> None:
                        "damping": w["damping"], "index_mode": args.index_mode,
                        "mass_mode": "u64 fixed point", "parallelism":
                        "single GPU" if world == 1 else f"{world} independent replicas",
-                       "l2": "flushed between timed steps (256 MiB write)"},
+                       "l2": "flushed between timed steps (256 MiB write)",
+                       "tuning": sim.tuning()},
             "phase_ms": {nm: float(v) for nm, v in zip(names, mean_ph)},
             "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved,
                          "peak": peaks["hbm_gbs"], "unit": "GB/s",
@@ -333,6 +341,8 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--index-mode", default="fast", choices=["fast", "exact"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tuning", default="", help="JSON object of mog_tuning fields to apply")
+    ap.add_argument("--autotune", action="store_true", help="pick launch shapes before timing")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

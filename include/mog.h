@@ -109,7 +109,7 @@ typedef struct mog_tuning {
     int32_t sort_every;             /* spatial re-ordering period in steps; 0 = never (default) */
     int32_t update_direct_ppt;      /* particles per thread of the L2-gather update: 1, 2, 4 */
     int32_t deposit_aggregate;      /* warp-merge runs of equal cells: -1 auto, 0 off, 1 on  */
-    int32_t reserved;
+    int32_t deposit_generic;        /* 1: never use the specialised g <= 16 deposit kernel    */
 } mog_tuning;
 
 /* Fill a config with the reference's in-code defaults (main.py:179-189). */
@@ -213,6 +213,23 @@ int mog_diagnostics(mog_handle* h, const float* pos4, const float* vel4,
  */
 int mog_direct_sum(const float* targets4, int64_t nt, const float* sources4, int64_t ns,
                    double world, double g_eff, double soft, double* out3, void* stream);
+
+/*
+ * Batched independent simulations (BASELINE config "batched uneven
+ * ensemble"; no counterpart in the reference, which runs one simulation per
+ * window).  A batch groups `count` handles on one device.  mog_batch_step
+ * advances every simulation n_steps steps; each ensemble step is ONE CUDA
+ * graph launch in which every simulation's kernels run on its own branch,
+ * so small and large simulations overlap on the GPU.  The graph is captured
+ * once per combination of (pos4[i], vel4[i], n[i], dt_eff[i]).  Spatial
+ * re-ordering inside a batch happens on every step when a handle's
+ * sort_every is 1 and never otherwise.
+ */
+typedef struct mog_batch mog_batch;
+int mog_batch_create(mog_handle* const* handles, int32_t count, mog_batch** out);
+int mog_batch_step(mog_batch* b, float* const* pos4, float* const* vel4, const int64_t* n,
+                   const float* dt_eff, int32_t n_steps, void* stream);
+int mog_batch_destroy(mog_batch* b);
 
 /*
  * Learned correction of a cheap ensemble (no counterpart in the reference,

@@ -1,0 +1,110 @@
+"""Autotuner for the launch shapes of a Simulation (no counterpart in the
+reference, whose dispatch shapes are fixed in main.py:596-668).
+
+The knobs of ``mog_tuning`` (include/mog.h) never change a result — every
+variant is bit-identical (tests/test_gpu_parity.py checks that) — only its
+speed.  ``autotune(sim)`` measures candidate shapes with
+``mog_step_profiled`` (per-kernel device times), one knob group at a time
+(coordinate search: deposit shape, gather variant, spatial ordering), keeps
+the fastest, restores the particles it advanced, and caches the choice in
+a JSON file keyed by device, particle-count bucket, k, g and modes.
+"""
+from __future__ import annotations
+
+import ctypes
+import itertools
+import json
+import math
+import os
+from pathlib import Path
+
+import numpy as np
+
+from . import _lib
+from .simulation import Simulation, torch_device
+
+CACHE = Path(os.environ.get("MOG_TUNING_CACHE", Path(__file__).resolve().parent / "tuning_cache.json"))
+
+
+def _key(sim: Simulation) -> str:
+    import torch
+
+    c = sim.cfg
+    name = torch.cuda.get_device_name(sim.device).replace(" ", "_")
+    bucket = 1 << max(0, math.ceil(math.log2(max(1, sim.n_particles))))
+    return f"{name}|n{bucket}|k{c.n_grids}|g{c.grid_size}|{c.mass_mode}|{c.index_mode}|{c.solver}"
+
+
+def _measure(sim: Simulation, reps: int) -> np.ndarray:
+    """Mean per-phase device ms over `reps` profiled steps (after 2 warm-ups)."""
+    lib = _lib.lib()
+    h = sim.handle
+    ph = (ctypes.c_float * 4)()
+    rows = []
+    with torch_device(sim.device):
+        for i in range(reps + 2):
+            _lib.check(lib.mog_step_profiled(h, sim.pos.data_ptr(), sim.vel.data_ptr(),
+                                             sim.n_particles, float(sim.cfg.dt), ph,
+                                             sim._stream()), "mog_step_profiled")
+            if i >= 2:
+                rows.append(list(ph))
+    return np.array(rows).mean(axis=0)
+
+
+def _candidates(sim: Simulation) -> dict[str, list[dict]]:
+    g = sim.cfg.grid_size
+    dep = [dict(deposit_grids_per_cta=gpc, deposit_ppt=ppt, deposit_threads=thr)
+           for gpc, ppt, thr in itertools.product([0, 3, 6] if g <= 16 else [0],
+                                                  [2, 4], [512, 1024])]
+    dep.append(dict(deposit_grids_per_cta=-1))
+    upd = [dict(update_staged=0, update_direct_ppt=1), dict(update_staged=0, update_direct_ppt=4)]
+    if g <= 16:
+        upd.append(dict(update_staged=1))
+    order = [dict(sort_every=0), dict(sort_every=16)]
+    return {"deposit": dep, "update": upd, "order": order}
+
+
+def autotune(sim: Simulation, reps: int = 4, cache: Path | None = CACHE, force: bool = False) -> dict:
+    """Pick and apply the fastest launch shapes for sim's current particles."""
+    key = _key(sim)
+    table = {}
+    if cache is not None and cache.exists():
+        try:
+            table = json.loads(cache.read_text())
+        except (OSError, json.JSONDecodeError):
+            table = {}
+    if key in table and not force:
+        sim.tune(**table[key]["tuning"])
+        return table[key]
+    p0, v0 = sim.pos.clone(), sim.vel.clone()
+    best: dict = {}
+    phase = {"deposit": 1, "update": 3, "order": None}
+    try:
+        for group, cands in _candidates(sim).items():
+            results = []
+            for cand in cands:
+                trial = {**best, **cand}
+                try:
+                    sim.tune(**trial)
+                    ms = _measure(sim, reps)
+                except _lib.MogError:
+                    continue
+                t = float(ms.sum()) if phase[group] is None else float(ms[phase[group]])
+                results.append((t, cand))
+                sim.pos.copy_(p0)
+                sim.vel.copy_(v0)
+            if results:
+                best.update(min(results, key=lambda r: r[0])[1])
+        sim.tune(**best)
+        total = float(_measure(sim, reps).sum())
+    finally:
+        sim.pos.copy_(p0)
+        sim.vel.copy_(v0)
+    entry = {"tuning": best, "step_ms": total}
+    if cache is not None:
+        table[key] = entry
+        try:
+            cache.write_text(json.dumps(table, indent=1, sort_keys=True))
+        except OSError:
+            pass
+    return entry

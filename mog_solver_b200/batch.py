@@ -1,0 +1,67 @@
+"""Several independent simulations advanced together (one CUDA graph per
+ensemble step, one branch per simulation; mog_batch_* in include/mog.h).
+
+The reference runs one simulation per window; this is the batched uneven
+ensemble of the benchmark configurations: simulations of different N, k and
+g step in a single graph launch so that small ones fill the GPU around
+large ones.
+"""
+from __future__ import annotations
+
+import ctypes
+
+from . import _lib
+from .simulation import Simulation, torch_device
+
+
+class Batch:
+    def __init__(self, sims: list[Simulation]):
+        if not sims:
+            raise ValueError("a batch needs at least one simulation")
+        self.sims = list(sims)
+        self._h = ctypes.c_void_p()
+        self._built_for = None
+
+    def _handles(self):
+        hs = [s.handle for s in self.sims]  # creates / refreshes each handle
+        key = tuple(h.value for h in hs)
+        if self._built_for != key:
+            self.close()
+            arr = (ctypes.c_void_p * len(hs))(*[h.value for h in hs])
+            _lib.check(_lib.lib().mog_batch_create(arr, len(hs), ctypes.byref(self._h)),
+                       "mog_batch_create")
+            self._built_for = key
+        return self._h
+
+    def step(self, n_steps: int = 1) -> None:
+        import torch
+
+        h = self._handles()
+        k = len(self.sims)
+        pos = (ctypes.c_void_p * k)(*[s.pos.data_ptr() for s in self.sims])
+        vel = (ctypes.c_void_p * k)(*[s.vel.data_ptr() for s in self.sims])
+        n = (ctypes.c_int64 * k)(*[s.n_particles for s in self.sims])
+        dt = (ctypes.c_float * k)(*[float(s.cfg.dt * s.timescale) for s in self.sims])
+        dev = self.sims[0].device
+        with torch_device(dev):
+            stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+            _lib.check(_lib.lib().mog_batch_step(h, pos, vel, n, dt, int(n_steps), stream),
+                       "mog_batch_step")
+        for s in self.sims:
+            s.steps_taken += n_steps
+
+    @property
+    def n_particles(self) -> int:
+        return sum(s.n_particles for s in self.sims)
+
+    def close(self) -> None:
+        if self._h:
+            _lib.lib().mog_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+            self._built_for = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -220,6 +220,131 @@ __global__ void __launch_bounds__(1024) deposit_smem_kernel(const float4* __rest
     }
 }
 
+// Specialised deposit for the common case: g <= 16 known at compile time,
+// FAST cell indices, whole grids in shared memory.  Cell offsets use
+// compile-time masks and shifts, shared adds are red.shared.add.u32 on
+// 32-bit shared addresses, full batches run without bounds checks, and
+// when every lane of a warp has a zero low word (equal power-of-two
+// fixed-point masses) the 64-bit add is a single add of the high word.
+__device__ __forceinline__ void red_shared(uint32_t addr, unsigned v) {
+    asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned atom_shared(uint32_t addr, unsigned v) {
+    unsigned old;
+    asm volatile("atom.shared.add.u32 %0, [%1], %2;" : "=r"(old) : "r"(addr), "r"(v) : "memory");
+    return old;
+}
+
+template <int LG>
+__device__ __forceinline__ uint32_t cell_byte_offset(const float4& r0, const float4& r1,
+                                                     const float4& r2, float cx, float cy,
+                                                     float cz) {
+    constexpr uint32_t M = (1u << LG) - 1u;
+    const float tx = __fmaf_rn(r0.z, cz, __fmaf_rn(r0.y, cy, __fmaf_rn(r0.x, cx, r0.w)));
+    const float ty = __fmaf_rn(r1.z, cz, __fmaf_rn(r1.y, cy, __fmaf_rn(r1.x, cx, r1.w)));
+    const float tz = __fmaf_rn(r2.z, cz, __fmaf_rn(r2.y, cy, __fmaf_rn(r2.x, cx, r2.w)));
+    const uint32_t bx = __float_as_uint(__fadd_rd(tx, 12582912.0f));
+    const uint32_t by = __float_as_uint(__fadd_rd(ty, 12582912.0f));
+    const uint32_t bz = __float_as_uint(__fadd_rd(tz, 12582912.0f));
+    // 4 * (x | y << LG | z << 2 LG)
+    return ((bx & M) << 2) | ((by & M) << (LG + 2)) | ((bz & M) << (2 * LG + 2));
+}
+
+template <int LG, int MODE, int PPT>
+__global__ void __launch_bounds__(1024) deposit_fast_kernel(const float4* __restrict__ pos,
+                                                            int64_t n, int64_t chunk, Ensemble e,
+                                                            int gpc,
+                                                            typename SmemHist<MODE>::Acc* __restrict__ mass) {
+    using H = SmemHist<MODE>;
+    using Acc = typename H::Acc;
+    constexpr int G3 = 1 << (3 * LG);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int g0 = blockIdx.y * gpc;
+    const int ng = min(gpc, e.k - g0);
+    const uint32_t words = (uint32_t)ng * G3;
+    float4* rows = reinterpret_cast<float4*>(smem_raw);                       // gpc * 3 rows
+    unsigned* lo_w = reinterpret_cast<unsigned*>(smem_raw + (size_t)gpc * 48);
+    unsigned* hi_w = lo_w + (size_t)gpc * G3;
+    const uint32_t lo_base = (uint32_t)__cvta_generic_to_shared(lo_w);
+    const uint32_t hi_base = (uint32_t)__cvta_generic_to_shared(hi_w);
+
+    for (int i = threadIdx.x; i < ng * 3; i += blockDim.x) rows[i] = e.fast[g0 + i / 3].row[i % 3];
+    for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) {
+        lo_w[i] = 0u;
+        if (H::kWords == 2) hi_w[i] = 0u;
+    }
+    __syncthreads();
+
+    const float half_l = e.world * 0.5f;
+    const int64_t lo = (int64_t)blockIdx.x * chunk;
+    const int64_t hi = min(n, lo + chunk);
+    const int T = blockDim.x;
+    unsigned bad = 0;
+    double qsum = 0.0;
+    for (int64_t base = lo; base < hi; base += (int64_t)T * PPT) {
+        const bool full = base + (int64_t)T * PPT <= hi;  // block-uniform
+        float cx[PPT], cy[PPT], cz[PPT];
+        unsigned ql[PPT], qh[PPT];
+#pragma unroll
+        for (int u = 0; u < PPT; ++u) {
+            const int64_t slot = base + (int64_t)u * T + threadIdx.x;
+            const bool valid = full || slot < hi;
+            const float4 P = valid ? __ldg(pos + slot) : make_float4(0.f, 0.f, 0.f, 0.f);
+            unsigned b = 0;
+            Acc q;
+            if (MODE == 1)
+                q = valid ? quantize_u64(P.w, e.scale, b) : 0ull;
+            else
+                q = valid ? quantize_u32(P.w, b) : 0u;
+            bad |= b;
+            qsum += (double)q;
+            ql[u] = (unsigned)q;
+            qh[u] = MODE == 1 ? (unsigned)((unsigned long long)q >> 32) : 0u;
+            cx[u] = __fsub_rn(P.x, half_l);
+            cy[u] = __fsub_rn(P.y, half_l);
+            cz[u] = __fsub_rn(P.z, half_l);
+        }
+        // one vote per batch: can the low words be skipped for the whole warp?
+        bool hi_only = false;
+        if (MODE == 1) {
+            unsigned any_lo = 0;
+#pragma unroll
+            for (int u = 0; u < PPT; ++u) any_lo |= ql[u];
+            hi_only = __all_sync(kFull, any_lo == 0u);
+        }
+        for (int j = 0; j < ng; ++j) {
+            const float4 r0 = rows[3 * j], r1 = rows[3 * j + 1], r2 = rows[3 * j + 2];
+            const uint32_t gbyte = (uint32_t)j * (G3 * 4u);
+#pragma unroll
+            for (int u = 0; u < PPT; ++u) {
+                const uint32_t off = gbyte + cell_byte_offset<LG>(r0, r1, r2, cx[u], cy[u], cz[u]);
+                if (MODE == 0) {
+                    if (ql[u]) red_shared(lo_base + off, ql[u]);   // zero for padding lanes
+                } else if (hi_only) {
+                    if (qh[u]) red_shared(hi_base + off, qh[u]);
+                } else {
+                    unsigned h = qh[u];
+                    if (ql[u]) {
+                        const unsigned old = atom_shared(lo_base + off, ql[u]);
+                        h += (old > ~ql[u]) ? 1u : 0u;
+                    }
+                    if (h) red_shared(hi_base + off, h);
+                }
+            }
+        }
+    }
+    if (MODE == 1 && blockIdx.y == 0) {
+        for (int o = 16; o > 0; o >>= 1) qsum += __shfl_xor_sync(kFull, qsum, o);
+        if ((threadIdx.x & 31) == 0 && qsum != 0.0) atomicAdd(e.mass_total, qsum);
+    }
+    if (bad) raise_flags(e.flags, bad);
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) {
+        const Acc v = H::read(lo_w, hi_w, i);
+        if (v) atomicAdd(mass + (size_t)g0 * G3 + i, v);
+    }
+}
+
 // Direct global-atomic deposit (any g): one thread per particle, all grids.
 template <typename Acc, int IDX>
 __global__ void __launch_bounds__(256) deposit_global_kernel(const float4* __restrict__ pos,
@@ -284,6 +409,35 @@ static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, const int
     const size_t smem = (size_t)gpc * 16 * sizeof(float) + ((size_t)gpc * word_bytes << slab_lg);
     const int ppt = sh.ppt == 1 || sh.ppt == 2 || sh.ppt == 4 ? sh.ppt : 4;
     const bool agg = sh.aggregate < 0 ? ordered : sh.aggregate != 0;
+    if (IDX == 0 && !agg && !perm && slab_lg == cells_lg && (e.g == 8 || e.g == 16) &&
+        sh.fast != 0) {
+        auto launch_fast = [&](auto kern) -> cudaError_t {
+            const size_t fsmem = (size_t)gpc * 48 + ((size_t)gpc * word_bytes << cells_lg);
+            cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)fsmem);
+            if (err != cudaSuccess) return err;
+            const int groups = (e.k + gpc - 1) / gpc;
+            int chunks = sh.chunks;
+            if (chunks <= 0) {
+                const int per_sm = fsmem > 110 * 1024 ? 1 : 2;
+                const int64_t target = (int64_t)num_sms() * per_sm * 8;
+                int64_t c = (target + groups - 1) / groups;
+                const int64_t max_c = (n + 4095) / 4096;
+                chunks = (int)std::max<int64_t>(1, std::min<int64_t>(std::max<int64_t>(c, 32), max_c));
+            }
+            const int64_t chunk = (n + chunks - 1) / chunks;
+            kern<<<dim3(chunks, groups, 1), sh.threads, fsmem, s>>>(pos, n, chunk, e, gpc, mass);
+            return cudaGetLastError();
+        };
+        if (e.g == 16) {
+            if (ppt == 1) return launch_fast(deposit_fast_kernel<4, MODE, 1>);
+            if (ppt == 2) return launch_fast(deposit_fast_kernel<4, MODE, 2>);
+            return launch_fast(deposit_fast_kernel<4, MODE, 4>);
+        }
+        if (ppt == 1) return launch_fast(deposit_fast_kernel<3, MODE, 1>);
+        if (ppt == 2) return launch_fast(deposit_fast_kernel<3, MODE, 2>);
+        return launch_fast(deposit_fast_kernel<3, MODE, 4>);
+    }
     auto launch = [&](auto kern) -> cudaError_t {
         cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                (int)smem);

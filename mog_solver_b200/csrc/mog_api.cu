@@ -671,6 +671,7 @@ int mog_get_tuning(const mog_handle* h, mog_tuning* out) {
     out->update_ctas = h->ushape.ctas;
     out->sort_every = h->sort_every;
     out->deposit_aggregate = h->dshape.aggregate;
+    out->deposit_generic = h->dshape.fast ? 0 : 1;
     out->update_direct_ppt = h->ushape.direct_ppt;
     return MOG_OK;
 }
@@ -696,6 +697,7 @@ int mog_set_tuning(mog_handle* h, const mog_tuning* t) {
     h->ushape.direct_ppt = t->update_direct_ppt ? t->update_direct_ppt : 4;
     h->sort_every = t->sort_every < 0 ? 0 : t->sort_every;
     h->dshape.aggregate = t->deposit_aggregate;
+    h->dshape.fast = t->deposit_generic ? 0 : 1;
     for (auto& g : h->graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);
     h->graphs.clear();
@@ -960,3 +962,143 @@ int mog_learned_step(mog_handle* h, const mog_model* m, float* pos4, float* vel4
 }
 
 }  // extern "C"
+
+// ---- batched simulations -------------------------------------------------
+
+struct mog_batch {
+    std::vector<mog_handle*> sims;
+    int device = 0;
+    cudaStream_t cap = nullptr;
+    std::vector<cudaStream_t> branch;
+    std::vector<cudaEvent_t> done;
+    cudaEvent_t fork = nullptr;
+    struct Entry {
+        std::vector<float*> pos, vel;
+        std::vector<int64_t> n;
+        std::vector<float> dt;
+        cudaGraphExec_t exec = nullptr;
+    };
+    std::vector<Entry> graphs;
+};
+
+extern "C" {
+
+int mog_batch_destroy(mog_batch* b) {
+    if (!b) return MOG_OK;
+    for (auto& g : b->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    for (auto s : b->branch)
+        if (s) cudaStreamDestroy(s);
+    for (auto e : b->done)
+        if (e) cudaEventDestroy(e);
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->cap) cudaStreamDestroy(b->cap);
+    delete b;
+    return MOG_OK;
+}
+
+int mog_batch_create(mog_handle* const* handles, int32_t count, mog_batch** out) {
+    if (!handles || !out || count <= 0) return fail(MOG_ERR_ARG, "need handles and count > 0");
+    *out = nullptr;
+    mog_batch* b = new mog_batch();
+    b->device = handles[0] ? handles[0]->device : 0;
+    for (int i = 0; i < count; ++i) {
+        if (!handles[i]) {
+            mog_batch_destroy(b);
+            return fail(MOG_ERR_ARG, "null handle in batch");
+        }
+        if (handles[i]->device != b->device) {
+            mog_batch_destroy(b);
+            return fail(MOG_ERR_ARG, "all handles of a batch must be on one device");
+        }
+        for (int j = 0; j < i; ++j)
+            if (handles[j] == handles[i]) {
+                mog_batch_destroy(b);
+                return fail(MOG_ERR_ARG, "a handle appears twice in the batch");
+            }
+        b->sims.push_back(handles[i]);
+    }
+    cudaError_t err = cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking);
+    if (!err) err = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+    b->branch.assign(count, nullptr);
+    b->done.assign(count, nullptr);
+    for (int i = 0; i < count && !err; ++i) {
+        err = cudaStreamCreateWithFlags(&b->branch[i], cudaStreamNonBlocking);
+        if (!err) err = cudaEventCreateWithFlags(&b->done[i], cudaEventDisableTiming);
+    }
+    if (err) {
+        mog_batch_destroy(b);
+        return cuda_fail(err, "mog_batch_create");
+    }
+    *out = b;
+    return MOG_OK;
+}
+
+int mog_batch_step(mog_batch* b, float* const* pos4, float* const* vel4, const int64_t* n,
+                   const float* dt_eff, int32_t n_steps, void* stream) {
+    if (!b || !pos4 || !vel4 || !n || !dt_eff) return fail(MOG_ERR_ARG, "null argument");
+    if (n_steps < 0) return fail(MOG_ERR_ARG, "n_steps must be >= 0");
+    const int count = (int)b->sims.size();
+    for (int i = 0; i < count; ++i) {
+        int rc = check_particles(b->sims[i], pos4[i], vel4[i], n[i], true);
+        if (rc) return rc;
+        if (!std::isfinite(dt_eff[i])) return fail(MOG_ERR_ARG, "dt_eff must be finite");
+    }
+    if (n_steps == 0) return MOG_OK;
+    int rc = set_device(b->sims[0]);
+    if (rc) return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    mog_batch::Entry* ge = nullptr;
+    for (auto& g : b->graphs) {
+        bool same = true;
+        for (int i = 0; i < count && same; ++i)
+            same = g.pos[i] == pos4[i] && g.vel[i] == vel4[i] && g.n[i] == n[i] && g.dt[i] == dt_eff[i];
+        if (same) ge = &g;
+    }
+    if (!ge) {
+        // buffers that a captured step cannot allocate
+        for (int i = 0; i < count; ++i) {
+            mog_handle* h = b->sims[i];
+            if (h->sort_every == 1 && n[i] > h->perm_cap)
+                return fail(MOG_ERR_ARG, "batch: n exceeds a handle's num_particles");
+        }
+        cudaGraph_t graph = nullptr;
+        MOG_CUDA(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal), "begin capture");
+        cudaError_t err = cudaEventRecord(b->fork, b->cap);
+        for (int i = 0; i < count && !err && !rc; ++i) {
+            err = cudaStreamWaitEvent(b->branch[i], b->fork, 0);
+            if (err) break;
+            mog_handle* h = b->sims[i];
+            rc = run_pipeline(h, reinterpret_cast<float4*>(pos4[i]), reinterpret_cast<float4*>(vel4[i]),
+                              n[i], dt_eff[i], nullptr, b->branch[i], h->sort_every == 1);
+            if (!rc) err = cudaEventRecord(b->done[i], b->branch[i]);
+            if (!err && !rc) err = cudaStreamWaitEvent(b->cap, b->done[i], 0);
+        }
+        cudaError_t end = cudaStreamEndCapture(b->cap, &graph);
+        if (rc || err || end) {
+            if (graph) cudaGraphDestroy(graph);
+            if (rc) return rc;
+            return cuda_fail(err ? err : end, "batch capture");
+        }
+        mog_batch::Entry entry;
+        entry.pos.assign(pos4, pos4 + count);
+        entry.vel.assign(vel4, vel4 + count);
+        entry.n.assign(n, n + count);
+        entry.dt.assign(dt_eff, dt_eff + count);
+        err = cudaGraphInstantiate(&entry.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (err) return cuda_fail(err, "batch graph instantiate");
+        if (b->graphs.size() >= 4) {
+            cudaGraphExecDestroy(b->graphs.front().exec);
+            b->graphs.erase(b->graphs.begin());
+        }
+        b->graphs.push_back(std::move(entry));
+        ge = &b->graphs.back();
+    }
+    for (int t = 0; t < n_steps; ++t) MOG_CUDA(cudaGraphLaunch(ge->exec, s), "batch graph launch");
+    for (auto* h : b->sims) h->step_count += (uint64_t)n_steps;
+    return MOG_OK;
+}
+
+}  // extern "C"
+

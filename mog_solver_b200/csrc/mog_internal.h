@@ -50,6 +50,7 @@ struct DepositShape {
     int chunks = 0;         // particle chunks; 0 = derived from n
     int ppt = 4;            // particles per thread carried through the grid loop
     int aggregate = -1;     // warp-merge runs of equal cells: -1 auto (when ordered), 0, 1
+    int fast = 1;           // use the specialised kernel where it applies
 };
 struct UpdateShape {
     int threads = 512;

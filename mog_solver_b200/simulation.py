@@ -183,7 +183,7 @@ class Simulation:
         """Current launch shapes of the handle (mog_get_tuning)."""
         t = _lib.MogTuningC()
         _lib.check(_lib.lib().mog_get_tuning(self.handle, ctypes.byref(t)), "mog_get_tuning")
-        return {name: getattr(t, name) for name, _ in t._fields_ if name != "reserved"}
+        return {name: getattr(t, name) for name, _ in t._fields_}
 
     def tune(self, **shapes: int) -> None:
         """Set launch shapes (mog_set_tuning); results never depend on them."""

@@ -65,13 +65,15 @@ DEPOSIT_TUNINGS = {
     "sorted+plain": dict(sort_every=1, deposit_aggregate=0, deposit_ppt=1),
     "unsorted+merged": dict(sort_every=0, deposit_aggregate=1, deposit_ppt=2),
     "global": dict(sort_every=0, deposit_grids_per_cta=-1),
+    "generic": dict(sort_every=0, deposit_generic=1),
+    "fast-ppt1": dict(sort_every=0, deposit_ppt=1, deposit_grids_per_cta=2),
 }
 
 
 @pytest.mark.parametrize("mass_mode,index_mode", MODES)
 @pytest.mark.parametrize("n,k,g", SHAPES)
 @pytest.mark.parametrize("equal_mass", [True, False])
-@pytest.mark.parametrize("tuning", ["sorted+merged", "unsorted"])
+@pytest.mark.parametrize("tuning", ["sorted+merged", "unsorted", "generic"])
 def test_deposit_bit_exact(mass_mode, index_mode, n, k, g, equal_mass, tuning):
     L = 100.0
     sim = make_sim(k=k, g=g, L=L, n=n, mass_mode=mass_mode, index_mode=index_mode, seed=n + k)
