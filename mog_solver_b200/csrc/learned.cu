@@ -5,12 +5,11 @@
 // GELU) predicts, from statistics of a cheap ensemble (k = 32), the residual
 // to an expensive one (k = 240):
 //
-//   features  per particle, from the k grids it touches:
-//             mean world force F (3), its per-component spread over the
-//             grids (3), mean distance of the particle from its cells'
-//             centres per grid axis (3), mean cell mass (1), |F| (1) and
-//             the mean per-grid force magnitude (1); standardised with the
-//             model's statistics;
+//   features  per particle, from the k grids it touches: the mean world
+//             force, a least-squares correction of it from the particle's
+//             offsets to its cells' centres, the per-grid force spread, the
+//             mean cell mass and two scalars (see features_kernel);
+//             standardised with the model's statistics;
 //   inference BF16 tensor-core MLP (mma.sync m16n8k16, FP32 accumulate).
 //             A warp carries 16 particles through all three layers in
 //             registers: the accumulator fragment of one layer is, pair of
@@ -61,6 +60,23 @@ __device__ __forceinline__ float gelu_fast(float x) {
 
 // ---------------------------------------------------------------------------
 // Feature gather.  One thread per particle; grids read from L2.
+//
+// Each grid samples the force at the centre of the particle's cell, not at
+// the particle, so the k per-grid forces F_i scatter around the force at
+// the particle roughly linearly in the particle's offset from those cell
+// centres, d_i (world frame).  A per-particle least-squares fit
+// F_i ~ a + B d_i over the k grids gives an intercept a, the force
+// extrapolated to the particle itself:
+//     a = Fbar - C_Fd (C_dd + ridge)^-1 dbar
+// with dbar, C_dd = cov(d, d) and C_Fd = cov(F, d) over the grids.
+// The features are
+//   0-2  Fbar / s            plain ensemble mean (update.glsl order)
+//   3-5  (a - Fbar) / s      regression correction from the in-cell offsets
+//   6-8  std_i(F_i) / s      per-component spread of the per-grid forces
+//   9    log1p(rho / rho_ref) mean mass of the particle's cells
+//   10   |Fbar| / s
+//   11   sqrt(tr C_dd) / h   spread of the in-cell offsets
+// then standardised with the model's mu / sigma.
 template <typename Acc>
 __global__ void __launch_bounds__(256) features_kernel(const float4* __restrict__ pos, int64_t n,
                                                        const float4* __restrict__ W,
@@ -75,10 +91,14 @@ __global__ void __launch_bounds__(256) features_kernel(const float4* __restrict_
                 cz = __fsub_rn(P.z, ip.half_l);
     const int G3 = 1 << (3 * e.lg);
     const uint32_t mask = (1u << e.lg) - 1u;
-    float sx = 0.f, sy = 0.f, sz = 0.f;      // plain average, update.glsl order
-    float qx = 0.f, qy = 0.f, qz = 0.f;      // second moments
-    float fx = 0.f, fy = 0.f, fz = 0.f;      // |frac - 1/2|
-    float rho = 0.f, mag = 0.f;
+    const float h = e.voxel;
+    float sx = 0.f, sy = 0.f, sz = 0.f;            // plain sum, update.glsl order
+    float qx = 0.f, qy = 0.f, qz = 0.f;            // sum F^2 per component
+    float dx = 0.f, dy = 0.f, dz = 0.f;            // sum d
+    float dxx = 0.f, dxy = 0.f, dxz = 0.f, dyy = 0.f, dyz = 0.f, dzz = 0.f;
+    float fxdx = 0.f, fxdy = 0.f, fxdz = 0.f, fydx = 0.f, fydy = 0.f, fydz = 0.f,
+          fzdx = 0.f, fzdy = 0.f, fzdz = 0.f;      // sum F d^T
+    float rho = 0.f;
     for (int i = 0; i < e.k; ++i) {
         const FastXf x = e.fast[i];
         const float tx = __fmaf_rn(x.row[0].z, cz, __fmaf_rn(x.row[0].y, cy, __fmaf_rn(x.row[0].x, cx, x.row[0].w)));
@@ -97,29 +117,59 @@ __global__ void __launch_bounds__(256) features_kernel(const float4* __restrict_
         qx += f.x * f.x;
         qy += f.y * f.y;
         qz += f.z * f.z;
-        mag += sqrtf(f.x * f.x + f.y * f.y + f.z * f.z);
-        fx += fabsf(tx - floorf(tx) - 0.5f);
-        fy += fabsf(ty - floorf(ty) - 0.5f);
-        fz += fabsf(tz - floorf(tz) - 0.5f);
+        // offset from the cell centre, grid frame -> world frame (M d)
+        const float gx = (tx - floorf(tx) - 0.5f) * h, gy = (ty - floorf(ty) - 0.5f) * h,
+                    gz = (tz - floorf(tz) - 0.5f) * h;
+        const float* R = e.rot12 + 12 * i;
+        const float wx = R[0] * gx + R[1] * gy + R[2] * gz;
+        const float wy = R[4] * gx + R[5] * gy + R[6] * gz;
+        const float wz = R[8] * gx + R[9] * gy + R[10] * gz;
+        dx += wx; dy += wy; dz += wz;
+        dxx += wx * wx; dxy += wx * wy; dxz += wx * wz;
+        dyy += wy * wy; dyz += wy * wz; dzz += wz * wz;
+        fxdx += f.x * wx; fxdy += f.x * wy; fxdz += f.x * wz;
+        fydx += f.y * wx; fydy += f.y * wy; fydz += f.y * wz;
+        fzdx += f.z * wx; fzdy += f.z * wy; fzdz += f.z * wz;
         rho += mass_value(__ldg(mass + (size_t)i * G3 + c), e.inv_scale);
     }
     const float kf = (float)e.k, ik = 1.0f / kf;
     const float mx = __fdiv_rn(sx, kf), my = __fdiv_rn(sy, kf), mz = __fdiv_rn(sz, kf);
     mean_out[p] = make_float4(mx, my, mz, 0.f);
+    const float ax_ = dx * ik, ay_ = dy * ik, az_ = dz * ik;  // dbar
+    // covariances
+    const float ridge = 1e-3f * h * h;
+    const float cxx = dxx * ik - ax_ * ax_ + ridge, cxy = dxy * ik - ax_ * ay_,
+                cxz = dxz * ik - ax_ * az_, cyy = dyy * ik - ay_ * ay_ + ridge,
+                cyz = dyz * ik - ay_ * az_, czz = dzz * ik - az_ * az_ + ridge;
+    // solve C_dd w = dbar (symmetric 3x3, adjugate)
+    const float A00 = cyy * czz - cyz * cyz, A01 = cxz * cyz - cxy * czz, A02 = cxy * cyz - cxz * cyy;
+    const float A11 = cxx * czz - cxz * cxz, A12 = cxy * cxz - cxx * cyz, A22 = cxx * cyy - cxy * cxy;
+    const float det = cxx * A00 + cxy * A01 + cxz * A02;
+    float wx = 0.f, wy = 0.f, wz = 0.f;
+    if (det > 0.f) {
+        const float id = 1.0f / det;
+        wx = (A00 * ax_ + A01 * ay_ + A02 * az_) * id;
+        wy = (A01 * ax_ + A11 * ay_ + A12 * az_) * id;
+        wz = (A02 * ax_ + A12 * ay_ + A22 * az_) * id;
+    }
+    // correction = -C_Fd w,  C_Fd = sum(F d^T)/k - Fbar dbar^T
+    const float ex = -((fxdx * ik - mx * ax_) * wx + (fxdy * ik - mx * ay_) * wy + (fxdz * ik - mx * az_) * wz);
+    const float ey = -((fydx * ik - my * ax_) * wx + (fydy * ik - my * ay_) * wy + (fydz * ik - my * az_) * wz);
+    const float ez = -((fzdx * ik - mz * ax_) * wx + (fzdy * ik - mz * ay_) * wy + (fzdz * ik - mz * az_) * wz);
     const float is = 1.0f / norm.force_scale;
     float f[kIn];
     f[0] = mx * is;
     f[1] = my * is;
     f[2] = mz * is;
-    f[3] = sqrtf(fmaxf(qx * ik - mx * mx, 0.f)) * is;
-    f[4] = sqrtf(fmaxf(qy * ik - my * my, 0.f)) * is;
-    f[5] = sqrtf(fmaxf(qz * ik - mz * mz, 0.f)) * is;
-    f[6] = fx * ik;
-    f[7] = fy * ik;
-    f[8] = fz * ik;
+    f[3] = ex * is;
+    f[4] = ey * is;
+    f[5] = ez * is;
+    f[6] = sqrtf(fmaxf(qx * ik - mx * mx, 0.f)) * is;
+    f[7] = sqrtf(fmaxf(qy * ik - my * my, 0.f)) * is;
+    f[8] = sqrtf(fmaxf(qz * ik - mz * mz, 0.f)) * is;
     f[9] = log1pf(rho * ik / norm.rho_ref);
     f[10] = sqrtf(mx * mx + my * my + mz * mz) * is;
-    f[11] = mag * ik * is;
+    f[11] = sqrtf(fmaxf(cxx + cyy + czz - 3.f * ridge, 0.f)) / h;
     float* o = feat_out + (size_t)p * 16;
 #pragma unroll
     for (int j = 0; j < kIn; ++j) o[j] = (f[j] - norm.mu[j]) * norm.inv_sigma[j];

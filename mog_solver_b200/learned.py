@@ -27,8 +27,10 @@ import numpy as np
 from . import _lib
 from .simulation import Simulation, torch_device
 
-FEATURES = ("Fx", "Fy", "Fz", "sFx", "sFy", "sFz", "dx", "dy", "dz", "log_rho", "|F|", "mean|Fi|")
-FORCE_COLS = [0, 1, 2, 3, 4, 5, 10, 11]   # features proportional to 1/force_scale
+FEATURES = ("Fx", "Fy", "Fz", "cFx", "cFy", "cFz", "sFx", "sFy", "sFz", "log_rho", "|F|",
+            "offset_spread")
+FORCE_COLS = [0, 1, 2, 3, 4, 5, 6, 7, 8, 10]   # features proportional to 1/force_scale
+SPREAD_COLS = slice(6, 9)
 
 
 def _torch():
@@ -198,7 +200,7 @@ def generate_dataset(n_sets: int = 64, n: int = 262144, k_small: int = 32, k_big
     feat16[:, :12] = Fz
     norm = norm_vector(mu.cpu().numpy(), (1.0 / sd).cpu().numpy(), s, rho_ref, out_scale)
     stats = {"force_scale": s, "out_scale": out_scale, "samples": int(Fz.shape[0]),
-             "spread_mean": float(F[:, 3:6].double().mean().item())}
+             "spread_mean": float(F[:, SPREAD_COLS].double().mean().item())}
     return Dataset(feat16, T, norm, stats)
 
 
@@ -226,7 +228,7 @@ class LearnedSimulation:
     expensive ensemble as fallback when the variance gate fires.
 
     Gate: the mean grid-to-grid force spread of the current particles
-    (feature block 3-5, in units of the model's force scale) exceeds
+    (features 6-8, in units of the model's force scale) exceeds
     ``gate_factor`` times its training mean.
     """
 
@@ -256,9 +258,9 @@ class LearnedSimulation:
         torch = _torch()
         _, norm = self.model.get()
         mean, feat = features(self.cheap, self.model)
-        sd = 1.0 / norm[15:18]
-        spread = (feat[:, 3:6].double() * torch.from_numpy(sd.astype(np.float64)).to(feat.device)
-                  + torch.from_numpy(norm[3:6].astype(np.float64)).to(feat.device)).mean()
+        sd = 1.0 / norm[18:21]
+        spread = (feat[:, SPREAD_COLS].double() * torch.from_numpy(sd.astype(np.float64)).to(feat.device)
+                  + torch.from_numpy(norm[6:9].astype(np.float64)).to(feat.device)).mean()
         return float(spread.item()) > self.gate_factor * self.spread_train_mean
 
     def step(self, n_steps: int = 1) -> None:

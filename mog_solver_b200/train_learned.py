@@ -1,0 +1,146 @@
+"""Train and evaluate the learned correction (k = 32 -> k = 240, g = 16).
+
+    python -m mog_solver_b200.train_learned [--sets 64] [--n 262144] [--steps 2000]
+           [--out mog_solver_b200/models/learned_k32_g16.npz] [--report report.json]
+
+Training data are pairs the method generates itself: seeded Gaussian-clump
+sets (20 clumps, log-uniform widths 1..8, 10 % uniform background), features
+of a k = 32 ensemble and the k = 240 force minus the k = 32 mean
+(learned.generate_dataset).  Adam, lr 1e-3, batch 8192.
+
+Evaluation on the colliding-disk set (N = 1,048,576): relative RMS error
+against the FP64 direct sum (mog_direct_sum, 16,384 sampled targets, all
+sources; softening 0, h/4, h/2) and against plain k = 240, for plain
+k = 240, plain k = 32 and learned k = 32; and device time per step of the
+plain k = 240 step and the learned k = 32 step.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import time
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+DEFAULT_MODEL = HERE / "models" / "learned_k32_g16.npz"
+
+
+def evaluate(model, n: int = 1 << 20, k_small: int = 32, k_big: int = 240, g: int = 16,
+             world: float = 100.0, G: float = 100.0, steps_timed: int = 50, targets: int = 16384,
+             small_seed: int = 1000, big_seed: int = 2000) -> dict:
+    import torch
+
+    from . import _lib, ics
+    from .learned import _cfg, direct_sum, learned_forces, rms_error
+    from .simulation import Simulation
+
+    small = Simulation(_cfg(k_small, g, world, G, n, small_seed))
+    big = Simulation(_cfg(k_big, g, world, G, n, big_seed))
+    pos, vel = ics.two_disks(n, world, seed=1, g_eff=big.effective_g())
+    small.set_particles(pos, vel)
+    big.set_particles(pos, vel)
+    h = world / g
+    tid = torch.from_numpy(np.random.default_rng(0).choice(n, targets, replace=False)).cuda()
+    P = small.pos
+    T = P[tid].contiguous()
+    f_big = big.forces()
+    f_small = small.forces()
+    f_learn = learned_forces(small, model)
+    # the least-squares correction alone (feature block 3-5), without the network
+    from .learned import Model, features, norm_vector
+
+    raw = Model(norm=norm_vector(np.zeros(12), np.ones(12), 1.0, 1.0 / g ** 3, 1.0))
+    mean, feat = features(small, raw)
+    f_reg = mean.clone()
+    f_reg[:, :3] += feat[:, 3:6]
+    raw.close()
+    report = {"n": n, "k_small": k_small, "k_big": k_big, "g": g, "targets": targets}
+    for soft_name, soft in (("0", 0.0), ("h/4", h / 4), ("h/2", h / 2)):
+        D = direct_sum(T, P, world, big.effective_g(), soft)
+        report[f"rms_vs_direct[soft={soft_name}]"] = {
+            "plain_k240": rms_error(f_big[tid], D), "plain_k32": rms_error(f_small[tid], D),
+            "learned_k32": rms_error(f_learn[tid], D),
+            "regression_only_k32": rms_error(f_reg[tid], D)}
+    report["rms_vs_k240"] = {"plain_k32": rms_error(f_small, f_big), "learned_k32": rms_error(f_learn, f_big),
+                             "regression_only_k32": rms_error(f_reg, f_big)}
+
+    # device time per step (L2 flushed between steps)
+    lib = _lib.lib()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        tot = 0.0
+        for _ in range(steps_timed):
+            flush.zero_()
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            tot += e0.elapsed_time(e1)
+        return tot / steps_timed
+
+    def plain_step():
+        _lib.check(lib.mog_step(big.handle, big.pos.data_ptr(), big.vel.data_ptr(), n, 1e-5, sptr), "step")
+
+    def learned_step():
+        _lib.check(lib.mog_learned_step(small.handle, model.handle, small.pos.data_ptr(),
+                                        small.vel.data_ptr(), n, 1e-5, sptr), "learned step")
+
+    ms_big = timed(plain_step)
+    ms_learn = timed(learned_step)
+    report["ms_per_step"] = {"plain_k240": ms_big, "learned_k32": ms_learn}
+    report["particle_steps_per_s"] = {"plain_k240": n / (ms_big / 1e3), "learned_k32": n / (ms_learn / 1e3)}
+    report["speedup_learned_over_plain_k240"] = ms_big / ms_learn
+    small.close()
+    big.close()
+    return report
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--sets", type=int, default=64)
+    ap.add_argument("--n", type=int, default=262144)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--batch", type=int, default=8192)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--out", default=str(DEFAULT_MODEL))
+    ap.add_argument("--report", default="")
+    ap.add_argument("--eval-only", action="store_true")
+    args = ap.parse_args()
+
+    from .learned import Model, generate_dataset, train
+
+    t0 = time.time()
+    if args.eval_only:
+        model = Model.load(args.out)
+        hist, stats = [], {}
+    else:
+        data = generate_dataset(n_sets=args.sets, n=args.n)
+        t1 = time.time()
+        model = Model(seed=0)
+        hist = train(model, data, steps=args.steps, batch=args.batch, lr=args.lr)
+        stats = dict(data.stats, dataset_seconds=t1 - t0, train_seconds=time.time() - t1)
+        Path(args.out).parent.mkdir(parents=True, exist_ok=True)
+        model.save(args.out)
+        del data
+    rep = evaluate(model)
+    rep["training"] = {"sets": args.sets, "n": args.n, "steps": args.steps, "batch": args.batch,
+                       "lr": args.lr, "loss_history": hist, **stats}
+    text = json.dumps(rep, indent=2)
+    print(text)
+    if args.report:
+        Path(args.report).write_text(text)
+    model.close()
+
+
+if __name__ == "__main__":
+    main()

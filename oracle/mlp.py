@@ -79,28 +79,36 @@ def loss_and_grad(params, x, t):
     return loss, pack(g)
 
 
-def features(pos4, cells, fgrid_world, mass_values, norm):
+def features(cells, fgrid_world, mass_values, t, rot12, h, norm):
     """Per-particle features (n, 12) and plain mean force (n, 3), FP64.
 
     cells: (n, k) cell indices; fgrid_world: (k, g^3, 3) world-frame forces;
-    mass_values: (k, g^3) cell masses; norm: dict with force_scale, rho_ref,
-    mu (12), inv_sigma (12); t_frac: (n, k, 3) scaled coordinates t for the
-    in-cell offsets (passed in norm["t"]).
+    mass_values: (k, g^3) cell masses; t: (n, k, 3) scaled grid coordinates
+    (cell = floor(t)); rot12: (k, 12) packed rotations; h: voxel size;
+    norm: dict with force_scale, rho_ref, mu (12), inv_sigma (12).
+    Definitions follow features_kernel in learned.cu.
     """
     k = cells.shape[1]
     gi = np.arange(k)[None, :]
-    F = fgrid_world[gi, cells]                     # (n, k, 3)
+    F = fgrid_world[gi, cells]                        # (n, k, 3)
     mean = F.mean(axis=1)
     var = np.maximum((F * F).mean(axis=1) - mean * mean, 0.0)
-    s = norm["force_scale"]
-    t = norm["t"]
-    frac = np.abs(t - np.floor(t) - 0.5).mean(axis=1)
+    M = np.asarray(rot12, dtype=np.float32).reshape(-1, 3, 4)[:, :, :3].astype(np.float64)
+    dg = (t - np.floor(t) - 0.5) * h
+    d = np.einsum("kab,nkb->nka", M, dg)              # world-frame offsets
+    dbar = d.mean(axis=1)
+    ridge = 1e-3 * h * h
+    Cdd = np.einsum("nki,nkj->nij", d, d) / k - dbar[:, :, None] * dbar[:, None, :] + ridge * np.eye(3)
+    CFd = np.einsum("nki,nkj->nij", F, d) / k - mean[:, :, None] * dbar[:, None, :]
+    w = np.linalg.solve(Cdd, dbar[:, :, None])[:, :, 0]
+    corr = -np.einsum("nij,nj->ni", CFd, w)
     rho = mass_values[gi, cells].mean(axis=1)
+    s = norm["force_scale"]
     f = np.empty((cells.shape[0], 12))
     f[:, 0:3] = mean / s
-    f[:, 3:6] = np.sqrt(var) / s
-    f[:, 6:9] = frac
+    f[:, 3:6] = corr / s
+    f[:, 6:9] = np.sqrt(var) / s
     f[:, 9] = np.log1p(rho / norm["rho_ref"])
     f[:, 10] = np.linalg.norm(mean, axis=1) / s
-    f[:, 11] = np.linalg.norm(F, axis=2).mean(axis=1) / s
+    f[:, 11] = np.sqrt(np.maximum(np.trace(Cdd, axis1=1, axis2=2) - 3 * ridge, 0.0)) / h
     return (f - norm["mu"]) * norm["inv_sigma"], mean

@@ -115,8 +115,8 @@ def test_features_match_fp64_oracle():
     rows = oracle.fast_rows(sim.rotations, sim.offsets, L, g).astype(np.float64).reshape(k, 3, 4)
     c = pos[:, :3].astype(np.float64) - L / 2
     t = np.einsum("krj,nj->nkr", rows[:, :, :3], c) + rows[:, :, 3][None]
-    ref, ref_mean = mlp.features(pos, cells, Fw, mass.reshape(k, -1),
-                                 {"force_scale": fs, "rho_ref": rho_ref, "mu": mu, "inv_sigma": isd, "t": t})
+    ref, ref_mean = mlp.features(cells, Fw, mass.reshape(k, -1), t, sim.rotations, L / g,
+                                 {"force_scale": fs, "rho_ref": rho_ref, "mu": mu, "inv_sigma": isd})
     got = feat.cpu().numpy()[:, :12].astype(np.float64)
     err = np.abs(got - ref)
     assert np.quantile(err, 0.999) < 1e-3 * (1 + np.abs(ref).max())
