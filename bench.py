@@ -44,6 +44,13 @@ WORKLOADS = {
     "c2": dict(desc="plain MOG k=240 g=16, two colliding exponential disks, N=1,048,576",
                n=1 << 20, k=240, g=16, L=100.0, G=100.0, dt=1e-5, damping=0.999, ic="disks",
                seed=1),
+    "c3": dict(desc="batched uneven ensemble: 8 simulations (N 65,536..2,097,152; (k,g) round-robin "
+                    "over (64,16),(128,16),(240,16),(64,32),(128,32)), Plummer spheres a=5, one CUDA "
+                    "graph per ensemble step",
+               sims=[(65536, 64, 16), (131072, 128, 16), (262144, 240, 16), (524288, 64, 32),
+                     (1048576, 128, 32), (1048576, 64, 16), (2097152, 128, 16),
+                     (2097152, 240, 16)],
+               L=100.0, G=100.0, dt=1e-5, damping=0.999, ic="plummer", seed=0),
     "c1": dict(desc="plain MOG k=16 g=16, uniform cube, N=65,536",
                n=1 << 16, k=16, g=16, L=100.0, G=100.0, dt=1e-5, damping=0.999, ic="uniform",
                seed=0),
@@ -52,6 +59,15 @@ WORKLOADS = {
 CLOCK_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+
+def step_bytes(n: int, k: int, g: int) -> int:
+    """B = 64 N + 16 N k + 20 k g^3 bytes per step."""
+    return 64 * n + 16 * n * k + 20 * k * g ** 3
+
+
+def launches_per_step(g: int) -> int:
+    return 3 if g <= 16 else 10   # deposit, solve (1 fused or 8 passes), update
 
 
 def phase_bytes(w: dict) -> dict:
@@ -332,6 +348,113 @@ def run_ours(args, w: dict) -> None:
         dist.destroy_process_group()
 
 
+def run_batch(args, w: dict) -> None:
+    import torch
+
+    from mog_solver_b200 import Simulation, ics
+    from mog_solver_b200.batch import Batch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    sims = []
+    for i, (n, k, g) in enumerate(w["sims"]):
+        s = Simulation({"n_grids": k, "grid_size": g, "world_size": w["L"], "num_particles": n,
+                        "G": w["G"], "dt": w["dt"], "damping": w["damping"], "seed": 100 + i},
+                       device=dev)
+        pos, vel = ics.plummer(n, w["L"], seed=w["seed"] + i + 1000 * rank)
+        s.set_particles(pos, vel)
+        sims.append(s)
+    if args.autotune:
+        from mog_solver_b200.autotune import autotune
+
+        for s in sims:
+            autotune(s, reps=2, cache=None)
+    torch.cuda.synchronize()
+    batch = Batch(sims)
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    n_tot = sum(s.n_particles for s in sims)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            batch.step(1)
+        stream.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        times = []
+        with ClockSampler(local) as clocks:
+            for _ in range(args.steps):
+                flush.zero_()
+                e0.record(stream)
+                batch.step(1)
+                e1.record(stream)
+                e1.synchronize()
+                times.append(e0.elapsed_time(e1))
+        # end to end: all particles copied from pinned host memory and back every step
+        hp = [torch.empty((s.n_particles, 4), dtype=torch.float32).pin_memory() for s in sims]
+        hv = [torch.empty((s.n_particles, 4), dtype=torch.float32).pin_memory() for s in sims]
+        for s, a, b in zip(sims, hp, hv):
+            a.copy_(s.pos)
+            b.copy_(s.vel)
+        torch.cuda.synchronize()
+        e2e = []
+        for _ in range(args.steps):
+            e0.record(stream)
+            for s, a, b in zip(sims, hp, hv):
+                s.pos.copy_(a, non_blocking=True)
+                s.vel.copy_(b, non_blocking=True)
+            batch.step(1)
+            for s, a, b in zip(sims, hp, hv):
+                a.copy_(s.pos, non_blocking=True)
+                b.copy_(s.vel, non_blocking=True)
+            e1.record(stream)
+            e1.synchronize()
+            e2e.append(e0.elapsed_time(e1))
+    tot = torch.tensor([sum(times), sum(e2e)], dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(tot, op=torch.distributed.ReduceOp.MAX)
+    total_ms, total_e2e = float(tot[0]), float(tot[1])
+    for s in sims:
+        s.check()
+    if rank == 0:
+        peaks = measured_peaks()
+        B = sum(step_bytes(n, k, g) for n, k, g in w["sims"])
+        ms = total_ms / args.steps
+        achieved = B / (ms / 1e3) / 1e9
+        line = {
+            "metric": METRIC, "value": n_tot * world * args.steps / (total_ms / 1e3), "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded Plummer spheres)",
+            "config": {"workload": w["desc"], "sims": w["sims"], "particles": n_tot,
+                       "parallelism": "single GPU" if world == 1 else f"{world} independent replicas",
+                       "l2": "flushed between timed steps (256 MiB write)",
+                       "autotuned": bool(args.autotune)},
+            "roofline": {"bound": "hbm", "kernel": "whole ensemble step", "achieved": achieved,
+                         "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                         "peak_source": peaks["source"], "algorithmic_bytes": B, "traffic": None},
+            "e2e": {"value": n_tot * world * args.steps / (total_e2e / 1e3), "unit": UNIT,
+                    "h2d_bytes_per_step": 32 * n_tot, "d2h_bytes_per_step": 32 * n_tot,
+                    "ms_per_step": total_e2e / args.steps},
+            "gpu_launches": sum(launches_per_step(g) for _, _, g in w["sims"]) * args.steps,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    batch.close()
+    for s in sims:
+        s.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -348,7 +471,13 @@ def main() -> None:
         args.warmup = 3
     w = WORKLOADS[args.workload]
     if args.impl == "reference":
+        if "sims" in w:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference runs one "
+                              "simulation per window; no batched path to time"}))
+            return
         run_reference(args, w)
+    elif "sims" in w:
+        run_batch(args, w)
     else:
         run_ours(args, w)
 

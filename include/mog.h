@@ -110,6 +110,8 @@ typedef struct mog_tuning {
     int32_t update_direct_ppt;      /* particles per thread of the L2-gather update: 1, 2, 4 */
     int32_t deposit_aggregate;      /* warp-merge runs of equal cells: -1 auto, 0 off, 1 on  */
     int32_t deposit_generic;        /* 1: never use the specialised g <= 16 deposit kernel    */
+    int32_t deposit_sorted;         /* 1: deposit from the spatially ordered copy too         */
+    int32_t update_threads;         /* staged gather block: 512, 768 or 1024                  */
 } mog_tuning;
 
 /* Fill a config with the reference's in-code defaults (main.py:179-189). */
@@ -239,9 +241,12 @@ int mog_batch_destroy(mog_batch* b);
  *   params: MOG_MODEL_PARAMS floats, W1[64][12] b1[64] W2[64][64] b2[64]
  *           W3[3][64] b3[3] (FP32 master copy; inference runs in BF16).
  *   norm:   MOG_MODEL_NORM floats, mu[12] inv_sigma[12] force_scale
- *           rho_ref out_scale pad — features are (f - mu) * inv_sigma with
- *           forces divided by force_scale and densities by rho_ref; the
- *           predicted residual is y * out_scale.
+ *           rho_ref out_scale base_mode — features are (f - mu) * inv_sigma
+ *           with forces divided by force_scale and densities by rho_ref;
+ *           the predicted residual is y * out_scale, added to the plain
+ *           ensemble mean (base_mode 0) or to the mean plus the per-particle
+ *           least-squares correction carried in feature slots 12-14
+ *           (base_mode 1).
  */
 #define MOG_MODEL_PARAMS 5187
 #define MOG_MODEL_NORM 28
@@ -265,11 +270,12 @@ int mog_model_train_step(mog_model* m, const float* feat16, const float* target4
 /*
  * Deposit + solve with the handle's ensemble, then per-particle features:
  * mean4_out (device n float4, the plain ensemble force) and feat16_out
- * (device n x 16 floats, standardised with m's norm).
+ * (device n x 16 floats: 0-11 standardised with m's norm, 12-14 the
+ * least-squares correction in force units, 15 zero).
  */
 int mog_features(mog_handle* h, const mog_model* m, const float* pos4, int64_t n,
                  float* mean4_out, float* feat16_out, void* stream);
-/* Corrected force (plain ensemble force + predicted residual) at every
+/* Corrected force (base force of m's base_mode + predicted residual) at every
  * particle, and one damped leapfrog step with it (update.glsl:83-89). */
 int mog_learned_forces(mog_handle* h, const mog_model* m, const float* pos4, float* acc4,
                        int64_t n, void* stream);

@@ -95,6 +95,8 @@ class MogTuningC(ctypes.Structure):
         ("update_direct_ppt", ctypes.c_int32),
         ("deposit_aggregate", ctypes.c_int32),
         ("deposit_generic", ctypes.c_int32),
+        ("deposit_sorted", ctypes.c_int32),
+        ("update_threads", ctypes.c_int32),
     ]
 
 

@@ -76,7 +76,9 @@ __device__ __forceinline__ float gelu_fast(float x) {
 //   9    log1p(rho / rho_ref) mean mass of the particle's cells
 //   10   |Fbar| / s
 //   11   sqrt(tr C_dd) / h   spread of the in-cell offsets
-// then standardised with the model's mu / sigma.
+// then standardised with the model's mu / sigma; slots 12-14 carry the
+// regression correction a - Fbar itself (world units, not standardised;
+// the first layer's weights for slots 12-15 are zero) and slot 15 is 0.
 template <typename Acc>
 __global__ void __launch_bounds__(256) features_kernel(const float4* __restrict__ pos, int64_t n,
                                                        const float4* __restrict__ W,
@@ -173,8 +175,10 @@ __global__ void __launch_bounds__(256) features_kernel(const float4* __restrict_
     float* o = feat_out + (size_t)p * 16;
 #pragma unroll
     for (int j = 0; j < kIn; ++j) o[j] = (f[j] - norm.mu[j]) * norm.inv_sigma[j];
-#pragma unroll
-    for (int j = kIn; j < 16; ++j) o[j] = 0.f;
+    o[12] = ex;
+    o[13] = ey;
+    o[14] = ez;
+    o[15] = 0.f;
 }
 
 // ---------------------------------------------------------------------------
@@ -223,13 +227,16 @@ __device__ __forceinline__ void mma_bf16(float (&d)[4], uint32_t a0, uint32_t a1
 }
 
 // Tensor-core inference.  Each warp owns 16 consecutive particles (one
-// m16 tile).  Output: acc[p] = mean[p] + out_scale * y  (the corrected
-// ensemble force), written for the update to apply.
+// m16 tile).  Output: acc[p] = base + out_scale * y  (the corrected
+// ensemble force), written for the update to apply; base is mean[p], or
+// mean[p] + the regression correction (feature slots 12-14) when
+// with_correction is set.
 __global__ void __launch_bounds__(128) mlp_infer_kernel(const float* __restrict__ feat, int64_t n,
                                                         const uint2* __restrict__ frags,
                                                         const float* __restrict__ params,
                                                         const float4* __restrict__ mean,
-                                                        float out_scale, float4* __restrict__ acc) {
+                                                        float out_scale, bool with_correction,
+                                                        float4* __restrict__ acc) {
     __shared__ uint2 sf[kFragTotal];
     __shared__ float sb[kH + kH + 8];
     for (int i = threadIdx.x; i < kFragTotal; i += blockDim.x) sf[i] = frags[i];
@@ -302,13 +309,23 @@ __global__ void __launch_bounds__(128) mlp_infer_kernel(const float* __restrict_
         const float o2a = __shfl_sync(kFull, y[0], (g << 2) | 1);
         const float o0b = __shfl_sync(kFull, y[2], (g << 2) | 0), o1b = __shfl_sync(kFull, y[3], (g << 2) | 0);
         const float o2b = __shfl_sync(kFull, y[2], (g << 2) | 1);
+        auto base = [&](int64_t r) {
+            float4 m = mean[r];
+            if (with_correction) {
+                const float4 c = *reinterpret_cast<const float4*>(feat + r * 16 + 12);
+                m.x += c.x;
+                m.y += c.y;
+                m.z += c.z;
+            }
+            return m;
+        };
         if (tg == 0) {
             if (r0 < n) {
-                const float4 m = mean[r0];
+                const float4 m = base(r0);
                 acc[r0] = make_float4(m.x + out_scale * o0a, m.y + out_scale * o1a, m.z + out_scale * o2a, 0.f);
             }
             if (r1 < n) {
-                const float4 m = mean[r1];
+                const float4 m = base(r1);
                 acc[r1] = make_float4(m.x + out_scale * o0b, m.y + out_scale * o1b, m.z + out_scale * o2b, 0.f);
             }
         }
@@ -478,12 +495,13 @@ cudaError_t launch_pack_fragments(const float* params, void* frags, cudaStream_t
 }
 
 cudaError_t launch_mlp_infer(const float* feat, int64_t n, const void* frags, const float* params,
-                             const float4* mean, float out_scale, float4* acc, cudaStream_t s) {
+                             const float4* mean, float out_scale, bool with_correction, float4* acc,
+                             cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
     const int64_t tiles = (n + 15) / 16;
     const int64_t blocks = std::min<int64_t>((tiles + 3) / 4, (int64_t)num_sms() * 16);
     mlp_infer_kernel<<<(unsigned)blocks, 128, 0, s>>>(feat, n, static_cast<const uint2*>(frags),
-                                                      params, mean, out_scale, acc);
+                                                      params, mean, out_scale, with_correction, acc);
     return cudaGetLastError();
 }
 

@@ -300,8 +300,13 @@ int run_pipeline(mog_handle* h, float4* pos, float4* vel, int64_t n, float dt, f
     const float4* pos_s = nullptr;
     int rc = order_particles(h, pos, n, sort, s, &perm, &pos_s);
     if (rc) return rc;
-    cudaError_t err = pos_s ? mog::launch_deposit(e, pos_s, nullptr, n, true, h->d_mass, h->dshape, s)
-                            : mog::launch_deposit(e, pos, nullptr, n, false, h->d_mass, h->dshape, s);
+    // The mass grid does not depend on the order; shared atomics from
+    // spatially ordered lanes collide on one address, so by default the
+    // deposit keeps the caller's order and only the gather uses the ordering.
+    const bool dep_sorted = pos_s && h->dshape.sorted_input;
+    cudaError_t err = dep_sorted
+                          ? mog::launch_deposit(e, pos_s, nullptr, n, true, h->d_mass, h->dshape, s)
+                          : mog::launch_deposit(e, pos, nullptr, n, false, h->d_mass, h->dshape, s);
     if (err != cudaSuccess) return cuda_fail(err, "deposit");
     if (h->cfg.solver == MOG_SOLVER_FFT)
         err = mog::launch_spectral(e, h->d_mass, h->d_force, true, true, h->d_scratch, s);
@@ -566,8 +571,9 @@ int mog_step_profiled(mog_handle* h, float* pos4, float* vel4, int64_t n, float 
     }
     if (!err) err = cudaEventRecord(ev[1], s);
     if (!err)
-        err = pos_s ? mog::launch_deposit(e, pos_s, nullptr, n, true, h->d_mass, h->dshape, s)
-                    : mog::launch_deposit(e, pos, nullptr, n, false, h->d_mass, h->dshape, s);
+        err = (pos_s && h->dshape.sorted_input)
+                  ? mog::launch_deposit(e, pos_s, nullptr, n, true, h->d_mass, h->dshape, s)
+                  : mog::launch_deposit(e, pos, nullptr, n, false, h->d_mass, h->dshape, s);
     if (!err) err = cudaEventRecord(ev[2], s);
     if (!err)
         err = h->cfg.solver == MOG_SOLVER_FFT
@@ -610,9 +616,10 @@ int mog_deposit(mog_handle* h, const float* pos4, int64_t n, void* mass_out, voi
                               &perm, &pos_s)))
         return rc;
     cudaError_t err =
-        pos_s ? mog::launch_deposit(h->e, pos_s, nullptr, n, true, mass_out, h->dshape, s)
-              : mog::launch_deposit(h->e, reinterpret_cast<const float4*>(pos4), nullptr, n, false,
-                                    mass_out, h->dshape, s);
+        (pos_s && h->dshape.sorted_input)
+            ? mog::launch_deposit(h->e, pos_s, nullptr, n, true, mass_out, h->dshape, s)
+            : mog::launch_deposit(h->e, reinterpret_cast<const float4*>(pos4), nullptr, n, false,
+                                  mass_out, h->dshape, s);
     if (err != cudaSuccess) return cuda_fail(err, "deposit");
     mog::check_total_kernel<<<1, 1, 0, s>>>(h->e);
     MOG_CUDA(cudaGetLastError(), "check total");
@@ -672,6 +679,8 @@ int mog_get_tuning(const mog_handle* h, mog_tuning* out) {
     out->sort_every = h->sort_every;
     out->deposit_aggregate = h->dshape.aggregate;
     out->deposit_generic = h->dshape.fast ? 0 : 1;
+    out->deposit_sorted = h->dshape.sorted_input;
+    out->update_threads = h->ushape.threads;
     out->update_direct_ppt = h->ushape.direct_ppt;
     return MOG_OK;
 }
@@ -685,6 +694,8 @@ int mog_set_tuning(mog_handle* h, const mog_tuning* t) {
         t->update_staged < -1 || t->update_staged > 1 ||
         (t->deposit_ppt != 0 && t->deposit_ppt != 1 && t->deposit_ppt != 2 && t->deposit_ppt != 4) ||
         t->sort_every < -1 || t->deposit_aggregate < -1 || t->deposit_aggregate > 1 ||
+        (t->update_threads != 0 && t->update_threads != 512 && t->update_threads != 768 &&
+         t->update_threads != 1024) ||
         (t->update_direct_ppt != 0 && t->update_direct_ppt != 1 && t->update_direct_ppt != 2 &&
          t->update_direct_ppt != 4))
         return fail(MOG_ERR_ARG, "tuning value out of range");
@@ -698,6 +709,8 @@ int mog_set_tuning(mog_handle* h, const mog_tuning* t) {
     h->sort_every = t->sort_every < 0 ? 0 : t->sort_every;
     h->dshape.aggregate = t->deposit_aggregate;
     h->dshape.fast = t->deposit_generic ? 0 : 1;
+    h->dshape.sorted_input = t->deposit_sorted ? 1 : 0;
+    h->ushape.threads = t->update_threads ? t->update_threads : 512;
     for (auto& g : h->graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);
     h->graphs.clear();
@@ -851,6 +864,7 @@ int mog_model_set(mog_model* m, const float* params, const float* norm) {
         if (!std::isfinite(norm[i])) return fail(MOG_ERR_ARG, "norm must be finite");
     if (!(norm[24] > 0.f) || !(norm[25] > 0.f))
         return fail(MOG_ERR_ARG, "force_scale and rho_ref must be positive");
+    if (norm[27] != 0.f && norm[27] != 1.f) return fail(MOG_ERR_ARG, "norm[27] (base mode) must be 0 or 1");
     const size_t pb = sizeof(float) * mog::mlp_param_count();
     MOG_CUDA(cudaMemcpy(m->d_params, params, pb, cudaMemcpyHostToDevice), "upload params");
     MOG_CUDA(cudaMemset(m->d_m, 0, pb), "reset adam");
@@ -935,7 +949,7 @@ int mog_learned_forces(mog_handle* h, const mog_model* m, const float* pos4, flo
     if ((rc = run_features(h, m, reinterpret_cast<const float4*>(pos4), n, h->d_mean, h->d_feat, s)))
         return rc;
     cudaError_t err = mog::launch_mlp_infer(h->d_feat, n, m->d_frags, m->d_params, h->d_mean,
-                                            m->norm.out_scale, reinterpret_cast<float4*>(acc4), s);
+                                            m->norm.out_scale, m->norm.base_mode != 0.f, reinterpret_cast<float4*>(acc4), s);
     if (err != cudaSuccess) return cuda_fail(err, "mlp inference");
     return MOG_OK;
 }
@@ -952,7 +966,7 @@ int mog_learned_step(mog_handle* h, const mog_model* m, float* pos4, float* vel4
     if ((rc = run_features(h, m, reinterpret_cast<const float4*>(pos4), n, h->d_mean, h->d_feat, s)))
         return rc;
     cudaError_t err = mog::launch_mlp_infer(h->d_feat, n, m->d_frags, m->d_params, h->d_mean,
-                                            m->norm.out_scale, h->d_acc, s);
+                                            m->norm.out_scale, m->norm.base_mode != 0.f, h->d_acc, s);
     if (err != cudaSuccess) return cuda_fail(err, "mlp inference");
     err = mog::launch_apply_force(reinterpret_cast<float4*>(pos4), reinterpret_cast<float4*>(vel4), n,
                                   h->d_acc, dt_eff, h->cfg.damping, h->e.world, h->d_flags, s);

@@ -51,9 +51,10 @@ struct DepositShape {
     int ppt = 4;            // particles per thread carried through the grid loop
     int aggregate = -1;     // warp-merge runs of equal cells: -1 auto (when ordered), 0, 1
     int fast = 1;           // use the specialised kernel where it applies
+    int sorted_input = 0;   // read the spatially ordered copy (else the caller's order)
 };
 struct UpdateShape {
-    int threads = 512;
+    int threads = 512;      // staged gather block size: 512, 768 or 1024
     int staged = -1;        // -1 auto, 0 global gathers, 1 smem-staged grids
     int ctas = 0;           // staged kernel CTAs; 0 = one per SM
     int direct_ppt = 4;     // particles per thread of the direct gather
@@ -127,7 +128,7 @@ struct ModelNorm {
     float force_scale;   // s: forces enter the features as F / s
     float rho_ref;       // mean cell mass (total mass / g^3)
     float out_scale;     // residual = y * out_scale
-    float pad;
+    float base_mode;     // 0: residual to the plain mean; 1: to mean + regression correction
 };
 
 
@@ -139,7 +140,8 @@ cudaError_t launch_features(const Ensemble& e, const float4* pos, int64_t n, con
                             cudaStream_t s);
 cudaError_t launch_pack_fragments(const float* params, void* frags, cudaStream_t s);
 cudaError_t launch_mlp_infer(const float* feat, int64_t n, const void* frags, const float* params,
-                             const float4* mean, float out_scale, float4* acc, cudaStream_t s);
+                             const float4* mean, float out_scale, bool with_correction, float4* acc,
+                             cudaStream_t s);
 cudaError_t launch_mlp_train_step(const float* feat, const float* target, const int* idx,
                                   int batch, float* params, float* partial, float* loss_partial,
                                   float* grad, float* m, float* v, float lr, int t,

@@ -171,8 +171,8 @@ __device__ __forceinline__ void issue_grid(int i, int s, const float4* __restric
 // ordering they fall in the same few cells and their shared-memory loads
 // broadcast instead of conflicting, and the CTA's particles occupy a small
 // box, so only the z-slabs of each grid that the box reaches are staged.
-template <int IDX, int PPT, bool ACC_OUT>
-__global__ void __launch_bounds__(512, 1)
+template <int IDX, int PPT, bool ACC_OUT, int THREADS>
+__global__ void __launch_bounds__(THREADS, 1)
     update_staged_kernel(float4* __restrict__ pos, float4* __restrict__ vel,
                          const float4* __restrict__ pos_s, const int* __restrict__ perm,
                          int64_t n, int64_t per_cta, const float4* __restrict__ W, Ensemble e,
@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(512, 1)
     float* xf = reinterpret_cast<float*>(full + 8);
     __shared__ int abort_flag;
     __shared__ float box[6];        // min c.xyz, max c.xyz of the CTA's particles
-    __shared__ float wbox[16][6];   // per-warp partial boxes
+    __shared__ float wbox[THREADS / 32][6];   // per-warp partial boxes
 
     const int tid = threadIdx.x;
     const int T = blockDim.x;
@@ -376,12 +376,13 @@ __global__ void __launch_bounds__(256) update_direct_kernel(float4* __restrict__
     if (bad) raise_flags(e.flags, bad);
 }
 
-template <int IDX, int PPT, bool ACC>
+template <int IDX, int PPT, bool ACC, int THREADS>
 cudaError_t launch_staged(const Ensemble& e, float4* pos, float4* vel, const float4* pos_s,
                           const int* perm, int64_t n, const float4* W, float dt, float damp,
-                          float4* acc, int ctas, int threads, int nstage, size_t smem,
-                          int sparse, cudaStream_t s) {
-    auto kern = update_staged_kernel<IDX, PPT, ACC>;
+                          float4* acc, int ctas, int nstage, size_t smem, int sparse,
+                          cudaStream_t s) {
+    auto kern = update_staged_kernel<IDX, PPT, ACC, THREADS>;
+    const int threads = THREADS;
     cudaError_t err =
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess) return err;
@@ -398,7 +399,7 @@ cudaError_t update_mode(const Ensemble& e, float4* pos, float4* vel, const float
     if (n <= 0) return cudaSuccess;
     const size_t grid_bytes = (size_t)16 << (3 * e.lg);
     const int sms = num_sms();
-    const int threads = 512;
+    const int threads = 512;  // minimum staged launch, for the auto choice below
     const int nstage = 3;
     const size_t smem = nstage * grid_bytes + 8 * sizeof(uint64_t) + (size_t)e.k * 16 * sizeof(float);
     bool staged;
@@ -424,25 +425,31 @@ cudaError_t update_mode(const Ensemble& e, float4* pos, float4* vel, const float
     }
     // Sparse staging only pays when the CTAs' particles are spatially compact.
     const int sparse = (pos_s || perm) ? 1 : 0;
-    // Enough CTAs that the particles per thread stay within the template.
+    // Block size (occupancy) against particles per thread (registers): the
+    // launch bounds give 512 threads ~128 registers, 768 ~85, 1024 64.
+    const int T = sh.threads == 768 || sh.threads == 1024 ? sh.threads : 512;
+    const int max_ppt = T == 512 ? 16 : (T == 768 ? 10 : 7);
     int ctas = sh.ctas > 0 ? sh.ctas : sms;
-    const int64_t per_thread = (n + (int64_t)ctas * threads - 1) / ((int64_t)ctas * threads);
-    if (per_thread > 16) ctas = (int)((n + 16LL * threads - 1) / (16LL * threads));
-    const int64_t ppt = (n + (int64_t)ctas * threads - 1) / ((int64_t)ctas * threads);
-    if (ppt <= 4)
-        return launch_staged<IDX, 4, ACC>(e, pos, vel, pos_s, perm, n, W, dt, damp, acc, ctas,
-                                              threads, nstage, smem, sparse, s);
-    if (ppt <= 8)
-        return launch_staged<IDX, 8, ACC>(e, pos, vel, pos_s, perm, n, W, dt, damp, acc, ctas,
-                                              threads, nstage, smem, sparse, s);
-    if (ppt <= 12)
-        return launch_staged<IDX, 12, ACC>(e, pos, vel, pos_s, perm, n, W, dt, damp, acc, ctas,
-                                              threads, nstage, smem, sparse, s);
-    if (ppt <= 14)
-        return launch_staged<IDX, 14, ACC>(e, pos, vel, pos_s, perm, n, W, dt, damp, acc, ctas,
-                                              threads, nstage, smem, sparse, s);
-    return launch_staged<IDX, 16, ACC>(e, pos, vel, pos_s, perm, n, W, dt, damp, acc, ctas,
-                                              threads, nstage, smem, sparse, s);
+    const int64_t per_thread = (n + (int64_t)ctas * T - 1) / ((int64_t)ctas * T);
+    if (per_thread > max_ppt) ctas = (int)((n + (int64_t)max_ppt * T - 1) / ((int64_t)max_ppt * T));
+    const int64_t ppt = (n + (int64_t)ctas * T - 1) / ((int64_t)ctas * T);
+#define MOG_STAGED(P, TH) \
+    return launch_staged<IDX, P, ACC, TH>(e, pos, vel, pos_s, perm, n, W, dt, damp, acc, ctas, nstage, smem, sparse, s)
+    if (T == 1024) {
+        if (ppt <= 4) MOG_STAGED(4, 1024);
+        MOG_STAGED(7, 1024);
+    }
+    if (T == 768) {
+        if (ppt <= 4) MOG_STAGED(4, 768);
+        if (ppt <= 8) MOG_STAGED(8, 768);
+        MOG_STAGED(10, 768);
+    }
+    if (ppt <= 4) MOG_STAGED(4, 512);
+    if (ppt <= 8) MOG_STAGED(8, 512);
+    if (ppt <= 12) MOG_STAGED(12, 512);
+    if (ppt <= 14) MOG_STAGED(14, 512);
+    MOG_STAGED(16, 512);
+#undef MOG_STAGED
 }
 
 }  // namespace

@@ -9,7 +9,8 @@ statistics of the cheap ensemble.  Everything runs in libmog.so:
 * ``mog_learned_step``   features + BF16 tensor-core inference + leapfrog.
 
 ``generate_dataset`` builds training pairs from the method itself (features
-of a k = 32 ensemble, targets = k = 240 force minus the k = 32 mean);
+of a k = 32 ensemble, targets = k = 240 force minus the k = 32 mean and
+its per-particle least-squares correction);
 ``train`` fits the model; ``LearnedSimulation`` steps with the corrected
 force and falls back to the plain expensive ensemble when a variance gate
 fires (the particles' grid-to-grid force spread is far outside what the
@@ -39,13 +40,18 @@ def _torch():
     return torch
 
 
-def norm_vector(mu, inv_sigma, force_scale: float, rho_ref: float, out_scale: float) -> np.ndarray:
+def norm_vector(mu, inv_sigma, force_scale: float, rho_ref: float, out_scale: float,
+                base_mode: int = 0) -> np.ndarray:
+    """The model's normalisation (MOG_MODEL_NORM floats).  base_mode 0: the
+    residual is added to the plain mean force; 1: to the mean plus the
+    least-squares correction (feature slots 12-14)."""
     v = np.zeros(_lib.MODEL_NORM, dtype=np.float32)
     v[0:12] = mu
     v[12:24] = inv_sigma
     v[24] = force_scale
     v[25] = rho_ref
     v[26] = out_scale
+    v[27] = float(base_mode)
     return v
 
 
@@ -122,7 +128,9 @@ class Model:
 
 
 def features(sim: Simulation, model: Model, pos=None):
-    """(mean force (n, 4), standardised features (n, 16)) of sim's ensemble."""
+    """(mean force (n, 4), features (n, 16)) of sim's ensemble: columns 0-11
+    standardised with model's norm, 12-14 the least-squares correction in
+    force units, 15 zero."""
     torch = _torch()
     p = sim.pos if pos is None else pos
     n = int(p.shape[0])
@@ -165,7 +173,8 @@ def generate_dataset(n_sets: int = 64, n: int = 262144, k_small: int = 32, k_big
                      small_seed: int = 1000, big_seed: int = 2000) -> Dataset:
     """Training pairs the method generates itself: for seeded clump sets,
     features of the k_small ensemble and the k_big force minus the k_small
-    mean.  Returns standardised tensors and the matching normalisation."""
+    base force (mean + least-squares correction, base_mode 1).  Returns
+    standardised tensors and the matching normalisation."""
     from . import ics
 
     torch = _torch()
@@ -181,7 +190,7 @@ def generate_dataset(n_sets: int = 64, n: int = 262144, k_small: int = 32, k_big
         mean, f = features(small, raw)
         fb = big.forces()
         feats.append(f[:, :12].clone())
-        resid.append((fb - mean)[:, :3].clone())
+        resid.append((fb[:, :3] - mean[:, :3] - f[:, 12:15]).clone())
     raw.close()
     small.close()
     big.close()
@@ -198,7 +207,7 @@ def generate_dataset(n_sets: int = 64, n: int = 262144, k_small: int = 32, k_big
     T[:, :3] = (R / out_scale).float()
     feat16 = torch.zeros((Fz.shape[0], 16), dtype=torch.float32, device=Fz.device)
     feat16[:, :12] = Fz
-    norm = norm_vector(mu.cpu().numpy(), (1.0 / sd).cpu().numpy(), s, rho_ref, out_scale)
+    norm = norm_vector(mu.cpu().numpy(), (1.0 / sd).cpu().numpy(), s, rho_ref, out_scale, base_mode=1)
     stats = {"force_scale": s, "out_scale": out_scale, "samples": int(Fz.shape[0]),
              "spread_mean": float(F[:, SPREAD_COLS].double().mean().item())}
     return Dataset(feat16, T, norm, stats)

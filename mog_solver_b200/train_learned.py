@@ -49,14 +49,10 @@ def evaluate(model, n: int = 1 << 20, k_small: int = 32, k_big: int = 240, g: in
     f_big = big.forces()
     f_small = small.forces()
     f_learn = learned_forces(small, model)
-    # the least-squares correction alone (feature block 3-5), without the network
-    from .learned import Model, features, norm_vector
-
-    raw = Model(norm=norm_vector(np.zeros(12), np.ones(12), 1.0, 1.0 / g ** 3, 1.0))
-    mean, feat = features(small, raw)
+    # the least-squares correction alone (feature slots 12-14), without the network
+    mean, feat = features(small, model)
     f_reg = mean.clone()
-    f_reg[:, :3] += feat[:, 3:6]
-    raw.close()
+    f_reg[:, :3] += feat[:, 12:15]
     report = {"n": n, "k_small": k_small, "k_big": k_big, "g": g, "targets": targets}
     for soft_name, soft in (("0", 0.0), ("h/4", h / 4), ("h/2", h / 2)):
         D = direct_sum(T, P, world, big.effective_g(), soft)

@@ -80,7 +80,8 @@ def loss_and_grad(params, x, t):
 
 
 def features(cells, fgrid_world, mass_values, t, rot12, h, norm):
-    """Per-particle features (n, 12) and plain mean force (n, 3), FP64.
+    """Per-particle features (n, 12), plain mean force (n, 3) and the
+    least-squares correction (n, 3), FP64.
 
     cells: (n, k) cell indices; fgrid_world: (k, g^3, 3) world-frame forces;
     mass_values: (k, g^3) cell masses; t: (n, k, 3) scaled grid coordinates
@@ -111,4 +112,4 @@ def features(cells, fgrid_world, mass_values, t, rot12, h, norm):
     f[:, 9] = np.log1p(rho / norm["rho_ref"])
     f[:, 10] = np.linalg.norm(mean, axis=1) / s
     f[:, 11] = np.sqrt(np.maximum(np.trace(Cdd, axis1=1, axis2=2) - 3 * ridge, 0.0)) / h
-    return (f - norm["mu"]) * norm["inv_sigma"], mean
+    return (f - norm["mu"]) * norm["inv_sigma"], mean, corr

@@ -60,9 +60,10 @@ SHAPES = [(1, 1, 8), (7, 3, 16), (257, 16, 16), (65536, 16, 16), (5000, 5, 32), 
 
 # launch shapes that take different code paths; none may change a bit
 DEPOSIT_TUNINGS = {
-    "sorted+merged": dict(sort_every=1, deposit_aggregate=-1),
+    "sorted+merged": dict(sort_every=1, deposit_aggregate=-1, deposit_sorted=1),
     "unsorted": dict(sort_every=0, deposit_aggregate=0),
-    "sorted+plain": dict(sort_every=1, deposit_aggregate=0, deposit_ppt=1),
+    "sorted+plain": dict(sort_every=1, deposit_aggregate=0, deposit_ppt=1, deposit_sorted=1),
+    "sorted-update-only": dict(sort_every=1),
     "unsorted+merged": dict(sort_every=0, deposit_aggregate=1, deposit_ppt=2),
     "global": dict(sort_every=0, deposit_grids_per_cta=-1),
     "generic": dict(sort_every=0, deposit_generic=1),
@@ -125,6 +126,8 @@ UPDATE_TUNINGS = {
     "unsorted": dict(sort_every=0),
     "direct4": dict(update_staged=0, update_direct_ppt=4),
     "direct1-unsorted": dict(update_staged=0, update_direct_ppt=1, sort_every=0),
+    "staged768": dict(update_staged=1, update_threads=768, sort_every=0),
+    "staged1024-sorted": dict(update_staged=1, update_threads=1024, sort_every=1),
 }
 
 

@@ -12,11 +12,11 @@ torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
 
 
-def _model(seed=0):
+def _model(seed=0, base_mode=0):
     from mog_solver_b200.learned import Model, norm_vector
 
     p = (mlp.init(seed) + np.random.default_rng(seed).normal(0, 0.05, mlp.N_PARAMS)).astype(np.float32)
-    return Model(p, norm_vector(np.zeros(12), np.ones(12), 1.0, 1.0, 1.0)), p
+    return Model(p, norm_vector(np.zeros(12), np.ones(12), 1.0, 1.0, 1.0, base_mode)), p
 
 
 def _batch(n, seed=0):
@@ -63,12 +63,13 @@ def test_adam_step_matches_fp64():
     m.close()
 
 
-def test_bf16_inference_matches_fp64_forward():
+@pytest.mark.parametrize("base_mode", [0, 1])
+def test_bf16_inference_matches_fp64_forward(base_mode):
     from mog_solver_b200 import Simulation
     from mog_solver_b200.learned import features, learned_forces
 
     n, k, g, L = 5000, 8, 16, 100.0
-    m, p = _model(4)
+    m, p = _model(4, base_mode)
     sim = Simulation({"n_grids": k, "grid_size": g, "world_size": L, "num_particles": n, "G": 100.0,
                       "dt": 1e-5, "seed": 3})
     rng = np.random.default_rng(4)
@@ -79,11 +80,14 @@ def test_bf16_inference_matches_fp64_forward():
     mean, feat = features(sim, m)
     acc = learned_forces(sim, m)
     y, _ = mlp.forward(p.astype(np.float64), feat.cpu().numpy()[:, :12].astype(np.float64))
-    ref = mean.cpu().numpy()[:, :3].astype(np.float64) + y
+    base = mean.cpu().numpy()[:, :3].astype(np.float64)
+    if base_mode:
+        base = base + feat.cpu().numpy()[:, 12:15].astype(np.float64)
+    ref = base + y
     got = acc.cpu().numpy()[:, :3].astype(np.float64)
     # BF16 weights and activations: a few parts in 1e3 of the output scale
     assert np.abs(got - ref).max() <= 2e-2 * max(1.0, np.abs(y).max())
-    assert pl.relative_l2(got - mean.cpu().numpy()[:, :3], y) < 2e-2
+    assert pl.relative_l2(got - base, y) < 2e-2
     sim.close()
     m.close()
 
@@ -115,12 +119,15 @@ def test_features_match_fp64_oracle():
     rows = oracle.fast_rows(sim.rotations, sim.offsets, L, g).astype(np.float64).reshape(k, 3, 4)
     c = pos[:, :3].astype(np.float64) - L / 2
     t = np.einsum("krj,nj->nkr", rows[:, :, :3], c) + rows[:, :, 3][None]
-    ref, ref_mean = mlp.features(cells, Fw, mass.reshape(k, -1), t, sim.rotations, L / g,
-                                 {"force_scale": fs, "rho_ref": rho_ref, "mu": mu, "inv_sigma": isd})
+    ref, ref_mean, ref_corr = mlp.features(cells, Fw, mass.reshape(k, -1), t, sim.rotations, L / g,
+                                           {"force_scale": fs, "rho_ref": rho_ref, "mu": mu,
+                                            "inv_sigma": isd})
     got = feat.cpu().numpy()[:, :12].astype(np.float64)
     err = np.abs(got - ref)
     assert np.quantile(err, 0.999) < 1e-3 * (1 + np.abs(ref).max())
-    assert np.abs(feat.cpu().numpy()[:, 12:]).max() == 0
+    corr = feat.cpu().numpy()[:, 12:15].astype(np.float64)
+    assert np.quantile(np.abs(corr - ref_corr), 0.999) < 1e-3 * fs * (1 + np.abs(ref_corr / fs).max())
+    assert np.abs(feat.cpu().numpy()[:, 15]).max() == 0
     sim.close()
     m.close()
 
