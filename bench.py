@@ -62,7 +62,7 @@ CLOCK_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.a
 
 
 def step_bytes(n: int, k: int, g: int) -> int:
-    """B = 64 N + 16 N k + 20 k g^3 bytes per step."""
+    """Algorithmic bytes of one plain step: B = 64 N + 16 N k + 20 k g^3."""
     return 64 * n + 16 * n * k + 20 * k * g ** 3
 
 

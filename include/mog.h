@@ -217,7 +217,7 @@ int mog_direct_sum(const float* targets4, int64_t nt, const float* sources4, int
                    double world, double g_eff, double soft, double* out3, void* stream);
 
 /*
- * Batched independent simulations (BASELINE config "batched uneven
+ * Batched independent simulations (the "batched uneven
  * ensemble"; no counterpart in the reference, which runs one simulation per
  * window).  A batch groups `count` handles on one device.  mog_batch_step
  * advances every simulation n_steps steps; each ensemble step is ONE CUDA

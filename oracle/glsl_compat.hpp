@@ -1,5 +1,5 @@
 // glsl_compat.hpp — enough of GLSL 4.60 compute for the reference's
-// hot-path shaders to compile as C++ and run on the CPU.  TEST / BASELINE
+// hot-path shaders to compile as C++ and run on the CPU.  TEST AND CPU-BASELINE
 // INFRASTRUCTURE ONLY (oracle/_ref is the checker and the timed reference
 // arm, never the product).
 //

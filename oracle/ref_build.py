@@ -1,6 +1,6 @@
 """Build oracle/_ref: the reference's own GLSL compute shaders compiled as C++.
 
-TEST / BASELINE INFRASTRUCTURE ONLY.  Reads the seven hot-path shaders
+TEST AND CPU-BASELINE INFRASTRUCTURE ONLY.  Reads the seven hot-path shaders
 (shaders/{mass,complex,fft_batched,fourier,greens,pack,update}.glsl) from a
 reference checkout (default /root/reference, or $MOG_REFERENCE), rewrites
 their GLSL-only declarations with a handful of regular expressions (SSBO

@@ -2,7 +2,7 @@
 // to C++ by ref_build.py into _ref/gen/*.inc) on the CPU, dispatch by
 // dispatch, exactly in the order and with the bindings and uniforms of
 // Simulation.step_fft (main.py:592-669) and run_fft_3d_batched
-// (main.py:564-590), including its texture ping-pong.  TEST / BASELINE
+// (main.py:564-590), including its texture ping-pong.  TEST AND CPU-BASELINE
 // INFRASTRUCTURE ONLY.  Invocations of one dispatch run in parallel with
 // OpenMP (they are independent except for the atomics of mass.glsl); each
 // dispatch completes before the next starts (the memory_barrier calls).

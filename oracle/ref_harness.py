@@ -1,4 +1,4 @@
-"""ctypes wrapper of oracle/_ref/libmogref.so — TEST / BASELINE INFRASTRUCTURE ONLY.
+"""ctypes wrapper of oracle/_ref/libmogref.so — TEST AND CPU-BASELINE INFRASTRUCTURE ONLY.
 
 The library runs the reference's own compute shaders (compiled as C++ by
 ref_build.py) with the dispatch order, bindings and texture ping-pong of
