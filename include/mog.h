@@ -217,6 +217,32 @@ int mog_direct_sum(const float* targets4, int64_t nt, const float* sources4, int
                    double world, double g_eff, double soft, double* out3, void* stream);
 
 /*
+ * mog_direct_sum without any device allocation.  No counterpart in the
+ * reference.  mog_direct_sum takes its partial sums from a stream-ordered
+ * allocation, which some callers cannot make: a process whose device memory
+ * is already held by its own caching allocator (a framework that has grown
+ * its pool to fill the GPU), or a device or driver without stream-ordered
+ * memory pools.  This entry point writes the partial sums into a fixed
+ * 12 MiB scratch that is part of the library image on each device instead,
+ * and returns the same result as mog_direct_sum bit for bit (same source
+ * chunking, same summation order).
+ *
+ * Limit: nt * chunks <= 524288, chunks = min(32, ceil(ns / 8192)) (at least
+ * 1); so at most 16384 targets once ns > 253952.  Larger requests return
+ * MOG_ERR_ARG with the limit in mog_last_error() and launch nothing.
+ * The first call on each device does a one-time set-up (it looks up the
+ * scratch's device address); make that first call before any stream
+ * capture begins.  Nothing in the scratch needs to start at zero: every
+ * partial sum a call reads was written earlier in the same call.  All
+ * calls on one device share the one scratch, so calls that overlap in time
+ * (other streams, other threads) race with one another and must be
+ * serialised by the caller.
+ */
+int mog_direct_sum_noalloc(const float* targets4, int64_t nt, const float* sources4,
+                           int64_t ns, double world, double g_eff, double soft, double* out3,
+                           void* stream);
+
+/*
  * Batched independent simulations (the "batched uneven
  * ensemble"; no counterpart in the reference, which runs one simulation per
  * window).  A batch groups `count` handles on one device.  mog_batch_step

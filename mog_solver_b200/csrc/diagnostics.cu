@@ -12,6 +12,8 @@
 // subtracts it).  Sources are tiled through shared memory in FP64; each
 // target accumulates the sources of one chunk, and the chunks' partial sums
 // are added in a fixed order, so the result is deterministic.
+#include <mutex>
+
 #include "mog_internal.h"
 
 namespace mog {
@@ -80,7 +82,33 @@ __global__ void direct_reduce_kernel(const double* __restrict__ partial, int64_t
     out3[i] = s;
 }
 
+// Fixed scratch of mog_direct_sum_noalloc: the per-chunk partial sums of up
+// to kDirectScratchPairs (target, chunk) pairs, 3 doubles each (12 MiB).
+// One copy exists on every device the library runs on.
+__device__ __align__(256) static double g_direct_scratch[3 * kDirectScratchPairs];
+
 }  // namespace
+
+// Device address of g_direct_scratch on the current device, looked up once
+// per device (cudaGetSymbolAddress, with that device current) and cached.
+cudaError_t direct_sum_scratch(double** out) {
+    constexpr int kMaxDevices = 64;
+    static std::mutex mu;
+    static double* addr[kMaxDevices] = {};
+    int dev = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err != cudaSuccess) return err;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void* p = nullptr;
+        err = cudaGetSymbolAddress(&p, g_direct_scratch);
+        if (err != cudaSuccess) return err;
+        addr[dev] = static_cast<double*>(p);
+    }
+    *out = addr[dev];
+    return cudaSuccess;
+}
 
 cudaError_t launch_direct_sum(const float4* targets, int64_t nt, const float4* sources, int64_t ns,
                               double world, double g_eff, double soft, double* partial, int chunks,

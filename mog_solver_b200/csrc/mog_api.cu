@@ -766,6 +766,32 @@ int mog_direct_sum(const float* targets4, int64_t nt, const float* sources4, int
     return MOG_OK;
 }
 
+int mog_direct_sum_noalloc(const float* targets4, int64_t nt, const float* sources4, int64_t ns,
+                           double world, double g_eff, double soft, double* out3, void* stream) {
+    if (nt < 0 || ns < 0) return fail(MOG_ERR_ARG, "negative size");
+    if ((nt && (!targets4 || !out3)) || (ns && !sources4)) return fail(MOG_ERR_ARG, "null buffer");
+    if (!(world > 0.0) || !std::isfinite(g_eff) || !(soft >= 0.0))
+        return fail(MOG_ERR_ARG, "world must be positive, g_eff finite, soft >= 0");
+    if (nt == 0) return MOG_OK;
+    // same source chunking as mog_direct_sum, so the two agree bit for bit
+    const int chunks = (int)std::max<int64_t>(1, std::min<int64_t>(32, (ns + 8191) / 8192));
+    if (nt > mog::kDirectScratchPairs / chunks)
+        return fail(MOG_ERR_ARG, "mog_direct_sum_noalloc: " + std::to_string(nt) + " targets x " +
+                                     std::to_string(chunks) + " source chunks exceeds the fixed scratch of " +
+                                     std::to_string(mog::kDirectScratchPairs) +
+                                     " target-chunk pairs (at most " +
+                                     std::to_string(mog::kDirectScratchPairs / chunks) +
+                                     " targets for this source count)");
+    double* partial = nullptr;
+    cudaError_t err = mog::direct_sum_scratch(&partial);
+    if (err != cudaSuccess) return cuda_fail(err, "direct-sum scratch address");
+    err = mog::launch_direct_sum(reinterpret_cast<const float4*>(targets4), nt,
+                                 reinterpret_cast<const float4*>(sources4), ns, world, g_eff, soft,
+                                 partial, chunks, out3, static_cast<cudaStream_t>(stream));
+    if (err != cudaSuccess) return cuda_fail(err, "direct sum");
+    return MOG_OK;
+}
+
 const char* mog_strerror(int code) {
     switch (code) {
         case MOG_OK: return "ok";

@@ -118,6 +118,10 @@ cudaError_t launch_diagnostics(const float4* pos, const float4* vel, int64_t n, 
 cudaError_t launch_direct_sum(const float4* targets, int64_t nt, const float4* sources, int64_t ns,
                               double world, double g_eff, double soft, double* partial, int chunks,
                               double* out3, cudaStream_t s);
+// Scratch of the allocation-free direct sum (diagnostics.cu): room for
+// kDirectScratchPairs (target, chunk) partial sums of 3 doubles.
+constexpr int64_t kDirectScratchPairs = int64_t(1) << 19;
+cudaError_t direct_sum_scratch(double** out);
 
 // ---- learned correction (learned.cu) ------------------------------------
 constexpr int kModelIn = 12;
