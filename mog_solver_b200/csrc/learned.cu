@@ -3,17 +3,24 @@
 // No counterpart in the reference: its force is always the plain average
 // over k grids (update.glsl:67-81).  Here a small network (12 -> 64 -> 64 -> 3,
 // GELU) predicts, from statistics of a cheap ensemble (k = 32), the residual
-// to an expensive one (k = 240):
+// to an expensive one (k = 240).
 //
-//   features  per particle, from the k grids it touches: the mean world
-//             force, a least-squares correction of it from the particle's
-//             offsets to its cells' centres, the per-grid force spread, the
-//             mean cell mass and two scalars (see features_kernel);
-//             standardised with the model's statistics;
-//   inference BF16 tensor-core MLP (mma.sync m16n8k16, FP32 accumulate).
-//             A warp carries 16 particles through all three layers in
-//             registers: the accumulator fragment of one layer is, pair of
-//             n-tiles by pair, exactly the A fragment of the next;
+// One fused kernel (learned_kernel) does, per particle:
+//   gather    the k world-frame grid forces and cell masses it touches (L2),
+//             accumulating the statistics of the features: the mean force,
+//             a least-squares correction of it from the particle's offsets
+//             to its cells' centres, the per-grid force spread, the mean
+//             cell mass and two scalars (see gather_features);
+//   inference the standardised features through the network on the tensor
+//             cores (mma.sync m16n8k16 BF16, FP32 accumulate): a warp's 32
+//             particles are two m16 tiles; the accumulator fragment of one
+//             layer is, pair of n-tiles by pair, exactly the A fragment of
+//             the next;
+//   update    force = base + out_scale * y, then update.glsl:83-89.
+// so nothing per particle but its position and velocity touches HBM.
+// The same kernel also writes the features only (mog_features) or the
+// corrected force only (mog_learned_forces).
+//
 //   training  FP32 fused forward + backward over a minibatch, one CTA per
 //             128 samples, per-CTA partial gradients reduced in a fixed
 //             order (deterministic), then Adam.
@@ -56,129 +63,6 @@ __device__ __forceinline__ float tanh_fast(float x) {
 __device__ __forceinline__ float gelu_fast(float x) {
     const float u = 0.7978845608028654f * (x + 0.044715f * x * x * x);
     return 0.5f * x * (1.0f + tanh_fast(u));
-}
-
-// ---------------------------------------------------------------------------
-// Feature gather.  One thread per particle; grids read from L2.
-//
-// Each grid samples the force at the centre of the particle's cell, not at
-// the particle, so the k per-grid forces F_i scatter around the force at
-// the particle roughly linearly in the particle's offset from those cell
-// centres, d_i (world frame).  A per-particle least-squares fit
-// F_i ~ a + B d_i over the k grids gives an intercept a, the force
-// extrapolated to the particle itself:
-//     a = Fbar - C_Fd (C_dd + ridge)^-1 dbar
-// with dbar, C_dd = cov(d, d) and C_Fd = cov(F, d) over the grids.
-// The features are
-//   0-2  Fbar / s            plain ensemble mean (update.glsl order)
-//   3-5  (a - Fbar) / s      regression correction from the in-cell offsets
-//   6-8  std_i(F_i) / s      per-component spread of the per-grid forces
-//   9    log1p(rho / rho_ref) mean mass of the particle's cells
-//   10   |Fbar| / s
-//   11   sqrt(tr C_dd) / h   spread of the in-cell offsets
-// then standardised with the model's mu / sigma; slots 12-14 carry the
-// regression correction a - Fbar itself (world units, not standardised;
-// the first layer's weights for slots 12-15 are zero) and slot 15 is 0.
-template <typename Acc>
-__global__ void __launch_bounds__(256) features_kernel(const float4* __restrict__ pos, int64_t n,
-                                                       const float4* __restrict__ W,
-                                                       const Acc* __restrict__ mass, Ensemble e,
-                                                       ModelNorm norm, float4* __restrict__ mean_out,
-                                                       float* __restrict__ feat_out) {
-    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
-    const IndexParams ip = e.index_params();
-    const float4 P = pos[p];
-    const float cx = __fsub_rn(P.x, ip.half_l), cy = __fsub_rn(P.y, ip.half_l),
-                cz = __fsub_rn(P.z, ip.half_l);
-    const int G3 = 1 << (3 * e.lg);
-    const uint32_t mask = (1u << e.lg) - 1u;
-    const float h = e.voxel;
-    float sx = 0.f, sy = 0.f, sz = 0.f;            // plain sum, update.glsl order
-    float qx = 0.f, qy = 0.f, qz = 0.f;            // sum F^2 per component
-    float dx = 0.f, dy = 0.f, dz = 0.f;            // sum d
-    float dxx = 0.f, dxy = 0.f, dxz = 0.f, dyy = 0.f, dyz = 0.f, dzz = 0.f;
-    float fxdx = 0.f, fxdy = 0.f, fxdz = 0.f, fydx = 0.f, fydy = 0.f, fydz = 0.f,
-          fzdx = 0.f, fzdy = 0.f, fzdz = 0.f;      // sum F d^T
-    float rho = 0.f;
-    for (int i = 0; i < e.k; ++i) {
-        const FastXf x = e.fast[i];
-        const float tx = __fmaf_rn(x.row[0].z, cz, __fmaf_rn(x.row[0].y, cy, __fmaf_rn(x.row[0].x, cx, x.row[0].w)));
-        const float ty = __fmaf_rn(x.row[1].z, cz, __fmaf_rn(x.row[1].y, cy, __fmaf_rn(x.row[1].x, cx, x.row[1].w)));
-        const float tz = __fmaf_rn(x.row[2].z, cz, __fmaf_rn(x.row[2].y, cy, __fmaf_rn(x.row[2].x, cx, x.row[2].w)));
-        uint32_t c;
-        if (e.index_mode == 0)
-            c = floor_mod_pow2(tx, mask) | (floor_mod_pow2(ty, mask) << e.lg) |
-                (floor_mod_pow2(tz, mask) << (2 * e.lg));
-        else
-            c = cell_exact(e.rot12 + 12 * i, e.off4 + 4 * i, cx, cy, cz, ip);
-        const float4 f = __ldg(W + (size_t)i * G3 + c);
-        sx = __fadd_rn(sx, f.x);
-        sy = __fadd_rn(sy, f.y);
-        sz = __fadd_rn(sz, f.z);
-        qx += f.x * f.x;
-        qy += f.y * f.y;
-        qz += f.z * f.z;
-        // offset from the cell centre, grid frame -> world frame (M d)
-        const float gx = (tx - floorf(tx) - 0.5f) * h, gy = (ty - floorf(ty) - 0.5f) * h,
-                    gz = (tz - floorf(tz) - 0.5f) * h;
-        const float* R = e.rot12 + 12 * i;
-        const float wx = R[0] * gx + R[1] * gy + R[2] * gz;
-        const float wy = R[4] * gx + R[5] * gy + R[6] * gz;
-        const float wz = R[8] * gx + R[9] * gy + R[10] * gz;
-        dx += wx; dy += wy; dz += wz;
-        dxx += wx * wx; dxy += wx * wy; dxz += wx * wz;
-        dyy += wy * wy; dyz += wy * wz; dzz += wz * wz;
-        fxdx += f.x * wx; fxdy += f.x * wy; fxdz += f.x * wz;
-        fydx += f.y * wx; fydy += f.y * wy; fydz += f.y * wz;
-        fzdx += f.z * wx; fzdy += f.z * wy; fzdz += f.z * wz;
-        rho += mass_value(__ldg(mass + (size_t)i * G3 + c), e.inv_scale);
-    }
-    const float kf = (float)e.k, ik = 1.0f / kf;
-    const float mx = __fdiv_rn(sx, kf), my = __fdiv_rn(sy, kf), mz = __fdiv_rn(sz, kf);
-    mean_out[p] = make_float4(mx, my, mz, 0.f);
-    const float ax_ = dx * ik, ay_ = dy * ik, az_ = dz * ik;  // dbar
-    // covariances
-    const float ridge = 1e-3f * h * h;
-    const float cxx = dxx * ik - ax_ * ax_ + ridge, cxy = dxy * ik - ax_ * ay_,
-                cxz = dxz * ik - ax_ * az_, cyy = dyy * ik - ay_ * ay_ + ridge,
-                cyz = dyz * ik - ay_ * az_, czz = dzz * ik - az_ * az_ + ridge;
-    // solve C_dd w = dbar (symmetric 3x3, adjugate)
-    const float A00 = cyy * czz - cyz * cyz, A01 = cxz * cyz - cxy * czz, A02 = cxy * cyz - cxz * cyy;
-    const float A11 = cxx * czz - cxz * cxz, A12 = cxy * cxz - cxx * cyz, A22 = cxx * cyy - cxy * cxy;
-    const float det = cxx * A00 + cxy * A01 + cxz * A02;
-    float wx = 0.f, wy = 0.f, wz = 0.f;
-    if (det > 0.f) {
-        const float id = 1.0f / det;
-        wx = (A00 * ax_ + A01 * ay_ + A02 * az_) * id;
-        wy = (A01 * ax_ + A11 * ay_ + A12 * az_) * id;
-        wz = (A02 * ax_ + A12 * ay_ + A22 * az_) * id;
-    }
-    // correction = -C_Fd w,  C_Fd = sum(F d^T)/k - Fbar dbar^T
-    const float ex = -((fxdx * ik - mx * ax_) * wx + (fxdy * ik - mx * ay_) * wy + (fxdz * ik - mx * az_) * wz);
-    const float ey = -((fydx * ik - my * ax_) * wx + (fydy * ik - my * ay_) * wy + (fydz * ik - my * az_) * wz);
-    const float ez = -((fzdx * ik - mz * ax_) * wx + (fzdy * ik - mz * ay_) * wy + (fzdz * ik - mz * az_) * wz);
-    const float is = 1.0f / norm.force_scale;
-    float f[kIn];
-    f[0] = mx * is;
-    f[1] = my * is;
-    f[2] = mz * is;
-    f[3] = ex * is;
-    f[4] = ey * is;
-    f[5] = ez * is;
-    f[6] = sqrtf(fmaxf(qx * ik - mx * mx, 0.f)) * is;
-    f[7] = sqrtf(fmaxf(qy * ik - my * my, 0.f)) * is;
-    f[8] = sqrtf(fmaxf(qz * ik - mz * mz, 0.f)) * is;
-    f[9] = log1pf(rho * ik / norm.rho_ref);
-    f[10] = sqrtf(mx * mx + my * my + mz * mz) * is;
-    f[11] = sqrtf(fmaxf(cxx + cyy + czz - 3.f * ridge, 0.f)) / h;
-    float* o = feat_out + (size_t)p * 16;
-#pragma unroll
-    for (int j = 0; j < kIn; ++j) o[j] = (f[j] - norm.mu[j]) * norm.inv_sigma[j];
-    o[12] = ex;
-    o[13] = ey;
-    o[14] = ez;
-    o[15] = 0.f;
 }
 
 // ---------------------------------------------------------------------------
@@ -226,112 +110,322 @@ __device__ __forceinline__ void mma_bf16(float (&d)[4], uint32_t a0, uint32_t a1
         : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
-// Tensor-core inference.  Each warp owns 16 consecutive particles (one
-// m16 tile).  Output: acc[p] = base + out_scale * y  (the corrected
-// ensemble force), written for the update to apply; base is mean[p], or
-// mean[p] + the regression correction (feature slots 12-14) when
-// with_correction is set.
-__global__ void __launch_bounds__(128) mlp_infer_kernel(const float* __restrict__ feat, int64_t n,
-                                                        const uint2* __restrict__ frags,
-                                                        const float* __restrict__ params,
-                                                        const float4* __restrict__ mean,
-                                                        float out_scale, bool with_correction,
-                                                        float4* __restrict__ acc) {
-    __shared__ uint2 sf[kFragTotal];
-    __shared__ float sb[kH + kH + 8];
-    for (int i = threadIdx.x; i < kFragTotal; i += blockDim.x) sf[i] = frags[i];
-    for (int i = threadIdx.x; i < kH; i += blockDim.x) {
-        sb[i] = params[kB1 + i];
-        sb[kH + i] = params[kB2 + i];
+// ---------------------------------------------------------------------------
+// Fused gather + features + inference + update.
+
+// Per-grid data of the gather, staged in shared memory once per CTA: the
+// pre-scaled index rows (t = A c + b, cell = floor(t), as cell_fast) and
+// the grid's rotation times the voxel size (world-frame offset from the
+// cell centre = (h M) (t - floor(t) - 1/2)).
+struct GridRows {
+    float4 r[3];
+    float m[9];
+    float pad[3];
+};
+static_assert(sizeof(GridRows) == 96, "GridRows layout");
+
+// Statistics of one particle over the k grids.
+//
+// Each grid samples the force at the centre of the particle's cell, not at
+// the particle, so the k per-grid forces F_i scatter around the force at
+// the particle roughly linearly in the particle's offset from those cell
+// centres, d_i (world frame).  A per-particle least-squares fit
+// F_i ~ a + B d_i over the k grids gives an intercept a, the force
+// extrapolated to the particle itself:
+//     a = Fbar - C_Fd (C_dd + ridge)^-1 dbar
+// with dbar, C_dd = cov(d, d) and C_Fd = cov(F, d) over the grids.
+// The features (before standardisation with the model's mu / sigma) are
+//   0-2  Fbar / s            plain ensemble mean (update.glsl order)
+//   3-5  (a - Fbar) / s      regression correction from the in-cell offsets
+//   6-8  std_i(F_i) / s      per-component spread of the per-grid forces
+//   9    log1p(rho / rho_ref) mean mass of the particle's cells
+//   10   |Fbar| / s
+//   11   sqrt(tr C_dd) / h   spread of the in-cell offsets
+// The cell masses come from the .w lane of the world-frame force grid
+// (density_w_kernel puts them there).
+struct Features {
+    float f[kIn];
+    float mx, my, mz;  // Fbar
+    float ex, ey, ez;  // a - Fbar
+};
+
+template <int IDX>
+__device__ __forceinline__ void gather_features(const float4* __restrict__ W,
+                                                const GridRows* __restrict__ xf, const Ensemble& e,
+                                                const IndexParams& ip, float cx, float cy, float cz,
+                                                float inv_fs, float rho_ref, Features& out) {
+    const int G3 = 1 << (3 * e.lg);
+    const uint32_t mask = (1u << e.lg) - 1u;
+    const float h = e.voxel;
+    float sx = 0.f, sy = 0.f, sz = 0.f;            // plain sum, update.glsl order
+    float qx = 0.f, qy = 0.f, qz = 0.f;            // sum F^2 per component
+    float dx = 0.f, dy = 0.f, dz = 0.f;            // sum d
+    float dxx = 0.f, dxy = 0.f, dxz = 0.f, dyy = 0.f, dyz = 0.f, dzz = 0.f;
+    float fxdx = 0.f, fxdy = 0.f, fxdz = 0.f, fydx = 0.f, fydy = 0.f, fydz = 0.f,
+          fzdx = 0.f, fzdy = 0.f, fzdz = 0.f;      // sum F d^T
+    float rho = 0.f;
+#pragma unroll 4
+    for (int i = 0; i < e.k; ++i) {
+        const GridRows& x = xf[i];
+        const float tx = __fmaf_rn(x.r[0].z, cz, __fmaf_rn(x.r[0].y, cy, __fmaf_rn(x.r[0].x, cx, x.r[0].w)));
+        const float ty = __fmaf_rn(x.r[1].z, cz, __fmaf_rn(x.r[1].y, cy, __fmaf_rn(x.r[1].x, cx, x.r[1].w)));
+        const float tz = __fmaf_rn(x.r[2].z, cz, __fmaf_rn(x.r[2].y, cy, __fmaf_rn(x.r[2].x, cx, x.r[2].w)));
+        uint32_t c;
+        if (IDX == 0)
+            c = floor_mod_pow2(tx, mask) | (floor_mod_pow2(ty, mask) << e.lg) |
+                (floor_mod_pow2(tz, mask) << (2 * e.lg));
+        else
+            c = cell_exact(e.rot12 + 12 * i, e.off4 + 4 * i, cx, cy, cz, ip);
+        const float4 f = __ldg(W + (size_t)i * G3 + c);
+        sx = __fadd_rn(sx, f.x);
+        sy = __fadd_rn(sy, f.y);
+        sz = __fadd_rn(sz, f.z);
+        qx += f.x * f.x;
+        qy += f.y * f.y;
+        qz += f.z * f.z;
+        const float gx = tx - floorf(tx) - 0.5f, gy = ty - floorf(ty) - 0.5f,
+                    gz = tz - floorf(tz) - 0.5f;
+        const float wx = x.m[0] * gx + x.m[1] * gy + x.m[2] * gz;
+        const float wy = x.m[3] * gx + x.m[4] * gy + x.m[5] * gz;
+        const float wz = x.m[6] * gx + x.m[7] * gy + x.m[8] * gz;
+        dx += wx; dy += wy; dz += wz;
+        dxx += wx * wx; dxy += wx * wy; dxz += wx * wz;
+        dyy += wy * wy; dyz += wy * wz; dzz += wz * wz;
+        fxdx += f.x * wx; fxdy += f.x * wy; fxdz += f.x * wz;
+        fydx += f.y * wx; fydy += f.y * wy; fydz += f.y * wz;
+        fzdx += f.z * wx; fzdy += f.z * wy; fzdz += f.z * wz;
+        rho += f.w;
     }
-    if (threadIdx.x < 8) sb[2 * kH + threadIdx.x] = threadIdx.x < kOut ? params[kB3 + threadIdx.x] : 0.f;
-    __syncthreads();
-    const int lane = threadIdx.x & 31, g = lane >> 2, tg = lane & 3;
-    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    for (int64_t tile = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-         tile * 16 < n; tile += warps) {
-        const int64_t r0 = tile * 16 + g, r1 = r0 + 8;
-        // layer 1 A fragment straight from the feature rows (16 floats each)
-        auto ld2 = [&](int64_t r, int c) -> uint32_t {
-            if (r >= n) return 0u;
-            const float2 v = *reinterpret_cast<const float2*>(feat + r * 16 + c);
-            return pack_bf16(v.x, v.y);
-        };
-        const uint32_t a0 = ld2(r0, 2 * tg), a1 = ld2(r1, 2 * tg), a2 = ld2(r0, 2 * tg + 8),
-                       a3 = ld2(r1, 2 * tg + 8);
-        float h[8][4];
+    const float kf = (float)e.k, ik = 1.0f / kf;
+    const float mx = __fdiv_rn(sx, kf), my = __fdiv_rn(sy, kf), mz = __fdiv_rn(sz, kf);
+    const float ax_ = dx * ik, ay_ = dy * ik, az_ = dz * ik;  // dbar
+    const float ridge = 1e-3f * h * h;
+    const float cxx = dxx * ik - ax_ * ax_ + ridge, cxy = dxy * ik - ax_ * ay_,
+                cxz = dxz * ik - ax_ * az_, cyy = dyy * ik - ay_ * ay_ + ridge,
+                cyz = dyz * ik - ay_ * az_, czz = dzz * ik - az_ * az_ + ridge;
+    // solve C_dd w = dbar (symmetric 3x3, adjugate)
+    const float A00 = cyy * czz - cyz * cyz, A01 = cxz * cyz - cxy * czz, A02 = cxy * cyz - cxz * cyy;
+    const float A11 = cxx * czz - cxz * cxz, A12 = cxy * cxz - cxx * cyz, A22 = cxx * cyy - cxy * cxy;
+    const float det = cxx * A00 + cxy * A01 + cxz * A02;
+    float wx = 0.f, wy = 0.f, wz = 0.f;
+    if (det > 0.f) {
+        const float id = 1.0f / det;
+        wx = (A00 * ax_ + A01 * ay_ + A02 * az_) * id;
+        wy = (A01 * ax_ + A11 * ay_ + A12 * az_) * id;
+        wz = (A02 * ax_ + A12 * ay_ + A22 * az_) * id;
+    }
+    // correction = -C_Fd w,  C_Fd = sum(F d^T)/k - Fbar dbar^T
+    out.ex = -((fxdx * ik - mx * ax_) * wx + (fxdy * ik - mx * ay_) * wy + (fxdz * ik - mx * az_) * wz);
+    out.ey = -((fydx * ik - my * ax_) * wx + (fydy * ik - my * ay_) * wy + (fydz * ik - my * az_) * wz);
+    out.ez = -((fzdx * ik - mz * ax_) * wx + (fzdy * ik - mz * ay_) * wy + (fzdz * ik - mz * az_) * wz);
+    out.mx = mx;
+    out.my = my;
+    out.mz = mz;
+    out.f[0] = mx * inv_fs;
+    out.f[1] = my * inv_fs;
+    out.f[2] = mz * inv_fs;
+    out.f[3] = out.ex * inv_fs;
+    out.f[4] = out.ey * inv_fs;
+    out.f[5] = out.ez * inv_fs;
+    out.f[6] = sqrtf(fmaxf(qx * ik - mx * mx, 0.f)) * inv_fs;
+    out.f[7] = sqrtf(fmaxf(qy * ik - my * my, 0.f)) * inv_fs;
+    out.f[8] = sqrtf(fmaxf(qz * ik - mz * mz, 0.f)) * inv_fs;
+    out.f[9] = log1pf(rho * ik / rho_ref);
+    out.f[10] = sqrtf(mx * mx + my * my + mz * mz) * inv_fs;
+    out.f[11] = sqrtf(fmaxf(cxx + cyy + czz - 3.f * ridge, 0.f)) / h;
+}
+
+// The network on one m16 tile of a warp: A fragment (a0..a3) of the
+// standardised features in, y fragment of the 8-wide output tile out
+// (outputs 0..2 live).  sf: weight fragments, sb: b1 | b2 | b3 (padded to 8).
+__device__ __forceinline__ void mlp_tile(const uint2* __restrict__ sf, const float* __restrict__ sb,
+                                         uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                         int lane, float (&y)[4]) {
+    const int tg = lane & 3;
+    float h[8][4];
 #pragma unroll
-        for (int nt = 0; nt < 8; ++nt) {
-            const float b0 = sb[nt * 8 + 2 * tg], b1 = sb[nt * 8 + 2 * tg + 1];
-            h[nt][0] = b0; h[nt][1] = b1; h[nt][2] = b0; h[nt][3] = b1;
-            const uint2 w = sf[(0 * 8 + nt) * 32 + lane];
-            mma_bf16(h[nt], a0, a1, a2, a3, w.x, w.y);
-        }
-        uint32_t A[4][4];
+    for (int nt = 0; nt < 8; ++nt) {
+        const float b0 = sb[nt * 8 + 2 * tg], b1 = sb[nt * 8 + 2 * tg + 1];
+        h[nt][0] = b0; h[nt][1] = b1; h[nt][2] = b0; h[nt][3] = b1;
+        const uint2 w = sf[(0 * 8 + nt) * 32 + lane];
+        mma_bf16(h[nt], a0, a1, a2, a3, w.x, w.y);
+    }
+    uint32_t A[4][4];
+#pragma unroll
+    for (int ks = 0; ks < 4; ++ks) {
+        A[ks][0] = pack_bf16(gelu_fast(h[2 * ks][0]), gelu_fast(h[2 * ks][1]));
+        A[ks][1] = pack_bf16(gelu_fast(h[2 * ks][2]), gelu_fast(h[2 * ks][3]));
+        A[ks][2] = pack_bf16(gelu_fast(h[2 * ks + 1][0]), gelu_fast(h[2 * ks + 1][1]));
+        A[ks][3] = pack_bf16(gelu_fast(h[2 * ks + 1][2]), gelu_fast(h[2 * ks + 1][3]));
+    }
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+        const float b0 = sb[kH + nt * 8 + 2 * tg], b1 = sb[kH + nt * 8 + 2 * tg + 1];
+        h[nt][0] = b0; h[nt][1] = b1; h[nt][2] = b0; h[nt][3] = b1;
 #pragma unroll
         for (int ks = 0; ks < 4; ++ks) {
-            A[ks][0] = pack_bf16(gelu_fast(h[2 * ks][0]), gelu_fast(h[2 * ks][1]));
-            A[ks][1] = pack_bf16(gelu_fast(h[2 * ks][2]), gelu_fast(h[2 * ks][3]));
-            A[ks][2] = pack_bf16(gelu_fast(h[2 * ks + 1][0]), gelu_fast(h[2 * ks + 1][1]));
-            A[ks][3] = pack_bf16(gelu_fast(h[2 * ks + 1][2]), gelu_fast(h[2 * ks + 1][3]));
+            const uint2 w = sf[(kFrag1 + ks * 8 + nt) * 32 + lane];
+            mma_bf16(h[nt], A[ks][0], A[ks][1], A[ks][2], A[ks][3], w.x, w.y);
         }
-        // layer 2
+    }
 #pragma unroll
-        for (int nt = 0; nt < 8; ++nt) {
-            const float b0 = sb[kH + nt * 8 + 2 * tg], b1 = sb[kH + nt * 8 + 2 * tg + 1];
-            h[nt][0] = b0; h[nt][1] = b1; h[nt][2] = b0; h[nt][3] = b1;
+    for (int ks = 0; ks < 4; ++ks) {
+        A[ks][0] = pack_bf16(gelu_fast(h[2 * ks][0]), gelu_fast(h[2 * ks][1]));
+        A[ks][1] = pack_bf16(gelu_fast(h[2 * ks][2]), gelu_fast(h[2 * ks][3]));
+        A[ks][2] = pack_bf16(gelu_fast(h[2 * ks + 1][0]), gelu_fast(h[2 * ks + 1][1]));
+        A[ks][3] = pack_bf16(gelu_fast(h[2 * ks + 1][2]), gelu_fast(h[2 * ks + 1][3]));
+    }
+    y[0] = sb[2 * kH + 2 * tg];
+    y[1] = sb[2 * kH + 2 * tg + 1];
+    y[2] = y[0];
+    y[3] = y[1];
 #pragma unroll
-            for (int ks = 0; ks < 4; ++ks) {
-                const uint2 w = sf[(kFrag1 + ks * 8 + nt) * 32 + lane];
-                mma_bf16(h[nt], A[ks][0], A[ks][1], A[ks][2], A[ks][3], w.x, w.y);
-            }
-        }
-#pragma unroll
-        for (int ks = 0; ks < 4; ++ks) {
-            A[ks][0] = pack_bf16(gelu_fast(h[2 * ks][0]), gelu_fast(h[2 * ks][1]));
-            A[ks][1] = pack_bf16(gelu_fast(h[2 * ks][2]), gelu_fast(h[2 * ks][3]));
-            A[ks][2] = pack_bf16(gelu_fast(h[2 * ks + 1][0]), gelu_fast(h[2 * ks + 1][1]));
-            A[ks][3] = pack_bf16(gelu_fast(h[2 * ks + 1][2]), gelu_fast(h[2 * ks + 1][3]));
-        }
-        // layer 3 (n = 8, outputs 0..2 live)
-        float y[4];
-        y[0] = sb[2 * kH + 2 * tg];
-        y[1] = sb[2 * kH + 2 * tg + 1];
-        y[2] = y[0];
-        y[3] = y[1];
-#pragma unroll
-        for (int ks = 0; ks < 4; ++ks) {
-            const uint2 w = sf[(kFrag1 + kFrag2 + ks) * 32 + lane];
-            mma_bf16(y, A[ks][0], A[ks][1], A[ks][2], A[ks][3], w.x, w.y);
-        }
-        // lanes with tg == 0 hold outputs 0,1 of rows g, g+8; tg == 1 holds output 2
-        const float o0a = __shfl_sync(kFull, y[0], (g << 2) | 0), o1a = __shfl_sync(kFull, y[1], (g << 2) | 0);
-        const float o2a = __shfl_sync(kFull, y[0], (g << 2) | 1);
-        const float o0b = __shfl_sync(kFull, y[2], (g << 2) | 0), o1b = __shfl_sync(kFull, y[3], (g << 2) | 0);
-        const float o2b = __shfl_sync(kFull, y[2], (g << 2) | 1);
-        auto base = [&](int64_t r) {
-            float4 m = mean[r];
-            if (with_correction) {
-                const float4 c = *reinterpret_cast<const float4*>(feat + r * 16 + 12);
-                m.x += c.x;
-                m.y += c.y;
-                m.z += c.z;
-            }
-            return m;
-        };
-        if (tg == 0) {
-            if (r0 < n) {
-                const float4 m = base(r0);
-                acc[r0] = make_float4(m.x + out_scale * o0a, m.y + out_scale * o1a, m.z + out_scale * o2a, 0.f);
-            }
-            if (r1 < n) {
-                const float4 m = base(r1);
-                acc[r1] = make_float4(m.x + out_scale * o0b, m.y + out_scale * o1b, m.z + out_scale * o2b, 0.f);
-            }
-        }
+    for (int ks = 0; ks < 4; ++ks) {
+        const uint2 w = sf[(kFrag1 + kFrag2 + ks) * 32 + lane];
+        mma_bf16(y, A[ks][0], A[ks][1], A[ks][2], A[ks][3], w.x, w.y);
     }
 }
 
+constexpr int kLT = 256;       // threads of learned_kernel
+constexpr int kLW = kLT / 32;  // warps
+constexpr int kARow = 12;      // u32 per A-tile row (8 used; 12 keeps the fragment loads conflict-free)
+constexpr size_t kLearnedFixedSmem = sizeof(uint2) * kFragTotal + sizeof(float) * (2 * kH + 8) +
+                                     sizeof(uint32_t) * kLW * 32 * kARow + sizeof(float4) * kLW * 32;
+static_assert(kLearnedFixedSmem % 16 == 0, "GridRows must stay 16-byte aligned");
+
+// OUT 0: one damped leapfrog step with the corrected force (pos, vel);
+// OUT 1: the corrected force into out4;  OUT 2: the features (out4 = Fbar,
+// feat = 16 floats: 0-11 standardised, 12-14 a - Fbar, 15 zero), no network.
+// One thread per particle; a persistent grid walks blocks of kLT particles.
+template <int IDX, int OUT>
+__global__ void __launch_bounds__(kLT, 2) learned_kernel(
+    float4* __restrict__ pos, float4* __restrict__ vel, int64_t n, const float4* __restrict__ W,
+    Ensemble e, ModelNorm norm, const uint2* __restrict__ frags, const float* __restrict__ params,
+    float dt, float damp, float4* __restrict__ out4, float* __restrict__ feat_out) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint2* sf = reinterpret_cast<uint2*>(smem_raw);
+    float* sb = reinterpret_cast<float*>(sf + kFragTotal);
+    uint32_t* sA = reinterpret_cast<uint32_t*>(sb + 2 * kH + 8);
+    float4* sY = reinterpret_cast<float4*>(sA + kLW * 32 * kARow);
+    GridRows* xf = reinterpret_cast<GridRows*>(smem_raw + kLearnedFixedSmem);
+    const float h = e.voxel;
+    for (int i = threadIdx.x; i < e.k; i += kLT) {
+        const FastXf x = e.fast[i];
+        const float* R = e.rot12 + 12 * i;
+        GridRows g;
+        g.r[0] = x.row[0];
+        g.r[1] = x.row[1];
+        g.r[2] = x.row[2];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) g.m[3 * a + b] = R[4 * a + b] * h;
+        g.pad[0] = g.pad[1] = g.pad[2] = 0.f;
+        xf[i] = g;
+    }
+    if (OUT != 2) {
+        for (int i = threadIdx.x; i < kFragTotal; i += kLT) sf[i] = frags[i];
+        for (int i = threadIdx.x; i < kH; i += kLT) {
+            sb[i] = params[kB1 + i];
+            sb[kH + i] = params[kB2 + i];
+        }
+        if (threadIdx.x < 8) sb[2 * kH + threadIdx.x] = threadIdx.x < kOut ? params[kB3 + threadIdx.x] : 0.f;
+    }
+    __syncthreads();
+    const IndexParams ip = e.index_params();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, tg = lane & 3;
+    uint32_t* A = sA + warp * 32 * kARow;
+    float4* Y = sY + warp * 32;
+    const float inv_fs = 1.0f / norm.force_scale;
+    unsigned bad = 0;
+    for (int64_t base = (int64_t)blockIdx.x * kLT; base < n; base += (int64_t)gridDim.x * kLT) {
+        if (base + warp * 32 >= n) continue;  // whole warp past the end (warp-uniform)
+        const int64_t p = base + threadIdx.x;
+        const bool live = p < n;
+        const float4 P = live ? pos[p] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float cx = __fsub_rn(P.x, ip.half_l), cy = __fsub_rn(P.y, ip.half_l),
+                    cz = __fsub_rn(P.z, ip.half_l);
+        Features F;
+        gather_features<IDX>(W, xf, e, ip, cx, cy, cz, inv_fs, norm.rho_ref, F);
+        float z[kIn];
+#pragma unroll
+        for (int j = 0; j < kIn; ++j) z[j] = (F.f[j] - norm.mu[j]) * norm.inv_sigma[j];
+        if (OUT == 2) {
+            if (live) {
+                out4[p] = make_float4(F.mx, F.my, F.mz, 0.f);
+                float4* o = reinterpret_cast<float4*>(feat_out + (size_t)p * 16);
+                o[0] = make_float4(z[0], z[1], z[2], z[3]);
+                o[1] = make_float4(z[4], z[5], z[6], z[7]);
+                o[2] = make_float4(z[8], z[9], z[10], z[11]);
+                o[3] = make_float4(F.ex, F.ey, F.ez, 0.f);
+            }
+            continue;
+        }
+        // this particle's row of the warp's A tile (BF16 pairs; columns 12-15 zero)
+        uint4* row = reinterpret_cast<uint4*>(A + lane * kARow);
+        row[0] = make_uint4(pack_bf16(z[0], z[1]), pack_bf16(z[2], z[3]), pack_bf16(z[4], z[5]),
+                            pack_bf16(z[6], z[7]));
+        row[1] = make_uint4(pack_bf16(z[8], z[9]), pack_bf16(z[10], z[11]), 0u, 0u);
+        __syncwarp();
+#pragma unroll
+        for (int m = 0; m < 2; ++m) {
+            const uint32_t* Am = A + 16 * m * kARow;
+            float y[4];
+            mlp_tile(sf, sb, Am[g * kARow + tg], Am[(g + 8) * kARow + tg], Am[g * kARow + tg + 4],
+                     Am[(g + 8) * kARow + tg + 4], lane, y);
+            // y: rows g and g+8, outputs 2tg and 2tg+1
+            if (tg == 0) {
+                Y[16 * m + g].x = y[0];
+                Y[16 * m + g].y = y[1];
+                Y[16 * m + g + 8].x = y[2];
+                Y[16 * m + g + 8].y = y[3];
+            } else if (tg == 1) {
+                Y[16 * m + g].z = y[0];
+                Y[16 * m + g + 8].z = y[2];
+            }
+        }
+        __syncwarp();
+        const float4 yv = Y[lane];
+        __syncwarp();  // the next block of particles reuses A and Y
+        if (!live) continue;
+        float bx = F.mx, by = F.my, bz = F.mz;
+        if (norm.base_mode != 0.f) {
+            bx += F.ex;
+            by += F.ey;
+            bz += F.ez;
+        }
+        const float ax = bx + norm.out_scale * yv.x, ay = by + norm.out_scale * yv.y,
+                    az = bz + norm.out_scale * yv.z;
+        if (OUT == 1) {
+            out4[p] = make_float4(ax, ay, az, 0.f);
+            continue;
+        }
+        // update.glsl:83-89 with the corrected force
+        const float4 V = vel[p];
+        const float vx = __fmul_rn(__fsub_rn(V.x, __fmul_rn(ax, dt)), damp);
+        const float vy = __fmul_rn(__fsub_rn(V.y, __fmul_rn(ay, dt)), damp);
+        const float vz = __fmul_rn(__fsub_rn(V.z, __fmul_rn(az, dt)), damp);
+        const float px = glsl_mod(__fadd_rn(P.x, __fmul_rn(vx, dt)), e.world);
+        const float py = glsl_mod(__fadd_rn(P.y, __fmul_rn(vy, dt)), e.world);
+        const float pz = glsl_mod(__fadd_rn(P.z, __fmul_rn(vz, dt)), e.world);
+        if (!(isfinite(px) && isfinite(py) && isfinite(pz))) bad |= 1u;  // MOG_FLAG_NONFINITE
+        pos[p] = make_float4(px, py, pz, P.w);
+        vel[p] = make_float4(vx, vy, vz, 0.f);
+    }
+    if (bad) raise_flags(e.flags, bad);
+}
+
+// Cell masses into the .w lane of the world-frame force grid (which the
+// world-frame solve leaves 0), clearing the mass grid for the next deposit.
+template <typename Acc>
+__global__ void density_w_kernel(Acc* __restrict__ mass, float4* __restrict__ W, int64_t cells,
+                                 float inv_scale) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cells;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        reinterpret_cast<float*>(W + i)[3] = mass_value(mass[i], inv_scale);
+        mass[i] = 0;
+    }
+}
 // ---------------------------------------------------------------------------
 // FP32 training: forward + backward for 128 samples per CTA.
 constexpr int kTB = 128;   // samples per CTA
@@ -449,24 +543,6 @@ __global__ void adam_kernel(float* __restrict__ params, const float* __restrict_
     params[q] -= lr * (mq / bc1) / (sqrtf(vq / bc2) + eps);
 }
 
-// Apply a per-particle force with the update.glsl:83-89 arithmetic.
-__global__ void apply_force_kernel(float4* __restrict__ pos, float4* __restrict__ vel, int64_t n,
-                                   const float4* __restrict__ acc, float dt, float damp,
-                                   float world, unsigned* flags) {
-    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
-    const float4 P = pos[p], V = vel[p], A = acc[p];
-    float vx = __fmul_rn(__fsub_rn(V.x, __fmul_rn(A.x, dt)), damp);
-    float vy = __fmul_rn(__fsub_rn(V.y, __fmul_rn(A.y, dt)), damp);
-    float vz = __fmul_rn(__fsub_rn(V.z, __fmul_rn(A.z, dt)), damp);
-    const float px = glsl_mod(__fadd_rn(P.x, __fmul_rn(vx, dt)), world);
-    const float py = glsl_mod(__fadd_rn(P.y, __fmul_rn(vy, dt)), world);
-    const float pz = glsl_mod(__fadd_rn(P.z, __fmul_rn(vz, dt)), world);
-    if (!(isfinite(px) && isfinite(py) && isfinite(pz))) atomicOr(flags, 1u);
-    pos[p] = make_float4(px, py, pz, P.w);
-    vel[p] = make_float4(vx, vy, vz, 0.f);
-}
-
 }  // namespace
 
 int mlp_param_count() { return kParams; }
@@ -475,33 +551,61 @@ size_t mlp_train_smem() {
     return sizeof(float) * ((size_t)kParams + kTB * kIn + 4 * kTB * kLd + kTB * 4);
 }
 
-cudaError_t launch_features(const Ensemble& e, const float4* pos, int64_t n, const float4* W,
-                            const void* mass, const ModelNorm& norm, float4* mean, float* feat,
-                            cudaStream_t s) {
-    if (n <= 0) return cudaSuccess;
-    const unsigned blocks = (unsigned)((n + 255) / 256);
+cudaError_t launch_density_w(const Ensemble& e, void* mass, float4* W, cudaStream_t s) {
+    const int64_t cells = e.cells();  // k * g^3
+    const unsigned blocks = (unsigned)std::min<int64_t>((cells + 255) / 256, (int64_t)num_sms() * 8);
     if (e.mass_mode == 0)
-        features_kernel<unsigned long long><<<blocks, 256, 0, s>>>(
-            pos, n, W, static_cast<const unsigned long long*>(mass), e, norm, mean, feat);
+        density_w_kernel<<<blocks, 256, 0, s>>>(static_cast<unsigned long long*>(mass), W, cells,
+                                                e.inv_scale);
     else
-        features_kernel<unsigned><<<blocks, 256, 0, s>>>(pos, n, W, static_cast<const unsigned*>(mass),
-                                                         e, norm, mean, feat);
+        density_w_kernel<<<blocks, 256, 0, s>>>(static_cast<unsigned*>(mass), W, cells, e.inv_scale);
     return cudaGetLastError();
+}
+
+namespace {
+template <int IDX, int OUT>
+cudaError_t launch_learned_t(const Ensemble& e, float4* pos, float4* vel, int64_t n,
+                             const float4* W, const ModelNorm& norm, const void* frags,
+                             const float* params, float dt, float damp, float4* out4, float* feat,
+                             cudaStream_t s) {
+    auto kern = learned_kernel<IDX, OUT>;
+    const size_t smem = kLearnedFixedSmem + sizeof(GridRows) * (size_t)e.k;
+    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return err;
+    int per_sm = 0;
+    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kLT, smem);
+    if (err != cudaSuccess) return err;
+    const int64_t blocks = std::min<int64_t>((n + kLT - 1) / kLT, (int64_t)num_sms() * std::max(per_sm, 1));
+    kern<<<(unsigned)blocks, kLT, smem, s>>>(pos, vel, n, W, e, norm, static_cast<const uint2*>(frags),
+                                            params, dt, damp, out4, feat);
+    return cudaGetLastError();
+}
+
+template <int IDX>
+cudaError_t launch_learned_i(int out_mode, const Ensemble& e, float4* pos, float4* vel, int64_t n,
+                             const float4* W, const ModelNorm& norm, const void* frags,
+                             const float* params, float dt, float damp, float4* out4, float* feat,
+                             cudaStream_t s) {
+    switch (out_mode) {
+        case 0: return launch_learned_t<IDX, 0>(e, pos, vel, n, W, norm, frags, params, dt, damp, out4, feat, s);
+        case 1: return launch_learned_t<IDX, 1>(e, pos, vel, n, W, norm, frags, params, dt, damp, out4, feat, s);
+        default: return launch_learned_t<IDX, 2>(e, pos, vel, n, W, norm, frags, params, dt, damp, out4, feat, s);
+    }
+}
+}  // namespace
+
+cudaError_t launch_learned(int out_mode, const Ensemble& e, float4* pos, float4* vel, int64_t n,
+                           const float4* W, const ModelNorm& norm, const void* frags,
+                           const float* params, float dt, float damp, float4* out4, float* feat,
+                           cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    if (e.index_mode == 0)
+        return launch_learned_i<0>(out_mode, e, pos, vel, n, W, norm, frags, params, dt, damp, out4, feat, s);
+    return launch_learned_i<1>(out_mode, e, pos, vel, n, W, norm, frags, params, dt, damp, out4, feat, s);
 }
 
 cudaError_t launch_pack_fragments(const float* params, void* frags, cudaStream_t s) {
     pack_fragments_kernel<<<(kFragTotal + 255) / 256, 256, 0, s>>>(params, static_cast<uint2*>(frags));
-    return cudaGetLastError();
-}
-
-cudaError_t launch_mlp_infer(const float* feat, int64_t n, const void* frags, const float* params,
-                             const float4* mean, float out_scale, bool with_correction, float4* acc,
-                             cudaStream_t s) {
-    if (n <= 0) return cudaSuccess;
-    const int64_t tiles = (n + 15) / 16;
-    const int64_t blocks = std::min<int64_t>((tiles + 3) / 4, (int64_t)num_sms() * 16);
-    mlp_infer_kernel<<<(unsigned)blocks, 128, 0, s>>>(feat, n, static_cast<const uint2*>(frags),
-                                                      params, mean, out_scale, with_correction, acc);
     return cudaGetLastError();
 }
 
@@ -521,13 +625,6 @@ cudaError_t launch_mlp_train_step(const float* feat, const float* target, const 
         const float bc1 = 1.f - powf(b1, (float)t), bc2 = 1.f - powf(b2, (float)t);
         adam_kernel<<<(kParams + 255) / 256, 256, 0, s>>>(params, grad, m, v, lr, b1, b2, 1e-8f, bc1, bc2);
     }
-    return cudaGetLastError();
-}
-
-cudaError_t launch_apply_force(float4* pos, float4* vel, int64_t n, const float4* acc, float dt,
-                               float damp, float world, unsigned* flags, cudaStream_t s) {
-    if (n <= 0) return cudaSuccess;
-    apply_force_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(pos, vel, n, acc, dt, damp, world, flags);
     return cudaGetLastError();
 }
 

@@ -162,10 +162,6 @@ struct mog_handle {
     double* d_diag = nullptr;    // diagnostics partials + result
     int* d_perm = nullptr;       // spatial order of the particles (slot -> particle)
     float4* d_pos_s = nullptr;   // positions in spatial order (refreshed every step)
-    float4* d_mean = nullptr;    // learned path: plain ensemble force
-    float* d_feat = nullptr;     // learned path: features (n x 16)
-    float4* d_acc = nullptr;     // learned path: corrected force
-    int64_t learn_cap = 0;
     void* d_sort = nullptr;      // counting-sort scratch
     int64_t perm_cap = 0;        // capacity of d_perm
     int64_t perm_n = -1;         // n the permutation was built for
@@ -329,8 +325,7 @@ void release(mog_handle* h) {
     h->graphs.clear();
     void* ptrs[] = {h->d_rot12, h->d_off4, h->d_fast, h->d_green, h->d_ktab, h->d_conv,
                     h->d_flags, h->d_total, h->d_mass, h->d_force, h->d_force2, h->d_scratch,
-                    h->d_diag, h->d_perm, h->d_sort, h->d_pos_s, h->d_mean, h->d_feat,
-                    h->d_acc};
+                    h->d_diag, h->d_perm, h->d_sort, h->d_pos_s};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }
@@ -814,29 +809,10 @@ const char* mog_version(void) { return "mog-b200 0.1 (sm_100a)"; }
 
 // ---- learned correction ---------------------------------------------------
 
-static int learn_buffers(mog_handle* h, int64_t n, cudaStream_t s) {
-    if (n <= h->learn_cap) return MOG_OK;
-    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    cudaStreamIsCapturing(s, &cs);
-    if (cs != cudaStreamCaptureStatusNone)
-        return fail(MOG_ERR_ARG, "learned-path buffers must exist before stream capture");
-    cudaFree(h->d_mean);
-    cudaFree(h->d_feat);
-    cudaFree(h->d_acc);
-    h->d_mean = nullptr;
-    h->d_feat = nullptr;
-    h->d_acc = nullptr;
-    h->learn_cap = 0;
-    MOG_CUDA(cudaMalloc((void**)&h->d_mean, sizeof(float4) * n), "cudaMalloc mean");
-    MOG_CUDA(cudaMalloc((void**)&h->d_feat, sizeof(float) * 16 * n), "cudaMalloc features");
-    MOG_CUDA(cudaMalloc((void**)&h->d_acc, sizeof(float4) * n), "cudaMalloc acc");
-    h->learn_cap = n;
-    return MOG_OK;
-}
-
-// deposit + solve (mass grid kept for the density feature) + features
-static int run_features(mog_handle* h, const mog_model* m, const float4* pos, int64_t n,
-                        float4* mean, float* feat, cudaStream_t s) {
+// Deposit + world-frame solve with the handle's ensemble, then the cell
+// masses into the force grid's .w lane (the mass grid is cleared for the
+// next deposit).  The learned kernel gathers everything from that grid.
+static int run_learned_grids(mog_handle* h, const float4* pos, int64_t n, cudaStream_t s) {
     const mog::Ensemble& e = h->e;
     cudaError_t err = mog::launch_deposit(e, pos, nullptr, n, false, h->d_mass, h->dshape, s);
     if (err != cudaSuccess) return cuda_fail(err, "deposit");
@@ -845,10 +821,20 @@ static int run_features(mog_handle* h, const mog_model* m, const float4* pos, in
     else
         err = mog::launch_convolution(e, h->d_mass, h->d_force, true, false, s);
     if (err != cudaSuccess) return cuda_fail(err, "solve");
-    err = mog::launch_features(e, pos, n, h->d_force, h->d_mass, m->norm, mean, feat, s);
-    if (err != cudaSuccess) return cuda_fail(err, "features");
-    MOG_CUDA(cudaMemsetAsync(h->d_mass, 0, mass_bytes(h), s), "clear mass");
+    err = mog::launch_density_w(e, h->d_mass, h->d_force, s);
+    if (err != cudaSuccess) return cuda_fail(err, "cell masses");
     if (e.mass_mode == 0 && e.mass_total) MOG_CUDA(cudaMemsetAsync(e.mass_total, 0, sizeof(double), s), "clear total");
+    return MOG_OK;
+}
+
+static int run_learned(mog_handle* h, const mog_model* m, int out_mode, float* pos4, float* vel4,
+                       int64_t n, float dt, float4* out4, float* feat, cudaStream_t s) {
+    int rc = run_learned_grids(h, reinterpret_cast<const float4*>(pos4), n, s);
+    if (rc) return rc;
+    cudaError_t err = mog::launch_learned(out_mode, h->e, reinterpret_cast<float4*>(pos4),
+                                          reinterpret_cast<float4*>(vel4), n, h->d_force, m->norm,
+                                          m->d_frags, m->d_params, dt, h->cfg.damping, out4, feat, s);
+    if (err != cudaSuccess) return cuda_fail(err, "learned kernel");
     return MOG_OK;
 }
 
@@ -959,9 +945,9 @@ int mog_features(mog_handle* h, const mog_model* m, const float* pos4, int64_t n
     if (rc) return rc;
     if (n > 0 && !feat16_out) return fail(MOG_ERR_ARG, "feat16_out is null");
     if ((rc = set_device(h))) return rc;
-    return run_features(h, m, reinterpret_cast<const float4*>(pos4), n,
-                        reinterpret_cast<float4*>(mean4_out), feat16_out,
-                        static_cast<cudaStream_t>(stream));
+    return run_learned(h, m, 2, const_cast<float*>(pos4), nullptr, n, 0.f,
+                       reinterpret_cast<float4*>(mean4_out), feat16_out,
+                       static_cast<cudaStream_t>(stream));
 }
 
 int mog_learned_forces(mog_handle* h, const mog_model* m, const float* pos4, float* acc4, int64_t n,
@@ -970,14 +956,8 @@ int mog_learned_forces(mog_handle* h, const mog_model* m, const float* pos4, flo
     int rc = check_particles(h, pos4, acc4, n, true);
     if (rc) return rc;
     if ((rc = set_device(h))) return rc;
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    if ((rc = learn_buffers(h, n, s))) return rc;
-    if ((rc = run_features(h, m, reinterpret_cast<const float4*>(pos4), n, h->d_mean, h->d_feat, s)))
-        return rc;
-    cudaError_t err = mog::launch_mlp_infer(h->d_feat, n, m->d_frags, m->d_params, h->d_mean,
-                                            m->norm.out_scale, m->norm.base_mode != 0.f, reinterpret_cast<float4*>(acc4), s);
-    if (err != cudaSuccess) return cuda_fail(err, "mlp inference");
-    return MOG_OK;
+    return run_learned(h, m, 1, const_cast<float*>(pos4), nullptr, n, 0.f,
+                       reinterpret_cast<float4*>(acc4), nullptr, static_cast<cudaStream_t>(stream));
 }
 
 int mog_learned_step(mog_handle* h, const mog_model* m, float* pos4, float* vel4, int64_t n,
@@ -987,16 +967,9 @@ int mog_learned_step(mog_handle* h, const mog_model* m, float* pos4, float* vel4
     if (rc) return rc;
     if (!std::isfinite(dt_eff)) return fail(MOG_ERR_ARG, "dt_eff must be finite");
     if ((rc = set_device(h))) return rc;
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    if ((rc = learn_buffers(h, n, s))) return rc;
-    if ((rc = run_features(h, m, reinterpret_cast<const float4*>(pos4), n, h->d_mean, h->d_feat, s)))
+    if ((rc = run_learned(h, m, 0, pos4, vel4, n, dt_eff, nullptr, nullptr,
+                          static_cast<cudaStream_t>(stream))))
         return rc;
-    cudaError_t err = mog::launch_mlp_infer(h->d_feat, n, m->d_frags, m->d_params, h->d_mean,
-                                            m->norm.out_scale, m->norm.base_mode != 0.f, h->d_acc, s);
-    if (err != cudaSuccess) return cuda_fail(err, "mlp inference");
-    err = mog::launch_apply_force(reinterpret_cast<float4*>(pos4), reinterpret_cast<float4*>(vel4), n,
-                                  h->d_acc, dt_eff, h->cfg.damping, h->e.world, h->d_flags, s);
-    if (err != cudaSuccess) return cuda_fail(err, "apply force");
     ++h->step_count;
     return MOG_OK;
 }

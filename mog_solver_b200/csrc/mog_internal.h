@@ -139,18 +139,19 @@ struct ModelNorm {
 int mlp_param_count();
 size_t mlp_fragment_bytes();
 size_t mlp_train_smem();
-cudaError_t launch_features(const Ensemble& e, const float4* pos, int64_t n, const float4* W,
-                            const void* mass, const ModelNorm& norm, float4* mean, float* feat,
-                            cudaStream_t s);
+// Cell masses into W's .w lane (and the mass grid cleared) after a
+// world-frame solve; then the fused gather + features + network + update
+// (out_mode 0: step pos/vel; 1: corrected force into out4; 2: features,
+// out4 = plain mean force, feat = n x 16).
+cudaError_t launch_density_w(const Ensemble& e, void* mass, float4* W, cudaStream_t s);
+cudaError_t launch_learned(int out_mode, const Ensemble& e, float4* pos, float4* vel, int64_t n,
+                           const float4* W, const ModelNorm& norm, const void* frags,
+                           const float* params, float dt, float damp, float4* out4, float* feat,
+                           cudaStream_t s);
 cudaError_t launch_pack_fragments(const float* params, void* frags, cudaStream_t s);
-cudaError_t launch_mlp_infer(const float* feat, int64_t n, const void* frags, const float* params,
-                             const float4* mean, float out_scale, bool with_correction, float4* acc,
-                             cudaStream_t s);
 cudaError_t launch_mlp_train_step(const float* feat, const float* target, const int* idx,
                                   int batch, float* params, float* partial, float* loss_partial,
                                   float* grad, float* m, float* v, float lr, int t,
                                   cudaStream_t s);
-cudaError_t launch_apply_force(float4* pos, float4* vel, int64_t n, const float4* acc, float dt,
-                               float damp, float world, unsigned* flags, cudaStream_t s);
 
 }  // namespace mog

@@ -34,7 +34,7 @@ def evaluate(model, n: int = 1 << 20, k_small: int = 32, k_big: int = 240, g: in
     import torch
 
     from . import _lib, ics
-    from .learned import _cfg, direct_sum, learned_forces, rms_error
+    from .learned import _cfg, direct_sum, features, learned_forces, rms_error
     from .simulation import Simulation
 
     small = Simulation(_cfg(k_small, g, world, G, n, small_seed))
