@@ -265,7 +265,7 @@ int mog_batch_destroy(mog_batch* b);
  * A model is a 12 -> 64 -> 64 -> 3 GELU network predicting, from per-particle
  * statistics of the handle's ensemble, the residual to a larger ensemble.
  *   params: MOG_MODEL_PARAMS floats, W1[64][12] b1[64] W2[64][64] b2[64]
- *           W3[3][64] b3[3] (FP32 master copy; inference runs in BF16).
+ *           W3[3][64] b3[3] (FP32 master copy; inference runs in FP16).
  *   norm:   MOG_MODEL_NORM floats, mu[12] inv_sigma[12] force_scale
  *           rho_ref out_scale base_mode — features are (f - mu) * inv_sigma
  *           with forces divided by force_scale and densities by rho_ref;

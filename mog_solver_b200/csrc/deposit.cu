@@ -380,6 +380,18 @@ __global__ void __launch_bounds__(256) deposit_global_kernel(const float4* __res
 
 }  // namespace
 
+// Particle chunks per grid group.  Every chunk costs one histogram flush
+// (gpc * g^3 global atomics), so chunks stay few, but the CTAs (groups x
+// chunks, `per_sm` resident per SM) should fill whole waves: 2 waves when
+// there are few groups, 5 when there are many (measured on k = 32 / 240,
+// g = 16, 2^20 particles).  At least 4096 particles per chunk.
+static int auto_chunks(int64_t n, int64_t groups, int per_sm) {
+    const int64_t waves = groups <= 16 ? 2 : 5;
+    const int64_t c = waves * num_sms() * per_sm / std::max<int64_t>(groups, 1);
+    const int64_t max_c = (n + 4095) / 4096;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(c, max_c));
+}
+
 template <int MODE, int IDX>
 static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, const int* perm, int64_t n,
                                  bool ordered, void* mass_v, const DepositShape& sh,
@@ -400,7 +412,17 @@ static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, const int
     }
     int gpc = sh.grids_per_cta;
     int slab_lg = cells_lg;
-    if (gpc == 0) gpc = (int)std::max<size_t>(1, std::min<size_t>((size_t)e.k, budget / grid_bytes));
+    if (gpc == 0) {
+        // as many grids as fit, lowered to a divisor of k when one is at
+        // least half that, so every grid group carries the same work
+        const int most = (int)std::max<size_t>(1, std::min<size_t>((size_t)e.k, budget / grid_bytes));
+        gpc = most;
+        for (int d = most; d * 2 >= most && d >= 1; --d)
+            if (e.k % d == 0) {
+                gpc = d;
+                break;
+            }
+    }
     if (grid_bytes * gpc > budget) {
         gpc = 1;
         while ((word_bytes << slab_lg) > 128 * 1024) --slab_lg;
@@ -418,13 +440,7 @@ static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, const int
             if (err != cudaSuccess) return err;
             const int groups = (e.k + gpc - 1) / gpc;
             int chunks = sh.chunks;
-            if (chunks <= 0) {
-                const int per_sm = fsmem > 110 * 1024 ? 1 : 2;
-                const int64_t target = (int64_t)num_sms() * per_sm * 8;
-                int64_t c = (target + groups - 1) / groups;
-                const int64_t max_c = (n + 4095) / 4096;
-                chunks = (int)std::max<int64_t>(1, std::min<int64_t>(std::max<int64_t>(c, 32), max_c));
-            }
+            if (chunks <= 0) chunks = auto_chunks(n, groups, fsmem > 110 * 1024 ? 1 : 2);
             const int64_t chunk = (n + chunks - 1) / chunks;
             kern<<<dim3(chunks, groups, 1), sh.threads, fsmem, s>>>(pos, n, chunk, e, gpc, mass);
             return cudaGetLastError();
@@ -445,14 +461,7 @@ static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, const int
         const int groups = (e.k + gpc - 1) / gpc;
         const int slabs = 1 << (cells_lg - slab_lg);
         int chunks = sh.chunks;
-        if (chunks <= 0) {
-            // a few waves of CTAs; each extra chunk costs one histogram flush
-            const int per_sm = smem > 110 * 1024 ? 1 : 2;
-            const int64_t target = (int64_t)num_sms() * per_sm * 8;
-            int64_t c = (target + (int64_t)groups * slabs - 1) / ((int64_t)groups * slabs);
-            const int64_t max_c = (n + 4095) / 4096;
-            chunks = (int)std::max<int64_t>(1, std::min<int64_t>(std::max<int64_t>(c, 32), max_c));
-        }
+        if (chunks <= 0) chunks = auto_chunks(n, groups * slabs, smem > 110 * 1024 ? 1 : 2);
         const int64_t chunk = (n + chunks - 1) / chunks;
         dim3 grid(chunks, groups, slabs);
         kern<<<grid, sh.threads, smem, s>>>(pos, perm, n, chunk, e, gpc, slab_lg, mass);

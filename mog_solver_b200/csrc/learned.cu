@@ -12,7 +12,7 @@
 //             to its cells' centres, the per-grid force spread, the mean
 //             cell mass and two scalars (see gather_features);
 //   inference the standardised features through the network on the tensor
-//             cores (mma.sync m16n8k16 BF16, FP32 accumulate): a warp's 32
+//             cores (mma.sync m16n8k16 FP16, FP32 accumulate): a warp's 32
 //             particles are two m16 tiles; the accumulator fragment of one
 //             layer is, pair of n-tiles by pair, exactly the A fragment of
 //             the next;
@@ -29,7 +29,7 @@
 //   W1[64][12] b1[64] W2[64][64] b2[64] W3[3][64] b3[3]
 #include <algorithm>
 #include <cstdint>
-#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include "mog_internal.h"
 
@@ -53,20 +53,8 @@ __device__ __forceinline__ float gelu_grad(float x) {
     const float t = tanhf(u);
     return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * 0.7978845608028654f * (1.0f + 0.134145f * x2);
 }
-// Inference: the hardware tanh approximation (relative error ~2^-11, far
-// below BF16 resolution).
-__device__ __forceinline__ float tanh_fast(float x) {
-    float y;
-    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-__device__ __forceinline__ float gelu_fast(float x) {
-    const float u = 0.7978845608028654f * (x + 0.044715f * x * x * x);
-    return 0.5f * x * (1.0f + tanh_fast(u));
-}
-
 // ---------------------------------------------------------------------------
-// BF16 weight fragments for mma.sync.m16n8k16 (B operand, "col" layout):
+// FP16 weight fragments for mma.sync.m16n8k16 (B operand, "col" layout):
 // for k-step ks and n-tile nt, lane l holds
 //   b0 = {W[n][k], W[n][k+1]} with n = nt*8 + l/4, k = ks*16 + 2*(l%4)
 //   b1 = the same at k + 8.
@@ -74,9 +62,24 @@ __device__ __forceinline__ float gelu_fast(float x) {
 constexpr int kFrag1 = 1 * 8, kFrag2 = 4 * 8, kFrag3 = 4 * 1;  // (k-steps x n-tiles)
 constexpr int kFragTotal = (kFrag1 + kFrag2 + kFrag3) * 32;     // uint2 per model
 
-__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
-    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+__device__ __forceinline__ uint32_t pack_h2(float lo, float hi) {
+    const __half2 v = __floats2half2_rn(lo, hi);
     return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+// GELU (tanh form) of two FP32 pre-activations, evaluated in packed FP16
+// (x * (c + c*0.044715*x^2), tanh.approx.f16x2, 0.5x + 0.5x*t): the result
+// is the FP16 A operand of the next layer either way.
+__device__ __forceinline__ uint32_t gelu_h2(float a, float b, uint32_t c1, uint32_t c2, uint32_t half) {
+    const uint32_t x = pack_h2(a, b);
+    uint32_t x2, p, u, t, hx, y;
+    asm("mul.rn.f16x2 %0, %1, %1;" : "=r"(x2) : "r"(x));
+    asm("fma.rn.f16x2 %0, %1, %2, %3;" : "=r"(p) : "r"(x2), "r"(c2), "r"(c1));
+    asm("mul.rn.f16x2 %0, %1, %2;" : "=r"(u) : "r"(x), "r"(p));
+    asm("tanh.approx.f16x2 %0, %1;" : "=r"(t) : "r"(u));
+    asm("mul.rn.f16x2 %0, %1, %2;" : "=r"(hx) : "r"(x), "r"(half));
+    asm("fma.rn.f16x2 %0, %1, %2, %1;" : "=r"(y) : "r"(hx), "r"(t));
+    return y;
 }
 
 __global__ void pack_fragments_kernel(const float* __restrict__ params, uint2* __restrict__ frags) {
@@ -98,13 +101,13 @@ __global__ void pack_fragments_kernel(const float* __restrict__ params, uint2* _
     const int n = nt * 8 + (lane >> 2);
     const int k = ks * 16 + 2 * (lane & 3);
     auto w = [&](int nn, int kk) { return (nn < out && kk < in) ? Wm[nn * in + kk] : 0.f; };
-    frags[t] = make_uint2(pack_bf16(w(n, k), w(n, k + 1)), pack_bf16(w(n, k + 8), w(n, k + 9)));
+    frags[t] = make_uint2(pack_h2(w(n, k), w(n, k + 1)), pack_h2(w(n, k + 8), w(n, k + 9)));
 }
 
-__device__ __forceinline__ void mma_bf16(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2,
+__device__ __forceinline__ void mma_f16(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2,
                                          uint32_t a3, uint32_t b0, uint32_t b1) {
     asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
+        "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 "
         "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
         : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
         : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
@@ -113,16 +116,6 @@ __device__ __forceinline__ void mma_bf16(float (&d)[4], uint32_t a0, uint32_t a1
 // ---------------------------------------------------------------------------
 // Fused gather + features + inference + update.
 
-// Per-grid data of the gather, staged in shared memory once per CTA: the
-// pre-scaled index rows (t = A c + b, cell = floor(t), as cell_fast) and
-// the grid's rotation times the voxel size (world-frame offset from the
-// cell centre = (h M) (t - floor(t) - 1/2)).
-struct GridRows {
-    float4 r[3];
-    float m[9];
-    float pad[3];
-};
-static_assert(sizeof(GridRows) == 96, "GridRows layout");
 
 // Statistics of one particle over the k grids.
 //
@@ -149,54 +142,92 @@ struct Features {
     float ex, ey, ez;  // a - Fbar
 };
 
-template <int IDX>
-__device__ __forceinline__ void gather_features(const float4* __restrict__ W,
-                                                const GridRows* __restrict__ xf, const Ensemble& e,
-                                                const IndexParams& ip, float cx, float cy, float cz,
-                                                float inv_fs, float rho_ref, Features& out) {
-    const int G3 = 1 << (3 * e.lg);
-    const uint32_t mask = (1u << e.lg) - 1u;
-    const float h = e.voxel;
-    float sx = 0.f, sy = 0.f, sz = 0.f;            // plain sum, update.glsl order
-    float qx = 0.f, qy = 0.f, qz = 0.f;            // sum F^2 per component
-    float dx = 0.f, dy = 0.f, dz = 0.f;            // sum d
+__device__ __forceinline__ GridRows make_grid_rows_dev(const Ensemble& e, int i) {
+    const FastXf x = e.fast[i];
+    const float* R = e.rot12 + 12 * i;
+    GridRows g;
+    g.r[0] = x.row[0];
+    g.r[1] = x.row[1];
+    g.r[2] = x.row[2];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+#pragma unroll
+        for (int b = 0; b < 3; ++b) g.m[3 * a + b] = R[4 * a + b] * e.voxel;
+        g.o[a] = -0.5f * (g.m[3 * a] + g.m[3 * a + 1] + g.m[3 * a + 2]);
+    }
+    return g;
+}
+
+// Running sums of one particle over the grids.
+struct GatherAcc {
+    float sx = 0.f, sy = 0.f, sz = 0.f;  // plain sum, update.glsl order
+    float qx = 0.f, qy = 0.f, qz = 0.f;  // sum F^2 per component
+    float dx = 0.f, dy = 0.f, dz = 0.f;  // sum d
     float dxx = 0.f, dxy = 0.f, dxz = 0.f, dyy = 0.f, dyz = 0.f, dzz = 0.f;
     float fxdx = 0.f, fxdy = 0.f, fxdz = 0.f, fydx = 0.f, fydy = 0.f, fydz = 0.f,
-          fzdx = 0.f, fzdy = 0.f, fzdz = 0.f;      // sum F d^T
+          fzdx = 0.f, fzdy = 0.f, fzdz = 0.f;  // sum F d^T
     float rho = 0.f;
-#pragma unroll 4
-    for (int i = 0; i < e.k; ++i) {
-        const GridRows& x = xf[i];
-        const float tx = __fmaf_rn(x.r[0].z, cz, __fmaf_rn(x.r[0].y, cy, __fmaf_rn(x.r[0].x, cx, x.r[0].w)));
-        const float ty = __fmaf_rn(x.r[1].z, cz, __fmaf_rn(x.r[1].y, cy, __fmaf_rn(x.r[1].x, cx, x.r[1].w)));
-        const float tz = __fmaf_rn(x.r[2].z, cz, __fmaf_rn(x.r[2].y, cy, __fmaf_rn(x.r[2].x, cx, x.r[2].w)));
-        uint32_t c;
-        if (IDX == 0)
-            c = floor_mod_pow2(tx, mask) | (floor_mod_pow2(ty, mask) << e.lg) |
-                (floor_mod_pow2(tz, mask) << (2 * e.lg));
-        else
-            c = cell_exact(e.rot12 + 12 * i, e.off4 + 4 * i, cx, cy, cz, ip);
-        const float4 f = __ldg(W + (size_t)i * G3 + c);
-        sx = __fadd_rn(sx, f.x);
-        sy = __fadd_rn(sy, f.y);
-        sz = __fadd_rn(sz, f.z);
-        qx += f.x * f.x;
-        qy += f.y * f.y;
-        qz += f.z * f.z;
-        const float gx = tx - floorf(tx) - 0.5f, gy = ty - floorf(ty) - 0.5f,
-                    gz = tz - floorf(tz) - 0.5f;
-        const float wx = x.m[0] * gx + x.m[1] * gy + x.m[2] * gz;
-        const float wy = x.m[3] * gx + x.m[4] * gy + x.m[5] * gz;
-        const float wz = x.m[6] * gx + x.m[7] * gy + x.m[8] * gz;
-        dx += wx; dy += wy; dz += wz;
-        dxx += wx * wx; dxy += wx * wy; dxz += wx * wz;
-        dyy += wy * wy; dyz += wy * wz; dzz += wz * wz;
-        fxdx += f.x * wx; fxdy += f.x * wy; fxdz += f.x * wz;
-        fydx += f.y * wx; fydy += f.y * wy; fydz += f.y * wz;
-        fzdx += f.z * wx; fzdy += f.z * wy; fzdz += f.z * wz;
-        rho += f.w;
+};
+
+// Grid i's contribution.  IDX 0: FAST cells (LG = log2 g, or 0 for a
+// run-time g); IDX 1: EXACT cells.  In FAST mode the floor that picks the
+// cell also gives the offset: r = t + 1.5*2^23 rounded down holds floor(t)
+// in its low bits (the cell, as floor_mod_pow2) and r - 1.5*2^23 = floor(t)
+// exactly, for |t| < 2^22.
+template <int IDX, int LG>
+__device__ __forceinline__ void gather_one(const GridRows& x, int i, const float4* __restrict__ W,
+                                           const Ensemble& e, const IndexParams& ip, float cx,
+                                           float cy, float cz, GatherAcc& a) {
+    const int lg = LG > 0 ? LG : e.lg;
+    const int G3 = 1 << (3 * lg);
+    const uint32_t mask = (1u << lg) - 1u;
+    constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23
+    const float tx = __fmaf_rn(x.r[0].z, cz, __fmaf_rn(x.r[0].y, cy, __fmaf_rn(x.r[0].x, cx, x.r[0].w)));
+    const float ty = __fmaf_rn(x.r[1].z, cz, __fmaf_rn(x.r[1].y, cy, __fmaf_rn(x.r[1].x, cx, x.r[1].w)));
+    const float tz = __fmaf_rn(x.r[2].z, cz, __fmaf_rn(x.r[2].y, cy, __fmaf_rn(x.r[2].x, cx, x.r[2].w)));
+    uint32_t c;
+    float gx, gy, gz;  // frac(t)
+    if (IDX == 0) {
+        const float rx = __fadd_rd(tx, kMagic), ry = __fadd_rd(ty, kMagic), rz = __fadd_rd(tz, kMagic);
+        c = (__float_as_uint(rx) & mask) | ((__float_as_uint(ry) & mask) << lg) |
+            ((__float_as_uint(rz) & mask) << (2 * lg));
+        gx = tx - (rx - kMagic);
+        gy = ty - (ry - kMagic);
+        gz = tz - (rz - kMagic);
+    } else {
+        c = cell_exact(e.rot12 + 12 * i, e.off4 + 4 * i, cx, cy, cz, ip);
+        gx = tx - floorf(tx);
+        gy = ty - floorf(ty);
+        gz = tz - floorf(tz);
     }
-    const float kf = (float)e.k, ik = 1.0f / kf;
+    const float4 f = __ldg(W + (size_t)i * G3 + c);
+    a.sx = __fadd_rn(a.sx, f.x);
+    a.sy = __fadd_rn(a.sy, f.y);
+    a.sz = __fadd_rn(a.sz, f.z);
+    a.qx += f.x * f.x;
+    a.qy += f.y * f.y;
+    a.qz += f.z * f.z;
+    const float wx = x.m[0] * gx + x.m[1] * gy + x.m[2] * gz + x.o[0];
+    const float wy = x.m[3] * gx + x.m[4] * gy + x.m[5] * gz + x.o[1];
+    const float wz = x.m[6] * gx + x.m[7] * gy + x.m[8] * gz + x.o[2];
+    a.dx += wx; a.dy += wy; a.dz += wz;
+    a.dxx += wx * wx; a.dxy += wx * wy; a.dxz += wx * wz;
+    a.dyy += wy * wy; a.dyz += wy * wz; a.dzz += wz * wz;
+    a.fxdx += f.x * wx; a.fxdy += f.x * wy; a.fxdz += f.x * wz;
+    a.fydx += f.y * wx; a.fydy += f.y * wy; a.fydz += f.y * wz;
+    a.fzdx += f.z * wx; a.fzdy += f.z * wy; a.fzdz += f.z * wz;
+    a.rho += f.w;
+}
+
+// Features from the sums over k grids of voxel size h.
+__device__ __forceinline__ void finish_features(const GatherAcc& a, int k, float h, float inv_fs,
+                                                float rho_ref, Features& out) {
+    const float sx = a.sx, sy = a.sy, sz = a.sz, qx = a.qx, qy = a.qy, qz = a.qz;
+    const float dx = a.dx, dy = a.dy, dz = a.dz, dxx = a.dxx, dxy = a.dxy, dxz = a.dxz,
+                dyy = a.dyy, dyz = a.dyz, dzz = a.dzz;
+    const float fxdx = a.fxdx, fxdy = a.fxdy, fxdz = a.fxdz, fydx = a.fydx, fydy = a.fydy,
+                fydz = a.fydz, fzdx = a.fzdx, fzdy = a.fzdy, fzdz = a.fzdz, rho = a.rho;
+    const float kf = (float)k, ik = 1.0f / kf;
     const float mx = __fdiv_rn(sx, kf), my = __fdiv_rn(sy, kf), mz = __fdiv_rn(sz, kf);
     const float ax_ = dx * ik, ay_ = dy * ik, az_ = dz * ik;  // dbar
     const float ridge = 1e-3f * h * h;
@@ -242,21 +273,24 @@ __device__ __forceinline__ void mlp_tile(const uint2* __restrict__ sf, const flo
                                          uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
                                          int lane, float (&y)[4]) {
     const int tg = lane & 3;
+    const uint32_t c1 = pack_h2(0.7978845608028654f, 0.7978845608028654f);
+    const uint32_t c2 = pack_h2(0.7978845608028654f * 0.044715f, 0.7978845608028654f * 0.044715f);
+    const uint32_t hf = pack_h2(0.5f, 0.5f);
     float h[8][4];
 #pragma unroll
     for (int nt = 0; nt < 8; ++nt) {
         const float b0 = sb[nt * 8 + 2 * tg], b1 = sb[nt * 8 + 2 * tg + 1];
         h[nt][0] = b0; h[nt][1] = b1; h[nt][2] = b0; h[nt][3] = b1;
         const uint2 w = sf[(0 * 8 + nt) * 32 + lane];
-        mma_bf16(h[nt], a0, a1, a2, a3, w.x, w.y);
+        mma_f16(h[nt], a0, a1, a2, a3, w.x, w.y);
     }
     uint32_t A[4][4];
 #pragma unroll
     for (int ks = 0; ks < 4; ++ks) {
-        A[ks][0] = pack_bf16(gelu_fast(h[2 * ks][0]), gelu_fast(h[2 * ks][1]));
-        A[ks][1] = pack_bf16(gelu_fast(h[2 * ks][2]), gelu_fast(h[2 * ks][3]));
-        A[ks][2] = pack_bf16(gelu_fast(h[2 * ks + 1][0]), gelu_fast(h[2 * ks + 1][1]));
-        A[ks][3] = pack_bf16(gelu_fast(h[2 * ks + 1][2]), gelu_fast(h[2 * ks + 1][3]));
+        A[ks][0] = gelu_h2(h[2 * ks][0], h[2 * ks][1], c1, c2, hf);
+        A[ks][1] = gelu_h2(h[2 * ks][2], h[2 * ks][3], c1, c2, hf);
+        A[ks][2] = gelu_h2(h[2 * ks + 1][0], h[2 * ks + 1][1], c1, c2, hf);
+        A[ks][3] = gelu_h2(h[2 * ks + 1][2], h[2 * ks + 1][3], c1, c2, hf);
     }
 #pragma unroll
     for (int nt = 0; nt < 8; ++nt) {
@@ -265,15 +299,15 @@ __device__ __forceinline__ void mlp_tile(const uint2* __restrict__ sf, const flo
 #pragma unroll
         for (int ks = 0; ks < 4; ++ks) {
             const uint2 w = sf[(kFrag1 + ks * 8 + nt) * 32 + lane];
-            mma_bf16(h[nt], A[ks][0], A[ks][1], A[ks][2], A[ks][3], w.x, w.y);
+            mma_f16(h[nt], A[ks][0], A[ks][1], A[ks][2], A[ks][3], w.x, w.y);
         }
     }
 #pragma unroll
     for (int ks = 0; ks < 4; ++ks) {
-        A[ks][0] = pack_bf16(gelu_fast(h[2 * ks][0]), gelu_fast(h[2 * ks][1]));
-        A[ks][1] = pack_bf16(gelu_fast(h[2 * ks][2]), gelu_fast(h[2 * ks][3]));
-        A[ks][2] = pack_bf16(gelu_fast(h[2 * ks + 1][0]), gelu_fast(h[2 * ks + 1][1]));
-        A[ks][3] = pack_bf16(gelu_fast(h[2 * ks + 1][2]), gelu_fast(h[2 * ks + 1][3]));
+        A[ks][0] = gelu_h2(h[2 * ks][0], h[2 * ks][1], c1, c2, hf);
+        A[ks][1] = gelu_h2(h[2 * ks][2], h[2 * ks][3], c1, c2, hf);
+        A[ks][2] = gelu_h2(h[2 * ks + 1][0], h[2 * ks + 1][1], c1, c2, hf);
+        A[ks][3] = gelu_h2(h[2 * ks + 1][2], h[2 * ks + 1][3], c1, c2, hf);
     }
     y[0] = sb[2 * kH + 2 * tg];
     y[1] = sb[2 * kH + 2 * tg + 1];
@@ -282,7 +316,7 @@ __device__ __forceinline__ void mlp_tile(const uint2* __restrict__ sf, const flo
 #pragma unroll
     for (int ks = 0; ks < 4; ++ks) {
         const uint2 w = sf[(kFrag1 + kFrag2 + ks) * 32 + lane];
-        mma_bf16(y, A[ks][0], A[ks][1], A[ks][2], A[ks][3], w.x, w.y);
+        mma_f16(y, A[ks][0], A[ks][1], A[ks][2], A[ks][3], w.x, w.y);
     }
 }
 
@@ -297,31 +331,30 @@ static_assert(kLearnedFixedSmem % 16 == 0, "GridRows must stay 16-byte aligned")
 // OUT 1: the corrected force into out4;  OUT 2: the features (out4 = Fbar,
 // feat = 16 floats: 0-11 standardised, 12-14 a - Fbar, 15 zero), no network.
 // One thread per particle; a persistent grid walks blocks of kLT particles.
-template <int IDX, int OUT>
+// The grid rows of a K-grid ensemble as a launch parameter: read through
+// the constant cache with compile-time offsets once the grid loop is
+// unrolled, so the gather issues no shared-memory loads for them.
+template <int K>
+struct GridTable {
+    GridRows r[K > 0 ? K : 1];
+};
+
+// K > 0: k == K and the rows come from `tab`; K == 0: any k, rows staged in
+// shared memory.
+template <int IDX, int LG, int OUT, int K>
 __global__ void __launch_bounds__(kLT, 2) learned_kernel(
     float4* __restrict__ pos, float4* __restrict__ vel, int64_t n, const float4* __restrict__ W,
     Ensemble e, ModelNorm norm, const uint2* __restrict__ frags, const float* __restrict__ params,
-    float dt, float damp, float4* __restrict__ out4, float* __restrict__ feat_out) {
+    float dt, float damp, float4* __restrict__ out4, float* __restrict__ feat_out,
+    const __grid_constant__ GridTable<K> tab) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint2* sf = reinterpret_cast<uint2*>(smem_raw);
     float* sb = reinterpret_cast<float*>(sf + kFragTotal);
     uint32_t* sA = reinterpret_cast<uint32_t*>(sb + 2 * kH + 8);
     float4* sY = reinterpret_cast<float4*>(sA + kLW * 32 * kARow);
     GridRows* xf = reinterpret_cast<GridRows*>(smem_raw + kLearnedFixedSmem);
-    const float h = e.voxel;
-    for (int i = threadIdx.x; i < e.k; i += kLT) {
-        const FastXf x = e.fast[i];
-        const float* R = e.rot12 + 12 * i;
-        GridRows g;
-        g.r[0] = x.row[0];
-        g.r[1] = x.row[1];
-        g.r[2] = x.row[2];
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-            for (int b = 0; b < 3; ++b) g.m[3 * a + b] = R[4 * a + b] * h;
-        g.pad[0] = g.pad[1] = g.pad[2] = 0.f;
-        xf[i] = g;
+    if constexpr (K == 0) {
+        for (int i = threadIdx.x; i < e.k; i += kLT) xf[i] = make_grid_rows_dev(e, i);
     }
     if (OUT != 2) {
         for (int i = threadIdx.x; i < kFragTotal; i += kLT) sf[i] = frags[i];
@@ -345,12 +378,20 @@ __global__ void __launch_bounds__(kLT, 2) learned_kernel(
         const float4 P = live ? pos[p] : make_float4(0.f, 0.f, 0.f, 0.f);
         const float cx = __fsub_rn(P.x, ip.half_l), cy = __fsub_rn(P.y, ip.half_l),
                     cz = __fsub_rn(P.z, ip.half_l);
+        GatherAcc acc;
+        if constexpr (K > 0) {
+#pragma unroll
+            for (int i = 0; i < K; ++i) gather_one<IDX, LG>(tab.r[i], i, W, e, ip, cx, cy, cz, acc);
+        } else {
+#pragma unroll 4
+            for (int i = 0; i < e.k; ++i) gather_one<IDX, LG>(xf[i], i, W, e, ip, cx, cy, cz, acc);
+        }
         Features F;
-        gather_features<IDX>(W, xf, e, ip, cx, cy, cz, inv_fs, norm.rho_ref, F);
+        finish_features(acc, e.k, e.voxel, inv_fs, norm.rho_ref, F);
         float z[kIn];
 #pragma unroll
         for (int j = 0; j < kIn; ++j) z[j] = (F.f[j] - norm.mu[j]) * norm.inv_sigma[j];
-        if (OUT == 2) {
+        if constexpr (OUT == 2) {
             if (live) {
                 out4[p] = make_float4(F.mx, F.my, F.mz, 0.f);
                 float4* o = reinterpret_cast<float4*>(feat_out + (size_t)p * 16);
@@ -359,58 +400,62 @@ __global__ void __launch_bounds__(kLT, 2) learned_kernel(
                 o[2] = make_float4(z[8], z[9], z[10], z[11]);
                 o[3] = make_float4(F.ex, F.ey, F.ez, 0.f);
             }
-            continue;
-        }
-        // this particle's row of the warp's A tile (BF16 pairs; columns 12-15 zero)
-        uint4* row = reinterpret_cast<uint4*>(A + lane * kARow);
-        row[0] = make_uint4(pack_bf16(z[0], z[1]), pack_bf16(z[2], z[3]), pack_bf16(z[4], z[5]),
-                            pack_bf16(z[6], z[7]));
-        row[1] = make_uint4(pack_bf16(z[8], z[9]), pack_bf16(z[10], z[11]), 0u, 0u);
-        __syncwarp();
+        } else {
+            // this particle's row of the warp's A tile (FP16 pairs, clamped to the
+            // FP16 range; columns 12-15 zero)
+            float zc[kIn];
 #pragma unroll
-        for (int m = 0; m < 2; ++m) {
-            const uint32_t* Am = A + 16 * m * kARow;
-            float y[4];
-            mlp_tile(sf, sb, Am[g * kARow + tg], Am[(g + 8) * kARow + tg], Am[g * kARow + tg + 4],
-                     Am[(g + 8) * kARow + tg + 4], lane, y);
-            // y: rows g and g+8, outputs 2tg and 2tg+1
-            if (tg == 0) {
-                Y[16 * m + g].x = y[0];
-                Y[16 * m + g].y = y[1];
-                Y[16 * m + g + 8].x = y[2];
-                Y[16 * m + g + 8].y = y[3];
-            } else if (tg == 1) {
-                Y[16 * m + g].z = y[0];
-                Y[16 * m + g + 8].z = y[2];
+            for (int j = 0; j < kIn; ++j) zc[j] = fminf(fmaxf(z[j], -60000.f), 60000.f);
+            uint4* row = reinterpret_cast<uint4*>(A + lane * kARow);
+            row[0] = make_uint4(pack_h2(zc[0], zc[1]), pack_h2(zc[2], zc[3]), pack_h2(zc[4], zc[5]),
+                                pack_h2(zc[6], zc[7]));
+            row[1] = make_uint4(pack_h2(zc[8], zc[9]), pack_h2(zc[10], zc[11]), 0u, 0u);
+            __syncwarp();
+#pragma unroll
+            for (int m = 0; m < 2; ++m) {
+                const uint32_t* Am = A + 16 * m * kARow;
+                float y[4];
+                mlp_tile(sf, sb, Am[g * kARow + tg], Am[(g + 8) * kARow + tg], Am[g * kARow + tg + 4],
+                         Am[(g + 8) * kARow + tg + 4], lane, y);
+                // y: rows g and g+8, outputs 2tg and 2tg+1
+                if (tg == 0) {
+                    Y[16 * m + g].x = y[0];
+                    Y[16 * m + g].y = y[1];
+                    Y[16 * m + g + 8].x = y[2];
+                    Y[16 * m + g + 8].y = y[3];
+                } else if (tg == 1) {
+                    Y[16 * m + g].z = y[0];
+                    Y[16 * m + g + 8].z = y[2];
+                }
             }
+            __syncwarp();
+            const float4 yv = Y[lane];
+            __syncwarp();  // the next block of particles reuses A and Y
+            if (!live) continue;
+            float bx = F.mx, by = F.my, bz = F.mz;
+            if (norm.base_mode != 0.f) {
+                bx += F.ex;
+                by += F.ey;
+                bz += F.ez;
+            }
+            const float ax = bx + norm.out_scale * yv.x, ay = by + norm.out_scale * yv.y,
+                        az = bz + norm.out_scale * yv.z;
+            if (OUT == 1) {
+                out4[p] = make_float4(ax, ay, az, 0.f);
+                continue;
+            }
+            // update.glsl:83-89 with the corrected force
+            const float4 V = vel[p];
+            const float vx = __fmul_rn(__fsub_rn(V.x, __fmul_rn(ax, dt)), damp);
+            const float vy = __fmul_rn(__fsub_rn(V.y, __fmul_rn(ay, dt)), damp);
+            const float vz = __fmul_rn(__fsub_rn(V.z, __fmul_rn(az, dt)), damp);
+            const float px = glsl_mod(__fadd_rn(P.x, __fmul_rn(vx, dt)), e.world);
+            const float py = glsl_mod(__fadd_rn(P.y, __fmul_rn(vy, dt)), e.world);
+            const float pz = glsl_mod(__fadd_rn(P.z, __fmul_rn(vz, dt)), e.world);
+            if (!(isfinite(px) && isfinite(py) && isfinite(pz))) bad |= 1u;  // MOG_FLAG_NONFINITE
+            pos[p] = make_float4(px, py, pz, P.w);
+            vel[p] = make_float4(vx, vy, vz, 0.f);
         }
-        __syncwarp();
-        const float4 yv = Y[lane];
-        __syncwarp();  // the next block of particles reuses A and Y
-        if (!live) continue;
-        float bx = F.mx, by = F.my, bz = F.mz;
-        if (norm.base_mode != 0.f) {
-            bx += F.ex;
-            by += F.ey;
-            bz += F.ez;
-        }
-        const float ax = bx + norm.out_scale * yv.x, ay = by + norm.out_scale * yv.y,
-                    az = bz + norm.out_scale * yv.z;
-        if (OUT == 1) {
-            out4[p] = make_float4(ax, ay, az, 0.f);
-            continue;
-        }
-        // update.glsl:83-89 with the corrected force
-        const float4 V = vel[p];
-        const float vx = __fmul_rn(__fsub_rn(V.x, __fmul_rn(ax, dt)), damp);
-        const float vy = __fmul_rn(__fsub_rn(V.y, __fmul_rn(ay, dt)), damp);
-        const float vz = __fmul_rn(__fsub_rn(V.z, __fmul_rn(az, dt)), damp);
-        const float px = glsl_mod(__fadd_rn(P.x, __fmul_rn(vx, dt)), e.world);
-        const float py = glsl_mod(__fadd_rn(P.y, __fmul_rn(vy, dt)), e.world);
-        const float pz = glsl_mod(__fadd_rn(P.z, __fmul_rn(vz, dt)), e.world);
-        if (!(isfinite(px) && isfinite(py) && isfinite(pz))) bad |= 1u;  // MOG_FLAG_NONFINITE
-        pos[p] = make_float4(px, py, pz, P.w);
-        vel[p] = make_float4(vx, vy, vz, 0.f);
     }
     if (bad) raise_flags(e.flags, bad);
 }
@@ -562,14 +607,29 @@ cudaError_t launch_density_w(const Ensemble& e, void* mass, float4* W, cudaStrea
     return cudaGetLastError();
 }
 
+GridRows make_grid_rows(const FastXf& fast, const float* R, float voxel) {
+    GridRows g;
+    g.r[0] = fast.row[0];
+    g.r[1] = fast.row[1];
+    g.r[2] = fast.row[2];
+    for (int a = 0; a < 3; ++a) {
+        for (int b = 0; b < 3; ++b) g.m[3 * a + b] = R[4 * a + b] * voxel;
+        g.o[a] = -0.5f * (g.m[3 * a] + g.m[3 * a + 1] + g.m[3 * a + 2]);
+    }
+    return g;
+}
+
 namespace {
-template <int IDX, int OUT>
-cudaError_t launch_learned_t(const Ensemble& e, float4* pos, float4* vel, int64_t n,
-                             const float4* W, const ModelNorm& norm, const void* frags,
+template <int IDX, int LG, int OUT, int K>
+cudaError_t launch_learned_t(const Ensemble& e, const GridRows* rows, float4* pos, float4* vel,
+                             int64_t n, const float4* W, const ModelNorm& norm, const void* frags,
                              const float* params, float dt, float damp, float4* out4, float* feat,
                              cudaStream_t s) {
-    auto kern = learned_kernel<IDX, OUT>;
-    const size_t smem = kLearnedFixedSmem + sizeof(GridRows) * (size_t)e.k;
+    auto kern = learned_kernel<IDX, LG, OUT, K>;
+    GridTable<K> tab{};
+    if (K > 0)
+        for (int i = 0; i < K; ++i) tab.r[i] = rows[i];
+    const size_t smem = kLearnedFixedSmem + (K > 0 ? 0 : sizeof(GridRows) * (size_t)e.k);
     cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess) return err;
     int per_sm = 0;
@@ -577,31 +637,38 @@ cudaError_t launch_learned_t(const Ensemble& e, float4* pos, float4* vel, int64_
     if (err != cudaSuccess) return err;
     const int64_t blocks = std::min<int64_t>((n + kLT - 1) / kLT, (int64_t)num_sms() * std::max(per_sm, 1));
     kern<<<(unsigned)blocks, kLT, smem, s>>>(pos, vel, n, W, e, norm, static_cast<const uint2*>(frags),
-                                            params, dt, damp, out4, feat);
+                                            params, dt, damp, out4, feat, tab);
     return cudaGetLastError();
 }
 
-template <int IDX>
-cudaError_t launch_learned_i(int out_mode, const Ensemble& e, float4* pos, float4* vel, int64_t n,
-                             const float4* W, const ModelNorm& norm, const void* frags,
-                             const float* params, float dt, float damp, float4* out4, float* feat,
-                             cudaStream_t s) {
+template <int IDX, int LG, int K>
+cudaError_t launch_learned_i(int out_mode, const Ensemble& e, const GridRows* rows, float4* pos,
+                             float4* vel, int64_t n, const float4* W, const ModelNorm& norm,
+                             const void* frags, const float* params, float dt, float damp,
+                             float4* out4, float* feat, cudaStream_t s) {
     switch (out_mode) {
-        case 0: return launch_learned_t<IDX, 0>(e, pos, vel, n, W, norm, frags, params, dt, damp, out4, feat, s);
-        case 1: return launch_learned_t<IDX, 1>(e, pos, vel, n, W, norm, frags, params, dt, damp, out4, feat, s);
-        default: return launch_learned_t<IDX, 2>(e, pos, vel, n, W, norm, frags, params, dt, damp, out4, feat, s);
+        case 0: return launch_learned_t<IDX, LG, 0, K>(e, rows, pos, vel, n, W, norm, frags, params, dt, damp, out4, feat, s);
+        case 1: return launch_learned_t<IDX, LG, 1, K>(e, rows, pos, vel, n, W, norm, frags, params, dt, damp, out4, feat, s);
+        default: return launch_learned_t<IDX, LG, 2, K>(e, rows, pos, vel, n, W, norm, frags, params, dt, damp, out4, feat, s);
     }
 }
 }  // namespace
 
-cudaError_t launch_learned(int out_mode, const Ensemble& e, float4* pos, float4* vel, int64_t n,
-                           const float4* W, const ModelNorm& norm, const void* frags,
-                           const float* params, float dt, float damp, float4* out4, float* feat,
-                           cudaStream_t s) {
+cudaError_t launch_learned(int out_mode, const Ensemble& e, const GridRows* rows, float4* pos,
+                           float4* vel, int64_t n, const float4* W, const ModelNorm& norm,
+                           const void* frags, const float* params, float dt, float damp,
+                           float4* out4, float* feat, cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
-    if (e.index_mode == 0)
-        return launch_learned_i<0>(out_mode, e, pos, vel, n, W, norm, frags, params, dt, damp, out4, feat, s);
-    return launch_learned_i<1>(out_mode, e, pos, vel, n, W, norm, frags, params, dt, damp, out4, feat, s);
+#define MOG_LEARNED(IDX, LG, K) \
+    return launch_learned_i<IDX, LG, K>(out_mode, e, rows, pos, vel, n, W, norm, frags, params, dt, damp, out4, feat, s)
+    // the k = 32, g = 16 FAST ensemble (the cheap ensemble the models are
+    // trained for) gets its rows as launch parameters and an unrolled loop
+    if (e.index_mode == 0 && e.lg == 4 && e.k == 32 && rows) MOG_LEARNED(0, 4, 32);
+    if (e.index_mode != 0) MOG_LEARNED(1, 0, 0);
+    if (e.lg == 4) MOG_LEARNED(0, 4, 0);
+    if (e.lg == 3) MOG_LEARNED(0, 3, 0);
+    MOG_LEARNED(0, 0, 0);
+#undef MOG_LEARNED
 }
 
 cudaError_t launch_pack_fragments(const float* params, void* frags, cudaStream_t s) {

@@ -168,6 +168,7 @@ struct mog_handle {
     int sort_every = 0;          // re-order every this many steps (0 = never)
     uint64_t step_count = 0;     // steps issued (decides when to re-order)
     std::vector<GraphEntry> graphs;
+    std::vector<mog::GridRows> rows;  // learned-gather rows of the k grids (host)
 };
 
 namespace {
@@ -400,6 +401,8 @@ int mog_create(const mog_config* cfg, const float* rot12, const float* off4, mog
             rows[4 * r + 3] = (float)((half_l - (double)off4[4 * i + r]) / hv);
         }
     }
+    h->rows.resize(k);
+    for (int i = 0; i < k; ++i) h->rows[i] = mog::make_grid_rows(fast[i], rot12 + 12 * i, e.voxel);
     const size_t cells = (size_t)e.cells();
     const size_t g3 = (size_t)g * g * g;
     auto fail_free = [&](cudaError_t err, const char* where) {
@@ -831,7 +834,7 @@ static int run_learned(mog_handle* h, const mog_model* m, int out_mode, float* p
                        int64_t n, float dt, float4* out4, float* feat, cudaStream_t s) {
     int rc = run_learned_grids(h, reinterpret_cast<const float4*>(pos4), n, s);
     if (rc) return rc;
-    cudaError_t err = mog::launch_learned(out_mode, h->e, reinterpret_cast<float4*>(pos4),
+    cudaError_t err = mog::launch_learned(out_mode, h->e, h->rows.data(), reinterpret_cast<float4*>(pos4),
                                           reinterpret_cast<float4*>(vel4), n, h->d_force, m->norm,
                                           m->d_frags, m->d_params, dt, h->cfg.damping, out4, feat, s);
     if (err != cudaSuccess) return cuda_fail(err, "learned kernel");

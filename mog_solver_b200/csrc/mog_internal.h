@@ -136,6 +136,20 @@ struct ModelNorm {
 };
 
 
+// Per-grid data of the learned gather: the pre-scaled index rows (t = A c
+// + b, cell = floor(t), as cell_fast), the grid's rotation times the voxel
+// size and the cell-centre shift, so that the world-frame offset from the
+// cell centre is
+//     (h M) (t - floor(t) - 1/2) = (h M) frac(t) + o,  o = -(h M) (1/2, 1/2, 1/2).
+struct GridRows {
+    float4 r[3];
+    float m[9];
+    float o[3];
+};
+static_assert(sizeof(GridRows) == 96, "GridRows layout");
+// rows[i] for grid i of an ensemble (host), from its FAST rows and rotation.
+GridRows make_grid_rows(const FastXf& fast, const float* rot12, float voxel);
+
 int mlp_param_count();
 size_t mlp_fragment_bytes();
 size_t mlp_train_smem();
@@ -144,10 +158,12 @@ size_t mlp_train_smem();
 // (out_mode 0: step pos/vel; 1: corrected force into out4; 2: features,
 // out4 = plain mean force, feat = n x 16).
 cudaError_t launch_density_w(const Ensemble& e, void* mass, float4* W, cudaStream_t s);
-cudaError_t launch_learned(int out_mode, const Ensemble& e, float4* pos, float4* vel, int64_t n,
-                           const float4* W, const ModelNorm& norm, const void* frags,
-                           const float* params, float dt, float damp, float4* out4, float* feat,
-                           cudaStream_t s);
+// rows: the ensemble's k GridRows in host memory (they travel in the launch
+// parameters when k is one of the compiled ensemble sizes).
+cudaError_t launch_learned(int out_mode, const Ensemble& e, const GridRows* rows, float4* pos,
+                           float4* vel, int64_t n, const float4* W, const ModelNorm& norm,
+                           const void* frags, const float* params, float dt, float damp,
+                           float4* out4, float* feat, cudaStream_t s);
 cudaError_t launch_pack_fragments(const float* params, void* frags, cudaStream_t s);
 cudaError_t launch_mlp_train_step(const float* feat, const float* target, const int* idx,
                                   int batch, float* params, float* partial, float* loss_partial,

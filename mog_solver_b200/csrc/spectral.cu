@@ -232,6 +232,143 @@ __global__ void __launch_bounds__(G * G, (G == 16 ? 2 : 1))
 }
 
 // ---------------------------------------------------------------------
+// Fused path, g = 8 and 16: 3 g^2 threads per pair of grids.  The forward
+// transform (one complex field) runs on the first g^2 threads; the Green's
+// multiply and the inverse transforms run one gradient field per third of
+// the threads; the epilogue stores with consecutive threads on consecutive
+// cells.  The arithmetic of every line is that of spectral_fused_kernel.
+template <int G, typename Acc, bool WORLD, bool ZERO>
+__global__ void __launch_bounds__(3 * G * G, (G == 16 ? 1 : 4))
+    spectral_fused3_kernel(Acc* __restrict__ mass, float4* __restrict__ force, Ensemble e) {
+    constexpr int P = G + 1, BUF = G * G * P, G3 = G * G * G, L = G * G;
+    extern __shared__ float2 sm[];
+    __shared__ float Rs[2][12];
+    float2* S0 = sm;
+    const int t = threadIdx.x;
+    const int f = t / L;  // gradient field of this thread in the inverse passes
+    const int l = t % L;  // line within a pass
+    const int ga = 2 * blockIdx.x, gb = ga + 1;
+    const bool hasb = gb < e.k;
+    if (blockIdx.x == 0 && t == 0 && ZERO) check_mass_total(e);
+    if (WORLD && t < 24) Rs[t / 12][t % 12] = (t < 12 || hasb) ? __ldg(e.rot12 + 12 * ga + t) : 0.f;
+
+    // forward, x axis: line = row (y, z)
+    if (f == 0) {
+        const int y = l % G, z = l / G;
+        const size_t row = (size_t)(z * G + y) * G;
+        Acc* ra = mass + (size_t)ga * G3 + row;
+        Acc* rb = mass + (size_t)gb * G3 + row;
+        float2 v[G];
+#pragma unroll
+        for (int x = 0; x < G; ++x) {
+            v[x].x = load_mass(ra + x, e.inv_scale);
+            v[x].y = hasb ? load_mass(rb + x, e.inv_scale) : 0.f;
+        }
+        if (ZERO) {
+#pragma unroll
+            for (int x = 0; x < G; ++x) {
+                ra[x] = 0;
+                if (hasb) rb[x] = 0;
+            }
+        }
+        fft_reg<G, false>(v);
+#pragma unroll
+        for (int x = 0; x < G; ++x) S0[(z * G + y) * P + x] = v[x];
+    }
+    __syncthreads();
+    // forward, y axis: line = column (x, z)
+    if (f == 0) {
+        const int x = l % G, z = l / G;
+        float2 v[G];
+#pragma unroll
+        for (int y = 0; y < G; ++y) v[y] = S0[(z * G + y) * P + x];
+        fft_reg<G, false>(v);
+#pragma unroll
+        for (int y = 0; y < G; ++y) S0[(z * G + y) * P + x] = v[y];
+    }
+    __syncthreads();
+    // forward, z axis: line = column (kx, ky)
+    const int kx = l % G, ky = l / G;
+    if (f == 0) {
+        float2 v[G];
+#pragma unroll
+        for (int z = 0; z < G; ++z) v[z] = S0[(z * G + ky) * P + kx];
+        fft_reg<G, false>(v);
+#pragma unroll
+        for (int z = 0; z < G; ++z) S0[(z * G + ky) * P + kx] = v[z];
+    }
+    __syncthreads();
+    // Green's factor and gradient of field f from X^(k) and X^(-k), inverse z
+    {
+        const float kxn = (kx == G / 2) ? 0.f : e.ktab[kx];
+        const float kyn = (ky == G / 2) ? 0.f : e.ktab[ky];
+        const int xm = (G - kx) & (G - 1), ym = (G - ky) & (G - 1);
+        float2 v[G];
+#pragma unroll
+        for (int kz = 0; kz < G; ++kz) {
+            const float2 own = S0[(kz * G + ky) * P + kx];
+            const float2 mir = S0[(((G - kz) & (G - 1)) * G + ym) * P + xm];
+            const float gk = __ldg(e.green + (kz * G + ky) * G + kx);
+            const float kzn = (kz == G / 2) ? 0.f : __ldg(e.ktab + kz);
+            const Bins b = gradient_bins(own, mir, gk, kxn, kyn, kzn);
+            v[kz] = f == 0 ? b.z1 : (f == 1 ? b.z2 : b.z3);
+        }
+        fft_reg<G, true>(v);
+        __syncthreads();  // every thread has read X^ before field 0 overwrites it
+        float2* S = sm + f * BUF;
+#pragma unroll
+        for (int z = 0; z < G; ++z) S[(z * G + ky) * P + kx] = v[z];
+    }
+    __syncthreads();
+    // inverse, y axis of field f: line = column (x, z)
+    {
+        const int x = l % G, z = l / G;
+        float2* S = sm + f * BUF;
+        float2 v[G];
+#pragma unroll
+        for (int y = 0; y < G; ++y) v[y] = S[(z * G + y) * P + x];
+        fft_reg<G, true>(v);
+#pragma unroll
+        for (int y = 0; y < G; ++y) S[(z * G + y) * P + x] = v[y];
+    }
+    __syncthreads();
+    // inverse, x axis of field f: line = row (y, z)
+    {
+        const int y = l % G, z = l / G;
+        float2* S = sm + f * BUF;
+        float2 v[G];
+#pragma unroll
+        for (int x = 0; x < G; ++x) v[x] = S[(z * G + y) * P + x];
+        fft_reg<G, true>(v);
+#pragma unroll
+        for (int x = 0; x < G; ++x) S[(z * G + y) * P + x] = v[x];
+    }
+    __syncthreads();
+    // epilogue (pack.glsl:20-29): grid a from Z1 and Re Z2, grid b from Z3
+    // and Im Z2; 1/g^3 of pack.glsl:20-21 (exact)
+    const float invn = 1.0f / (float)G3;
+    const int cells = (hasb ? 2 : 1) * G3;
+    for (int idx = t; idx < cells; idx += 3 * L) {
+        const int gsel = idx / G3, c = idx % G3;
+        const int srow = (c / G) * P + (c % G);
+        const float2 z2 = sm[BUF + srow];
+        float fx, fy, fz;
+        if (gsel == 0) {
+            const float2 z1 = sm[srow];
+            fx = (e.alias_xz ? z2.x : z1.x) * invn;
+            fy = z1.y * invn;
+            fz = z2.x * invn;
+        } else {
+            const float2 z3 = sm[2 * BUF + srow];
+            fx = (e.alias_xz ? z2.y : z3.x) * invn;
+            fy = z3.y * invn;
+            fz = z2.y * invn;
+        }
+        force[(size_t)(ga + gsel) * G3 + c] = make_out(WORLD, Rs[gsel], fx, fy, fz);
+    }
+}
+
+// ---------------------------------------------------------------------
 // Multi-pass path (any g up to 64, used for g >= 32): the same algebra,
 // with each axis pass a separate launch over global (L2-resident) scratch.
 
@@ -357,18 +494,26 @@ cudaError_t run_fused(const Ensemble& e, Acc* mass, float4* force, bool world, b
                       cudaStream_t s) {
     const int pairs = (e.k + 1) / 2;
     const size_t smem = (size_t)3 * G * G * (G + 1) * sizeof(float2);
-    auto pick = [&](auto kern) -> cudaError_t {
+    auto pick = [&](auto kern, int threads) -> cudaError_t {
         cudaError_t err =
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (err != cudaSuccess) return err;
-        kern<<<pairs, G * G, smem, s>>>(mass, force, e);
+        kern<<<pairs, threads, smem, s>>>(mass, force, e);
         return cudaGetLastError();
     };
+    if constexpr (G >= 8) {
+        constexpr int T = 3 * G * G;
+        if (world)
+            return zero ? pick(spectral_fused3_kernel<G, Acc, true, true>, T)
+                        : pick(spectral_fused3_kernel<G, Acc, true, false>, T);
+        return zero ? pick(spectral_fused3_kernel<G, Acc, false, true>, T)
+                    : pick(spectral_fused3_kernel<G, Acc, false, false>, T);
+    }
     if (world)
-        return zero ? pick(spectral_fused_kernel<G, Acc, true, true>)
-                    : pick(spectral_fused_kernel<G, Acc, true, false>);
-    return zero ? pick(spectral_fused_kernel<G, Acc, false, true>)
-                : pick(spectral_fused_kernel<G, Acc, false, false>);
+        return zero ? pick(spectral_fused_kernel<G, Acc, true, true>, G * G)
+                    : pick(spectral_fused_kernel<G, Acc, true, false>, G * G);
+    return zero ? pick(spectral_fused_kernel<G, Acc, false, true>, G * G)
+                : pick(spectral_fused_kernel<G, Acc, false, false>, G * G);
 }
 
 template <int G, typename Acc>

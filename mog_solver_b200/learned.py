@@ -6,7 +6,7 @@ statistics of the cheap ensemble.  Everything runs in libmog.so:
 
 * ``mog_features``       deposit + solve + feature gather of the cheap ensemble;
 * ``mog_model_train_step`` fused FP32 forward/backward + Adam (deterministic);
-* ``mog_learned_step``   features + BF16 tensor-core inference + leapfrog.
+* ``mog_learned_step``   features + FP16 tensor-core inference + leapfrog, one fused kernel.
 
 ``generate_dataset`` builds training pairs from the method itself (features
 of a k = 32 ensemble, targets = k = 240 force minus the k = 32 mean and

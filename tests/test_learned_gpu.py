@@ -1,5 +1,5 @@
 """The learned correction on the GPU against the FP64 oracle (oracle/mlp.py):
-gradients of the fused training kernel, one Adam step, BF16 tensor-core
+gradients of the fused training kernel, one Adam step, FP16 tensor-core
 inference, the feature gather, and what training gains over the plain
 cheap ensemble."""
 import numpy as np
@@ -64,7 +64,7 @@ def test_adam_step_matches_fp64():
 
 
 @pytest.mark.parametrize("base_mode", [0, 1])
-def test_bf16_inference_matches_fp64_forward(base_mode):
+def test_fp16_inference_matches_fp64_forward(base_mode):
     from mog_solver_b200 import Simulation
     from mog_solver_b200.learned import features, learned_forces
 
@@ -85,7 +85,7 @@ def test_bf16_inference_matches_fp64_forward(base_mode):
         base = base + feat.cpu().numpy()[:, 12:15].astype(np.float64)
     ref = base + y
     got = acc.cpu().numpy()[:, :3].astype(np.float64)
-    # BF16 weights and activations: a few parts in 1e3 of the output scale
+    # FP16 weights and activations, GELU in FP16: a few parts in 1e3 of the output scale
     assert np.abs(got - ref).max() <= 2e-2 * max(1.0, np.abs(y).max())
     assert pl.relative_l2(got - base, y) < 2e-2
     sim.close()
