@@ -307,6 +307,24 @@ int mog_learned_forces(mog_handle* h, const mog_model* m, const float* pos4, flo
                        int64_t n, void* stream);
 int mog_learned_step(mog_handle* h, const mog_model* m, float* pos4, float* vel4, int64_t n,
                      float dt_eff, void* stream);
+/*
+ * mog_learned_step with CUDA events between its kernels: phase_ms[0..3]
+ * receive the device time of the deposit, the solve, the cell-mass pass and
+ * the fused gather + network + update kernel.  Synchronises the stream.
+ */
+int mog_learned_step_profiled(mog_handle* h, const mog_model* m, float* pos4, float* vel4,
+                              int64_t n, float dt_eff, float* phase_ms, void* stream);
+/*
+ * Statistics of the particles of the last mog_learned_step, summed per CTA
+ * by that step's own kernel in a fixed order: out2[0] = the mean over
+ * particles of their grid-to-grid force spread (mean of features 6-8
+ * before standardisation), out2[1] = the mean of their ensemble-mean force
+ * magnitude (feature 10); both in units of the model's force_scale.  The
+ * variance gate of the learned path compares their ratio with the one of
+ * its training data.  Zeros before the first learned step.  Synchronises
+ * the stream.
+ */
+int mog_learned_spread(mog_handle* h, double* out2, void* stream);
 
 /* Human-readable text for a status code, and the calling thread's last
  * error message. */

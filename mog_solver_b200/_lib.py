@@ -50,6 +50,7 @@ EXPORTS = (
     "mog_batch_create", "mog_batch_step", "mog_batch_destroy",
     "mog_model_create", "mog_model_destroy", "mog_model_set", "mog_model_get",
     "mog_model_train_step", "mog_features", "mog_learned_forces", "mog_learned_step",
+    "mog_learned_step_profiled", "mog_learned_spread",
     "mog_strerror", "mog_last_error", "mog_version",
 )
 
@@ -138,6 +139,8 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.mog_features.argtypes = [P, P, P, I64, P, P, P]
     lib.mog_learned_forces.argtypes = [P, P, P, P, I64, P]
     lib.mog_learned_step.argtypes = [P, P, P, P, I64, F, P]
+    lib.mog_learned_step_profiled.argtypes = [P, P, P, P, I64, F, ctypes.POINTER(ctypes.c_float), P]
+    lib.mog_learned_spread.argtypes = [P, ctypes.POINTER(ctypes.c_double), P]
     lib.mog_strerror.argtypes = [I]
     lib.mog_strerror.restype = ctypes.c_char_p
     lib.mog_last_error.argtypes = []

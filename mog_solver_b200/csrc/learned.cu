@@ -346,7 +346,7 @@ __global__ void __launch_bounds__(kLT, 2) learned_kernel(
     float4* __restrict__ pos, float4* __restrict__ vel, int64_t n, const float4* __restrict__ W,
     Ensemble e, ModelNorm norm, const uint2* __restrict__ frags, const float* __restrict__ params,
     float dt, float damp, float4* __restrict__ out4, float* __restrict__ feat_out,
-    const __grid_constant__ GridTable<K> tab) {
+    float* __restrict__ spread_part, const __grid_constant__ GridTable<K> tab) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint2* sf = reinterpret_cast<uint2*>(smem_raw);
     float* sb = reinterpret_cast<float*>(sf + kFragTotal);
@@ -371,6 +371,8 @@ __global__ void __launch_bounds__(kLT, 2) learned_kernel(
     float4* Y = sY + warp * 32;
     const float inv_fs = 1.0f / norm.force_scale;
     unsigned bad = 0;
+    float spread = 0.f;  // sum over this thread's particles of mean(features 6-8)
+    float fmag = 0.f;    // sum over this thread's particles of feature 10
     for (int64_t base = (int64_t)blockIdx.x * kLT; base < n; base += (int64_t)gridDim.x * kLT) {
         if (base + warp * 32 >= n) continue;  // whole warp past the end (warp-uniform)
         const int64_t p = base + threadIdx.x;
@@ -432,6 +434,8 @@ __global__ void __launch_bounds__(kLT, 2) learned_kernel(
             const float4 yv = Y[lane];
             __syncwarp();  // the next block of particles reuses A and Y
             if (!live) continue;
+            spread += (F.f[6] + F.f[7] + F.f[8]) * (1.0f / 3.0f);
+            fmag += F.f[10];
             float bx = F.mx, by = F.my, bz = F.mz;
             if (norm.base_mode != 0.f) {
                 bx += F.ex;
@@ -458,13 +462,43 @@ __global__ void __launch_bounds__(kLT, 2) learned_kernel(
         }
     }
     if (bad) raise_flags(e.flags, bad);
+    if (spread_part) {
+        // per-CTA sums in a fixed order (warp shuffles, then thread 0)
+        __shared__ float red[2][kLW];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            spread += __shfl_xor_sync(kFull, spread, o);
+            fmag += __shfl_xor_sync(kFull, fmag, o);
+        }
+        if (lane == 0) {
+            red[0][warp] = spread;
+            red[1][warp] = fmag;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            float a = 0.f, b = 0.f;
+#pragma unroll
+            for (int w = 0; w < kLW; ++w) {
+                a += red[0][w];
+                b += red[1][w];
+            }
+            spread_part[2 * blockIdx.x] = a;
+            spread_part[2 * blockIdx.x + 1] = b;
+        }
+    }
 }
 
 // Cell masses into the .w lane of the world-frame force grid (which the
 // world-frame solve leaves 0), clearing the mass grid for the next deposit.
+// Also checks the deposit's fixed-point total for overflow and clears it,
+// as the solve does when it clears the mass grid itself.
 template <typename Acc>
 __global__ void density_w_kernel(Acc* __restrict__ mass, float4* __restrict__ W, int64_t cells,
-                                 float inv_scale) {
+                                 float inv_scale, double* mass_total, unsigned* flags) {
+    if (blockIdx.x == 0 && threadIdx.x == 0 && mass_total) {
+        if (*mass_total >= 18446744073709551616.0) atomicOr(flags, 2u);  // MOG_FLAG_OVERFLOW
+        *mass_total = 0.0;
+    }
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cells;
          i += (int64_t)gridDim.x * blockDim.x) {
         reinterpret_cast<float*>(W + i)[3] = mass_value(mass[i], inv_scale);
@@ -601,9 +635,10 @@ cudaError_t launch_density_w(const Ensemble& e, void* mass, float4* W, cudaStrea
     const unsigned blocks = (unsigned)std::min<int64_t>((cells + 255) / 256, (int64_t)num_sms() * 8);
     if (e.mass_mode == 0)
         density_w_kernel<<<blocks, 256, 0, s>>>(static_cast<unsigned long long*>(mass), W, cells,
-                                                e.inv_scale);
+                                                e.inv_scale, e.mass_total, e.flags);
     else
-        density_w_kernel<<<blocks, 256, 0, s>>>(static_cast<unsigned*>(mass), W, cells, e.inv_scale);
+        density_w_kernel<<<blocks, 256, 0, s>>>(static_cast<unsigned*>(mass), W, cells, e.inv_scale,
+                                                nullptr, e.flags);
     return cudaGetLastError();
 }
 
@@ -623,7 +658,7 @@ namespace {
 template <int IDX, int LG, int OUT, int K>
 cudaError_t launch_learned_t(const Ensemble& e, const GridRows* rows, float4* pos, float4* vel,
                              int64_t n, const float4* W, const ModelNorm& norm, const void* frags,
-                             const float* params, float dt, float damp, float4* out4, float* feat,
+                             const float* params, float dt, float damp, LearnedOut& out,
                              cudaStream_t s) {
     auto kern = learned_kernel<IDX, LG, OUT, K>;
     GridTable<K> tab{};
@@ -635,9 +670,11 @@ cudaError_t launch_learned_t(const Ensemble& e, const GridRows* rows, float4* po
     int per_sm = 0;
     err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kLT, smem);
     if (err != cudaSuccess) return err;
-    const int64_t blocks = std::min<int64_t>((n + kLT - 1) / kLT, (int64_t)num_sms() * std::max(per_sm, 1));
+    int64_t blocks = std::min<int64_t>((n + kLT - 1) / kLT, (int64_t)num_sms() * std::max(per_sm, 1));
+    if (out.spread && blocks > out.spread_cap) blocks = out.spread_cap;
+    out.blocks = (int)blocks;
     kern<<<(unsigned)blocks, kLT, smem, s>>>(pos, vel, n, W, e, norm, static_cast<const uint2*>(frags),
-                                            params, dt, damp, out4, feat, tab);
+                                            params, dt, damp, out.out4, out.feat, out.spread, tab);
     return cudaGetLastError();
 }
 
@@ -645,11 +682,11 @@ template <int IDX, int LG, int K>
 cudaError_t launch_learned_i(int out_mode, const Ensemble& e, const GridRows* rows, float4* pos,
                              float4* vel, int64_t n, const float4* W, const ModelNorm& norm,
                              const void* frags, const float* params, float dt, float damp,
-                             float4* out4, float* feat, cudaStream_t s) {
+                             LearnedOut& out, cudaStream_t s) {
     switch (out_mode) {
-        case 0: return launch_learned_t<IDX, LG, 0, K>(e, rows, pos, vel, n, W, norm, frags, params, dt, damp, out4, feat, s);
-        case 1: return launch_learned_t<IDX, LG, 1, K>(e, rows, pos, vel, n, W, norm, frags, params, dt, damp, out4, feat, s);
-        default: return launch_learned_t<IDX, LG, 2, K>(e, rows, pos, vel, n, W, norm, frags, params, dt, damp, out4, feat, s);
+        case 0: return launch_learned_t<IDX, LG, 0, K>(e, rows, pos, vel, n, W, norm, frags, params, dt, damp, out, s);
+        case 1: return launch_learned_t<IDX, LG, 1, K>(e, rows, pos, vel, n, W, norm, frags, params, dt, damp, out, s);
+        default: return launch_learned_t<IDX, LG, 2, K>(e, rows, pos, vel, n, W, norm, frags, params, dt, damp, out, s);
     }
 }
 }  // namespace
@@ -657,10 +694,11 @@ cudaError_t launch_learned_i(int out_mode, const Ensemble& e, const GridRows* ro
 cudaError_t launch_learned(int out_mode, const Ensemble& e, const GridRows* rows, float4* pos,
                            float4* vel, int64_t n, const float4* W, const ModelNorm& norm,
                            const void* frags, const float* params, float dt, float damp,
-                           float4* out4, float* feat, cudaStream_t s) {
+                           LearnedOut& out, cudaStream_t s) {
+    out.blocks = 0;
     if (n <= 0) return cudaSuccess;
 #define MOG_LEARNED(IDX, LG, K) \
-    return launch_learned_i<IDX, LG, K>(out_mode, e, rows, pos, vel, n, W, norm, frags, params, dt, damp, out4, feat, s)
+    return launch_learned_i<IDX, LG, K>(out_mode, e, rows, pos, vel, n, W, norm, frags, params, dt, damp, out, s)
     // the k = 32, g = 16 FAST ensemble (the cheap ensemble the models are
     // trained for) gets its rows as launch parameters and an unrolled loop
     if (e.index_mode == 0 && e.lg == 4 && e.k == 32 && rows) MOG_LEARNED(0, 4, 32);

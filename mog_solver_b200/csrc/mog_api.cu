@@ -169,6 +169,10 @@ struct mog_handle {
     uint64_t step_count = 0;     // steps issued (decides when to re-order)
     std::vector<GraphEntry> graphs;
     std::vector<mog::GridRows> rows;  // learned-gather rows of the k grids (host)
+    float* d_spread = nullptr;        // per-CTA (spread, |mean force|) sums of the last learned step
+    int spread_cap = 0;               // CTAs d_spread has room for
+    int spread_blocks = 0;
+    int64_t spread_n = 0;
 };
 
 namespace {
@@ -326,7 +330,7 @@ void release(mog_handle* h) {
     h->graphs.clear();
     void* ptrs[] = {h->d_rot12, h->d_off4, h->d_fast, h->d_green, h->d_ktab, h->d_conv,
                     h->d_flags, h->d_total, h->d_mass, h->d_force, h->d_force2, h->d_scratch,
-                    h->d_diag, h->d_perm, h->d_sort, h->d_pos_s};
+                    h->d_diag, h->d_perm, h->d_sort, h->d_pos_s, h->d_spread};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }
@@ -436,6 +440,8 @@ int mog_create(const mog_config* cfg, const float* rot12, const float* off4, mog
         h->perm_cap = cfg->num_particles;
     }
     ALLOC(h->d_sort, mog::sort_scratch_bytes());
+    h->spread_cap = mog::num_sms() * 8;
+    ALLOC(h->d_spread, sizeof(float) * 2 * h->spread_cap);
 #undef ALLOC
     cudaError_t err;
     std::vector<float> convk = conv_kernel_table(g, hv);
@@ -814,30 +820,43 @@ const char* mog_version(void) { return "mog-b200 0.1 (sm_100a)"; }
 
 // Deposit + world-frame solve with the handle's ensemble, then the cell
 // masses into the force grid's .w lane (the mass grid is cleared for the
-// next deposit).  The learned kernel gathers everything from that grid.
-static int run_learned_grids(mog_handle* h, const float4* pos, int64_t n, cudaStream_t s) {
+// next deposit), then the learned kernel, which gathers everything from
+// that grid.  ev (optional): 5 events recorded around the deposit, the
+// solve, the cell-mass pass and the learned kernel.
+static int run_learned(mog_handle* h, const mog_model* m, int out_mode, float* pos4, float* vel4,
+                       int64_t n, float dt, float4* out4, float* feat, cudaStream_t s,
+                       cudaEvent_t* ev = nullptr) {
     const mog::Ensemble& e = h->e;
-    cudaError_t err = mog::launch_deposit(e, pos, nullptr, n, false, h->d_mass, h->dshape, s);
+    const float4* pos = reinterpret_cast<const float4*>(pos4);
+    cudaError_t err = ev ? cudaEventRecord(ev[0], s) : cudaSuccess;
+    if (!err) err = mog::launch_deposit(e, pos, nullptr, n, false, h->d_mass, h->dshape, s);
     if (err != cudaSuccess) return cuda_fail(err, "deposit");
+    if (ev && (err = cudaEventRecord(ev[1], s))) return cuda_fail(err, "event");
     if (h->cfg.solver == MOG_SOLVER_FFT)
         err = mog::launch_spectral(e, h->d_mass, h->d_force, true, false, h->d_scratch, s);
     else
         err = mog::launch_convolution(e, h->d_mass, h->d_force, true, false, s);
     if (err != cudaSuccess) return cuda_fail(err, "solve");
+    if (ev && (err = cudaEventRecord(ev[2], s))) return cuda_fail(err, "event");
     err = mog::launch_density_w(e, h->d_mass, h->d_force, s);
     if (err != cudaSuccess) return cuda_fail(err, "cell masses");
-    if (e.mass_mode == 0 && e.mass_total) MOG_CUDA(cudaMemsetAsync(e.mass_total, 0, sizeof(double), s), "clear total");
-    return MOG_OK;
-}
-
-static int run_learned(mog_handle* h, const mog_model* m, int out_mode, float* pos4, float* vel4,
-                       int64_t n, float dt, float4* out4, float* feat, cudaStream_t s) {
-    int rc = run_learned_grids(h, reinterpret_cast<const float4*>(pos4), n, s);
-    if (rc) return rc;
-    cudaError_t err = mog::launch_learned(out_mode, h->e, h->rows.data(), reinterpret_cast<float4*>(pos4),
-                                          reinterpret_cast<float4*>(vel4), n, h->d_force, m->norm,
-                                          m->d_frags, m->d_params, dt, h->cfg.damping, out4, feat, s);
+    if (ev && (err = cudaEventRecord(ev[3], s))) return cuda_fail(err, "event");
+    mog::LearnedOut out;
+    out.out4 = out4;
+    out.feat = feat;
+    if (out_mode == 0) {
+        out.spread = h->d_spread;
+        out.spread_cap = h->spread_cap;
+    }
+    err = mog::launch_learned(out_mode, e, h->rows.data(), reinterpret_cast<float4*>(pos4),
+                              reinterpret_cast<float4*>(vel4), n, h->d_force, m->norm, m->d_frags,
+                              m->d_params, dt, h->cfg.damping, out, s);
     if (err != cudaSuccess) return cuda_fail(err, "learned kernel");
+    if (ev && (err = cudaEventRecord(ev[4], s))) return cuda_fail(err, "event");
+    if (out_mode == 0) {
+        h->spread_blocks = out.blocks;
+        h->spread_n = n;
+    }
     return MOG_OK;
 }
 
@@ -974,6 +993,47 @@ int mog_learned_step(mog_handle* h, const mog_model* m, float* pos4, float* vel4
                           static_cast<cudaStream_t>(stream))))
         return rc;
     ++h->step_count;
+    return MOG_OK;
+}
+
+int mog_learned_step_profiled(mog_handle* h, const mog_model* m, float* pos4, float* vel4,
+                              int64_t n, float dt_eff, float* phase_ms, void* stream) {
+    if (!h || !m || !phase_ms) return fail(MOG_ERR_ARG, "null argument");
+    int rc = check_particles(h, pos4, vel4, n, true);
+    if (rc) return rc;
+    if (!std::isfinite(dt_eff)) return fail(MOG_ERR_ARG, "dt_eff must be finite");
+    if ((rc = set_device(h))) return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaEvent_t ev[5];
+    for (auto& x : ev) MOG_CUDA(cudaEventCreate(&x), "event create");
+    rc = run_learned(h, m, 0, pos4, vel4, n, dt_eff, nullptr, nullptr, s, ev);
+    cudaError_t err = rc ? cudaSuccess : cudaEventSynchronize(ev[4]);
+    for (int i = 0; i < 4 && !rc && !err; ++i) err = cudaEventElapsedTime(&phase_ms[i], ev[i], ev[i + 1]);
+    for (auto& x : ev) cudaEventDestroy(x);
+    if (rc) return rc;
+    if (err) return cuda_fail(err, "profiled learned step");
+    ++h->step_count;
+    return MOG_OK;
+}
+
+int mog_learned_spread(mog_handle* h, double* out2, void* stream) {
+    if (!h || !out2) return fail(MOG_ERR_ARG, "null argument");
+    int rc = set_device(h);
+    if (rc) return rc;
+    out2[0] = out2[1] = 0.0;
+    if (h->spread_blocks <= 0 || h->spread_n <= 0) return MOG_OK;
+    std::vector<float> part(2 * (size_t)h->spread_blocks);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    MOG_CUDA(cudaMemcpyAsync(part.data(), h->d_spread, sizeof(float) * part.size(),
+                             cudaMemcpyDeviceToHost, s), "read spread");
+    MOG_CUDA(cudaStreamSynchronize(s), "sync");
+    double a = 0.0, b = 0.0;
+    for (int i = 0; i < h->spread_blocks; ++i) {
+        a += part[2 * i];
+        b += part[2 * i + 1];
+    }
+    out2[0] = a / (double)h->spread_n;
+    out2[1] = b / (double)h->spread_n;
     return MOG_OK;
 }
 

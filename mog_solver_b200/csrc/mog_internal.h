@@ -158,12 +158,24 @@ size_t mlp_train_smem();
 // (out_mode 0: step pos/vel; 1: corrected force into out4; 2: features,
 // out4 = plain mean force, feat = n x 16).
 cudaError_t launch_density_w(const Ensemble& e, void* mass, float4* W, cudaStream_t s);
+// Outputs of the learned kernel: out4 / feat as out_mode says; spread (if
+// not null, room for 2 * spread_cap floats) receives per-CTA sums of the
+// particles' mean grid-to-grid force spread (mean of features 6-8) and of
+// their mean-force magnitude (feature 10), both in units of the model's
+// force scale, for `blocks` CTAs.
+struct LearnedOut {
+    float4* out4 = nullptr;
+    float* feat = nullptr;
+    float* spread = nullptr;
+    int spread_cap = 0;
+    int blocks = 0;
+};
 // rows: the ensemble's k GridRows in host memory (they travel in the launch
 // parameters when k is one of the compiled ensemble sizes).
 cudaError_t launch_learned(int out_mode, const Ensemble& e, const GridRows* rows, float4* pos,
                            float4* vel, int64_t n, const float4* W, const ModelNorm& norm,
                            const void* frags, const float* params, float dt, float damp,
-                           float4* out4, float* feat, cudaStream_t s);
+                           LearnedOut& out, cudaStream_t s);
 cudaError_t launch_pack_fragments(const float* params, void* frags, cudaStream_t s);
 cudaError_t launch_mlp_train_step(const float* feat, const float* target, const int* idx,
                                   int batch, float* params, float* partial, float* loss_partial,

@@ -232,26 +232,46 @@ def train(model: Model, data: Dataset, steps: int = 2000, batch: int = 8192, lr:
     return history
 
 
+def _gate_stats(feat, norm) -> tuple[float, float]:
+    """(mean spread, mean |mean force|) over particles from a feature pass:
+    features 6-8 and 10 before standardisation, in units of force_scale."""
+    torch = _torch()
+    sd = torch.from_numpy((1.0 / norm[12:24]).astype(np.float64)).to(feat.device)
+    mu = torch.from_numpy(norm[0:12].astype(np.float64)).to(feat.device)
+    raw = feat[:, :12].double() * sd + mu
+    return float(raw[:, 6:9].mean(dim=1).mean().item()), float(raw[:, 10].mean().item())
+
+
 class LearnedSimulation:
     """A cheap ensemble stepped with the learned correction, and the plain
     expensive ensemble as fallback when the variance gate fires.
 
-    Gate: the mean grid-to-grid force spread of the current particles
-    (features 6-8, in units of the model's force scale) exceeds
-    ``gate_factor`` times its training mean.
+    Gate: every ``gate_every`` steps, the relative grid-to-grid force spread
+    of the particles -- their mean force spread over their mean force
+    magnitude, both summed inside the last learned step's own kernel
+    (mog_learned_spread) -- is compared with ``gate_factor`` times the same
+    ratio on the training data (``train_ratio``; by default taken from the
+    model's normalisation offsets of features 6-8 and 10).  When it is
+    above, the fallback ensemble takes the next ``gate_every`` steps, after
+    which a feature pass of the cheap ensemble decides again.
     """
 
     def __init__(self, cheap: Simulation, model: Model, fallback: Simulation | None = None,
-                 spread_train_mean: float | None = None, gate_factor: float = 3.0,
+                 train_ratio: float | None = None, gate_factor: float = 3.0,
                  gate_every: int = 10):
         self.cheap = cheap
         self.model = model
         self.fallback = fallback
-        self.spread_train_mean = spread_train_mean
+        if train_ratio is None:
+            _, norm = model.get()
+            train_ratio = float(np.mean(norm[6:9]) / norm[10]) if norm[10] > 0 else 0.0
+        self.train_ratio = train_ratio
         self.gate_factor = gate_factor
         self.gate_every = gate_every
         self.steps = 0
         self.fallback_steps = 0
+        self.last_ratio = None
+        self._use_fallback = False
 
     @property
     def pos(self):
@@ -261,24 +281,36 @@ class LearnedSimulation:
     def vel(self):
         return self.cheap.vel
 
-    def gate_fires(self) -> bool:
-        if self.fallback is None or self.spread_train_mean is None:
-            return False
-        torch = _torch()
+    def step_stats(self) -> tuple[float, float]:
+        """(mean spread, mean |mean force|) of the last learned step."""
+        out = (ctypes.c_double * 2)()
+        with torch_device(self.cheap.device):
+            _lib.check(_lib.lib().mog_learned_spread(self.cheap.handle, out, self.cheap._stream()),
+                       "mog_learned_spread")
+        return float(out[0]), float(out[1])
+
+    def feature_stats(self) -> tuple[float, float]:
+        """The same statistics from a separate feature pass (mog_features)."""
         _, norm = self.model.get()
-        mean, feat = features(self.cheap, self.model)
-        sd = 1.0 / norm[18:21]
-        spread = (feat[:, SPREAD_COLS].double() * torch.from_numpy(sd.astype(np.float64)).to(feat.device)
-                  + torch.from_numpy(norm[6:9].astype(np.float64)).to(feat.device)).mean()
-        return float(spread.item()) > self.gate_factor * self.spread_train_mean
+        _, feat = features(self.cheap, self.model)
+        return _gate_stats(feat, norm)
+
+    def gate_fires(self) -> bool:
+        if self.fallback is None or not self.train_ratio:
+            return False
+        # after a learned step its kernel has summed the statistics already;
+        # after fallback steps a feature pass measures them
+        spread, fmag = self.feature_stats() if self._use_fallback else self.step_stats()
+        self.last_ratio = spread / fmag if fmag > 0 else float("inf")
+        return self.last_ratio > self.gate_factor * self.train_ratio
 
     def step(self, n_steps: int = 1) -> None:
         torch = _torch()
         lib = _lib.lib()
         for _ in range(n_steps):
-            use_fallback = (self.gate_every and self.steps % self.gate_every == 0
-                            and self.gate_fires())
-            if use_fallback:
+            if self.gate_every and self.steps % self.gate_every == 0 and self.steps > 0:
+                self._use_fallback = self.gate_fires()
+            if self._use_fallback:
                 fb = self.fallback
                 fb.pos, fb.vel = self.cheap.pos, self.cheap.vel
                 fb.step()

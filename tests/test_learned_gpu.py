@@ -159,3 +159,75 @@ def test_training_gains_over_plain_cheap_ensemble():
     small.close()
     big.close()
     model.close()
+
+
+def _clump_sim(k, n=20000, seed=7):
+    from mog_solver_b200 import Simulation, ics
+
+    sim = Simulation({"n_grids": k, "grid_size": 16, "world_size": 100.0, "num_particles": n,
+                      "G": 100.0, "dt": 1e-5, "seed": seed})
+    pos, _ = ics.clumps(n, 100.0, seed=seed)
+    sim.set_particles(pos)
+    return sim
+
+
+def test_step_statistics_match_feature_pass():
+    """The force spread and mean-force magnitude summed inside
+    mog_learned_step are the means that mog_features gives for the same
+    positions."""
+    from mog_solver_b200.learned import LearnedSimulation
+
+    sim = _clump_sim(16)
+    m, _ = _model(5)
+    ls = LearnedSimulation(sim, m)
+    before = ls.feature_stats()
+    ls.step()
+    after = ls.step_stats()
+    assert before[0] > 0 and before[1] > 0
+    for a, b in zip(after, before):
+        assert abs(a - b) <= 1e-4 * b
+    sim.close()
+    m.close()
+
+
+def test_learned_step_profiled_matches_step():
+    import ctypes
+
+    from mog_solver_b200 import _lib
+
+    a, b = _clump_sim(16), _clump_sim(16)
+    m, _ = _model(6)
+    lib = _lib.lib()
+    ph = (ctypes.c_float * 4)()
+    for _ in range(3):
+        _lib.check(lib.mog_learned_step(a.handle, m.handle, a.pos.data_ptr(), a.vel.data_ptr(),
+                                        a.n_particles, 1e-3, None), "step")
+        _lib.check(lib.mog_learned_step_profiled(b.handle, m.handle, b.pos.data_ptr(),
+                                                 b.vel.data_ptr(), b.n_particles, 1e-3, ph, None),
+                   "profiled")
+    torch.cuda.synchronize()
+    assert torch.equal(a.pos, b.pos) and torch.equal(a.vel, b.vel)
+    assert all(v >= 0 for v in ph) and ph[3] > 0
+    a.close()
+    b.close()
+    m.close()
+
+
+@pytest.mark.parametrize("factor,expect_fallback", [(0.0, True), (1e9, False)])
+def test_variance_gate(factor, expect_fallback):
+    """gate_factor 0 hands every step after a gate check to the plain
+    expensive ensemble; a huge factor never does."""
+    from mog_solver_b200.learned import LearnedSimulation
+
+    cheap, big = _clump_sim(16), _clump_sim(64)
+    m, _ = _model(7)
+    ls = LearnedSimulation(cheap, m, fallback=big, train_ratio=1.0, gate_factor=factor,
+                           gate_every=2)
+    ls.step(6)
+    torch.cuda.synchronize()
+    assert ls.steps == 6
+    assert (ls.fallback_steps == 4) if expect_fallback else (ls.fallback_steps == 0)
+    assert torch.isfinite(ls.pos).all()
+    cheap.close()
+    big.close()
+    m.close()
