@@ -1,25 +1,34 @@
 #!/usr/bin/env python
 """Throughput of the Mixture-of-Grids force-and-step path on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2|c1] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W]
+                    [--workload learned|c2|c3|c1] [--impl ours|reference]
 
-Default workload (one GPU): the plain MOG step of the colliding-disk set,
-N = 1,048,576 particles, k = 240 grids of 16^3, G = 100, dt = 1e-5,
-damping 0.999 (seeded synthetic particles: two exponential disks with scale
-radius 8 and sech^2 height 0.5, centres 40 apart, relative speed 5).
+Default workload (``learned``, one GPU): the headline metric, particle-steps/s
+of the learned k = 32 step at the RMS force error of plain k = 240, on the
+colliding-disk set: N = 1,048,576 particles, grids of 16^3, G = 100,
+dt = 1e-5, damping 0.999 (seeded synthetic particles: two exponential disks
+with scale radius 8 and sech^2 height 0.5, centres 40 apart, relative speed
+5).  Before timing, the RMS force error of learned k = 32 and of plain
+k = 240 against the FP64 direct sum is measured on 16,384 sampled particles
+at softening 0, h/4 and h/2 and reported in ``accuracy``.  ``value`` is the
+learned step's particle-steps/s with the particles resident in HBM (device
+time of K steps, CUDA events, L2 flushed between steps); the plain k = 240
+step is timed the same way and reported under ``plain_k240``.  ``e2e`` is
+the learned path through its public API (``LearnedSimulation.step``, with
+its variance gate) with the particles copied from pinned host memory and
+back every step.
 
-One JSON line is printed by rank 0.  ``value`` is particle-steps/s with
-particles resident in HBM (device time of K steps measured with CUDA events,
-L2 flushed between steps); ``e2e`` is the same metric through the public
-``Simulation.step`` call with the particles copied from pinned host memory
-and back every step.  Under torchrun (N > 1) every rank advances its own
-independent simulation of the same size (replicas; the step has no
-cross-GPU exchange in this mode) and the time is the maximum over ranks.
+``c2`` times the plain k = 240 step alone, ``c1`` the small uniform-cube
+case and ``c3`` the batched uneven ensemble.  Under torchrun (N > 1) every
+rank advances its own independent simulation of the same size (replicas;
+the step has no cross-GPU exchange) and the time is the maximum over ranks.
 
 ``--impl reference`` times the reference's own shader code on the host cores
 (the GLSL compute shaders compiled as C++ by oracle/, OpenMP over all
-threads) on a bounded sample of the same workload; without that build it
-falls back to the C/NumPy restatement in oracle/.
+threads) on a bounded sample of the plain k = 240 workload (the reference
+has no learned path); without that build it falls back to the C/NumPy
+restatement in oracle/.
 """
 from __future__ import annotations
 
@@ -41,6 +50,10 @@ METRIC = "particle-steps/s at fixed RMS force error vs FP64 direct sum: learned 
 UNIT = "particle-steps/s"
 
 WORKLOADS = {
+    "learned": dict(desc="learned k=32 vs plain k=240, g=16, two colliding exponential disks, "
+                         "N=1,048,576",
+                    n=1 << 20, k=240, k_small=32, g=16, L=100.0, G=100.0, dt=1e-5, damping=0.999,
+                    ic="disks", seed=1),
     "c2": dict(desc="plain MOG k=240 g=16, two colliding exponential disks, N=1,048,576",
                n=1 << 20, k=240, g=16, L=100.0, G=100.0, dt=1e-5, damping=0.999, ic="disks",
                seed=1),
@@ -120,10 +133,13 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={CLOCK_FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "20"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 5.0:  # sampling has started
+                time.sleep(0.01)
         except (OSError, FileNotFoundError):
             self.proc = None
         return self
@@ -348,6 +364,244 @@ def run_ours(args, w: dict) -> None:
         dist.destroy_process_group()
 
 
+def learned_bytes(n: int, k: int, g: int) -> dict:
+    """Algorithmic bytes per launch of the learned step's kernels.
+
+    deposit: position read (16 N) + one 4-byte cell update per (particle,
+    grid) (4 N k) + mass-grid write (4 k g^3); solve: mass read + force grid
+    written (16 k g^3); cell masses: mass read + w lane written (8 k g^3);
+    learned kernel: position and velocity read and written (64 N) + the
+    force grid read once (16 k g^3) (its per-particle gathers are L1/L2
+    hits).
+    """
+    g3 = g ** 3
+    return {"deposit": 16 * n + 4 * n * k + 4 * k * g3, "solve": 16 * k * g3,
+            "cell_masses": 8 * k * g3, "learned": 64 * n + 16 * k * g3,
+            "step": 64 * n + 4 * n * k + 44 * k * g3}
+
+
+def learned_model():
+    """The committed model (trained on the GPU by train_learned.py), or one
+    trained here on the same recipe when the file is missing."""
+    from mog_solver_b200.learned import Model, generate_dataset, train
+    from mog_solver_b200.train_learned import DEFAULT_MODEL
+
+    if DEFAULT_MODEL.exists():
+        return Model.load(DEFAULT_MODEL), str(DEFAULT_MODEL.relative_to(ROOT))
+    data = generate_dataset()
+    model = Model(seed=0)
+    train(model, data)
+    del data
+    return model, "trained in this run (64 clump sets x 262,144, 2,000 Adam steps)"
+
+
+def run_learned(args, w: dict) -> None:
+    import ctypes
+
+    import torch
+    import torch.distributed as dist
+
+    from mog_solver_b200 import Simulation, _lib, ics
+    from mog_solver_b200.learned import LearnedSimulation, direct_sum, learned_forces, rms_error
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+
+    def cfg(k, seed):
+        return {"n_grids": k, "grid_size": w["g"], "world_size": w["L"], "num_particles": w["n"],
+                "G": w["G"], "dt": w["dt"], "damping": w["damping"], "solver": "fft", "seed": seed}
+
+    cheap = Simulation(cfg(w["k_small"], 1000), device=dev)
+    big = Simulation(cfg(w["k"], 2000), device=dev)
+    pos, vel = ics.two_disks(w["n"], w["L"], seed=w["seed"] + rank, g_eff=big.effective_g())
+    cheap.set_particles(pos, vel)
+    big.set_particles(pos, vel)
+    model, model_src = learned_model()
+    n = cheap.n_particles
+    lib = _lib.lib()
+
+    # accuracy against the FP64 direct sum (untimed)
+    h = w["L"] / w["g"]
+    tid = torch.from_numpy(np.random.default_rng(0).choice(n, 16384, replace=False)).to(dev)
+    T = cheap.pos[tid].contiguous()
+    f_big = big.forces()[tid]
+    f_learn = learned_forces(cheap, model)[tid]
+    accuracy = {}
+    for name, soft in (("0", 0.0), ("h/4", h / 4), ("h/2", h / 2)):
+        D = direct_sum(T, cheap.pos, w["L"], big.effective_g(), soft)
+        e_l, e_b = rms_error(f_learn, D), rms_error(f_big, D)
+        accuracy[f"soft={name}"] = {"learned_k32": e_l, "plain_k240": e_b, "ratio": e_l / e_b}
+    within = all(v["ratio"] <= 1.10 for v in accuracy.values())
+
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    phase = (ctypes.c_float * 4)()
+    dt_eff = float(w["dt"])
+    p0, v0 = cheap.pos.clone(), cheap.vel.clone()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        sptr = ctypes.c_void_p(stream.cuda_stream)
+        hc, hb, hm = cheap.handle, big.handle, model.handle
+        for _ in range(args.warmup):
+            _lib.check(lib.mog_learned_step(hc, hm, cheap.pos.data_ptr(), cheap.vel.data_ptr(), n,
+                                            dt_eff, sptr), "warmup")
+            _lib.check(lib.mog_step(hb, big.pos.data_ptr(), big.vel.data_ptr(), n, dt_eff, sptr),
+                       "warmup")
+        stream.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        learn_ms, plain_ms = [], []
+        with ClockSampler(local) as clocks:
+            for _ in range(args.steps):
+                flush.zero_()  # evict L2 between timed steps
+                ev0.record(stream)
+                _lib.check(lib.mog_learned_step(hc, hm, cheap.pos.data_ptr(), cheap.vel.data_ptr(),
+                                                n, dt_eff, sptr), "timed learned step")
+                ev1.record(stream)
+                ev1.synchronize()
+                learn_ms.append(ev0.elapsed_time(ev1))
+            torch.cuda.synchronize()
+            barrier()
+            for _ in range(args.steps):
+                flush.zero_()
+                ev0.record(stream)
+                _lib.check(lib.mog_step(hb, big.pos.data_ptr(), big.vel.data_ptr(), n, dt_eff, sptr),
+                           "timed plain step")
+                ev1.record(stream)
+                ev1.synchronize()
+                plain_ms.append(ev0.elapsed_time(ev1))
+        torch.cuda.synchronize()
+        barrier()
+        # per-kernel device times from separate profiled steps (events
+        # between the kernels; not part of the timed region above)
+        learn_ph, plain_ph = [], []
+        for _ in range(min(args.steps, 50)):
+            flush.zero_()
+            _lib.check(lib.mog_learned_step_profiled(hc, hm, cheap.pos.data_ptr(),
+                                                     cheap.vel.data_ptr(), n, dt_eff, phase, sptr),
+                       "profiled learned step")
+            learn_ph.append(list(phase))
+            flush.zero_()
+            _lib.check(lib.mog_step_profiled(hb, big.pos.data_ptr(), big.vel.data_ptr(), n, dt_eff,
+                                             phase, sptr), "profiled plain step")
+            plain_ph.append(list(phase))
+        cheap.check()
+        big.check()
+
+        # end to end through the public API (variance gate every 10 steps),
+        # host buffers every step
+        cheap.pos.copy_(p0)
+        cheap.vel.copy_(v0)
+        ls = LearnedSimulation(cheap, model, fallback=big, gate_every=10)
+        host_pos = torch.empty((n, 4), dtype=torch.float32).pin_memory()
+        host_vel = torch.empty((n, 4), dtype=torch.float32).pin_memory()
+        host_pos.copy_(p0)
+        host_vel.copy_(v0)
+        torch.cuda.synchronize()
+        barrier()
+        e2e_ms = []
+        for _ in range(args.steps):
+            flush.zero_()
+            ev0.record(stream)
+            cheap.pos.copy_(host_pos, non_blocking=True)
+            cheap.vel.copy_(host_vel, non_blocking=True)
+            ls.step()
+            host_pos.copy_(cheap.pos, non_blocking=True)
+            host_vel.copy_(cheap.vel, non_blocking=True)
+            ev1.record(stream)
+            ev1.synchronize()
+            e2e_ms.append(ev0.elapsed_time(ev1))
+        barrier()
+
+    tot = torch.tensor([sum(learn_ms), sum(plain_ms), sum(e2e_ms)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(tot, op=dist.ReduceOp.MAX)
+    t_learn, t_plain, t_e2e = (float(x) for x in tot)
+    value = n * world * args.steps / (t_learn / 1e3)
+    plain_value = n * world * args.steps / (t_plain / 1e3)
+    e2e = n * world * args.steps / (t_e2e / 1e3)
+    lph = np.array(learn_ph).mean(axis=0)
+    pph = np.array(plain_ph).mean(axis=0)
+    lnames = ["deposit", "solve", "cell_masses", "learned"]
+    pnames = ["order", "deposit", "solve", "update"]
+    lb = learned_bytes(n, w["k_small"], w["g"])
+    pb = phase_bytes(w)
+    peaks = measured_peaks()
+    ldom, pdom = int(np.argmax(lph)), int(np.argmax(pph))
+    l_ach = lb[lnames[ldom]] / (lph[ldom] / 1e3) / 1e9
+    p_ach = pb[pnames[pdom]] / (pph[pdom] / 1e3) / 1e9
+    clk = clocks.summary()
+
+    if rank == 0:
+        base = None
+        if world == 1 and not args.no_cpu_baseline:
+            r = cpu_baseline(w)
+            base = {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": r["kind"],
+                    "sample": r["sample"] + "; the reference's plain k=240 step (it has no "
+                                            "learned path)"}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_learn / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded two-disk set)",
+            "config": {"workload": w["desc"], "n": w["n"], "k_small": w["k_small"], "k": w["k"],
+                       "g": w["g"], "G": w["G"], "dt": w["dt"], "damping": w["damping"],
+                       "network": "12-64-64-3 GELU, FP16 tensor-core inference, FP32 features",
+                       "model": model_src, "index_mode": "fast", "mass_mode": "u64 fixed point",
+                       "parallelism": "single GPU" if world == 1 else f"{world} independent replicas",
+                       "l2": "flushed between timed steps (256 MiB write)"},
+            "accuracy": {"judge": "relative RMS force error vs FP64 periodic direct sum, 16,384 "
+                                  "sampled particles, all sources",
+                         **accuracy, "learned_within_10pct_of_plain_k240": within},
+            "plain_k240": {"value": plain_value, "unit": UNIT,
+                           "ms_per_step": t_plain / args.steps,
+                           "phase_ms": {nm: float(v) for nm, v in zip(pnames, pph)},
+                           "speedup_learned_over_plain": value / plain_value,
+                           "roofline": {"bound": "hbm", "kernel": pnames[pdom], "achieved": p_ach,
+                                        "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                                        "frac": p_ach / peaks["hbm_gbs"],
+                                        "algorithmic_bytes": pb[pnames[pdom]],
+                                        "traffic": profiled_traffic(pnames[pdom], "c2")}},
+            "phase_ms": {nm: float(v) for nm, v in zip(lnames, lph)},
+            "roofline": {"bound": "hbm", "kernel": lnames[ldom], "achieved": l_ach,
+                         "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": l_ach / peaks["hbm_gbs"], "peak_source": peaks["source"],
+                         "algorithmic_bytes": lb[lnames[ldom]],
+                         "traffic": profiled_traffic(lnames[ldom], "learned"),
+                         "note": "the fused learned kernel is bound by FP32 instruction issue "
+                                 "(feature statistics over 32 gathered grids), not by HBM"},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 2 * 16 * n,
+                    "d2h_bytes_per_step": 2 * 16 * n, "ms_per_step": t_e2e / args.steps,
+                    "gate": f"variance gate every 10 steps, {ls.fallback_steps} fallback steps, "
+                            f"last relative spread {ls.last_ratio} vs training {ls.train_ratio}"},
+            "gpu_launches": 4 * args.steps,
+            "clocks": clk,
+        }
+        if base is not None:
+            line["cpu_baseline"] = base
+        print(json.dumps(line), flush=True)
+    model.close()
+    cheap.close()
+    big.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def run_batch(args, w: dict) -> None:
     import torch
 
@@ -458,9 +712,9 @@ def run_batch(args, w: dict) -> None:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="learned", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--index-mode", default="fast", choices=["fast", "exact"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -478,6 +732,8 @@ def main() -> None:
         run_reference(args, w)
     elif "sims" in w:
         run_batch(args, w)
+    elif "k_small" in w:
+        run_learned(args, w)
     else:
         run_ours(args, w)
 
