@@ -1,0 +1,52 @@
+"""A few steps of a fixed workload, for running under a profiler.
+
+    python -m mog_solver_b200.profile_step [--path plain|learned] [--steps 6]
+
+plain:   k = 240 grids of 16^3, the colliding-disk set (N = 1,048,576,
+         seeded two exponential disks), mog_step;
+learned: k = 32 grids of 16^3, the same particles, mog_learned_step with the
+         committed model (models/learned_k32_g16.npz).
+Everything is set up first; the steps run back to back on the default
+stream and the status flags are checked at the end.
+"""
+from __future__ import annotations
+
+import argparse
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--path", default="plain", choices=["plain", "learned"])
+    ap.add_argument("--steps", type=int, default=6)
+    ap.add_argument("--n", type=int, default=1 << 20)
+    a = ap.parse_args()
+
+    import torch
+
+    from . import _lib, ics
+    from .learned import Model
+    from .simulation import Simulation
+    from .train_learned import DEFAULT_MODEL
+
+    k, seed = (240, 2000) if a.path == "plain" else (32, 1000)
+    sim = Simulation({"n_grids": k, "grid_size": 16, "world_size": 100.0, "num_particles": a.n,
+                      "G": 100.0, "dt": 1e-5, "damping": 0.999, "seed": seed})
+    pos, vel = ics.two_disks(a.n, 100.0, seed=1, g_eff=sim.effective_g())
+    sim.set_particles(pos, vel)
+    lib = _lib.lib()
+    model = Model.load(DEFAULT_MODEL) if a.path == "learned" else None
+    torch.cuda.synchronize()
+    for _ in range(a.steps):
+        if model is None:
+            _lib.check(lib.mog_step(sim.handle, sim.pos.data_ptr(), sim.vel.data_ptr(), a.n, 1e-5,
+                                    None), "mog_step")
+        else:
+            _lib.check(lib.mog_learned_step(sim.handle, model.handle, sim.pos.data_ptr(),
+                                            sim.vel.data_ptr(), a.n, 1e-5, None), "mog_learned_step")
+    torch.cuda.synchronize()
+    sim.check()
+    print(f"{a.path}: {a.steps} steps of N={a.n}, k={k}: ok")
+
+
+if __name__ == "__main__":
+    main()
