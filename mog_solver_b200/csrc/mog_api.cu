@@ -158,7 +158,8 @@ struct mog_handle {
     void* d_mass = nullptr;      // k g^3 (u64 or u32)
     float4* d_force = nullptr;   // k g^3 world-frame forces
     float4* d_force2 = nullptr;  // stage-update staging (lazy)
-    void* d_scratch = nullptr;   // spectral scratch (g >= 32)
+    void* d_scratch = nullptr;   // spectral scratch (g >= 32, or tensor-core DFT passes)
+    void* d_dft = nullptr;       // DFT matrices of the tensor-core passes
     double* d_diag = nullptr;    // diagnostics partials + result
     int* d_perm = nullptr;       // spatial order of the particles (slot -> particle)
     float4* d_pos_s = nullptr;   // positions in spatial order (refreshed every step)
@@ -330,7 +331,7 @@ void release(mog_handle* h) {
     h->graphs.clear();
     void* ptrs[] = {h->d_rot12, h->d_off4, h->d_fast, h->d_green, h->d_ktab, h->d_conv,
                     h->d_flags, h->d_total, h->d_mass, h->d_force, h->d_force2, h->d_scratch,
-                    h->d_diag, h->d_perm, h->d_sort, h->d_pos_s, h->d_spread};
+                    h->d_diag, h->d_perm, h->d_sort, h->d_pos_s, h->d_spread, h->d_dft};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }
@@ -363,8 +364,9 @@ int mog_create(const mog_config* cfg, const float* rot12, const float* off4, mog
     *out = nullptr;
     int rc = validate(*cfg);
     if (rc) return rc;
-    if (cfg->dft_prec == MOG_DFT_TC_BF16X3)
-        return fail(MOG_ERR_UNSUPPORTED, "tensor-core DFT precision is not built in this library");
+    if (cfg->dft_prec == MOG_DFT_TC_BF16X3 &&
+        (cfg->solver != MOG_SOLVER_FFT || (cfg->grid_size != 16 && cfg->grid_size != 32)))
+        return fail(MOG_ERR_UNSUPPORTED, "tensor-core DFT precision needs the fft solver and grid_size 16 or 32");
     for (int i = 0; i < cfg->n_grids * 12; ++i)
         if (!std::isfinite(rot12[i])) return fail(MOG_ERR_CONFIG, "rotation entries must be finite");
     for (int i = 0; i < cfg->n_grids * 4; ++i)
@@ -392,6 +394,7 @@ int mog_create(const mog_config* cfg, const float* rot12, const float* off4, mog
     // the reference's ping-pong leaves the result in its scratch texture
     // after an odd number of passes, 3 (log2 g + 1)
     e.alias_xz = (cfg->compat_flags & MOG_COMPAT_FFT_TEXTURE_ALIAS) && ((3 * (lg + 1)) & 1) ? 1 : 0;
+    e.dft_tc = cfg->dft_prec == MOG_DFT_TC_BF16X3 ? 1 : 0;
 
     // FAST-mode rows: t_r = sum_j (M[j][r] / h) c_j + (L/2 - off_r) / h
     std::vector<mog::FastXf> fast(k);
@@ -430,6 +433,11 @@ int mog_create(const mog_config* cfg, const float* rot12, const float* off4, mog
     ALLOC(h->d_mass, cells * (cfg->mass_mode == MOG_MASS_U64_FIXED ? 8 : 4));
     ALLOC(h->d_force, sizeof(float4) * cells);
     ALLOC(h->d_diag, sizeof(double) * (kDiagBlocks * 8 + 8));
+    std::vector<uint16_t> dft_tab;
+    if (e.dft_tc) {
+        dft_tab = mog::dft_tc_tables(g);
+        ALLOC(h->d_dft, sizeof(uint16_t) * dft_tab.size());
+    }
     const size_t scratch = mog::spectral_scratch_bytes(e);
     if (scratch) ALLOC(h->d_scratch, scratch);
     // spatial-order buffers for the declared capacity (no allocation may
@@ -451,8 +459,11 @@ int mog_create(const mog_config* cfg, const float* rot12, const float* off4, mog
         (err = cudaMemcpy(h->d_conv, convk.data(), sizeof(float) * convk.size(), cudaMemcpyHostToDevice)) ||
         (err = cudaMemset(h->d_flags, 0, sizeof(unsigned) * 4)) ||
         (err = cudaMemset(h->d_total, 0, sizeof(double) * 2)) ||
-        (err = cudaMemset(h->d_mass, 0, mass_bytes(h))))
+        (err = cudaMemset(h->d_mass, 0, mass_bytes(h))) ||
+        (e.dft_tc && (err = cudaMemcpy(h->d_dft, dft_tab.data(), sizeof(uint16_t) * dft_tab.size(),
+                                       cudaMemcpyHostToDevice))))
         return fail_free(err, "mog_create upload");
+    e.dft_tables = h->d_dft;
     e.rot12 = h->d_rot12;
     e.off4 = h->d_off4;
     e.fast = h->d_fast;

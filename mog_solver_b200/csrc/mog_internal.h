@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cstdint>
+#include <vector>
 #include <cuda_runtime.h>
 
 #include "mog_device.cuh"
@@ -29,6 +30,8 @@ struct Ensemble {
     const float* green = nullptr;   // g^3 Green's factors -2 pi G / k^2 (0 when k^2 <= 1e-4)
     const float* ktab = nullptr;    // g wave numbers 2 pi shift(i) / L
     const float4* conv_kernel = nullptr;  // g^3 real-space kernel r/(4 pi r^3) (main.py:250-278)
+    int dft_tc = 0;                 // axis passes on the tensor cores (MOG_DFT_TC_BF16X3)
+    const void* dft_tables = nullptr;  // their DFT matrices (dft_tc_tables layout)
     unsigned* flags = nullptr;      // device status word
     double* mass_total = nullptr;   // running sum of q for the overflow check
 
@@ -83,6 +86,12 @@ cudaError_t launch_convolution(const Ensemble& e, void* mass, float4* force, boo
                                bool zero_mass, cudaStream_t s);
 
 // Rotate a grid-frame force grid into the world frame (stage entry point).
+// Tensor-core DFT passes (dft_tc.cu), g = 16 or 32: host-built B tables
+// (forward hi, lo, inverse hi, lo; BF16 bits) and one in-place axis pass
+// over the lines of nf fields of pairs x g^3 complex values.
+std::vector<uint16_t> dft_tc_tables(int g);
+cudaError_t launch_dft_tc(int g, float2* f0, float2* f1, float2* f2, int nf, int axis, int pairs,
+                          bool inverse, const void* tables, unsigned* flags, cudaStream_t s);
 cudaError_t launch_prerotate(const Ensemble& e, const float4* force_grid, float4* force_world,
                              cudaStream_t s);
 

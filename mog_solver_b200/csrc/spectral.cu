@@ -372,8 +372,9 @@ __global__ void __launch_bounds__(3 * G * G, (G == 16 ? 1 : 4))
 // Multi-pass path (any g up to 64, used for g >= 32): the same algebra,
 // with each axis pass a separate launch over global (L2-resident) scratch.
 
-// X[pair][z][y][x] = rho_a + i rho_b, transformed along x.
-template <int G, typename Acc, bool ZERO>
+// X[pair][z][y][x] = rho_a + i rho_b, transformed along x (XFFT) or not
+// (the tensor-core passes transform it afterwards).
+template <int G, typename Acc, bool ZERO, bool XFFT = true>
 __global__ void __launch_bounds__(128) mp_load_x_kernel(Acc* __restrict__ mass,
                                                         float2* __restrict__ X, Ensemble e,
                                                         int pairs) {
@@ -400,7 +401,7 @@ __global__ void __launch_bounds__(128) mp_load_x_kernel(Acc* __restrict__ mass,
             if (hasb) rb[x] = 0;
         }
     }
-    fft_reg<G, false>(v);
+    if (XFFT) fft_reg<G, false>(v);
     float2* out = X + (size_t)pair * G3 + (size_t)rowi * G;
 #pragma unroll
     for (int x = 0; x < G; ++x) out[x] = v[x];
@@ -528,16 +529,31 @@ cudaError_t run_multipass(const Ensemble& e, Acc* mass, float4* force, bool worl
     const int64_t lines = (int64_t)pairs * G * G;
     const unsigned lb = (unsigned)((lines + 127) / 128);
     const unsigned eb = (unsigned)(((int64_t)pairs * G3 + 255) / 256);
-    if (zero)
-        mp_load_x_kernel<G, Acc, true><<<lb, 128, 0, s>>>(mass, X, e, pairs);
-    else
-        mp_load_x_kernel<G, Acc, false><<<lb, 128, 0, s>>>(mass, X, e, pairs);
-    mp_line_kernel<G, false><<<dim3(lb, 1), 128, 0, s>>>(X, X, X, 1, pairs);
-    mp_line_kernel<G, false><<<dim3(lb, 1), 128, 0, s>>>(X, X, X, 2, pairs);
-    mp_green_kernel<G><<<eb, 256, 0, s>>>(X, Z1, Z2, Z3, e, pairs);
-    mp_line_kernel<G, true><<<dim3(lb, 3), 128, 0, s>>>(Z1, Z2, Z3, 2, pairs);
-    mp_line_kernel<G, true><<<dim3(lb, 3), 128, 0, s>>>(Z1, Z2, Z3, 1, pairs);
-    mp_line_kernel<G, true><<<dim3(lb, 3), 128, 0, s>>>(Z1, Z2, Z3, 0, pairs);
+    if (e.dft_tc) {
+        // every axis pass as a DFT-matrix GEMM on the tensor cores
+        const void* tb = e.dft_tables;
+        if (zero)
+            mp_load_x_kernel<G, Acc, true, false><<<lb, 128, 0, s>>>(mass, X, e, pairs);
+        else
+            mp_load_x_kernel<G, Acc, false, false><<<lb, 128, 0, s>>>(mass, X, e, pairs);
+        cudaError_t err;
+        for (int axis = 0; axis < 3; ++axis)
+            if ((err = launch_dft_tc(G, X, X, X, 1, axis, pairs, false, tb, e.flags, s))) return err;
+        mp_green_kernel<G><<<eb, 256, 0, s>>>(X, Z1, Z2, Z3, e, pairs);
+        for (int axis = 2; axis >= 0; --axis)
+            if ((err = launch_dft_tc(G, Z1, Z2, Z3, 3, axis, pairs, true, tb, e.flags, s))) return err;
+    } else {
+        if (zero)
+            mp_load_x_kernel<G, Acc, true><<<lb, 128, 0, s>>>(mass, X, e, pairs);
+        else
+            mp_load_x_kernel<G, Acc, false><<<lb, 128, 0, s>>>(mass, X, e, pairs);
+        mp_line_kernel<G, false><<<dim3(lb, 1), 128, 0, s>>>(X, X, X, 1, pairs);
+        mp_line_kernel<G, false><<<dim3(lb, 1), 128, 0, s>>>(X, X, X, 2, pairs);
+        mp_green_kernel<G><<<eb, 256, 0, s>>>(X, Z1, Z2, Z3, e, pairs);
+        mp_line_kernel<G, true><<<dim3(lb, 3), 128, 0, s>>>(Z1, Z2, Z3, 2, pairs);
+        mp_line_kernel<G, true><<<dim3(lb, 3), 128, 0, s>>>(Z1, Z2, Z3, 1, pairs);
+        mp_line_kernel<G, true><<<dim3(lb, 3), 128, 0, s>>>(Z1, Z2, Z3, 0, pairs);
+    }
     if (world)
         mp_store_kernel<G, true><<<eb, 256, 0, s>>>(Z1, Z2, Z3, force, e, pairs);
     else
@@ -548,6 +564,7 @@ cudaError_t run_multipass(const Ensemble& e, Acc* mass, float4* force, bool worl
 template <typename Acc>
 cudaError_t spectral_typed(const Ensemble& e, Acc* mass, float4* force, bool world, bool zero,
                            void* scratch, cudaStream_t s) {
+    if (e.dft_tc && e.g == 16) return run_multipass<16, Acc>(e, mass, force, world, zero, scratch, s);
     switch (e.g) {
         case 2: return run_fused<2, Acc>(e, mass, force, world, zero, s);
         case 4: return run_fused<4, Acc>(e, mass, force, world, zero, s);
@@ -598,7 +615,7 @@ __global__ void prerotate_kernel(const float4* __restrict__ in, float4* __restri
 }  // namespace
 
 size_t spectral_scratch_bytes(const Ensemble& e) {
-    if (e.g <= 16) return 0;
+    if (e.g <= 16 && !e.dft_tc) return 0;
     const size_t pairs = (size_t)(e.k + 1) / 2;
     return 4 * pairs * ((size_t)1 << (3 * e.lg)) * sizeof(float2);
 }
