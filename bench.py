@@ -2,7 +2,7 @@
 """Throughput of the Mixture-of-Grids force-and-step path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W]
-                    [--workload learned|c2|c3|c1] [--impl ours|reference]
+                    [--workload learned|c2|c3|c4|c1] [--impl ours|reference]
 
 Default workload (``learned``, one GPU): the headline metric, particle-steps/s
 of the learned k = 32 step at the RMS force error of plain k = 240, on the
@@ -20,7 +20,8 @@ its variance gate) with the particles copied from pinned host memory and
 back every step.
 
 ``c2`` times the plain k = 240 step alone, ``c1`` the small uniform-cube
-case and ``c3`` the batched uneven ensemble.  Under torchrun (N > 1) every
+case, ``c3`` the batched uneven ensemble and ``c4`` the plain k = 240, g = 32
+step with the DFT passes on the tensor cores (BF16 hi+lo x3).  Under torchrun (N > 1) every
 rank advances its own independent simulation of the same size (replicas;
 the step has no cross-GPU exchange) and the time is the maximum over ranks.
 
@@ -64,6 +65,10 @@ WORKLOADS = {
                      (1048576, 128, 32), (1048576, 64, 16), (2097152, 128, 16),
                      (2097152, 240, 16)],
                L=100.0, G=100.0, dt=1e-5, damping=0.999, ic="plummer", seed=0),
+    "c4": dict(desc="plain MOG k=240 g=32 with the DFT passes on the tensor cores (BF16 hi+lo x3), "
+                    "two colliding exponential disks, N=1,048,576",
+               n=1 << 20, k=240, g=32, L=100.0, G=100.0, dt=1e-5, damping=0.999, ic="disks",
+               seed=1, dft="bf16x3"),
     "c1": dict(desc="plain MOG k=16 g=16, uniform cube, N=65,536",
                n=1 << 16, k=16, g=16, L=100.0, G=100.0, dt=1e-5, damping=0.999, ic="uniform",
                seed=0),
@@ -106,8 +111,19 @@ def measured_peaks() -> dict:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
         d = json.loads(p.read_text())
-        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
-    return {"hbm_gbs": 6650.0, "source": "fallback"}
+        return {"hbm_gbs": float(d["hbm_gbs"]), "bf16_tflops": float(d["bf16_tflops"]),
+                "source": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
+
+
+def dft_tensor_flops(k: int, g: int) -> float:
+    """Tensor-core FLOPs of one solve with the BF16 x3 DFT passes: per
+    128-line tile a (128 x 2g) . (2g x 2g) real GEMM, three products; lines
+    per field pass = pairs g^2; one forward field and three inverse fields,
+    three axes each."""
+    pairs = (k + 1) // 2
+    lines = pairs * g * g
+    return 2.0 * lines * (2 * g) * (2 * g) * 3 * (3 + 9)
 
 
 def profiled_traffic(kernel: str, workload: str):
@@ -235,7 +251,7 @@ def run_ours(args, w: dict) -> None:
 
     cfg = {"n_grids": w["k"], "grid_size": w["g"], "world_size": w["L"], "num_particles": w["n"],
            "G": w["G"], "dt": w["dt"], "damping": w["damping"], "solver": "fft", "seed": 0,
-           "index_mode": args.index_mode}
+           "index_mode": args.index_mode, "dft_precision": w.get("dft", "fp32")}
     sim = Simulation(cfg, device=dev)
     pos, vel = make_particles(w, sim, seed_offset=rank)
     sim.set_particles(pos, vel)
@@ -330,7 +346,7 @@ def run_ours(args, w: dict) -> None:
             r = cpu_baseline(w)
             base = {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": r["kind"],
                     "sample": r["sample"]}
-        launches = 3 if w["g"] <= 16 else 10
+        launches = (3 if w["g"] <= 16 else 10) if w.get("dft") != "bf16x3" else 11
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
@@ -356,6 +372,15 @@ def run_ours(args, w: dict) -> None:
             "gpu_launches": launches * args.steps,
             "clocks": clk,
         }
+        if w.get("dft") == "bf16x3":
+            fl = dft_tensor_flops(w["k"], w["g"])
+            tf = fl / (mean_ph[2] / 1e3) / 1e12
+            line["dft"] = {"precision": "BF16 hi+lo x3, FP32 accumulation (tcgen05)",
+                           "solve_ms": float(mean_ph[2]), "tensor_flops_per_solve": fl,
+                           "achieved_tflops": tf, "peak_tflops": peaks["bf16_tflops"],
+                           "frac": tf / peaks["bf16_tflops"],
+                           "note": "whole solve (load, 6 DFT passes, Green's multiply, store) "
+                                   "timed; tensor-pipe share in profiles/"}
         if base is not None:
             line["cpu_baseline"] = base
         print(json.dumps(line), flush=True)

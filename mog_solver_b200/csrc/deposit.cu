@@ -250,13 +250,19 @@ __device__ __forceinline__ uint32_t cell_byte_offset(const float4& r0, const flo
     return ((bx & M) << 2) | ((by & M) << (LG + 2)) | ((bz & M) << (2 * LG + 2));
 }
 
-template <int LG, int MODE, int PPT>
+//
+// SPLIT (u64 mode, for grids whose two words per cell do not fit shared
+// memory, g = 32): only the high words live in shared memory; a non-zero
+// low half goes straight to the global 64-bit cell with one global atomic
+// (equal power-of-two masses have none).
+template <int LG, int MODE, int PPT, bool SPLIT = false>
 __global__ void __launch_bounds__(1024) deposit_fast_kernel(const float4* __restrict__ pos,
                                                             int64_t n, int64_t chunk, Ensemble e,
                                                             int gpc,
                                                             typename SmemHist<MODE>::Acc* __restrict__ mass) {
     using H = SmemHist<MODE>;
     using Acc = typename H::Acc;
+    static_assert(!SPLIT || MODE == 1, "the split histogram is for u64 grids");
     constexpr int G3 = 1 << (3 * LG);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int g0 = blockIdx.y * gpc;
@@ -264,14 +270,14 @@ __global__ void __launch_bounds__(1024) deposit_fast_kernel(const float4* __rest
     const uint32_t words = (uint32_t)ng * G3;
     float4* rows = reinterpret_cast<float4*>(smem_raw);                       // gpc * 3 rows
     unsigned* lo_w = reinterpret_cast<unsigned*>(smem_raw + (size_t)gpc * 48);
-    unsigned* hi_w = lo_w + (size_t)gpc * G3;
+    unsigned* hi_w = SPLIT ? lo_w : lo_w + (size_t)gpc * G3;
     const uint32_t lo_base = (uint32_t)__cvta_generic_to_shared(lo_w);
     const uint32_t hi_base = (uint32_t)__cvta_generic_to_shared(hi_w);
 
     for (int i = threadIdx.x; i < ng * 3; i += blockDim.x) rows[i] = e.fast[g0 + i / 3].row[i % 3];
     for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) {
         lo_w[i] = 0u;
-        if (H::kWords == 2) hi_w[i] = 0u;
+        if (H::kWords == 2 && !SPLIT) hi_w[i] = 0u;
     }
     __syncthreads();
 
@@ -320,6 +326,9 @@ __global__ void __launch_bounds__(1024) deposit_fast_kernel(const float4* __rest
                 const uint32_t off = gbyte + cell_byte_offset<LG>(r0, r1, r2, cx[u], cy[u], cz[u]);
                 if (MODE == 0) {
                     if (ql[u]) red_shared(lo_base + off, ql[u]);   // zero for padding lanes
+                } else if (SPLIT) {
+                    if (ql[u]) atomicAdd(mass + (size_t)g0 * G3 + (off >> 2), (Acc)ql[u]);
+                    if (qh[u]) red_shared(hi_base + off, qh[u]);
                 } else if (hi_only) {
                     if (qh[u]) red_shared(hi_base + off, qh[u]);
                 } else {
@@ -340,7 +349,7 @@ __global__ void __launch_bounds__(1024) deposit_fast_kernel(const float4* __rest
     if (bad) raise_flags(e.flags, bad);
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) {
-        const Acc v = H::read(lo_w, hi_w, i);
+        const Acc v = SPLIT ? (Acc)hi_w[i] << 32 : H::read(lo_w, hi_w, i);
         if (v) atomicAdd(mass + (size_t)g0 * G3 + i, v);
     }
 }
@@ -431,10 +440,17 @@ static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, const int
     const size_t smem = (size_t)gpc * 16 * sizeof(float) + ((size_t)gpc * word_bytes << slab_lg);
     const int ppt = sh.ppt == 1 || sh.ppt == 2 || sh.ppt == 4 ? sh.ppt : 4;
     const bool agg = sh.aggregate < 0 ? ordered : sh.aggregate != 0;
-    if (IDX == 0 && !agg && !perm && slab_lg == cells_lg && (e.g == 8 || e.g == 16) &&
+    // g = 32 in u64 mode: the split histogram (high words only) fits one
+    // grid per CTA where the two-word one needs two slabs
+    const bool split = MODE == 1 && e.g == 32 && sh.grids_per_cta <= 1;
+    if (split && IDX == 0 && !agg && !perm && sh.fast != 0) {
+        gpc = 1;
+        slab_lg = cells_lg;
+    }
+    if (IDX == 0 && !agg && !perm && slab_lg == cells_lg && (e.g == 8 || e.g == 16 || e.g == 32) &&
         sh.fast != 0) {
         auto launch_fast = [&](auto kern) -> cudaError_t {
-            const size_t fsmem = (size_t)gpc * 48 + ((size_t)gpc * word_bytes << cells_lg);
+            const size_t fsmem = (size_t)gpc * 48 + ((size_t)gpc * (split ? 4 : word_bytes) << cells_lg);
             cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                    (int)fsmem);
             if (err != cudaSuccess) return err;
@@ -445,6 +461,17 @@ static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, const int
             kern<<<dim3(chunks, groups, 1), sh.threads, fsmem, s>>>(pos, n, chunk, e, gpc, mass);
             return cudaGetLastError();
         };
+        if (e.g == 32) {
+            if constexpr (MODE == 1) {
+                if (ppt == 1) return launch_fast(deposit_fast_kernel<5, 1, 1, true>);
+                if (ppt == 2) return launch_fast(deposit_fast_kernel<5, 1, 2, true>);
+                return launch_fast(deposit_fast_kernel<5, 1, 4, true>);
+            } else {
+                if (ppt == 1) return launch_fast(deposit_fast_kernel<5, MODE, 1>);
+                if (ppt == 2) return launch_fast(deposit_fast_kernel<5, MODE, 2>);
+                return launch_fast(deposit_fast_kernel<5, MODE, 4>);
+            }
+        }
         if (e.g == 16) {
             if (ppt == 1) return launch_fast(deposit_fast_kernel<4, MODE, 1>);
             if (ppt == 2) return launch_fast(deposit_fast_kernel<4, MODE, 2>);

@@ -193,13 +193,27 @@ __global__ void __launch_bounds__(kTileLines) dft_tc_kernel(float2* f0, float2* 
             }
             p = buf + pair * G3 + base;
         }
-        // line t -> row t of A (hi and lo), 4 complex values per k-block
+        // line t -> registers (all loads in flight; 16-byte loads along x)
+        float2 v[G];
+        if (live && stride == 1) {
+            const float4* q = reinterpret_cast<const float4*>(p);
+#pragma unroll
+            for (int j = 0; j < G / 2; ++j) {
+                const float4 a = q[j];
+                v[2 * j] = make_float2(a.x, a.y);
+                v[2 * j + 1] = make_float2(a.z, a.w);
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < G; ++j) v[j] = live ? p[(int64_t)j * stride] : make_float2(0.f, 0.f);
+        }
+        // -> row t of A (hi and lo), 4 complex values per k-block
 #pragma unroll
         for (int kb = 0; kb < KB; ++kb) {
             uint32_t hi[4], lo[4];
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-                const float2 x = live ? p[(int64_t)(kb * 4 + j) * stride] : make_float2(0.f, 0.f);
+                const float2 x = v[kb * 4 + j];
                 const __nv_bfloat16 hr = __float2bfloat16_rn(x.x), hi_ = __float2bfloat16_rn(x.y);
                 hi[j] = bf16_pair(__bfloat162float(hr), __bfloat162float(hi_));
                 lo[j] = bf16_pair(x.x - __bfloat162float(hr), x.y - __bfloat162float(hi_));
@@ -239,7 +253,13 @@ __global__ void __launch_bounds__(kTileLines) dft_tc_kernel(float2* f0, float2* 
         for (int c = 0; c < KD; c += 32) {
             uint32_t r[32];
             tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, r);
-            if (live) {
+            if (live && stride == 1) {
+                float4* q = reinterpret_cast<float4*>(p) + c / 4;
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    q[j] = make_float4(__uint_as_float(r[4 * j]), __uint_as_float(r[4 * j + 1]),
+                                       __uint_as_float(r[4 * j + 2]), __uint_as_float(r[4 * j + 3]));
+            } else if (live) {
 #pragma unroll
                 for (int j = 0; j < 16; ++j)
                     p[(int64_t)(c / 2 + j) * stride] =
@@ -321,6 +341,8 @@ cudaError_t launch_dft_tc(int g, float2* f0, float2* f1, float2* f2, int nf, int
     const size_t smem = dft_tc_smem(g);
     auto go = [&](auto kern) -> cudaError_t {
         cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (err == cudaSuccess)
+            err = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         if (err != cudaSuccess) return err;
         int per_sm = 0;
         err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTileLines, smem);

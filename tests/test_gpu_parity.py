@@ -112,6 +112,26 @@ def test_deposit_tunings_bit_exact(tuning, mass_mode):
         assert np.array_equal(got.view(ref.dtype), ref)
 
 
+@pytest.mark.parametrize("mass_mode", ["u64", "u32x1000"])
+def test_deposit_g32_bit_exact(mass_mode):
+    """g = 32: the split histogram (u64: high words in shared memory, low
+    halves as global atomics) and the one-word histogram (u32)."""
+    n, k, g, L = 131072, 5, 32, 100.0  # 2^17: equal masses have a zero low half
+    sim = make_sim(k=k, g=g, L=L, n=n, mass_mode=mass_mode)
+    for equal in (True, False):
+        if mass_mode == "u32x1000":
+            m = None if equal else np.random.default_rng(4).uniform(0.5, 2, n)
+            pos, vel = particles(n, L, seed=8, equal_mass=equal, mass=1.0 if equal else m)
+        else:
+            m = None if equal else np.random.default_rng(4).uniform(0.5, 2, n) / n
+            pos, vel = particles(n, L, seed=8, equal_mass=equal, mass=m)
+        sim.set_particles(pos, vel)
+        got = sim.mass_grid().cpu().numpy()
+        mm = oracle.MASS_U64 if mass_mode == "u64" else oracle.MASS_U32
+        ref = oracle.deposit(pos, sim.rotations, sim.offsets, g, L, mm, sim.scale_bits)
+        assert np.array_equal(got.view(ref.dtype), ref)
+
+
 def test_deposit_repeat_is_identical():
     sim = make_sim(k=32, g=16, n=200000)
     pos, vel = particles(200000, seed=3)
