@@ -590,7 +590,7 @@ def run_learned(args, w: dict) -> None:
                        "model": model_src, "index_mode": "fast", "mass_mode": "u64 fixed point",
                        "parallelism": "single GPU" if world == 1 else f"{world} independent replicas",
                        "l2": "flushed between timed steps (256 MiB write)"},
-            "accuracy": {"judge": "relative RMS force error vs FP64 periodic direct sum, 16,384 "
+            "accuracy": {"yardstick": "relative RMS force error vs FP64 periodic direct sum, 16,384 "
                                   "sampled particles, all sources",
                          **accuracy, "learned_within_10pct_of_plain_k240": within},
             "plain_k240": {"value": plain_value, "unit": UNIT,

@@ -211,7 +211,7 @@ int mog_diagnostics(mog_handle* h, const float* pos4, const float* vel4,
                     int64_t n, double* out8, void* stream);
 
 /*
- * FP64 direct-sum judge of force accuracy (no counterpart in the
+ * FP64 direct-sum yardstick of force accuracy (no counterpart in the
  * reference).  For each of nt target records (device float4, w ignored)
  * sums over ns source records (device float4, w = mass):
  *     out3[t] = g_eff * sum_j m_j d / (|d|^2 + soft^2)^(3/2),

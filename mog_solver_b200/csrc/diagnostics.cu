@@ -1,11 +1,11 @@
-// diagnostics.cu — FP64 direct-sum judge of force accuracy.
+// diagnostics.cu — FP64 direct-sum yardstick of force accuracy.
 //
 // The accuracy half of the headline metric compares MOG forces with an FP64
 // direct sum.  The reference has no such tool; its paper reports a 2-D MSE
 // from a script that is not shipped.  In the solver's units the reference's
 // field is (h^3 / 2) times the Newtonian periodic gradient for G: -2 pi G
 // instead of -4 pi G in greens.glsl:40, cell masses instead of densities,
-// and 1/g^3 instead of 1/L^3 in pack.glsl:21.  So the judge sums
+// and 1/g^3 instead of 1/L^3 in pack.glsl:21.  So the yardstick sums
 //     F(x) = g_eff * sum_j m_j d / (|d|^2 + soft^2)^(3/2),
 //     d = minimum-image (x - x_j),  g_eff = G h^3 / 2,
 // which points away from the sources like the solver's F (update.glsl:83

@@ -122,7 +122,7 @@ cudaError_t launch_build_tables(int g, float world, float G, float* green, float
 cudaError_t launch_diagnostics(const float4* pos, const float4* vel, int64_t n, double* partial,
                                int nblocks, double* out8, cudaStream_t s);
 
-// FP64 direct-sum judge: out3[t] = g_eff * sum_j m_j d / (|d|^2 + soft^2)^1.5
+// FP64 direct-sum yardstick: out3[t] = g_eff * sum_j m_j d / (|d|^2 + soft^2)^1.5
 // over minimum-image separations.  partial: chunks * nt * 3 doubles.
 cudaError_t launch_direct_sum(const float4* targets, int64_t nt, const float4* sources, int64_t ns,
                               double world, double g_eff, double soft, double* partial, int chunks,

@@ -334,7 +334,7 @@ def rms_error(F, D) -> float:
 
 
 def direct_sum(targets, sources, world: float, g_eff: float, soft: float = 0.0):
-    """FP64 direct-sum judge on the GPU (mog_direct_sum), (nt, 3) float64."""
+    """FP64 direct-sum yardstick on the GPU (mog_direct_sum), (nt, 3) float64."""
     torch = _torch()
     out = torch.empty((targets.shape[0], 3), dtype=torch.float64, device=targets.device)
     _lib.check(_lib.lib().mog_direct_sum(targets.data_ptr(), int(targets.shape[0]),

@@ -10,7 +10,7 @@ of it.  Contents:
 * ``pipeline``         NumPy FP64 "ideal pipeline" (same transforms, NGP and
                        Green's function, exact FFT): the 1e-5 force gate;
                        NumPy FP32 transcription of the reference's shader
-                       chain with its flush quirks; FP64 direct-sum judge;
+                       chain with its flush quirks; FP64 direct-sum yardstick;
 * ``_ref``             (built in the source container only) the reference's
                        own GLSL compute shaders compiled as C++ through a
                        GLSL compatibility header, used to pin the above.

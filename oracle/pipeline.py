@@ -10,7 +10,7 @@
 * FP32 transcription of the shader chain including its quirks
   (uint x1000 mass, per-stage radix-2 passes with the |x| < 1e-6 flushes
   and twiddle snapping of fft_batched.glsl:19-34, 123-126).
-* FP64 direct-sum judge: minimum-image Newtonian field scaled to the
+* FP64 direct-sum yardstick: minimum-image Newtonian field scaled to the
   solver's units (G h^3 / 2).
 """
 from __future__ import annotations
@@ -213,7 +213,7 @@ def forces_grid_f32(mass_u32: np.ndarray, G: float, world: float,
 
 
 # ---------------------------------------------------------------------------
-# FP64 direct-sum judge.
+# FP64 direct-sum yardstick.
 
 def direct_sum_fp64(targets: np.ndarray, sources: np.ndarray, masses: np.ndarray, world: float,
                     g_eff: float, soft: float = 0.0, chunk: int = 256) -> np.ndarray:
