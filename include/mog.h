@@ -96,6 +96,10 @@ typedef struct mog_config {
     int32_t dft_prec;       /* MOG_DFT_*                                    */
     int32_t compat_flags;   /* MOG_COMPAT_* bits                            */
     int64_t num_particles;  /* capacity: largest n passed to the step calls */
+    float   softening;      /* fft solver: spectral softening radius a in voxels; 0 = the
+                               live greens.glsl:17-61 (-2 pi G / k^2); > 0 = the variant
+                               commented out in greens.glsl:63-115:
+                               -4 pi G exp(-k^2 a^2) / k^2                   */
 } mog_config;
 
 typedef struct mog_handle mog_handle;
@@ -332,6 +336,18 @@ int mog_learned_step_profiled(mog_handle* h, const mog_model* m, float* pos4, fl
  * the stream.
  */
 int mog_learned_spread(mog_handle* h, double* out2, void* stream);
+
+/*
+ * The Green's factor table the spectral solve multiplies by, g^3 floats in
+ * [kz][ky][kx] order, written to host memory `out`: -2 pi G / k^2
+ * (softening 0) or -4 pi G exp(-k^2 a^2) / k^2 with a = softening * L / g,
+ * in FP64 then rounded to FP32; 0 where the reference's FP32 k^2 <= 1e-4
+ * (greens.glsl:17-47).  Host only, no GPU needed.  No counterpart in the
+ * reference (it builds the factor per bin in the shader).  For softening 0
+ * the library builds the same table on the GPU, equal to this one up to the
+ * last bit of k^2.
+ */
+int mog_green_table(int32_t g, float world, float G, float softening, float* out);
 
 /* Human-readable text for a status code, and the calling thread's last
  * error message. */

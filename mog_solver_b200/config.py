@@ -25,6 +25,7 @@ include/mog.h MOG_COMPAT_FFT_TEXTURE_ALIAS).
 from __future__ import annotations
 
 import dataclasses
+import math
 from pathlib import Path
 from typing import Any, Mapping
 
@@ -79,6 +80,7 @@ class MogConfig:
     index_mode: str = "fast"
     dft_precision: str = "fp32"
     reference_texture_aliasing: bool = False
+    softening: float = 0.0
 
     @property
     def voxel_size(self) -> float:
@@ -114,6 +116,7 @@ class MogConfig:
             index_mode=str(cfg.get("index_mode", "fast")),
             dft_precision=str(cfg.get("dft_precision", "fp32")),
             reference_texture_aliasing=bool(cfg.get("reference_texture_aliasing", False)),
+            softening=float(cfg.get("softening", 0.0)),
         )
         out.validate()
         return out
@@ -138,6 +141,10 @@ class MogConfig:
             raise ValueError(f"dft_precision must be one of {_DFT}")
         if self.scale_bits is not None and not 0 <= self.scale_bits <= 100:
             raise ValueError("scale_bits must be in [0, 100]")
+        if not (math.isfinite(self.softening) and self.softening >= 0):
+            raise ValueError("softening must be finite and >= 0")
+        if self.softening > 0 and self.solver != "fft":
+            raise ValueError("softening applies to the fft solver only")
 
     def to_dict(self) -> dict[str, Any]:
         return dataclasses.asdict(self)

@@ -207,7 +207,39 @@ int validate(const mog_config& c) {
     if (c.num_particles < 0) return fail(MOG_ERR_CONFIG, "num_particles must be >= 0");
     if (c.compat_flags & ~MOG_COMPAT_FFT_TEXTURE_ALIAS)
         return fail(MOG_ERR_CONFIG, "unknown compat_flags bits");
+    if (!(std::isfinite(c.softening) && c.softening >= 0.f))
+        return fail(MOG_ERR_CONFIG, "softening must be finite and >= 0");
+    if (c.softening > 0.f && c.solver != MOG_SOLVER_FFT)
+        return fail(MOG_ERR_CONFIG, "softening applies to the fft solver only");
     return MOG_OK;
+}
+
+// Green's factors on [kz][ky][kx] (greens.glsl:17-47): FP64 values, the
+// reference's FP32 k^2 > 1e-4 test for which bins are kept.
+std::vector<float> green_table(int g, float world, float G, float softening) {
+    std::vector<float> out((size_t)g * g * g, 0.f);
+    auto shift = [g](int i) { return i <= g / 2 ? i : i - g; };
+    volatile float two_pi_f = 2.0f * 3.14159265359f;  // the shader's TWO_PI
+    const float step_f = two_pi_f / world;
+    const double two_pi = 6.283185307179586476925286766559;
+    const double step = two_pi / (double)world;
+    const double a = (double)softening * (double)world / (double)g;
+    for (int iz = 0; iz < g; ++iz)
+        for (int iy = 0; iy < g; ++iy)
+            for (int ix = 0; ix < g; ++ix) {
+                volatile float kxf = (float)shift(ix) * step_f, kyf = (float)shift(iy) * step_f,
+                               kzf = (float)shift(iz) * step_f;
+                volatile float kxx = kxf * kxf, kyy = kyf * kyf, kzz = kzf * kzf;
+                volatile float k2xy = kxx + kyy;
+                const float k2f = k2xy + kzz;
+                if (!(k2f > 1e-4f)) continue;
+                const double kx = shift(ix) * step, ky = shift(iy) * step, kz = shift(iz) * step;
+                const double k2 = kx * kx + ky * ky + kz * kz;
+                const double v = softening > 0.f ? -2.0 * two_pi * (double)G * std::exp(-k2 * a * a) / k2
+                                                 : -two_pi * (double)G / k2;
+                out[((size_t)iz * g + iy) * g + ix] = (float)v;
+            }
+    return out;
 }
 
 // Real-space kernel of init_greens_kernel (main.py:250-278), FP64 then f4,
@@ -475,6 +507,12 @@ int mog_create(const mog_config* cfg, const float* rot12, const float* off4, mog
     if ((err = mog::launch_build_tables(g, cfg->world_size, cfg->G, h->d_green, h->d_ktab, 0)) ||
         (err = cudaDeviceSynchronize()))
         return fail_free(err, "Green's table build");
+    if (cfg->softening > 0.f) {
+        // the softened variant's factors, built on the host in FP64
+        const std::vector<float> gt = green_table(g, cfg->world_size, cfg->G, cfg->softening);
+        if ((err = cudaMemcpy(h->d_green, gt.data(), sizeof(float) * gt.size(), cudaMemcpyHostToDevice)))
+            return fail_free(err, "softened Green's table upload");
+    }
     *out = h;
     return MOG_OK;
 }
@@ -804,6 +842,17 @@ int mog_direct_sum_noalloc(const float* targets4, int64_t nt, const float* sourc
                                  reinterpret_cast<const float4*>(sources4), ns, world, g_eff, soft,
                                  partial, chunks, out3, static_cast<cudaStream_t>(stream));
     if (err != cudaSuccess) return cuda_fail(err, "direct sum");
+    return MOG_OK;
+}
+
+int mog_green_table(int32_t g, float world, float G, float softening, float* out) {
+    if (!out) return fail(MOG_ERR_ARG, "out is null");
+    if (!is_pow2(g) || g < 2 || g > 64) return fail(MOG_ERR_ARG, "g must be a power of two in [2, 64]");
+    if (!(std::isfinite(world) && world > 0.f) || !std::isfinite(G) ||
+        !(std::isfinite(softening) && softening >= 0.f))
+        return fail(MOG_ERR_ARG, "world must be positive, G finite, softening >= 0");
+    const std::vector<float> t = green_table(g, world, G, softening);
+    std::memcpy(out, t.data(), sizeof(float) * t.size());
     return MOG_OK;
 }
 

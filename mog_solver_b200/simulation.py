@@ -124,6 +124,7 @@ class Simulation:
         cc.dft_prec = _DFT[c.dft_precision]
         cc.compat_flags = _lib.COMPAT_FFT_TEXTURE_ALIAS if c.reference_texture_aliasing else 0
         cc.num_particles = max(self.n_particles, c.num_particles)
+        cc.softening = c.softening
         return cc
 
     def _scale_bits(self) -> int:

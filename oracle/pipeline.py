@@ -38,24 +38,31 @@ def keep_mask(g: int, world: float) -> np.ndarray:
     return k2 > np.float32(1e-4)
 
 
-def green_fp64(g: int, world: float, G: float) -> np.ndarray:
-    """-2 pi G / k^2 on [kz][ky][kx], zero where the reference drops the bin."""
+def green_fp64(g: int, world: float, G: float, softening: float = 0.0) -> np.ndarray:
+    """-2 pi G / k^2 on [kz][ky][kx] (greens.glsl:39-47), or with softening a
+    (in voxels) the variant commented out in greens.glsl:63-115,
+    -4 pi G exp(-k^2 a^2) / k^2; zero where the reference drops the bin."""
     k = wavenumbers(g, world)
     kz, ky, kx = np.meshgrid(k, k, k, indexing="ij")
     k2 = kx * kx + ky * ky + kz * kz
     out = np.zeros((g, g, g))
     keep = keep_mask(g, world)
-    out[keep] = -2.0 * np.pi * float(np.float32(G)) / k2[keep]
+    Gf = float(np.float32(G))
+    if softening > 0:
+        a = float(np.float32(softening)) * float(np.float32(world)) / g
+        out[keep] = -4.0 * np.pi * Gf * np.exp(-k2[keep] * a * a) / k2[keep]
+    else:
+        out[keep] = -2.0 * np.pi * Gf / k2[keep]
     return out
 
 
-def forces_grid_fp64(rho: np.ndarray, G: float, world: float) -> np.ndarray:
+def forces_grid_fp64(rho: np.ndarray, G: float, world: float, softening: float = 0.0) -> np.ndarray:
     """Grid-frame forces (k, g, g, g, 3) in FP64 from cell masses (k, g, g, g)."""
     rho = np.asarray(rho, dtype=np.float64)
     g = rho.shape[-1]
     k = wavenumbers(g, world)
     rho_hat = np.fft.fftn(rho, axes=(1, 2, 3))
-    phi_hat = rho_hat * green_fp64(g, world, G)[None]
+    phi_hat = rho_hat * green_fp64(g, world, G, softening)[None]
     out = np.empty(rho.shape + (3,))
     # axis 3 is x, 2 is y, 1 is z ([z][y][x] layout, x fastest)
     shapes = {0: (1, 1, 1, g), 1: (1, 1, g, 1), 2: (1, g, 1, 1)}

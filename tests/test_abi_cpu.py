@@ -78,3 +78,39 @@ def test_strerror(lib):
     for code in range(8):
         assert lib.mog_strerror(code)
     assert b"sm_100a" in lib.mog_version()
+
+
+@pytest.mark.parametrize("g,softening", [(8, 0.0), (16, 0.0), (16, 0.5), (32, 1.5)])
+def test_green_table_matches_fp64(lib, g, softening):
+    """mog_green_table (host): the solve's Green's factors, plain and with the
+    reference's commented-out spectral softening, against the FP64 oracle."""
+    import numpy as np
+
+    from oracle import pipeline as pl
+
+    out = np.empty(g ** 3, dtype=np.float32)
+    assert lib.mog_green_table(g, 100.0, 3.0, softening, out.ctypes.data_as(ctypes.c_void_p)) == 0
+    ref = pl.green_fp64(g, 100.0, 3.0, softening).ravel()
+    assert np.array_equal(out == 0, ref == 0)
+    nz = ref != 0
+    assert np.abs(out[nz] / ref[nz] - 1).max() <= 1e-7
+
+
+def test_green_table_rejects_bad_arguments(lib):
+    import numpy as np
+
+    out = np.empty(8, dtype=np.float32)
+    assert lib.mog_green_table(3, 100.0, 1.0, 0.0, out.ctypes.data_as(ctypes.c_void_p)) == _lib.MOG_ERR_ARG
+    assert lib.mog_green_table(2, 100.0, 1.0, -1.0, out.ctypes.data_as(ctypes.c_void_p)) == _lib.MOG_ERR_ARG
+
+
+def test_config_softening_key():
+    from mog_solver_b200.config import MogConfig
+
+    base = {"grid_size": 16, "world_size": 100.0, "num_particles": 10, "G": 1.0, "dt": 1e-3}
+    assert MogConfig.from_dict(base).softening == 0.0
+    assert MogConfig.from_dict({**base, "softening": 0.5}).softening == 0.5
+    with pytest.raises(ValueError):
+        MogConfig.from_dict({**base, "softening": -1.0})
+    with pytest.raises(ValueError):
+        MogConfig.from_dict({**base, "softening": 0.5, "solver": "convolution"})

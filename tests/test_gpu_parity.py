@@ -196,6 +196,25 @@ def test_solve_matches_fp64(mass_mode, k, g):
     assert np.allclose(F[..., 3], mag, rtol=1e-5, atol=1e-30)
 
 
+@pytest.mark.parametrize("g", [16, 32])
+def test_softened_solve_matches_fp64(g):
+    """softening > 0: the variant commented out in greens.glsl:63-115."""
+    from mog_solver_b200 import Simulation
+
+    L, G, n, k, a = 100.0, 100.0, 20000, 3, 0.5
+    sim = Simulation({"n_grids": k, "grid_size": g, "world_size": L, "num_particles": n, "G": G,
+                      "dt": 1e-5, "seed": 1, "softening": a})
+    pos, vel = particles(n, L, seed=g + 1)
+    sim.set_particles(pos, vel)
+    m = sim.mass_grid()
+    F = sim.solve_grid(m).cpu().numpy()[..., :3]
+    rho = m.cpu().numpy().view(np.uint64).astype(np.float64) * 2.0 ** -sim.scale_bits
+    ref = pl.forces_grid_fp64(rho, G, L, softening=a)
+    assert pl.relative_l2(F, ref) <= FORCE_TOL
+    plain = pl.forces_grid_fp64(rho, G, L)
+    assert pl.relative_l2(ref, plain) > 0.05   # the softening changes the field
+
+
 @pytest.mark.parametrize("index_mode", ["fast", "exact"])
 def test_forces_match_fp64_pipeline(index_mode):
     """c1-like: N=65,536 uniform, k=16, g=16, G=100."""
