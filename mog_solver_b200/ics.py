@@ -12,7 +12,9 @@ use their own seeded distributions instead:
                       relative speed ``v_rel``;
 * ``plummer``         a Plummer sphere of scale radius a, at rest;
 * ``clumps``          a Gaussian mixture (log-uniform widths) plus a uniform
-                      background fraction.
+                      background fraction;
+* ``reference_two_galaxies`` the reference's own two-galaxy routine,
+                      seeded (bit-identical to it after np.random.seed).
 
 Every record is (x, y, z, m) for positions and (vx, vy, vz, 0) for
 velocities, the std430 vec4 layout of the reference's buffers
@@ -127,3 +129,44 @@ def clumps(n: int, world: float = 100.0, seed: int = 100, n_clumps: int = 20,
     xyz = wrap(np.concatenate([pts, bg]), world)
     xyz = xyz[rng.permutation(n)]
     return _records(xyz, total_mass / n)
+
+
+def reference_two_galaxies(n: int, world: float = 100.0, particle_mass: float = 1.0,
+                           seed: int = 0):
+    """The reference's numpy two-galaxy initialiser (main.py:312-357,
+    ``Simulation.init_particles2``) with its global ``np.random`` made an
+    explicit legacy ``RandomState(seed)``: the same draws in the same order,
+    so ``np.random.seed(seed)`` followed by the reference's routine gives the
+    same float32 buffers bit for bit.
+
+    Two spherical exponential blobs (scale 0.08 L) at ±0.2 L along x with
+    bulk velocities ±(0.3, 0.1, 0), each spinning about its own axis with
+    v = 0.3 sqrt(r / L + 0.01).  Masses are ``particle_mass`` each (the
+    reference's config value); with odd n the last record stays zero, as in
+    the reference.
+    """
+    rs = np.random.RandomState(seed)
+    pos = np.zeros((n, 4), dtype=np.float32)
+    vel = np.zeros((n, 4), dtype=np.float32)
+    centre = world / 2.0
+    per = n // 2
+    blobs = ((np.array([-0.2, 0.0, 0.0]), np.array([0.3, 0.1, 0.0]), np.array([0.3, 0.7, 0.5])),
+             (np.array([0.2, 0.0, 0.0]), np.array([-0.3, -0.1, 0.0]), np.array([-0.5, 0.2, 0.8])))
+    for i, (offset, v_bulk, axis) in enumerate(blobs):
+        lo, hi = i * per, (i + 1) * per
+        r = rs.exponential(scale=0.08, size=per) * world
+        theta = rs.uniform(0, 2 * np.pi, per)
+        phi = np.arccos(rs.uniform(-1, 1, per))
+        x = r * np.sin(phi) * np.cos(theta)
+        y = r * np.sin(phi) * np.sin(theta)
+        z = r * np.cos(phi)
+        for j, c in enumerate((x, y, z)):
+            pos[lo:hi, j] = centre + offset[j] * world + c
+        pos[lo:hi, 3] = particle_mass
+        axis = axis / np.linalg.norm(axis)
+        v_circ = 0.3 * np.sqrt(r / world + 0.01)
+        v_dir = np.cross(axis, np.stack([x, y, z], axis=1))
+        v_dir = v_dir / (np.linalg.norm(v_dir, axis=1, keepdims=True) + 1e-10)
+        for j in range(3):
+            vel[lo:hi, j] = v_circ * v_dir[:, j] + v_bulk[j]
+    return pos, vel

@@ -231,6 +231,8 @@ class Simulation:
             pos, vel = ics.plummer(n, L, seed=seed, **kw)
         elif kind == "clumps":
             pos, vel = ics.clumps(n, L, seed=seed, **kw)
+        elif kind == "two_galaxies":  # the reference's init_particles2 (main.py:312-357)
+            pos, vel = ics.reference_two_galaxies(n, L, self.cfg.particle_mass, seed=seed)
         else:
             raise ValueError(f"unknown particle set {kind!r}")
         self.set_particles(pos, vel)

@@ -3,12 +3,14 @@
 Run in a container that has the reference checkout (default /root/reference,
 or $MOG_REFERENCE) and the built oracle/_ref (python -m oracle.ref_build):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [transforms greens_kernel shaders two_galaxies]
 
 * transforms.npz   — Simulation.compute_transforms (main.py:157-172) with
                      the reference's own RandomSE3Sampler (main.py:9-62),
                      seeded; main.py is imported with its GL modules stubbed.
 * greens_kernel.npz — Simulation.init_greens_kernel (main.py:250-278).
+* two_galaxies.npz — Simulation.init_particles2 (main.py:312-357) after
+                     np.random.seed(seed), buffers captured from its writes.
 * shaders_g{8,16}.npz — the reference's compute shaders (compiled as C++ by
                      oracle/_ref) on small seeded particle sets: the mass
                      grid of mass.glsl, the gradient texture of the
@@ -124,11 +126,43 @@ def shaders():
                             params=np.array([L, G, dt, damping], dtype=np.float64))
 
 
+def initial_conditions(ref_main):
+    """Simulation.init_particles2 (main.py:312-357) after np.random.seed(s)."""
+    out = {}
+    for n, L, m, seed in [(1001, 100.0, 0.5, 3), (64, 250.0, 1.0, 0)]:
+        bufs = {}
+
+        class _Buf:
+            def __init__(self, name):
+                self.name = name
+
+            def write(self, data):
+                bufs[self.name] = data
+
+        fake = types.SimpleNamespace(num_particles=n, world_size=L, cfg={"particle_mass": m},
+                                     pos_buf=_Buf("pos"), vel_buf=_Buf("vel"))
+        np.random.seed(seed)
+        ref_main.Simulation.init_particles2(fake)
+        key = f"n{n}_L{int(L)}_s{seed}"
+        out[f"{key}_pos"] = np.frombuffer(bufs["pos"], dtype=np.float32).reshape(n, 4)
+        out[f"{key}_vel"] = np.frombuffer(bufs["vel"], dtype=np.float32).reshape(n, 4)
+        out[f"{key}_params"] = np.array([n, L, m, seed], dtype=np.float64)
+    np.savez_compressed(HERE / "two_galaxies.npz", **out)
+
+
+PARTS = {"transforms": transforms, "greens_kernel": greens_kernel, "shaders": None,
+         "two_galaxies": initial_conditions}
+
+
 def main():
+    """python tests/golden/make_golden.py [part ...]  (default: every part)"""
     ref_main = import_reference_main()
-    transforms(ref_main)
-    greens_kernel(ref_main)
-    shaders()
+    names = sys.argv[1:] or list(PARTS)
+    for name in names:
+        if name == "shaders":
+            shaders()
+        else:
+            PARTS[name](ref_main)
     for f in sorted(HERE.glob("*.npz")):
         print(f.name, f.stat().st_size)
 

@@ -94,3 +94,19 @@ def test_fp64_pipeline_matches_reference_components(shaders):
         assert pl.relative_l2(grad[..., 0], f64[..., 0]) > 0.5
     else:
         assert pl.relative_l2(grad[..., 0], f64[..., 0]) < 1e-5
+
+
+def test_two_galaxy_initialiser_matches_reference():
+    """ics.reference_two_galaxies == the reference's init_particles2
+    (main.py:312-357) after np.random.seed, bit for bit (fixture from the
+    reference itself)."""
+    from mog_solver_b200 import ics
+
+    d = np.load(GOLD / "two_galaxies.npz")
+    keys = sorted({k.rsplit("_", 1)[0] for k in d.files})
+    assert keys
+    for key in keys:
+        n, L, m, seed = d[f"{key}_params"]
+        pos, vel = ics.reference_two_galaxies(int(n), float(L), float(m), int(seed))
+        assert np.array_equal(pos.view(np.uint32), d[f"{key}_pos"].view(np.uint32)), key
+        assert np.array_equal(vel.view(np.uint32), d[f"{key}_vel"].view(np.uint32)), key
