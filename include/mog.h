@@ -349,6 +349,28 @@ int mog_learned_spread(mog_handle* h, double* out2, void* stream);
  */
 int mog_green_table(int32_t g, float world, float G, float softening, float* out);
 
+/*
+ * The reference's initial-condition sampler, init_particles.glsl (DIM 3) as
+ * init_particles_gpu dispatches it (main.py:283-310): particle i draws
+ * candidates from an integer hash of seed + 12345 i (inside a sphere,
+ * shape 1, or a cube, shape 0, of the world shrunk by spawn_buffer * L on
+ * every side), keeps the first whose random threshold falls below
+ * clamp(fbm + 1/2, 0, 1)^contrast (4-octave Perlin noise at
+ * noise_scale / L), falls back to a uniform draw after 64 tries, and gets
+ * a velocity uniform in [-L/2, L/2)^3.  pos4 / vel4: n float4 records
+ * (x, y, z, mass) and (vx, vy, vz, 0); n < 2^32.  The reference's default
+ * call is noise_scale 4, contrast 2, seed 12345, spawn_buffer 0.1, shape 1.
+ * mog_init_particles: device buffers, on `stream` (no synchronisation).
+ * mog_init_particles_host: host buffers, on the host (no GPU needed); the
+ * same arithmetic, with the host math library's cos, sin, acos and pow.
+ */
+int mog_init_particles(float* pos4, float* vel4, int64_t n, float world, float noise_scale,
+                       float contrast, uint32_t seed, float mass, float spawn_buffer,
+                       int32_t shape, void* stream);
+int mog_init_particles_host(float* pos4, float* vel4, int64_t n, float world, float noise_scale,
+                            float contrast, uint32_t seed, float mass, float spawn_buffer,
+                            int32_t shape);
+
 /* Human-readable text for a status code, and the calling thread's last
  * error message. */
 const char* mog_strerror(int code);

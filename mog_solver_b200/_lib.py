@@ -46,7 +46,7 @@ EXPORTS = (
     "mog_config_default", "mog_create", "mog_destroy", "mog_step", "mog_step_n",
     "mog_step_profiled", "mog_forces", "mog_deposit", "mog_solve", "mog_update", "mog_get_status",
     "mog_get_tuning", "mog_set_tuning", "mog_diagnostics", "mog_direct_sum",
-    "mog_direct_sum_noalloc", "mog_green_table",
+    "mog_direct_sum_noalloc", "mog_green_table", "mog_init_particles", "mog_init_particles_host",
     "mog_batch_create", "mog_batch_step", "mog_batch_destroy",
     "mog_model_create", "mog_model_destroy", "mog_model_set", "mog_model_get",
     "mog_model_train_step", "mog_features", "mog_learned_forces", "mog_learned_step",
@@ -129,6 +129,9 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.mog_direct_sum.argtypes = [P, I64, P, I64, D, D, D, P, P]
     lib.mog_direct_sum_noalloc.argtypes = [P, I64, P, I64, D, D, D, P, P]
     lib.mog_green_table.argtypes = [ctypes.c_int32, F, F, F, P]
+    U32 = ctypes.c_uint32
+    lib.mog_init_particles.argtypes = [P, P, I64, F, F, F, U32, F, F, ctypes.c_int32, P]
+    lib.mog_init_particles_host.argtypes = [P, P, I64, F, F, F, U32, F, F, ctypes.c_int32]
     FP = ctypes.POINTER(ctypes.c_float)
     lib.mog_batch_create.argtypes = [P, ctypes.c_int32, ctypes.POINTER(P)]
     lib.mog_batch_step.argtypes = [P, P, P, P, P, ctypes.c_int32, P]

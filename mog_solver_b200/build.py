@@ -20,7 +20,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 OUT = PKG / "libmog.so"
 SOURCES = ["mog_api.cu", "deposit.cu", "spectral.cu", "update.cu", "convolution.cu",
-           "diagnostics.cu", "sort.cu", "learned.cu", "dft_tc.cu"]
+           "diagnostics.cu", "sort.cu", "learned.cu", "dft_tc.cu", "ics.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

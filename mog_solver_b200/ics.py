@@ -14,7 +14,10 @@ use their own seeded distributions instead:
 * ``clumps``          a Gaussian mixture (log-uniform widths) plus a uniform
                       background fraction;
 * ``reference_two_galaxies`` the reference's own two-galaxy routine,
-                      seeded (bit-identical to it after np.random.seed).
+                      seeded (bit-identical to it after np.random.seed);
+* ``perlin_host``     the reference's GPU Perlin/fBm rejection sampler
+                      (init_particles.glsl) on the host through libmog;
+                      ``Simulation.init_particles("perlin")`` runs it on the GPU.
 
 Every record is (x, y, z, m) for positions and (vx, vy, vz, 0) for
 velocities, the std430 vec4 layout of the reference's buffers
@@ -169,4 +172,32 @@ def reference_two_galaxies(n: int, world: float = 100.0, particle_mass: float = 
         v_dir = v_dir / (np.linalg.norm(v_dir, axis=1, keepdims=True) + 1e-10)
         for j in range(3):
             vel[lo:hi, j] = v_circ * v_dir[:, j] + v_bulk[j]
+    return pos, vel
+
+
+def perlin_args(n: int, world: float, mass: float, spawn_buffer: float = 0.1, seed: int = 12345,
+                noise_scale: float = 4.0, density_contrast: float = 2.0, shape: str = "sphere"):
+    """Arguments of mog_init_particles after the buffers (stream excluded).
+    Defaults: the reference's call, init_particles_gpu(noise_scale=4.0,
+    density_contrast=2.0, seed=12345) with spawnShape 1 (main.py:280-305)."""
+    if shape not in ("sphere", "cube"):
+        raise ValueError("shape must be 'sphere' or 'cube'")
+    return (int(n), float(world), float(noise_scale), float(density_contrast),
+            int(seed) & 0xFFFFFFFF, float(mass), float(spawn_buffer), 1 if shape == "sphere" else 0)
+
+
+def perlin_host(n: int, world: float = 100.0, mass: float = 1.0, spawn_buffer: float = 0.1,
+                seed: int = 12345, noise_scale: float = 4.0, density_contrast: float = 2.0,
+                shape: str = "sphere"):
+    """init_particles.glsl on the host (mog_init_particles_host; no GPU needed)."""
+    import ctypes
+
+    from . import _lib
+
+    pos = np.zeros((n, 4), dtype=np.float32)
+    vel = np.zeros((n, 4), dtype=np.float32)
+    args = perlin_args(n, world, mass, spawn_buffer, seed, noise_scale, density_contrast, shape)
+    _lib.check(_lib.lib().mog_init_particles_host(pos.ctypes.data_as(ctypes.c_void_p),
+                                                  vel.ctypes.data_as(ctypes.c_void_p), *args),
+               "mog_init_particles_host")
     return pos, vel

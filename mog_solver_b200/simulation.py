@@ -218,10 +218,16 @@ class Simulation:
         self.vel = v
         self._auto_bits = None  # the fixed-point scale depends on the masses
 
-    def init_particles(self, kind: str = "uniform", seed: int = 0, **kw) -> None:
+    def init_particles(self, kind: str = "uniform", seed: int | None = None, **kw) -> None:
+        """Replace the particles with a named initial set: uniform, disks,
+        plummer, clumps (seed default 0), two_galaxies (the reference's
+        init_particles2) or perlin (the reference's GPU sampler,
+        init_particles.glsl, seed default 12345 as in main.py:281)."""
         from . import ics
 
         n, L = self.cfg.num_particles, self.cfg.world_size
+        if seed is None:
+            seed = 12345 if kind == "perlin" else 0
         if kind == "uniform":
             pos, vel = ics.uniform_cube(n, L, seed=seed, **kw)
         elif kind == "disks":
@@ -233,6 +239,15 @@ class Simulation:
             pos, vel = ics.clumps(n, L, seed=seed, **kw)
         elif kind == "two_galaxies":  # the reference's init_particles2 (main.py:312-357)
             pos, vel = ics.reference_two_galaxies(n, L, self.cfg.particle_mass, seed=seed)
+        elif kind == "perlin":  # the reference's GPU sampler (main.py:280-310), on this GPU
+            torch = _torch()
+            pos = torch.empty((n, 4), dtype=torch.float32, device=self.device)
+            vel = torch.empty_like(pos)
+            args = ics.perlin_args(n, L, self.cfg.particle_mass, self.cfg.spawn_buffer,
+                                   seed=seed, **kw)
+            with torch_device(self.device):
+                _lib.check(_lib.lib().mog_init_particles(pos.data_ptr(), vel.data_ptr(), *args,
+                                                         self._stream()), "mog_init_particles")
         else:
             raise ValueError(f"unknown particle set {kind!r}")
         self.set_particles(pos, vel)

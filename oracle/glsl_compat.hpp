@@ -8,10 +8,13 @@
 //    written (the harness is built with -ffp-contract=off);
 //  * mat3 * vec3 = (col0 * v.x + col1 * v.y) + col2 * v.z, component-wise;
 //  * mod(x, y) = x - y * floor(x / y) with IEEE division;
-//  * cos / sin are the C library's cosf / sinf;
+//  * cos / sin / acos / pow are the C library's cosf / sinf / acosf / powf;
+//  * mix(x, y, a) = x * (1 - a) + y * a; fract(x) = x - floor(x);
+//    clamp(x, lo, hi) = min(max(x, lo), hi);
 //  * rg32f images keep two channels and read back as (r, g, 0, 1).
 #pragma once
 
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdint>
@@ -53,12 +56,22 @@ struct uvec3 {
     uint x, y, z;
 };
 
+struct ivec2 {
+    int x, y;
+    ivec2() : x(0), y(0) {}
+    ivec2(int a, int b) : x(a), y(b) {}
+    explicit ivec2(const vec2& v) : x((int)v.x), y((int)v.y) {}
+};
+
 struct ivec3 {
     int x, y, z;
     ivec3() : x(0), y(0), z(0) {}
     ivec3(int a, int b, int c) : x(a), y(b), z(c) {}
     explicit ivec3(const uvec3& u) : x((int)u.x), y((int)u.y), z((int)u.z) {}
+    explicit ivec3(const vec3& v) : x((int)v.x), y((int)v.y), z((int)v.z) {}
 };
+inline ivec2 operator+(const ivec2& a, const ivec2& b) { return ivec2(a.x + b.x, a.y + b.y); }
+inline ivec3 operator+(const ivec3& a, const ivec3& b) { return ivec3(a.x + b.x, a.y + b.y, a.z + b.z); }
 
 struct bvec3 {
     bool x, y, z;
@@ -72,6 +85,10 @@ struct mat3 {
 inline vec2 operator+(const vec2& a, const vec2& b) { return vec2(a.x + b.x, a.y + b.y); }
 inline vec2 operator-(const vec2& a, const vec2& b) { return vec2(a.x - b.x, a.y - b.y); }
 inline vec2 operator*(const vec2& a, float s) { return vec2(a.x * s, a.y * s); }
+inline vec2 operator/(const vec2& a, float s) { return vec2(a.x / s, a.y / s); }
+inline vec2 operator+(const vec2& a, float s) { return vec2(a.x + s, a.y + s); }
+inline vec2 operator-(const vec2& a, float s) { return vec2(a.x - s, a.y - s); }
+inline float dot(const vec2& a, const vec2& b) { return a.x * b.x + a.y * b.y; }
 
 inline vec3 operator+(const vec3& a, const vec3& b) { return vec3(a.x + b.x, a.y + b.y, a.z + b.z); }
 inline vec3 operator-(const vec3& a, const vec3& b) { return vec3(a.x - b.x, a.y - b.y, a.z - b.z); }
@@ -89,6 +106,16 @@ inline mat3 transpose(const mat3& m) {
 }
 
 inline float floor(float x) { return std::floor(x); }
+inline vec2 floor(const vec2& v) { return vec2(floor(v.x), floor(v.y)); }
+inline vec3 floor(const vec3& v) { return vec3(floor(v.x), floor(v.y), floor(v.z)); }
+inline float fract(float x) { return x - floor(x); }
+inline vec2 fract(const vec2& v) { return vec2(fract(v.x), fract(v.y)); }
+inline vec3 fract(const vec3& v) { return vec3(fract(v.x), fract(v.y), fract(v.z)); }
+inline float dot(const vec3& a, const vec3& b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+inline float acos(float x) { return std::acos(x); }
+inline float pow(float x, float y) { return std::pow(x, y); }
+inline float clamp(float x, float lo, float hi) { return std::min(std::max(x, lo), hi); }
+inline float mix(float x, float y, float a) { return x * (1.0f - a) + y * a; }
 inline float abs(float x) { return std::fabs(x); }
 inline int abs(int x) { return x < 0 ? -x : x; }
 inline float cos(float x) { return std::cos(x); }

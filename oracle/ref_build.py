@@ -1,7 +1,8 @@
 """Build oracle/_ref: the reference's own GLSL compute shaders compiled as C++.
 
 TEST AND CPU-BASELINE INFRASTRUCTURE ONLY.  Reads the seven hot-path shaders
-(shaders/{mass,complex,fft_batched,fourier,greens,pack,update}.glsl) from a
+(shaders/{mass,complex,fft_batched,fourier,greens,pack,update}.glsl) and the
+initial-condition sampler (shaders/init_particles.glsl) from a
 reference checkout (default /root/reference, or $MOG_REFERENCE), rewrites
 their GLSL-only declarations with a handful of regular expressions (SSBO
 blocks -> SSBO<T>, image uniforms -> image references, layout qualifiers
@@ -26,7 +27,7 @@ HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
 GEN = OUT / "gen"
 LIB = OUT / "libmogref.so"
-SHADERS = ["mass", "complex", "fft_batched", "fourier", "greens", "pack", "update"]
+SHADERS = ["mass", "complex", "fft_batched", "fourier", "greens", "pack", "update", "init_particles"]
 
 
 def reference_root() -> Path:

@@ -22,6 +22,7 @@
 #include "greens.inc"
 #include "pack.inc"
 #include "update.inc"
+#include "init_particles.inc"
 
 namespace glsl {
 thread_local uvec3 gl_GlobalInvocationID;
@@ -217,6 +218,30 @@ __attribute__((visibility("default"))) void ref_step(float* pos4, float* vel4, i
     do_mass(pos4, n, off4, rot12, k, g, world, voxel, mass_scratch);
     do_solve(mass_scratch, k, g, world, Gc);
     do_update(pos4, vel4, n, off4, rot12, k, g, world, voxel, dt, damping);
+}
+
+// init_particles.glsl as init_particles_gpu (main.py:283-310) dispatches
+// it: numParticles, worldSize, noiseScale, densityContrast, seed, baseMass,
+// spawnBuffer, spawnShape as given; (n + 255) / 256 groups of 256.
+__attribute__((visibility("default"))) void ref_init_particles(float* pos4, float* vel4, int n,
+                                                               float world, float noise_scale,
+                                                               float contrast, uint32_t seed,
+                                                               float mass, float spawn_buffer,
+                                                               uint32_t shape) {
+    namespace S = init_particles_glsl;
+    S::numParticles = (uint)n;
+    S::worldSize = world;
+    S::noiseScale = noise_scale;
+    S::densityContrast = contrast;
+    S::seed = seed;
+    S::baseMass = mass;
+    S::spawnBuffer = spawn_buffer;
+    S::spawnShape = shape;
+    S::positions.data = reinterpret_cast<vec4*>(pos4);
+    S::positions.n = n;
+    S::velocities.data = reinterpret_cast<vec4*>(vel4);
+    S::velocities.n = n;
+    dispatch((n + 255) / 256, 1, 1, 256, 1, 1, [] { S::main(); });
 }
 
 }  // extern "C"

@@ -36,6 +36,8 @@ def lib() -> ctypes.CDLL:
         h.ref_update.argtypes = [P, P, I, P, P, I, I, F, F, F, F, P]
         h.ref_update.restype = None
         h.ref_step.argtypes = [P, P, I, P, P, I, I, F, F, F, F, F, P]
+        U = ctypes.c_uint32
+        h.ref_init_particles.argtypes = [P, P, I, F, F, F, U, F, F, U]
         h.ref_step.restype = None
         _lib = h
     return _lib
@@ -94,6 +96,19 @@ def step(pos4, vel4, off4, rot12, g: int, world: float, G: float, dt: float, dam
     lib().ref_step(_p(pos), _p(vel), pos.shape[0], _p(off), _p(rot), k, g, world,
                    voxel(world, g), G, dt, damping, _p(mass))
     return pos, vel, mass
+
+
+def init_particles(n: int, world: float, noise_scale: float = 4.0, contrast: float = 2.0,
+                   seed: int = 12345, mass: float = 1.0, spawn_buffer: float = 0.1,
+                   shape: int = 1):
+    """init_particles.glsl (DIM 3) as init_particles_gpu dispatches it; returns
+    (pos, vel) float32 (n, 4)."""
+    pos = np.zeros((n, 4), dtype=np.float32)
+    vel = np.zeros((n, 4), dtype=np.float32)
+    lib().ref_init_particles(_p(pos), _p(vel), n, float(world), float(noise_scale),
+                             float(contrast), int(seed) & 0xFFFFFFFF, float(mass),
+                             float(spawn_buffer), int(shape))
+    return pos, vel
 
 
 def time_steps(pos4, vel4, off4, rot12, w: dict, steps: int):

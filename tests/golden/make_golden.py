@@ -3,12 +3,14 @@
 Run in a container that has the reference checkout (default /root/reference,
 or $MOG_REFERENCE) and the built oracle/_ref (python -m oracle.ref_build):
 
-    python tests/golden/make_golden.py [transforms greens_kernel shaders two_galaxies]
+    python tests/golden/make_golden.py [transforms greens_kernel shaders two_galaxies init_particles]
 
 * transforms.npz   — Simulation.compute_transforms (main.py:157-172) with
                      the reference's own RandomSE3Sampler (main.py:9-62),
                      seeded; main.py is imported with its GL modules stubbed.
 * greens_kernel.npz — Simulation.init_greens_kernel (main.py:250-278).
+* init_particles.npz — init_particles.glsl, the GPU Perlin/fBm rejection
+                     sampler (compiled as C++ by oracle/_ref), two seeded cases.
 * two_galaxies.npz — Simulation.init_particles2 (main.py:312-357) after
                      np.random.seed(seed), buffers captured from its writes.
 * shaders_g{8,16}.npz — the reference's compute shaders (compiled as C++ by
@@ -150,8 +152,26 @@ def initial_conditions(ref_main):
     np.savez_compressed(HERE / "two_galaxies.npz", **out)
 
 
+def perlin_sampler(ref_main=None):
+    """init_particles.glsl (compiled as C++ by oracle/_ref): the reference's
+    default call (main.py:280-281: noise 4, contrast 2, seed 12345, sphere)
+    and a cube-shaped variant."""
+    from oracle import ref_harness as rh
+
+    assert rh.available(), "build oracle/_ref first (python -m oracle.ref_build)"
+    out = {}
+    for n, L, noise, contrast, seed, m, buf, shape in [(4096, 100.0, 4.0, 2.0, 12345, 1.0, 0.1, 1),
+                                                       (3000, 250.0, 2.5, 3.0, 7, 0.25, 0.05, 0)]:
+        pos, vel = rh.init_particles(n, L, noise, contrast, seed, m, buf, shape)
+        key = f"n{n}_shape{shape}"
+        out[f"{key}_pos"] = pos
+        out[f"{key}_vel"] = vel
+        out[f"{key}_params"] = np.array([n, L, noise, contrast, seed, m, buf, shape], dtype=np.float64)
+    np.savez_compressed(HERE / "init_particles.npz", **out)
+
+
 PARTS = {"transforms": transforms, "greens_kernel": greens_kernel, "shaders": None,
-         "two_galaxies": initial_conditions}
+         "two_galaxies": initial_conditions, "init_particles": perlin_sampler}
 
 
 def main():

@@ -110,3 +110,31 @@ def test_two_galaxy_initialiser_matches_reference():
         pos, vel = ics.reference_two_galaxies(int(n), float(L), float(m), int(seed))
         assert np.array_equal(pos.view(np.uint32), d[f"{key}_pos"].view(np.uint32)), key
         assert np.array_equal(vel.view(np.uint32), d[f"{key}_vel"].view(np.uint32)), key
+
+
+def test_perlin_sampler_host_matches_reference_shader():
+    """mog_init_particles_host == init_particles.glsl (the reference's GPU
+    initial-condition sampler, compiled as C++ by oracle/_ref), bit for bit,
+    for the reference's default call and a cube-shaped variant."""
+    from mog_solver_b200 import ics
+
+    d = np.load(GOLD / "init_particles.npz")
+    for key in sorted({k.rsplit("_", 1)[0] for k in d.files}):
+        n, L, noise, contrast, seed, m, buf, shape = d[f"{key}_params"]
+        pos, vel = ics.perlin_host(int(n), float(L), float(m), float(buf), int(seed), float(noise),
+                                   float(contrast), "sphere" if int(shape) == 1 else "cube")
+        assert np.array_equal(pos.view(np.uint32), d[f"{key}_pos"].view(np.uint32)), key
+        assert np.array_equal(vel.view(np.uint32), d[f"{key}_vel"].view(np.uint32)), key
+
+
+def test_perlin_sampler_rejects_bad_arguments():
+    import ctypes
+
+    from mog_solver_b200 import _lib
+
+    lib = _lib.lib()
+    buf = np.zeros((4, 4), np.float32)
+    p = buf.ctypes.data_as(ctypes.c_void_p)
+    assert lib.mog_init_particles_host(p, p, 4, -1.0, 4.0, 2.0, 1, 1.0, 0.1, 1) == _lib.MOG_ERR_ARG
+    assert lib.mog_init_particles_host(p, p, 4, 100.0, 4.0, 2.0, 1, 1.0, 0.1, 2) == _lib.MOG_ERR_ARG
+    assert lib.mog_init_particles_host(None, None, 0, 100.0, 4.0, 2.0, 1, 1.0, 0.1, 1) == _lib.MOG_OK
