@@ -221,8 +221,9 @@ def run_reference(args, w: dict) -> None:
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": res["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-        "config": {"workload": w["desc"], "n": w["n"], "k": w["k"], "g": w["g"],
-                   "sample_particles": res["sample_n"]},
+        "config": {"workload": w["desc"] + ("; the reference's plain k=240 step (it has no learned "
+                                            "path)" if "k_small" in w else ""),
+                   "n": w["n"], "k": w["k"], "g": w["g"], "sample_particles": res["sample_n"]},
         "cpu_baseline": {"value": res["value"], "unit": UNIT, "cores": res["cores"],
                          "kind": res["kind"], "sample": res["sample"]},
         "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
