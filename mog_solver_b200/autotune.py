@@ -53,13 +53,13 @@ def _measure(sim: Simulation, reps: int) -> np.ndarray:
 
 def _candidates(sim: Simulation) -> dict[str, list[dict]]:
     g = sim.cfg.grid_size
-    dep = [dict(deposit_grids_per_cta=gpc, deposit_ppt=ppt, deposit_threads=thr)
+    dep = [dict(deposit_grids_per_cta=gpc, deposit_ppt=ppt, deposit_threads=thr, deposit_chunks=0)
            for gpc, ppt, thr in itertools.product([0, 3, 6] if g <= 16 else [0],
                                                   [2, 4], [512, 1024])]
     dep.append(dict(deposit_grids_per_cta=-1))
     upd = [dict(update_staged=0, update_direct_ppt=1), dict(update_staged=0, update_direct_ppt=4)]
     if g <= 16:
-        upd.append(dict(update_staged=1))
+        upd += [dict(update_staged=1, update_threads=t) for t in (512, 768, 1024)]
     order = [dict(sort_every=0), dict(sort_every=16)]
     return {"deposit": dep, "update": upd, "order": order}
 
