@@ -1,9 +1,10 @@
 """A few steps of a fixed workload, for running under a profiler.
 
-    python -m mog_solver_b200.profile_step [--path plain|learned] [--steps 6]
+    python -m mog_solver_b200.profile_step [--path plain|learned] [--steps 6] [--n N]
+                                           [--k K] [--g 16|32] [--dft fp32|bf16x3]
 
-plain:   k = 240 grids of 16^3, the colliding-disk set (N = 1,048,576,
-         seeded two exponential disks), mog_step;
+plain:   k = 240 grids of 16^3 (or --k, --g, --dft), the colliding-disk set
+         (N = 1,048,576, seeded two exponential disks), mog_step;
 learned: k = 32 grids of 16^3, the same particles, mog_learned_step with the
          committed model (models/learned_k32_g16.npz).
 Everything is set up first; the steps run back to back on the default
@@ -19,6 +20,9 @@ def main() -> None:
     ap.add_argument("--path", default="plain", choices=["plain", "learned"])
     ap.add_argument("--steps", type=int, default=6)
     ap.add_argument("--n", type=int, default=1 << 20)
+    ap.add_argument("--k", type=int, default=0, help="grids (default 240 plain, 32 learned)")
+    ap.add_argument("--g", type=int, default=16)
+    ap.add_argument("--dft", default="fp32", choices=["fp32", "bf16x3"])
     a = ap.parse_args()
 
     import torch
@@ -29,8 +33,10 @@ def main() -> None:
     from .train_learned import DEFAULT_MODEL
 
     k, seed = (240, 2000) if a.path == "plain" else (32, 1000)
-    sim = Simulation({"n_grids": k, "grid_size": 16, "world_size": 100.0, "num_particles": a.n,
-                      "G": 100.0, "dt": 1e-5, "damping": 0.999, "seed": seed})
+    k = a.k or k
+    sim = Simulation({"n_grids": k, "grid_size": a.g, "world_size": 100.0, "num_particles": a.n,
+                      "G": 100.0, "dt": 1e-5, "damping": 0.999, "seed": seed,
+                      "dft_precision": a.dft})
     pos, vel = ics.two_disks(a.n, 100.0, seed=1, g_eff=sim.effective_g())
     sim.set_particles(pos, vel)
     lib = _lib.lib()
@@ -45,7 +51,7 @@ def main() -> None:
                                             sim.vel.data_ptr(), a.n, 1e-5, None), "mog_learned_step")
     torch.cuda.synchronize()
     sim.check()
-    print(f"{a.path}: {a.steps} steps of N={a.n}, k={k}: ok")
+    print(f"{a.path}: {a.steps} steps of N={a.n}, k={k}, g={a.g}, dft={a.dft}: ok")
 
 
 if __name__ == "__main__":
