@@ -76,6 +76,10 @@ extern "C" {
 #define MOG_FLAG_OVERFLOW   2u
 #define MOG_FLAG_TIMEOUT    4u
 #define MOG_FLAG_BADMASS    8u
+/* an index outside its buffer was caught and the access skipped; raised
+   only by a library built with -DMOG_CHECK (python -m mog_solver_b200.build
+   --check), whose kernels bounds-check their scatter and gather indices */
+#define MOG_FLAG_BOUNDS    16u
 
 /*
  * Configuration.  Field names follow config.yaml (config.yaml:2-18) and

@@ -11,8 +11,8 @@ The package mirrors the reference's operator surface (tbmo/mog-solver
 main.py: ``load_config``, ``RandomSE3Sampler``, ``compute_transforms``,
 ``Simulation.step``); every force evaluation runs in hand-written CUDA.
 """
-from ._lib import (MogError, MogLibraryError, FLAG_BADMASS, FLAG_NONFINITE, FLAG_OVERFLOW,
-                   FLAG_TIMEOUT)
+from ._lib import (MogError, MogLibraryError, FLAG_BADMASS, FLAG_BOUNDS, FLAG_NONFINITE,
+                   FLAG_OVERFLOW, FLAG_TIMEOUT)
 from .config import MogConfig, REFERENCE_DEFAULTS, load_config
 from .transforms import RandomSE3Sampler, compute_transforms, rotation_matrices
 from .simulation import Simulation, auto_scale_bits
@@ -20,6 +20,6 @@ from .simulation import Simulation, auto_scale_bits
 __all__ = [
     "MogConfig", "MogError", "MogLibraryError", "REFERENCE_DEFAULTS", "RandomSE3Sampler",
     "Simulation", "auto_scale_bits", "compute_transforms", "load_config", "rotation_matrices",
-    "FLAG_BADMASS", "FLAG_NONFINITE", "FLAG_OVERFLOW", "FLAG_TIMEOUT",
+    "FLAG_BADMASS", "FLAG_BOUNDS", "FLAG_NONFINITE", "FLAG_OVERFLOW", "FLAG_TIMEOUT",
 ]
 __version__ = "0.1.0"

@@ -40,6 +40,7 @@ FLAG_NONFINITE = 1
 FLAG_OVERFLOW = 2
 FLAG_TIMEOUT = 4
 FLAG_BADMASS = 8
+FLAG_BOUNDS = 16  # only from a library built with --check
 
 # Every symbol include/mog.h declares.
 EXPORTS = (

@@ -136,7 +136,10 @@ __global__ void __launch_bounds__(1024) deposit_smem_kernel(const float4* __rest
             const int64_t slot = base + (int64_t)u * T + threadIdx.x;
             valid[u] = slot < hi;
             float4 P = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (valid[u]) P = __ldg(pos + (perm ? (int64_t)__ldg(perm + slot) : slot));
+            if (valid[u]) {
+                const int64_t src = perm ? (int64_t)__ldg(perm + slot) : slot;
+                if (in_bounds(e.flags, (uint64_t)src, (uint64_t)n)) P = __ldg(pos + src);
+            }
             unsigned b = 0;
             if (MODE == 1)
                 q[u] = valid[u] ? quantize_u64(P.w, e.scale, b) : 0ull;
@@ -215,7 +218,8 @@ __global__ void __launch_bounds__(1024) deposit_smem_kernel(const float4* __rest
         const Acc v = H::read(lo_w, hi_w, i);
         if (v) {
             const uint32_t j = i >> slab_lg, c = i & (slab_cells - 1);
-            atomicAdd(mass + (size_t)(g0 + j) * gcells + slab_lo + c, v);
+            const size_t cell = (size_t)(g0 + j) * gcells + slab_lo + c;
+            if (in_bounds(e.flags, cell, (uint64_t)e.cells())) atomicAdd(mass + cell, v);
         }
     }
 }
@@ -324,6 +328,7 @@ __global__ void __launch_bounds__(1024) deposit_fast_kernel(const float4* __rest
 #pragma unroll
             for (int u = 0; u < PPT; ++u) {
                 const uint32_t off = gbyte + cell_byte_offset<LG>(r0, r1, r2, cx[u], cy[u], cz[u]);
+                if (!in_bounds(e.flags, off >> 2, words)) continue;
                 if (MODE == 0) {
                     if (ql[u]) red_shared(lo_base + off, ql[u]);   // zero for padding lanes
                 } else if (SPLIT) {
@@ -350,7 +355,8 @@ __global__ void __launch_bounds__(1024) deposit_fast_kernel(const float4* __rest
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) {
         const Acc v = SPLIT ? (Acc)hi_w[i] << 32 : H::read(lo_w, hi_w, i);
-        if (v) atomicAdd(mass + (size_t)g0 * G3 + i, v);
+        if (v && in_bounds(e.flags, (size_t)g0 * G3 + i, (uint64_t)e.cells()))
+            atomicAdd(mass + (size_t)g0 * G3 + i, v);
     }
 }
 
@@ -377,7 +383,8 @@ __global__ void __launch_bounds__(256) deposit_global_kernel(const float4* __res
         } else {
             cell = cell_exact(e.rot12 + 12 * i, e.off4 + 4 * i, cx, cy, cz, ip);
         }
-        if (q) atomicAdd(mass + (size_t)i * gcells + cell, q);
+        if (q && in_bounds(e.flags, (size_t)i * gcells + cell, (uint64_t)e.cells()))
+            atomicAdd(mass + (size_t)i * gcells + cell, q);
     }
     if (sizeof(Acc) == 8) {
         double qs = (double)q;  // blocks are whole warps, so every lane is present

@@ -200,6 +200,7 @@ __device__ __forceinline__ void gather_one(const GridRows& x, int i, const float
         gy = ty - floorf(ty);
         gz = tz - floorf(tz);
     }
+    if (!in_bounds(e.flags, c, (uint64_t)G3)) c = 0;
     const float4 f = __ldg(W + (size_t)i * G3 + c);
     a.sx = __fadd_rn(a.sx, f.x);
     a.sy = __fadd_rn(a.sy, f.y);

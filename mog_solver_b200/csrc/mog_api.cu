@@ -315,7 +315,7 @@ int order_particles(mog_handle* h, const float4* pos, int64_t n, bool sort, cuda
         h->perm_cap = n;
     }
     if (sort || h->perm_n != n) {
-        cudaError_t err = mog::launch_sort(pos, n, h->e.world, h->d_sort, h->d_perm, s);
+        cudaError_t err = mog::launch_sort(pos, n, h->e.world, h->d_sort, h->d_perm, h->d_flags, s);
         if (err != cudaSuccess) return cuda_fail(err, "spatial order");
         h->perm_n = n;
     }

@@ -221,4 +221,19 @@ __device__ __forceinline__ void raise_flags(unsigned* flags, unsigned bits) {
     if (any && (threadIdx.x & 31) == __ffs(__activemask()) - 1) atomicOr(flags, any);
 }
 
+// Debug bounds check of a computed index i into a buffer of n elements.
+// Built with -DMOG_CHECK, an index outside [0, n) raises MOG_FLAG_BOUNDS (16)
+// in the status word and the caller skips the access, so a wrong index
+// shows in mog_get_status instead of writing someone else's memory.
+// Without it the check is the constant true and costs nothing.
+#ifdef MOG_CHECK
+__device__ __forceinline__ bool in_bounds(unsigned* flags, uint64_t i, uint64_t n) {
+    if (i < n) return true;
+    atomicOr(flags, 16u);
+    return false;
+}
+#else
+__device__ __forceinline__ constexpr bool in_bounds(unsigned*, uint64_t, uint64_t) { return true; }
+#endif
+
 }  // namespace mog

@@ -112,7 +112,7 @@ size_t sort_scratch_bytes();
 cudaError_t launch_gather_sorted(const float4* pos, const int* perm, int64_t n, float4* out,
                                  cudaStream_t s);
 cudaError_t launch_sort(const float4* pos, int64_t n, float world, void* scratch, int* perm,
-                        cudaStream_t s);
+                        unsigned* flags, cudaStream_t s);
 
 // Green's-function and wave-number tables (FP64 arithmetic on the device).
 cudaError_t launch_build_tables(int g, float world, float G, float* green, float* ktab,

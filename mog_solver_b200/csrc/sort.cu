@@ -89,7 +89,8 @@ __global__ void __launch_bounds__(1024) sort_scan_kernel(const unsigned* __restr
 __global__ void __launch_bounds__(256) sort_scatter_kernel(const float4* __restrict__ pos,
                                                            int64_t n, float inv_cell,
                                                            unsigned* __restrict__ cursor,
-                                                           int* __restrict__ perm) {
+                                                           int* __restrict__ perm,
+                                                           unsigned* flags) {
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = p < n;
     const uint32_t key = valid ? bin_of(pos[p], inv_cell) : 0xffffffffu;
@@ -101,7 +102,7 @@ __global__ void __launch_bounds__(256) sort_scatter_kernel(const float4* __restr
     base = __shfl_sync(kFull, base, leader);
     if (valid) {
         const unsigned rank = __popc(m & ((1u << lane) - 1u));
-        perm[base + rank] = (int)p;
+        if (in_bounds(flags, (uint64_t)base + rank, (uint64_t)n)) perm[base + rank] = (int)p;
     }
 }
 
@@ -124,7 +125,7 @@ cudaError_t launch_gather_sorted(const float4* pos, const int* perm, int64_t n, 
 size_t sort_scratch_bytes() { return 2 * (size_t)kBins * sizeof(unsigned); }
 
 cudaError_t launch_sort(const float4* pos, int64_t n, float world, void* scratch, int* perm,
-                        cudaStream_t s) {
+                        unsigned* flags, cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
     unsigned* count = static_cast<unsigned*>(scratch);
     unsigned* cursor = count + kBins;
@@ -134,7 +135,7 @@ cudaError_t launch_sort(const float4* pos, int64_t n, float world, void* scratch
     const unsigned blocks = (unsigned)((n + 255) / 256);
     sort_count_kernel<<<blocks, 256, 0, s>>>(pos, n, inv_cell, count);
     sort_scan_kernel<<<1, 1024, 0, s>>>(count, cursor);
-    sort_scatter_kernel<<<blocks, 256, 0, s>>>(pos, n, inv_cell, cursor, perm);
+    sort_scatter_kernel<<<blocks, 256, 0, s>>>(pos, n, inv_cell, cursor, perm, flags);
     return cudaGetLastError();
 }
 

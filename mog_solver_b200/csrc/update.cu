@@ -104,8 +104,13 @@ __device__ __forceinline__ uint32_t cell_of(int idx_mode, const float* xf, float
     return cell_exact(xf, xf + 12, cx, cy, cz, ip);
 }
 
-__device__ __forceinline__ int64_t particle_of(const int* __restrict__ perm, int64_t slot) {
-    return perm ? (int64_t)__ldg(perm + slot) : slot;
+// Particle in slot `slot` (slot < n).  A checked build redirects a
+// permutation entry outside [0, n) to the slot itself and flags it.
+__device__ __forceinline__ int64_t particle_of(const int* __restrict__ perm, int64_t slot,
+                                               int64_t n, unsigned* flags) {
+    if (!perm) return slot;
+    const int64_t p = (int64_t)__ldg(perm + slot);
+    return in_bounds(flags, (uint64_t)p, (uint64_t)n) ? p : slot;
 }
 
 // Copy grid i's force field (or the z-slabs of it that the CTA's particles
@@ -219,7 +224,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         float4 P = make_float4(0.f, 0.f, 0.f, 0.f);
         if (j < cnt) {
             const int64_t slot = first + (int64_t)j * T;
-            P = pos_s ? pos_s[slot] : pos[particle_of(perm, slot)];
+            P = pos_s ? pos_s[slot] : pos[particle_of(perm, slot, n, e.flags)];
         }
         cx[j] = __fsub_rn(P.x, ip.half_l);
         cy[j] = __fsub_rn(P.y, ip.half_l);
@@ -273,7 +278,8 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
         for (int j = 0; j < PPT; ++j) {
             if (j < cnt) {
-                const uint32_t c = cell_of(IDX, x, cx[j], cy[j], cz[j], ip);
+                uint32_t c = cell_of(IDX, x, cx[j], cy[j], cz[j], ip);
+                if (!in_bounds(e.flags, c, (uint64_t)G3)) c = 0;
                 const float4 f = F[c];
                 ax[j] = __fadd_rn(ax[j], f.x);
                 ay[j] = __fadd_rn(ay[j], f.y);
@@ -307,7 +313,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     for (int j = 0; j < PPT; ++j) {
         if (j < cnt) {
             const int64_t slot = first + (int64_t)j * T;
-            const int64_t p = particle_of(perm, slot);
+            const int64_t p = particle_of(perm, slot, n, e.flags);
             const float4 P = pos_s ? pos_s[slot] : pos[p];
             finish_particle<ACC_OUT>(p, P, ax[j], ay[j], az[j], pos, vel, acc_out, kf, dt, damp,
                                      e.world, bad);
@@ -335,7 +341,7 @@ __global__ void __launch_bounds__(256) update_direct_kernel(float4* __restrict__
 #pragma unroll
     for (int j = 0; j < DPPT; ++j) {
         float4 P = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (j < cnt) P = pos_s ? pos_s[first + j] : pos[particle_of(perm, first + j)];
+        if (j < cnt) P = pos_s ? pos_s[first + j] : pos[particle_of(perm, first + j, n, e.flags)];
         cx[j] = __fsub_rn(P.x, ip.half_l);
         cy[j] = __fsub_rn(P.y, ip.half_l);
         cz[j] = __fsub_rn(P.z, ip.half_l);
@@ -356,6 +362,7 @@ __global__ void __launch_bounds__(256) update_direct_kernel(float4* __restrict__
                 } else {
                     c = cell_exact(e.rot12 + 12 * i, e.off4 + 4 * i, cx[j], cy[j], cz[j], ip);
                 }
+                if (!in_bounds(e.flags, c, (uint64_t)G3)) c = 0;
                 if (c != prev) f = __ldg(F + c);
                 prev = c;
                 ax[j] = __fadd_rn(ax[j], f.x);
@@ -368,7 +375,7 @@ __global__ void __launch_bounds__(256) update_direct_kernel(float4* __restrict__
 #pragma unroll
     for (int j = 0; j < DPPT; ++j) {
         if (j < cnt) {
-            const int64_t p = particle_of(perm, first + j);
+            const int64_t p = particle_of(perm, first + j, n, e.flags);
             finish_particle<ACC_OUT>(p, pos_s ? pos_s[first + j] : pos[p], ax[j], ay[j], az[j], pos, vel, acc_out,
                                      (float)e.k, dt, damp, e.world, bad);
         }

@@ -33,6 +33,13 @@ def test_every_declared_symbol_is_exported(lib):
         assert hasattr(lib, name), name
 
 
+def test_checked_library_exports_every_symbol():
+    """libmog_check.so (the -DMOG_CHECK build) has the same C ABI."""
+    checked = ctypes.CDLL(str(build(check=True)))
+    for name in _declared_functions():
+        assert hasattr(checked, name), name
+
+
 def test_config_default_matches_reference_defaults(lib):
     c = _lib.default_config()
     # main.py:179-189 defaults, damping 1.0 (main.py:667)
