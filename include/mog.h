@@ -15,8 +15,8 @@
  *    (update.glsl:88-89).
  *  - `stream` is a cudaStream_t passed as void* (0 = legacy default stream).
  *    All work is stream ordered; no entry point synchronises the host
- *    except mog_create, mog_get_status, mog_step_profiled and
- *    mog_diagnostics.
+ *    except mog_create, mog_get_status, mog_step_profiled,
+ *    mog_diagnostics and mog_render.
  *  - Every entry point returns MOG_OK (0) or an error code; the text of the
  *    last error on the calling thread is available from mog_last_error().
  */
@@ -374,6 +374,55 @@ int mog_init_particles(float* pos4, float* vel4, int64_t n, float world, float n
 int mog_init_particles_host(float* pos4, float* vel4, int64_t n, float world, float noise_scale,
                             float contrast, uint32_t seed, float mass, float spawn_buffer,
                             int32_t shape);
+
+/* ---- headless particle renderer ---------------------------------------
+ * Replaces the reference's particle draw (vertex and fragment shaders,
+ * main.py:359-423; on_render, main.py:678-703) with CUDA kernels writing
+ * an image into a device buffer, under OpenGL's rules for points: clip to
+ * the view volume, square points, gl_PointCoord, and SRC_ALPHA /
+ * ONE_MINUS_SRC_ALPHA blending in particle index order on every pixel.
+ * The reference never enables GL_PROGRAM_POINT_SIZE, so its points have
+ * the fixed size 1; point_mode 1 uses the shader's 800 / (w + 0.1).
+ * Rows are stored top row first; each pixel is 4 channels, RGBA. */
+#define MOG_RENDER_RGBA8   0  /* 8-bit target: round(clamp(c) * 255) after every blend */
+#define MOG_RENDER_RGBA32F 1  /* float target: no rounding, no clamping */
+
+typedef struct mog_render_params {
+    int32_t width, height;   /* pixels (the reference's window is 2560 x 1440, main.py:104) */
+    float   world_size;      /* the world_size uniform */
+    float   speed_scale;     /* the speed_scale uniform (main.py:419 sets 0.0) */
+    float   m_view[16];      /* the m_view uniform, column-major: the bytes on_render writes */
+    float   m_proj[16];      /* the m_proj uniform, column-major */
+    float   clear[4];        /* clear colour (main.py:681: 0.01, 0.01, 0.02; alpha 0) */
+    int32_t point_mode;      /* 0: every point point_size pixels wide; 1: the shader's size */
+    float   point_size;      /* 1.0, the GL default */
+    float   max_point_size;  /* sizes are clamped to [1, max_point_size] */
+    int32_t format;          /* MOG_RENDER_RGBA8 or MOG_RENDER_RGBA32F */
+} mog_render_params;
+
+typedef struct mog_renderer mog_renderer;
+
+/* Defaults: the reference's uniforms and GL state, 2560 x 1440, identity
+ * matrices (the caller writes the camera's). */
+void mog_render_params_default(mog_render_params* p);
+
+/* A renderer owns its device scratch (grown on demand). */
+int mog_renderer_create(mog_renderer** out);
+int mog_renderer_destroy(mog_renderer* r);
+
+/*
+ * Draws n particles (device pos4 / vel4, as the step uses them) into the
+ * device buffer `image` (width x height x 4 bytes for RGBA8, x 4 floats
+ * for RGBA32F), on `stream`.  It waits for the stream once, to size the
+ * tile lists.  MOG_ERR_UNSUPPORTED if the points touch more than 2^31 - 1
+ * (point, tile) pairs.
+ */
+int mog_render(mog_renderer* r, const mog_render_params* p, const float* pos4,
+               const float* vel4, int64_t n, void* image, void* stream);
+
+/* The same image from host buffers, on the host (no GPU needed), bit for bit. */
+int mog_render_host(const mog_render_params* p, const float* pos4, const float* vel4,
+                    int64_t n, void* image);
 
 /* Human-readable text for a status code, and the calling thread's last
  * error message. */

@@ -52,6 +52,8 @@ EXPORTS = (
     "mog_model_create", "mog_model_destroy", "mog_model_set", "mog_model_get",
     "mog_model_train_step", "mog_features", "mog_learned_forces", "mog_learned_step",
     "mog_learned_step_profiled", "mog_learned_spread",
+    "mog_render_params_default", "mog_renderer_create", "mog_renderer_destroy", "mog_render",
+    "mog_render_host",
     "mog_strerror", "mog_last_error", "mog_version",
 )
 
@@ -104,6 +106,28 @@ class MogTuningC(ctypes.Structure):
     ]
 
 
+RENDER_RGBA8 = 0
+RENDER_RGBA32F = 1
+
+
+class RenderParamsC(ctypes.Structure):
+    """mog_render_params (include/mog.h)."""
+
+    _fields_ = [
+        ("width", ctypes.c_int32),
+        ("height", ctypes.c_int32),
+        ("world_size", ctypes.c_float),
+        ("speed_scale", ctypes.c_float),
+        ("m_view", ctypes.c_float * 16),
+        ("m_proj", ctypes.c_float * 16),
+        ("clear", ctypes.c_float * 4),
+        ("point_mode", ctypes.c_int32),
+        ("point_size", ctypes.c_float),
+        ("max_point_size", ctypes.c_float),
+        ("format", ctypes.c_int32),
+    ]
+
+
 _lib = None
 
 
@@ -147,6 +171,13 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.mog_learned_step.argtypes = [P, P, P, P, I64, F, P]
     lib.mog_learned_step_profiled.argtypes = [P, P, P, P, I64, F, ctypes.POINTER(ctypes.c_float), P]
     lib.mog_learned_spread.argtypes = [P, ctypes.POINTER(ctypes.c_double), P]
+    RP = ctypes.POINTER(RenderParamsC)
+    lib.mog_render_params_default.argtypes = [RP]
+    lib.mog_render_params_default.restype = None
+    lib.mog_renderer_create.argtypes = [ctypes.POINTER(P)]
+    lib.mog_renderer_destroy.argtypes = [P]
+    lib.mog_render.argtypes = [P, RP, P, P, I64, P, P]
+    lib.mog_render_host.argtypes = [RP, P, P, I64, P]
     lib.mog_strerror.argtypes = [I]
     lib.mog_strerror.restype = ctypes.c_char_p
     lib.mog_last_error.argtypes = []
@@ -154,7 +185,7 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.mog_version.argtypes = []
     lib.mog_version.restype = ctypes.c_char_p
     for name in EXPORTS:
-        if name not in ("mog_strerror", "mog_last_error", "mog_version"):
+        if name not in ("mog_strerror", "mog_last_error", "mog_version", "mog_render_params_default"):
             getattr(lib, name).restype = ctypes.c_int
 
 

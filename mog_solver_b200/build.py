@@ -28,7 +28,7 @@ CSRC = PKG / "csrc"
 OUT = PKG / "libmog.so"
 OUT_CHECK = PKG / "libmog_check.so"
 SOURCES = ["mog_api.cu", "deposit.cu", "spectral.cu", "update.cu", "convolution.cu",
-           "diagnostics.cu", "sort.cu", "learned.cu", "dft_tc.cu", "ics.cu"]
+           "diagnostics.cu", "sort.cu", "learned.cu", "dft_tc.cu", "ics.cu", "render.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -56,7 +56,7 @@ def build(force: bool = False, ptxas_verbose: bool = False, quiet: bool = True,
     objdir = PKG / ("_build_check" if check else "_build")
     objdir.mkdir(exist_ok=True)
     common = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
-              "-Xcompiler", "-fPIC", "-I", str(ROOT / "include")]
+              "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-I", str(ROOT / "include")]
     if check:
         common += ["-DMOG_CHECK"]
     if ptxas_verbose:

@@ -32,6 +32,15 @@ int cuda_fail(cudaError_t err, const char* where) {
     return fail(MOG_ERR_CUDA, m);
 }
 
+}  // namespace
+
+namespace mog {
+// Sets the calling thread's mog_last_error() text; returns code.
+int report_error(int code, const char* msg) { return fail(code, msg); }
+}  // namespace mog
+
+namespace {
+
 #define MOG_CUDA(call, where)                          \
     do {                                               \
         cudaError_t err__ = (call);                    \

@@ -109,6 +109,9 @@ cudaError_t launch_update(const Ensemble& e, float4* pos, float4* vel, const flo
 size_t sort_scratch_bytes();
 // out[s] = pos[perm[s]]: the positions in spatial order, read coalesced by
 // the deposit and the gather.
+// Sets the calling thread's mog_last_error() text (mog_api.cu); returns code.
+int report_error(int code, const char* msg);
+
 cudaError_t launch_gather_sorted(const float4* pos, const int* perm, int64_t n, float4* out,
                                  cudaStream_t s);
 cudaError_t launch_sort(const float4* pos, int64_t n, float world, void* scratch, int* perm,

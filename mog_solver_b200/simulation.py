@@ -268,6 +268,17 @@ class Simulation:
                            "mog_step_n")
         self.steps_taken += n_steps
 
+    def render(self, width: int = 2560, height: int = 1440, **kw):
+        """The frame on_render draws (main.py:678-703), headless: an
+        (height, width, 4) image on this GPU.  Keywords as
+        mog_solver_b200.render.params (camera angles and distance,
+        speed_scale, point_mode, fmt)."""
+        from .render import render
+
+        kw.setdefault("world_size", self.cfg.world_size)
+        with torch_device(self.device):
+            return render(self.pos, self.vel, width=width, height=height, **kw)
+
     def forces(self, pos=None):
         """Ensemble-averaged force at each particle, (N, 4) with w = 0."""
         torch = _torch()

@@ -1,5 +1,6 @@
-// glsl_compat.hpp — enough of GLSL 4.60 compute for the reference's
-// hot-path shaders to compile as C++ and run on the CPU.  TEST AND CPU-BASELINE
+// glsl_compat.hpp — enough of GLSL 4.60 for the reference's hot-path
+// compute shaders and its particle vertex and fragment shaders to compile
+// as C++ and run on the CPU.  TEST AND CPU-BASELINE
 // INFRASTRUCTURE ONLY (oracle/_ref is the checker and the timed reference
 // arm, never the product).
 //
@@ -7,6 +8,8 @@
 //  * every float operation is an IEEE binary32 operation, evaluated as
 //    written (the harness is built with -ffp-contract=off);
 //  * mat3 * vec3 = (col0 * v.x + col1 * v.y) + col2 * v.z, component-wise;
+//    mat4 * vec4 = ((col0 * v.x + col1 * v.y) + col2 * v.z) + col3 * v.w;
+//    mat4 * mat4 applies the latter to each column of the right operand;
 //  * mod(x, y) = x - y * floor(x / y) with IEEE division;
 //  * cos / sin / acos / pow are the C library's cosf / sinf / acosf / powf;
 //  * mix(x, y, a) = x * (1 - a) + y * a; fract(x) = x - floor(x);
@@ -82,6 +85,24 @@ struct mat3 {
     mat3(const vec3& a, const vec3& b, const vec3& d) { c[0] = a; c[1] = b; c[2] = d; }
 };
 
+struct mat4 {
+    vec4 c[4];  // columns
+    mat4() {}
+};
+inline vec4 operator*(const mat4& m, const vec4& v) {
+    vec4 r;
+    r.x = ((m.c[0].x * v.x + m.c[1].x * v.y) + m.c[2].x * v.z) + m.c[3].x * v.w;
+    r.y = ((m.c[0].y * v.x + m.c[1].y * v.y) + m.c[2].y * v.z) + m.c[3].y * v.w;
+    r.z = ((m.c[0].z * v.x + m.c[1].z * v.y) + m.c[2].z * v.z) + m.c[3].z * v.w;
+    r.w = ((m.c[0].w * v.x + m.c[1].w * v.y) + m.c[2].w * v.z) + m.c[3].w * v.w;
+    return r;
+}
+inline mat4 operator*(const mat4& a, const mat4& b) {
+    mat4 r;
+    for (int j = 0; j < 4; ++j) r.c[j] = a * b.c[j];
+    return r;
+}
+
 inline vec2 operator+(const vec2& a, const vec2& b) { return vec2(a.x + b.x, a.y + b.y); }
 inline vec2 operator-(const vec2& a, const vec2& b) { return vec2(a.x - b.x, a.y - b.y); }
 inline vec2 operator*(const vec2& a, float s) { return vec2(a.x * s, a.y * s); }
@@ -116,6 +137,9 @@ inline float acos(float x) { return std::acos(x); }
 inline float pow(float x, float y) { return std::pow(x, y); }
 inline float clamp(float x, float lo, float hi) { return std::min(std::max(x, lo), hi); }
 inline float mix(float x, float y, float a) { return x * (1.0f - a) + y * a; }
+inline vec3 mix(const vec3& x, const vec3& y, float a) {
+    return vec3(mix(x.x, y.x, a), mix(x.y, y.y, a), mix(x.z, y.z, a));
+}
 inline float abs(float x) { return std::fabs(x); }
 inline int abs(int x) { return x < 0 ? -x : x; }
 inline float cos(float x) { return std::cos(x); }

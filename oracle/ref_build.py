@@ -3,7 +3,9 @@
 TEST AND CPU-BASELINE INFRASTRUCTURE ONLY.  Reads the seven hot-path shaders
 (shaders/{mass,complex,fft_batched,fourier,greens,pack,update}.glsl) and the
 initial-condition sampler (shaders/init_particles.glsl) from a
-reference checkout (default /root/reference, or $MOG_REFERENCE), rewrites
+reference checkout (default /root/reference, or $MOG_REFERENCE), and the
+particle vertex and fragment shaders embedded in main.py's init_render
+(main.py:359-410), rewrites
 their GLSL-only declarations with a handful of regular expressions (SSBO
 blocks -> SSBO<T>, image uniforms -> image references, layout qualifiers
 dropped, float literals suffixed ``f`` so they stay binary32, swizzles
@@ -51,20 +53,50 @@ def translate(src: str, name: str) -> str:
             "\n#undef DIM\n}  // namespace " + name + "_glsl\n}  // namespace glsl\n")
 
 
+# stage-specific declarations of the particle draw's shaders (main.py:359-410)
+POINT_STAGES = {"point_vs": "vec4 gl_Position;\nfloat gl_PointSize;\n",
+                "point_fs": "vec2 gl_PointCoord;\nbool discarded;\n"}
+
+
+def point_shader_sources() -> dict[str, str]:
+    """The vertex and fragment shader strings of render_prog (main.py:359-410)."""
+    text = (reference_root() / "main.py").read_text()
+    m = re.search(r'self\.render_prog\s*=\s*self\.ctx\.program\(\s*vertex_shader\s*=\s*"""(.*?)"""'
+                  r'\s*,\s*fragment_shader\s*=\s*"""(.*?)"""', text, re.S)
+    if not m:
+        raise RuntimeError("render_prog shaders not found in main.py")
+    return {"point_vs": m.group(1), "point_fs": m.group(2)}
+
+
+def translate_stage(src: str, name: str) -> str:
+    """A vertex or fragment shader: attributes, varyings and plain uniforms
+    become namespace variables the harness sets and reads; `discard` sets a
+    flag and returns."""
+    s = re.sub(r"layout\s*\([^)]*\)\s*in\s+", "", src)
+    s = re.sub(r"^(\s*)(?:uniform|in|out)\s+", r"\1", s, flags=re.M)
+    s = re.sub(r"\bdiscard\s*;", "{ discarded = true; return; }", s)
+    body = translate(s, name)
+    head = "namespace glsl {\nnamespace " + name + "_glsl {\n"
+    return body.replace(head, head + POINT_STAGES[name], 1)
+
+
 def sources_available() -> bool:
     root = reference_root() / "shaders"
-    return all((root / f"{n}.glsl").exists() for n in SHADERS)
+    return (all((root / f"{n}.glsl").exists() for n in SHADERS) and
+            (reference_root() / "main.py").exists())
 
 
 def build(force: bool = False) -> Path:
     root = reference_root() / "shaders"
     GEN.mkdir(parents=True, exist_ok=True)
     deps = [HERE / "glsl_compat.hpp", HERE / "ref_harness.cpp", Path(__file__)]
-    deps += [root / f"{n}.glsl" for n in SHADERS]
+    deps += [root / f"{n}.glsl" for n in SHADERS] + [reference_root() / "main.py"]
     if not force and LIB.exists() and all(d.stat().st_mtime <= LIB.stat().st_mtime for d in deps):
         return LIB
     for n in SHADERS:
         (GEN / f"{n}.inc").write_text(translate((root / f"{n}.glsl").read_text(), n))
+    for n, src in point_shader_sources().items():
+        (GEN / f"{n}.inc").write_text(translate_stage(src, n))
     tmp = LIB.with_suffix(".so.tmp")
     cmd = ["g++", "-O2", "-std=c++20", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC",
            "-shared", "-I", str(HERE), "-I", str(GEN), "-o", str(tmp),

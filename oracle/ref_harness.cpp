@@ -23,6 +23,8 @@
 #include "pack.inc"
 #include "update.inc"
 #include "init_particles.inc"
+#include "point_vs.inc"
+#include "point_fs.inc"
 
 namespace glsl {
 thread_local uvec3 gl_GlobalInvocationID;
@@ -242,6 +244,58 @@ __attribute__((visibility("default"))) void ref_init_particles(float* pos4, floa
     S::velocities.data = reinterpret_cast<vec4*>(vel4);
     S::velocities.n = n;
     dispatch((n + 255) / 256, 1, 1, 256, 1, 1, [] { S::main(); });
+}
+
+// The particle vertex shader of render_prog (main.py:360-383) on n vertices,
+// with the uniforms on_render sets (m_view, m_proj as the column-major bytes
+// it writes).  out: n x 6 = gl_Position (4), gl_PointSize, v_speed.
+// Serial: the shader's inputs and outputs are namespace variables.
+__attribute__((visibility("default"))) void ref_point_vertex(const float* pos4, const float* vel4,
+                                                             int n, float world,
+                                                             float speed_scale,
+                                                             const float* m_view,
+                                                             const float* m_proj, float* out) {
+    namespace S = point_vs_glsl;
+    S::world_size = world;
+    S::speed_scale = speed_scale;
+    for (int c = 0; c < 4; ++c) {
+        S::m_view.c[c] = vec4(m_view[4 * c], m_view[4 * c + 1], m_view[4 * c + 2], m_view[4 * c + 3]);
+        S::m_proj.c[c] = vec4(m_proj[4 * c], m_proj[4 * c + 1], m_proj[4 * c + 2], m_proj[4 * c + 3]);
+    }
+    for (int i = 0; i < n; ++i) {
+        S::in_pos = vec4(pos4[4 * i], pos4[4 * i + 1], pos4[4 * i + 2], pos4[4 * i + 3]);
+        S::in_vel = vec4(vel4[4 * i], vel4[4 * i + 1], vel4[4 * i + 2], vel4[4 * i + 3]);
+        S::main();
+        float* o = out + 6 * (size_t)i;
+        o[0] = S::gl_Position.x;
+        o[1] = S::gl_Position.y;
+        o[2] = S::gl_Position.z;
+        o[3] = S::gl_Position.w;
+        o[4] = S::gl_PointSize;
+        o[5] = S::v_speed;
+    }
+}
+
+// The particle fragment shader (main.py:385-410) on m fragments given
+// gl_PointCoord (m x 2) and v_speed (m).  out: m x 5 = fragColor (4) and 1
+// where the shader kept the fragment, 0 where it discarded it.
+__attribute__((visibility("default"))) void ref_point_fragment(const float* point_coord,
+                                                               const float* v_speed, int m,
+                                                               float* out) {
+    namespace S = point_fs_glsl;
+    for (int i = 0; i < m; ++i) {
+        S::gl_PointCoord = vec2(point_coord[2 * i], point_coord[2 * i + 1]);
+        S::v_speed = v_speed[i];
+        S::discarded = false;
+        S::fragColor = vec4();
+        S::main();
+        float* o = out + 5 * (size_t)i;
+        o[0] = S::fragColor.x;
+        o[1] = S::fragColor.y;
+        o[2] = S::fragColor.z;
+        o[3] = S::fragColor.w;
+        o[4] = S::discarded ? 0.f : 1.f;
+    }
 }
 
 }  // extern "C"

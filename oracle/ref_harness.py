@@ -39,6 +39,10 @@ def lib() -> ctypes.CDLL:
         U = ctypes.c_uint32
         h.ref_init_particles.argtypes = [P, P, I, F, F, F, U, F, F, U]
         h.ref_step.restype = None
+        h.ref_point_vertex.argtypes = [P, P, I, F, F, P, P, P]
+        h.ref_point_vertex.restype = None
+        h.ref_point_fragment.argtypes = [P, P, I, P]
+        h.ref_point_fragment.restype = None
         _lib = h
     return _lib
 
@@ -109,6 +113,25 @@ def init_particles(n: int, world: float, noise_scale: float = 4.0, contrast: flo
                              float(contrast), int(seed) & 0xFFFFFFFF, float(mass),
                              float(spawn_buffer), int(shape))
     return pos, vel
+
+
+def point_vertex(pos4, vel4, world: float, speed_scale: float, m_view, m_proj):
+    """The reference's particle vertex shader (main.py:360-383): (gl_Position
+    (n, 4), gl_PointSize (n), v_speed (n))."""
+    pos, vel = _f32(pos4), _f32(vel4)
+    out = np.zeros((pos.shape[0], 6), dtype=np.float32)
+    lib().ref_point_vertex(_p(pos), _p(vel), pos.shape[0], float(world), float(speed_scale),
+                           _p(_f32(m_view)), _p(_f32(m_proj)), _p(out))
+    return out[:, :4], out[:, 4], out[:, 5]
+
+
+def point_fragment(point_coord, v_speed):
+    """The reference's particle fragment shader (main.py:385-410): (fragColor
+    (m, 4), kept (m) bool)."""
+    pc, vs = _f32(point_coord), _f32(v_speed)
+    out = np.zeros((vs.shape[0], 5), dtype=np.float32)
+    lib().ref_point_fragment(_p(pc), _p(vs), vs.shape[0], _p(out))
+    return out[:, :4], out[:, 4] > 0.5
 
 
 def time_steps(pos4, vel4, off4, rot12, w: dict, steps: int):

@@ -3,7 +3,8 @@
 Run in a container that has the reference checkout (default /root/reference,
 or $MOG_REFERENCE) and the built oracle/_ref (python -m oracle.ref_build):
 
-    python tests/golden/make_golden.py [transforms greens_kernel shaders two_galaxies init_particles]
+    python tests/golden/make_golden.py [transforms greens_kernel shaders two_galaxies init_particles camera
+                                        point_shaders]
 
 * transforms.npz   — Simulation.compute_transforms (main.py:157-172) with
                      the reference's own RandomSE3Sampler (main.py:9-62),
@@ -13,6 +14,14 @@ or $MOG_REFERENCE) and the built oracle/_ref (python -m oracle.ref_build):
                      sampler (compiled as C++ by oracle/_ref), two seeded cases.
 * two_galaxies.npz — Simulation.init_particles2 (main.py:312-357) after
                      np.random.seed(seed), buffers captured from its writes.
+* camera.npz       — the m_view and m_proj uniform bytes that on_render
+                     (main.py:678-700) writes, for several orbit-camera
+                     angles, distances and aspect ratios (on_render run on a
+                     stand-in object that records the writes).
+* point_shaders.npz — the particle vertex and fragment shaders of render_prog
+                     (main.py:359-410, compiled as C++ by oracle/_ref) on
+                     seeded vertices for three cameras and two speed
+                     scales, and on seeded gl_PointCoord values.
 * shaders_g{8,16}.npz — the reference's compute shaders (compiled as C++ by
                      oracle/_ref) on small seeded particle sets: the mass
                      grid of mass.glsl, the gradient texture of the
@@ -170,8 +179,70 @@ def perlin_sampler(ref_main=None):
     np.savez_compressed(HERE / "init_particles.npz", **out)
 
 
+class _Uniform:
+    def __init__(self):
+        self.data = None
+
+    def write(self, data):
+        self.data = bytes(data)
+
+
+def camera(ref_main):
+    """The matrix uniforms on_render writes (main.py:678-700), per camera."""
+    for name in ("BLEND", "SRC_ALPHA", "ONE_MINUS_SRC_ALPHA", "POINTS", "LINES"):
+        setattr(ref_main.moderngl, name, 0)
+    out = {}
+    cases = [(0.0, 0.0, 3.0, 2560 / 1440), (30.0, 20.0, 3.0, 2560 / 1440), (-135.5, 95.0, 1.7, 4 / 3),
+             (250.0, -40.0, 6.25, 1.0), (12.0, -89.0, 0.1, 16 / 9)]
+    for idx, (rx, ry, dist, aspect) in enumerate(cases):
+        uniforms = {"m_view": _Uniform(), "m_proj": _Uniform()}
+        ctx = types.SimpleNamespace(clear=lambda *a, **k: None, enable=lambda *a, **k: None,
+                                    blend_func=None)
+        fake = types.SimpleNamespace(paused=True, ctx=ctx, cam_rot_x=rx, cam_rot_y=ry,
+                                     cam_dist=dist, aspect_ratio=aspect, render_prog=uniforms,
+                                     show_particles=False, show_grid_debug=False)
+        ref_main.Simulation.on_render(fake, 0.0, 0.0)
+        out[f"c{idx}_params"] = np.array([rx, ry, dist, aspect], dtype=np.float64)
+        out[f"c{idx}_m_view"] = np.frombuffer(uniforms["m_view"].data, np.float32)
+        out[f"c{idx}_m_proj"] = np.frombuffer(uniforms["m_proj"].data, np.float32)
+    np.savez_compressed(HERE / "camera.npz", **out)
+
+
+def point_shaders(ref_main=None):
+    """render_prog's vertex and fragment shaders (oracle/_ref) on seeded inputs."""
+    from oracle import ref_harness as rh
+    from mog_solver_b200.render import camera_matrices
+
+    assert rh.available(), "build oracle/_ref first (python -m oracle.ref_build)"
+    rng = np.random.default_rng(2024)
+    n = 512
+    pos = np.zeros((n, 4), np.float32)
+    pos[:, :3] = rng.uniform(-20.0, 120.0, (n, 3))
+    pos[:, 3] = 1.0
+    vel = np.zeros((n, 4), np.float32)
+    vel[:, :3] = rng.normal(0.0, 3.0, (n, 3)) * rng.uniform(0.0, 3.0, (n, 1))
+    out = {"pos": pos, "vel": vel}
+    for c, cam in enumerate([(0.0, 0.0, 3.0, 2560 / 1440), (30.0, 20.0, 2.0, 4 / 3),
+                             (-135.5, 95.0, 1.7, 1.0)]):
+        m_view, m_proj = camera_matrices(*cam)
+        out[f"cam{c}_m_view"], out[f"cam{c}_m_proj"] = m_view, m_proj
+        for s, scale in enumerate((0.13, 2.0)):
+            clip, size, v_speed = rh.point_vertex(pos, vel, 100.0, scale, m_view, m_proj)
+            out[f"cam{c}_s{s}_params"] = np.array([100.0, scale], np.float32)
+            out[f"cam{c}_s{s}_clip"], out[f"cam{c}_s{s}_size"] = clip, size
+            out[f"cam{c}_s{s}_v_speed"] = v_speed
+    m = 4000
+    pc = rng.uniform(-0.1, 1.1, (m, 2)).astype(np.float32)
+    vs = rng.uniform(0.0, 1.0, m).astype(np.float32)
+    vs[:8] = [0.0, 0.3, 0.7, 1.0, 0.29999998, 0.70000005, 0.5, 0.9]
+    colour, kept = rh.point_fragment(pc, vs)
+    out.update(frag_point_coord=pc, frag_v_speed=vs, frag_colour=colour, frag_kept=kept)
+    np.savez_compressed(HERE / "point_shaders.npz", **out)
+
+
 PARTS = {"transforms": transforms, "greens_kernel": greens_kernel, "shaders": None,
-         "two_galaxies": initial_conditions, "init_particles": perlin_sampler}
+         "two_galaxies": initial_conditions, "init_particles": perlin_sampler, "camera": camera,
+         "point_shaders": point_shaders}
 
 
 def main():
