@@ -2,7 +2,7 @@
 """Throughput of the Mixture-of-Grids force-and-step path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W]
-                    [--workload learned|c2|c3|c4|c1] [--impl ours|reference]
+                    [--workload learned|c2|c3|c4|c1|render] [--impl ours|reference]
 
 Default workload (``learned``, one GPU): the headline metric, particle-steps/s
 of the learned k = 32 step at the RMS force error of plain k = 240, on the
@@ -21,7 +21,9 @@ back every step.
 
 ``c2`` times the plain k = 240 step alone, ``c1`` the small uniform-cube
 case, ``c3`` the batched uneven ensemble and ``c4`` the plain k = 240, g = 32
-step with the DFT passes on the tensor cores (BF16 hi+lo x3).  Under torchrun (N > 1) every
+step with the DFT passes on the tensor cores (BF16 hi+lo x3), ``render`` one
+headless frame of the colliding-disk set (the reference's particle draw,
+2560 x 1440, 1-pixel points, 8-bit target).  Under torchrun (N > 1) every
 rank advances its own independent simulation of the same size (replicas;
 the step has no cross-GPU exchange) and the time is the maximum over ranks.
 
@@ -69,6 +71,11 @@ WORKLOADS = {
                     "two colliding exponential disks, N=1,048,576",
                n=1 << 20, k=240, g=32, L=100.0, G=100.0, dt=1e-5, damping=0.999, ic="disks",
                seed=1, dft="bf16x3"),
+    "render": dict(desc="headless frame of the particle draw (main.py:359-423 under GL point rules): "
+                        "two colliding exponential disks, N=1,048,576, 2560x1440, default camera, "
+                        "1-pixel points, RGBA8 target",
+                   n=1 << 20, k=16, g=16, L=100.0, G=100.0, dt=1e-5, damping=0.999, ic="disks",
+                   seed=1, width=2560, height=1440, speed_scale=0.2, frame=True),
     "c1": dict(desc="plain MOG k=16 g=16, uniform cube, N=65,536",
                n=1 << 16, k=16, g=16, L=100.0, G=100.0, dt=1e-5, damping=0.999, ic="uniform",
                seed=0),
@@ -735,6 +742,128 @@ def run_batch(args, w: dict) -> None:
         torch.distributed.destroy_process_group()
 
 
+def render_cpu_baseline(w: dict, pos, vel, budget_s: float = 15.0) -> dict:
+    """The oracle's draw (oracle/render.py, one core) on a growing prefix of
+    the particles until the budget is used; the frame time is extrapolated
+    linearly in the particle count (its cost is per point)."""
+    import oracle.render as orc
+    from mog_solver_b200.render import camera_matrices
+
+    v, p = camera_matrices(aspect=w["width"] / w["height"])
+    kw = dict(width=w["width"], height=w["height"], world_size=w["L"],
+              speed_scale=w["speed_scale"], m_view=v, m_proj=p)
+    t0 = time.perf_counter()
+    orc.render(pos[:0], vel[:0], **kw)
+    t_clear = time.perf_counter() - t0
+    m, t_pts = 1024, 0.0
+    while True:
+        t0 = time.perf_counter()
+        orc.render(pos[:m], vel[:m], **kw)
+        t_pts = time.perf_counter() - t0 - t_clear
+        if t_pts * 4 > budget_s or m >= len(pos):
+            break
+        m *= 4
+    frame_s = t_clear + max(t_pts, 0.0) * len(pos) / m
+    return {"value": 1.0 / frame_s, "unit": "frames/s", "cores": 1, "kind": "port",
+            "sample": f"first {m} of {len(pos)} particles drawn by the NumPy restatement "
+                      f"(oracle/render.py), time scaled to all particles"}
+
+
+def run_render(args, w: dict) -> None:
+    import torch
+
+    from mog_solver_b200 import Simulation, render as R
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    sim = Simulation({"n_grids": w["k"], "grid_size": w["g"], "world_size": w["L"],
+                      "num_particles": w["n"], "G": w["G"], "dt": w["dt"],
+                      "damping": w["damping"], "seed": w["seed"]}, device=dev)
+    pos_h, vel_h = make_particles(w, sim, seed_offset=1000 * rank)
+    sim.set_particles(pos_h, vel_h)
+    W, H = w["width"], w["height"]
+    p = R.params(W, H, world_size=w["L"], speed_scale=w["speed_scale"])
+    r = R.Renderer()
+    img = torch.empty((H, W, 4), dtype=torch.uint8, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    hp = torch.from_numpy(np.ascontiguousarray(pos_h, np.float32)).pin_memory()
+    hv = torch.from_numpy(np.ascontiguousarray(vel_h, np.float32)).pin_memory()
+    himg = torch.empty((H, W, 4), dtype=torch.uint8).pin_memory()
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            r.render(sim.pos, sim.vel, p=p, out=img)
+        stream.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        times = []
+        with ClockSampler(local) as clocks:
+            for _ in range(args.steps):
+                flush.zero_()
+                e0.record(stream)
+                r.render(sim.pos, sim.vel, p=p, out=img)
+                e1.record(stream)
+                e1.synchronize()
+                times.append(e0.elapsed_time(e1))
+        stats = r.stats()
+        e2e = []
+        for _ in range(args.steps):
+            e0.record(stream)
+            sim.pos.copy_(hp, non_blocking=True)
+            sim.vel.copy_(hv, non_blocking=True)
+            r.render(sim.pos, sim.vel, p=p, out=img)
+            himg.copy_(img, non_blocking=True)
+            e1.record(stream)
+            e1.synchronize()
+            e2e.append(e0.elapsed_time(e1))
+    tot = torch.tensor([sum(times), sum(e2e)], dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(tot, op=torch.distributed.ReduceOp.MAX)
+    total_ms, total_e2e = float(tot[0]), float(tot[1])
+    if rank == 0:
+        peaks = measured_peaks()
+        n = w["n"]
+        B = 32 * n + 4 * W * H  # particles read once, image written once
+        ms = total_ms / args.steps
+        achieved = B / (ms / 1e3) / 1e9
+        line = {
+            "metric": "frames/s of the headless particle draw", "unit": "frames/s",
+            "value": world * args.steps / (total_ms / 1e3), "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (u8 target)",
+            "data": "synthetic (seeded colliding disks)",
+            "config": {"workload": w["desc"], "n": n, "width": W, "height": H,
+                       "pairs_per_frame": stats["pairs"],
+                       "parallelism": "single GPU" if world == 1 else f"{world} independent replicas",
+                       "l2": "flushed between timed frames (256 MiB write)"},
+            "roofline": {"bound": "hbm", "kernel": "whole frame (6 kernels and the scans)",
+                         "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
+                         "algorithmic_bytes": B, "traffic": None},
+            "e2e": {"value": world * args.steps / (total_e2e / 1e3), "unit": "frames/s",
+                    "h2d_bytes_per_step": 32 * n, "d2h_bytes_per_step": 4 * W * H,
+                    "ms_per_step": total_e2e / args.steps},
+            "gpu_launches": stats["launches"] * args.steps,
+            "clocks": clocks.summary(),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = render_cpu_baseline(w, pos_h, vel_h)
+        print(json.dumps(line), flush=True)
+    r.close()
+    sim.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -751,11 +880,18 @@ def main() -> None:
         args.warmup = 3
     w = WORKLOADS[args.workload]
     if args.impl == "reference":
+        if w.get("frame"):
+            print(json.dumps({"impl": "reference", "unavailable": "the reference draws with OpenGL "
+                              "(main.py:359-423, 678-703); there is no graphics stack here: "
+                              "unavailable on this box"}))
+            return
         if "sims" in w:
             print(json.dumps({"impl": "reference", "unavailable": "the reference runs one "
                               "simulation per window; no batched path to time"}))
             return
         run_reference(args, w)
+    elif w.get("frame"):
+        run_render(args, w)
     elif "sims" in w:
         run_batch(args, w)
     elif "k_small" in w:

@@ -420,6 +420,9 @@ int mog_renderer_destroy(mog_renderer* r);
 int mog_render(mog_renderer* r, const mog_render_params* p, const float* pos4,
                const float* vel4, int64_t n, void* image, void* stream);
 
+/* The last frame's (point, tile) pair count and number of kernel launches. */
+int mog_renderer_stats(const mog_renderer* r, int64_t* pairs, int32_t* launches);
+
 /* The same image from host buffers, on the host (no GPU needed), bit for bit. */
 int mog_render_host(const mog_render_params* p, const float* pos4, const float* vel4,
                     int64_t n, void* image);

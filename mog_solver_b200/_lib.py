@@ -53,7 +53,7 @@ EXPORTS = (
     "mog_model_train_step", "mog_features", "mog_learned_forces", "mog_learned_step",
     "mog_learned_step_profiled", "mog_learned_spread",
     "mog_render_params_default", "mog_renderer_create", "mog_renderer_destroy", "mog_render",
-    "mog_render_host",
+    "mog_renderer_stats", "mog_render_host",
     "mog_strerror", "mog_last_error", "mog_version",
 )
 
@@ -178,6 +178,7 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.mog_renderer_destroy.argtypes = [P]
     lib.mog_render.argtypes = [P, RP, P, P, I64, P, P]
     lib.mog_render_host.argtypes = [RP, P, P, I64, P]
+    lib.mog_renderer_stats.argtypes = [P, ctypes.POINTER(I64), ctypes.POINTER(ctypes.c_int32)]
     lib.mog_strerror.argtypes = [I]
     lib.mog_strerror.restype = ctypes.c_char_p
     lib.mog_last_error.argtypes = []

@@ -126,6 +126,12 @@ int64_t scan_scratch(int64_t n) {
     return total;
 }
 
+// Kernel launches of scan_exclusive over n elements.
+int scan_launches(int64_t n) {
+    const int64_t nb = (n + kScanBlock - 1) / kScanBlock;
+    return nb <= 1 ? 1 : 2 + scan_launches(nb);
+}
+
 // out[i] = in[0] + ... + in[i-1]; *total = the sum of all n (if non-null).
 template <typename In, typename Out>
 cudaError_t scan_exclusive(const In* in, Out* out, int64_t n, Out* scratch, Out* total,
@@ -330,6 +336,8 @@ struct mog_renderer {
     void* buf[9] = {};
     size_t cap[9] = {};
     uint64_t* host_total = nullptr;  // pinned
+    int64_t last_pairs = 0;          // (point, tile) pairs of the last frame
+    int32_t last_launches = 0;       // kernels the last frame launched
 };
 
 namespace {
@@ -419,6 +427,8 @@ int mog_render(mog_renderer* r, const mog_render_params* p, const float* pos4, c
     if (cudaGetDevice(&dev) != cudaSuccess || dev != r->device)
         return report_error(MOG_ERR_ARG, "the renderer was created on another device");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    r->last_pairs = 0;
+    r->last_launches = 0;
     const Params R = make_params(p);
     const int tiles_x = (p->width + kTile - 1) / kTile;
     const int tiles_y = (p->height + kTile - 1) / kTile;
@@ -447,6 +457,7 @@ int mog_render(mog_renderer* r, const mog_render_params* p, const float* pos4, c
                                                     static_cast<Splat*>(splats),
                                                     static_cast<uint32_t*>(counts));
         MOG_R(cudaGetLastError(), "render vertex");
+        r->last_launches += 1 + scan_launches(n);
         MOG_R((scan_exclusive<uint32_t, uint64_t>(static_cast<uint32_t*>(counts),
                                                   static_cast<uint64_t*>(offsets), n,
                                                   static_cast<uint64_t*>(scan_tmp), total, s)),
@@ -456,6 +467,7 @@ int mog_render(mog_renderer* r, const mog_render_params* p, const float* pos4, c
           "render read pair count");
     MOG_R(cudaStreamSynchronize(s), "render read pair count");
     const uint64_t m = *r->host_total;
+    r->last_pairs = (int64_t)m;
     if (m > 0x7FFFFFFFull)
         return report_error(MOG_ERR_UNSUPPORTED, "the points touch more than 2^31 - 1 (point, tile) pairs");
     if (m > 0) {
@@ -490,18 +502,28 @@ int mog_render(mog_renderer* r, const mog_render_params* p, const float* pos4, c
             MOG_R(cudaGetLastError(), "render sort");
             std::swap(kin, kout);
             std::swap(vin, vout);
+            r->last_launches += 2 + scan_launches(hn);
         }
         tile_bounds_kernel<<<(unsigned)(((int64_t)m + 255) / 256), 256, 0, s>>>(kin, (int64_t)m,
                                                                                  start, end);
         MOG_R(cudaGetLastError(), "render bounds");
         render_composite_kernel<<<(unsigned)tiles, kTile * kTile, 0, s>>>(
             static_cast<Splat*>(splats), vin, start, end, R, tiles_x, image);
+        r->last_launches += 3;  // expand, bounds, composite
     } else {
         render_composite_kernel<<<(unsigned)tiles, kTile * kTile, 0, s>>>(
             static_cast<Splat*>(splats), nullptr, start, end, R, tiles_x, image);
+        r->last_launches += 1;
     }
     MOG_R(cudaGetLastError(), "render composite");
 #undef MOG_R
+    return MOG_OK;
+}
+
+int mog_renderer_stats(const mog_renderer* r, int64_t* pairs, int32_t* launches) {
+    if (!r) return mog::report_error(MOG_ERR_ARG, "null renderer");
+    if (pairs) *pairs = r->last_pairs;
+    if (launches) *launches = r->last_launches;
     return MOG_OK;
 }
 

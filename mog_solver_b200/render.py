@@ -140,6 +140,13 @@ class Renderer:
                                              stream), "mog_render")
         return out
 
+    def stats(self) -> dict:
+        """The last frame's (point, tile) pair count and kernel launches."""
+        pairs, launches = ctypes.c_int64(), ctypes.c_int32()
+        _lib.check(_lib.lib().mog_renderer_stats(self._h, ctypes.byref(pairs),
+                                                 ctypes.byref(launches)), "mog_renderer_stats")
+        return {"pairs": pairs.value, "launches": launches.value}
+
 
 _renderers: dict[int, Renderer] = {}
 

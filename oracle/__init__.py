@@ -11,9 +11,13 @@ of it.  Contents:
                        Green's function, exact FFT): the 1e-5 force gate;
                        NumPy FP32 transcription of the reference's shader
                        chain with its flush quirks; FP64 direct-sum yardstick;
+* ``mlp``              NumPy FP64 forward/backward of the learned correction;
+* ``render``           NumPy restatement of the reference's particle draw
+                       under OpenGL's point rules (the renderer's checker);
 * ``_ref``             (built in the source container only) the reference's
-                       own GLSL compute shaders compiled as C++ through a
-                       GLSL compatibility header, used to pin the above.
+                       own GLSL compute shaders, and the vertex and fragment
+                       shaders of its particle draw, compiled as C++ through
+                       a GLSL compatibility header, used to pin the above.
 
 Parity anchors: the transforms come from the reference's own
 ``RandomSE3Sampler`` (golden fixtures in tests/golden, generated by
