@@ -79,3 +79,51 @@ def test_simulation_render_matches_host():
     ref = R.render_host(sim.pos.cpu().numpy(), sim.vel.cpu().numpy(), width=320, height=180,
                         world_size=100.0, speed_scale=0.2)
     assert np.array_equal(img.cpu().numpy(), ref)
+
+
+def _expected_stats(pos, vel, W, H, scale, v, p):
+    """(point, tile) pairs and kernel launches of one frame, from the
+    oracle's vertex stage and the renderer's binning rule (a one-pixel
+    margin around each point's square, 16 x 16 tiles)."""
+    from oracle import render as O
+
+    clip, _, _ = O.vertex_stage(pos, vel, v, p, 100.0, scale)
+    x, y, z, w = (clip[:, i] for i in range(4))
+    keep = (w > 0) & (x >= -w) & (x <= w) & (y >= -w) & (y <= w) & (z >= -w) & (z <= w)
+    F = np.float32
+    xw = (x[keep] / w[keep]) * F(W * 0.5) + F(W * 0.5)
+    yw = (y[keep] / w[keep]) * F(H * 0.5) + F(H * 0.5)
+    h = F(1.0) * F(0.5)
+    i0 = np.maximum(np.floor(xw - h).astype(int) - 1, 0)
+    i1 = np.minimum(np.floor(xw + h).astype(int) + 1, W - 1)
+    j0 = np.maximum(np.floor(yw - h).astype(int) - 1, 0)
+    j1 = np.minimum(np.floor(yw + h).astype(int) + 1, H - 1)
+    ok = (i0 <= i1) & (j0 <= j1)
+    pairs = int(((i1 // 16 - i0 // 16 + 1) * (j1 // 16 - j0 // 16 + 1))[ok].sum())
+
+    def scans(m):
+        nb = -(-m // 2048)
+        return 1 if nb <= 1 else 2 + scans(nb)
+
+    tiles = -(-W // 16) * -(-H // 16)
+    passes = -(-int(np.ceil(np.log2(tiles))) // 8) if tiles > 1 else 0
+    hn = -(-pairs // 2048) * 256
+    launches = 1 + scans(len(pos)) + passes * (2 + scans(hn)) + 3 if pairs else 1 + scans(len(pos)) + 1
+    return pairs, launches
+
+
+def test_renderer_stats():
+    from mog_solver_b200 import render as R
+
+    n, W, H, scale = 50000, 700, 300, 0.3
+    pos, vel = _particles(n, 11)
+    v, p = R.camera_matrices(aspect=W / H)
+    r = R.Renderer()
+    try:
+        r.render(torch.from_numpy(pos).cuda(), torch.from_numpy(vel).cuda(), width=W, height=H,
+                 world_size=100.0, speed_scale=scale, m_view=v, m_proj=p)
+        torch.cuda.synchronize()
+        pairs, launches = _expected_stats(pos, vel, W, H, scale, v, p)
+        assert r.stats() == {"pairs": pairs, "launches": launches}
+    finally:
+        r.close()
