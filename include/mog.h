@@ -210,6 +210,15 @@ int mog_set_tuning(mog_handle* h, const mog_tuning* t);
 int mog_get_status(mog_handle* h, uint32_t* flags, void* stream);
 
 /*
+ * Failure-detection self-test (no counterpart in the reference): one
+ * device wait that nothing satisfies, bounded like every wait in the
+ * library's kernels (about 2^31 SM cycles, a second).  It gives up, raises
+ * MOG_FLAG_TIMEOUT in the handle's status word and returns, leaving the
+ * context usable; mog_get_status then reports it.  Stream ordered.
+ */
+int mog_selftest_wait_timeout(mog_handle* h, void* stream);
+
+/*
  * FP64 diagnostics of a particle set: out[0..2] = total momentum
  * sum(m v), out[3] = kinetic energy sum(m |v|^2 / 2), out[4] = total
  * mass, out[5..7] = centre of mass.  No counterpart in the reference,

@@ -46,6 +46,7 @@ FLAG_BOUNDS = 16  # only from a library built with --check
 EXPORTS = (
     "mog_config_default", "mog_create", "mog_destroy", "mog_step", "mog_step_n",
     "mog_step_profiled", "mog_forces", "mog_deposit", "mog_solve", "mog_update", "mog_get_status",
+    "mog_selftest_wait_timeout",
     "mog_get_tuning", "mog_set_tuning", "mog_diagnostics", "mog_direct_sum",
     "mog_direct_sum_noalloc", "mog_green_table", "mog_init_particles", "mog_init_particles_host",
     "mog_batch_create", "mog_batch_step", "mog_batch_destroy",
@@ -149,6 +150,7 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.mog_get_tuning.argtypes = [P, ctypes.POINTER(MogTuningC)]
     lib.mog_set_tuning.argtypes = [P, ctypes.POINTER(MogTuningC)]
     lib.mog_get_status.argtypes = [P, ctypes.POINTER(ctypes.c_uint32), P]
+    lib.mog_selftest_wait_timeout.argtypes = [P, P]
     lib.mog_diagnostics.argtypes = [P, P, P, I64, ctypes.POINTER(ctypes.c_double), P]
     D = ctypes.c_double
     lib.mog_direct_sum.argtypes = [P, I64, P, I64, D, D, D, P, P]

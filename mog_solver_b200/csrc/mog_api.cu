@@ -792,6 +792,15 @@ int mog_get_status(mog_handle* h, uint32_t* flags, void* stream) {
     return MOG_OK;
 }
 
+int mog_selftest_wait_timeout(mog_handle* h, void* stream) {
+    if (!h) return fail(MOG_ERR_ARG, "null argument");
+    int rc = set_device(h);
+    if (rc) return rc;
+    MOG_CUDA(mog::launch_wait_timeout_selftest(h->d_flags, static_cast<cudaStream_t>(stream)),
+             "wait self-test");
+    return MOG_OK;
+}
+
 int mog_diagnostics(mog_handle* h, const float* pos4, const float* vel4, int64_t n, double* out8,
                     void* stream) {
     if (!h || !out8) return fail(MOG_ERR_ARG, "null argument");

@@ -109,6 +109,10 @@ cudaError_t launch_update(const Ensemble& e, float4* pos, float4* vel, const flo
 size_t sort_scratch_bytes();
 // out[s] = pos[perm[s]]: the positions in spatial order, read coalesced by
 // the deposit and the gather.
+// One bounded device wait that nothing satisfies (update.cu); raises
+// MOG_FLAG_TIMEOUT in *flags after about a second.
+cudaError_t launch_wait_timeout_selftest(unsigned* flags, cudaStream_t s);
+
 // Sets the calling thread's mog_last_error() text (mog_api.cu); returns code.
 int report_error(int code, const char* msg);
 

@@ -459,7 +459,26 @@ cudaError_t update_mode(const Ensemble& e, float4* pos, float4* vel, const float
 #undef MOG_STAGED
 }
 
+// One bounded wait that nothing satisfies: a fresh mbarrier expecting one
+// arrival, waited on by thread 0 with the gather's own mbar_wait_bounded.
+// It gives up after its budget and raises MOG_FLAG_TIMEOUT (4), exactly as
+// the staged gather does when a bulk copy never lands.
+__global__ void __launch_bounds__(32) wait_timeout_selftest_kernel(unsigned* flags) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && !mbar_wait_bounded(&bar, 0)) atomicOr(flags, 4u);
+}
+
 }  // namespace
+
+cudaError_t launch_wait_timeout_selftest(unsigned* flags, cudaStream_t s) {
+    wait_timeout_selftest_kernel<<<1, 32, 0, s>>>(flags);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_update(const Ensemble& e, float4* pos, float4* vel, const float4* pos_s,
                           const int* perm, int64_t n, const float4* force_world, float dt,

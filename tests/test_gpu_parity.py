@@ -381,3 +381,31 @@ def test_checkpoint_resume_is_bit_identical(tmp_path):
     b.step(4)
     torch.cuda.synchronize()
     assert torch.equal(a.pos, b.pos) and torch.equal(a.vel, b.vel)
+
+
+def test_bounded_wait_times_out_and_the_context_survives():
+    """A device wait that nothing satisfies gives up within its budget,
+    raises MOG_FLAG_TIMEOUT, and the next step still runs and matches a
+    fresh handle's."""
+    import ctypes
+    import time
+
+    from mog_solver_b200 import FLAG_TIMEOUT, _lib
+
+    n = 4096
+    a = make_sim(k=4, g=16, n=n, dt=1e-3)
+    b = make_sim(k=4, g=16, n=n, dt=1e-3)
+    pos, vel = particles(n, seed=21)
+    a.set_particles(pos, vel)
+    b.set_particles(pos, vel)
+    assert a.status() == 0
+    t0 = time.time()
+    _lib.check(_lib.lib().mog_selftest_wait_timeout(a.handle, None), "selftest")
+    assert a.status() == FLAG_TIMEOUT
+    assert time.time() - t0 < 30.0
+    assert a.status() == 0  # read and cleared
+    a.step(2)
+    b.step(2)
+    torch.cuda.synchronize()
+    assert torch.equal(a.pos, b.pos) and torch.equal(a.vel, b.vel)
+    assert a.status() == 0
