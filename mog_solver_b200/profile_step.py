@@ -1,12 +1,16 @@
 """A few steps of a fixed workload, for running under a profiler.
 
-    python -m mog_solver_b200.profile_step [--path plain|learned] [--steps 6] [--n N]
+    python -m mog_solver_b200.profile_step [--path plain|learned|render] [--steps 6] [--n N]
                                            [--k K] [--g 16|32] [--dft fp32|bf16x3]
+                                           [--width W] [--height H]
 
 plain:   k = 240 grids of 16^3 (or --k, --g, --dft), the colliding-disk set
          (N = 1,048,576, seeded two exponential disks), mog_step;
 learned: k = 32 grids of 16^3, the same particles, mog_learned_step with the
-         committed model (models/learned_k32_g16.npz).
+         committed model (models/learned_k32_g16.npz);
+render:  frames of the same particles drawn headless (mog_render) at
+         --width x --height (default 2560 x 1440), default camera, 1-pixel
+         points, 8-bit target.
 Everything is set up first; the steps run back to back on the default
 stream and the status flags are checked at the end.
 """
@@ -17,12 +21,14 @@ import argparse
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--path", default="plain", choices=["plain", "learned"])
+    ap.add_argument("--path", default="plain", choices=["plain", "learned", "render"])
     ap.add_argument("--steps", type=int, default=6)
     ap.add_argument("--n", type=int, default=1 << 20)
     ap.add_argument("--k", type=int, default=0, help="grids (default 240 plain, 32 learned)")
     ap.add_argument("--g", type=int, default=16)
     ap.add_argument("--dft", default="fp32", choices=["fp32", "bf16x3"])
+    ap.add_argument("--width", type=int, default=2560)
+    ap.add_argument("--height", type=int, default=1440)
     a = ap.parse_args()
 
     import torch
@@ -42,6 +48,18 @@ def main() -> None:
     lib = _lib.lib()
     model = Model.load(DEFAULT_MODEL) if a.path == "learned" else None
     torch.cuda.synchronize()
+    if a.path == "render":
+        from .render import Renderer, params
+
+        r = Renderer()
+        p = params(a.width, a.height, world_size=100.0, speed_scale=0.2)
+        img = torch.empty((a.height, a.width, 4), dtype=torch.uint8, device=sim.pos.device)
+        for _ in range(a.steps):
+            r.render(sim.pos, sim.vel, p=p, out=img)
+        torch.cuda.synchronize()
+        print(f"render: {a.steps} frames of N={a.n} at {a.width}x{a.height}: {r.stats()}")
+        r.close()
+        return
     for _ in range(a.steps):
         if model is None:
             _lib.check(lib.mog_step(sim.handle, sim.pos.data_ptr(), sim.vel.data_ptr(), a.n, 1e-5,
