@@ -209,6 +209,43 @@ int mog_set_tuning(mog_handle* h, const mog_tuning* t);
  */
 int mog_get_status(mog_handle* h, uint32_t* flags, void* stream);
 
+/* ---- sharded step over peer memory --------------------------------------
+ * One simulation's particles split over `world` GPUs (<= 8), one handle per
+ * rank, every handle created with the same config, transforms and
+ * scale_bits (no counterpart in the reference, which runs on one GL
+ * context).  Grid i belongs to rank floor(i * world / k).  The deposit
+ * adds each rank's cells straight into the owner's accumulation buffer with
+ * system-scope atomics over NVLink; the exchange waits (bounded) for every
+ * rank's deposit and copies the owners' slices into the local grid.  The
+ * integer total is exact, so the trajectory is bit-identical to one handle
+ * stepping all particles, for any split.  Every rank must make the same
+ * calls in the same order.
+ *
+ * mog_shard_init       allocate this rank's accumulation (3 x k g^3 cells)
+ *                      and flags; synchronises.
+ * mog_shard_export     64-byte CUDA IPC handles of those two buffers.
+ * mog_shard_connect    open the other ranks' handles (world x 64 bytes
+ *                      each, in rank order; this rank's entry is ignored).
+ * mog_shard_connect_local  the same for ranks held in this process
+ *                      (peers[q] = rank q's handle; peer access is enabled
+ *                      between different devices).
+ * mog_shard_deposit    deposit this rank's particles, then signal.
+ * mog_shard_exchange   wait for all ranks, gather the total grid.  A wait
+ *                      that runs out raises MOG_FLAG_TIMEOUT.
+ * mog_shard_finish     solve and update this rank's particles.
+ * mog_shard_step       the last three in order.
+ * Destroy the handles only after every rank has finished its last step.
+ */
+int mog_shard_init(mog_handle* h, int32_t rank, int32_t world);
+int mog_shard_export(const mog_handle* h, uint8_t* accum_ipc, uint8_t* flags_ipc);
+int mog_shard_connect(mog_handle* h, const uint8_t* accum_ipcs, const uint8_t* flags_ipcs);
+int mog_shard_connect_local(mog_handle* h, mog_handle* const* peers);
+int mog_shard_deposit(mog_handle* h, const float* pos4, int64_t n, void* stream);
+int mog_shard_exchange(mog_handle* h, void* stream);
+int mog_shard_finish(mog_handle* h, float* pos4, float* vel4, int64_t n, float dt_eff,
+                     void* stream);
+int mog_shard_step(mog_handle* h, float* pos4, float* vel4, int64_t n, float dt_eff, void* stream);
+
 /*
  * Failure-detection self-test (no counterpart in the reference): one
  * device wait that nothing satisfies, bounded like every wait in the

@@ -46,7 +46,9 @@ FLAG_BOUNDS = 16  # only from a library built with --check
 EXPORTS = (
     "mog_config_default", "mog_create", "mog_destroy", "mog_step", "mog_step_n",
     "mog_step_profiled", "mog_forces", "mog_deposit", "mog_solve", "mog_update", "mog_get_status",
-    "mog_selftest_wait_timeout",
+    "mog_selftest_wait_timeout", "mog_shard_init", "mog_shard_export", "mog_shard_connect",
+    "mog_shard_connect_local", "mog_shard_deposit", "mog_shard_exchange", "mog_shard_finish",
+    "mog_shard_step",
     "mog_get_tuning", "mog_set_tuning", "mog_diagnostics", "mog_direct_sum",
     "mog_direct_sum_noalloc", "mog_green_table", "mog_init_particles", "mog_init_particles_host",
     "mog_batch_create", "mog_batch_step", "mog_batch_destroy",
@@ -151,6 +153,14 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.mog_set_tuning.argtypes = [P, ctypes.POINTER(MogTuningC)]
     lib.mog_get_status.argtypes = [P, ctypes.POINTER(ctypes.c_uint32), P]
     lib.mog_selftest_wait_timeout.argtypes = [P, P]
+    lib.mog_shard_init.argtypes = [P, ctypes.c_int32, ctypes.c_int32]
+    lib.mog_shard_export.argtypes = [P, P, P]
+    lib.mog_shard_connect.argtypes = [P, P, P]
+    lib.mog_shard_connect_local.argtypes = [P, ctypes.POINTER(P)]
+    lib.mog_shard_deposit.argtypes = [P, P, I64, P]
+    lib.mog_shard_exchange.argtypes = [P, P]
+    lib.mog_shard_finish.argtypes = [P, P, P, I64, F, P]
+    lib.mog_shard_step.argtypes = [P, P, P, I64, F, P]
     lib.mog_diagnostics.argtypes = [P, P, P, I64, ctypes.POINTER(ctypes.c_double), P]
     D = ctypes.c_double
     lib.mog_direct_sum.argtypes = [P, I64, P, I64, D, D, D, P, P]

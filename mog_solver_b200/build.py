@@ -28,7 +28,8 @@ CSRC = PKG / "csrc"
 OUT = PKG / "libmog.so"
 OUT_CHECK = PKG / "libmog_check.so"
 SOURCES = ["mog_api.cu", "deposit.cu", "spectral.cu", "update.cu", "convolution.cu",
-           "diagnostics.cu", "sort.cu", "learned.cu", "dft_tc.cu", "ics.cu", "render.cu"]
+           "diagnostics.cu", "sort.cu", "learned.cu", "dft_tc.cu", "ics.cu", "render.cu",
+           "shard.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -72,6 +72,30 @@ struct SmemHist<1> {
     }
 };
 
+// Sharded deposits (SHARD kernels): `mass` points at the step's
+// ShardTargets, and v is added to cell `cell` (index in the k g^3 layout)
+// of the owning rank's accumulation buffer with a system-scope atomic
+// (several GPUs add to one cell over NVLink).
+template <typename Acc>
+__device__ __forceinline__ void shard_add(const Ensemble& e, Acc* mass, uint64_t cell, Acc v) {
+    const ShardTargets* t = reinterpret_cast<const ShardTargets*>(mass);
+    const int grid = (int)(cell >> (3 * e.lg));
+    Acc* base = static_cast<Acc*>(t->base[shard_owner(grid, e.k, t->world)]);
+    atomicAdd_system(base + cell, v);
+}
+
+// A sharded deposit's CTA makes its remote adds visible system-wide before
+// it exits (the step's signal follows the kernel): the barrier orders every
+// thread's adds before thread 0's system-scope fence.  Every thread of the
+// CTA must reach it.
+template <bool SHARD>
+__device__ __forceinline__ void shard_release() {
+    if constexpr (SHARD) {
+        __syncthreads();
+        if (threadIdx.x == 0) __threadfence_system();
+    }
+}
+
 // Shared-memory histogram deposit.  blockIdx.x: particle chunk; blockIdx.y:
 // group of `gpc` grids; blockIdx.z: slab of (1 << slab_lg) consecutive
 // cells of each grid (slab_lg == 3*lg means the whole grid).  Each thread
@@ -80,7 +104,7 @@ struct SmemHist<1> {
 // and shared adds overlap.  With AGG (used when the particles come in
 // spatial order) the lanes of a warp merge runs of equal cells with a
 // ballot of run heads, so a run costs one shared add.
-template <int MODE, int IDX, int PPT, bool AGG>
+template <int MODE, int IDX, int PPT, bool AGG, bool SHARD = false>
 __global__ void __launch_bounds__(1024) deposit_smem_kernel(const float4* __restrict__ pos,
                                                             const int* __restrict__ perm,
                                                             int64_t n, int64_t chunk,
@@ -219,9 +243,15 @@ __global__ void __launch_bounds__(1024) deposit_smem_kernel(const float4* __rest
         if (v) {
             const uint32_t j = i >> slab_lg, c = i & (slab_cells - 1);
             const size_t cell = (size_t)(g0 + j) * gcells + slab_lo + c;
-            if (in_bounds(e.flags, cell, (uint64_t)e.cells())) atomicAdd(mass + cell, v);
+            if (in_bounds(e.flags, cell, (uint64_t)e.cells())) {
+                if constexpr (SHARD)
+                    shard_add(e, mass, cell, v);
+                else
+                    atomicAdd(mass + cell, v);
+            }
         }
     }
+    shard_release<SHARD>();
 }
 
 // Specialised deposit for the common case: g <= 16 known at compile time,
@@ -259,7 +289,7 @@ __device__ __forceinline__ uint32_t cell_byte_offset(const float4& r0, const flo
 // memory, g = 32): only the high words live in shared memory; a non-zero
 // low half goes straight to the global 64-bit cell with one global atomic
 // (equal power-of-two masses have none).
-template <int LG, int MODE, int PPT, bool SPLIT = false>
+template <int LG, int MODE, int PPT, bool SPLIT = false, bool SHARD = false>
 __global__ void __launch_bounds__(1024) deposit_fast_kernel(const float4* __restrict__ pos,
                                                             int64_t n, int64_t chunk, Ensemble e,
                                                             int gpc,
@@ -332,7 +362,12 @@ __global__ void __launch_bounds__(1024) deposit_fast_kernel(const float4* __rest
                 if (MODE == 0) {
                     if (ql[u]) red_shared(lo_base + off, ql[u]);   // zero for padding lanes
                 } else if (SPLIT) {
-                    if (ql[u]) atomicAdd(mass + (size_t)g0 * G3 + (off >> 2), (Acc)ql[u]);
+                    if (ql[u]) {
+                        if constexpr (SHARD)
+                            shard_add(e, mass, (uint64_t)g0 * G3 + (off >> 2), (Acc)ql[u]);
+                        else
+                            atomicAdd(mass + (size_t)g0 * G3 + (off >> 2), (Acc)ql[u]);
+                    }
                     if (qh[u]) red_shared(hi_base + off, qh[u]);
                 } else if (hi_only) {
                     if (qh[u]) red_shared(hi_base + off, qh[u]);
@@ -355,13 +390,18 @@ __global__ void __launch_bounds__(1024) deposit_fast_kernel(const float4* __rest
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) {
         const Acc v = SPLIT ? (Acc)hi_w[i] << 32 : H::read(lo_w, hi_w, i);
-        if (v && in_bounds(e.flags, (size_t)g0 * G3 + i, (uint64_t)e.cells()))
-            atomicAdd(mass + (size_t)g0 * G3 + i, v);
+        if (v && in_bounds(e.flags, (size_t)g0 * G3 + i, (uint64_t)e.cells())) {
+            if constexpr (SHARD)
+                shard_add(e, mass, (uint64_t)g0 * G3 + i, v);
+            else
+                atomicAdd(mass + (size_t)g0 * G3 + i, v);
+        }
     }
+    shard_release<SHARD>();
 }
 
 // Direct global-atomic deposit (any g): one thread per particle, all grids.
-template <typename Acc, int IDX>
+template <typename Acc, int IDX, bool SHARD = false>
 __global__ void __launch_bounds__(256) deposit_global_kernel(const float4* __restrict__ pos,
                                                              int64_t n, Ensemble e,
                                                              Acc* __restrict__ mass) {
@@ -383,9 +423,14 @@ __global__ void __launch_bounds__(256) deposit_global_kernel(const float4* __res
         } else {
             cell = cell_exact(e.rot12 + 12 * i, e.off4 + 4 * i, cx, cy, cz, ip);
         }
-        if (q && in_bounds(e.flags, (size_t)i * gcells + cell, (uint64_t)e.cells()))
-            atomicAdd(mass + (size_t)i * gcells + cell, q);
+        if (q && in_bounds(e.flags, (size_t)i * gcells + cell, (uint64_t)e.cells())) {
+            if constexpr (SHARD)
+                shard_add(e, mass, (uint64_t)i * gcells + cell, q);
+            else
+                atomicAdd(mass + (size_t)i * gcells + cell, q);
+        }
     }
+    shard_release<SHARD>();
     if (sizeof(Acc) == 8) {
         double qs = (double)q;  // blocks are whole warps, so every lane is present
         for (int o = 16; o > 0; o >>= 1) qs += __shfl_xor_sync(kFull, qs, o);
@@ -408,7 +453,7 @@ static int auto_chunks(int64_t n, int64_t groups, int per_sm) {
     return (int)std::max<int64_t>(1, std::min<int64_t>(c, max_c));
 }
 
-template <int MODE, int IDX>
+template <int MODE, int IDX, bool SHARD>
 static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, const int* perm, int64_t n,
                                  bool ordered, void* mass_v, const DepositShape& sh,
                                  cudaStream_t s) {
@@ -423,7 +468,7 @@ static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, const int
     if (sh.grids_per_cta < 0) {
         const int threads = 256;
         const int64_t blocks = (n + threads - 1) / threads;
-        deposit_global_kernel<Acc, IDX><<<(unsigned)blocks, threads, 0, s>>>(pos, n, e, mass);
+        deposit_global_kernel<Acc, IDX, SHARD><<<(unsigned)blocks, threads, 0, s>>>(pos, n, e, mass);
         return cudaGetLastError();
     }
     int gpc = sh.grids_per_cta;
@@ -445,7 +490,8 @@ static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, const int
     }
     gpc = std::max(1, std::min(gpc, e.k));
     const size_t smem = (size_t)gpc * 16 * sizeof(float) + ((size_t)gpc * word_bytes << slab_lg);
-    const int ppt = sh.ppt == 1 || sh.ppt == 2 || sh.ppt == 4 ? sh.ppt : 4;
+    // the sharded deposit is built for 4 particles per thread only
+    const int ppt = SHARD ? 4 : (sh.ppt == 1 || sh.ppt == 2 || sh.ppt == 4 ? sh.ppt : 4);
     const bool agg = sh.aggregate < 0 ? ordered : sh.aggregate != 0;
     // g = 32 in u64 mode: the split histogram (high words only) fits one
     // grid per CTA where the two-word one needs two slabs
@@ -468,25 +514,31 @@ static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, const int
             kern<<<dim3(chunks, groups, 1), sh.threads, fsmem, s>>>(pos, n, chunk, e, gpc, mass);
             return cudaGetLastError();
         };
-        if (e.g == 32) {
-            if constexpr (MODE == 1) {
-                if (ppt == 1) return launch_fast(deposit_fast_kernel<5, 1, 1, true>);
-                if (ppt == 2) return launch_fast(deposit_fast_kernel<5, 1, 2, true>);
-                return launch_fast(deposit_fast_kernel<5, 1, 4, true>);
-            } else {
-                if (ppt == 1) return launch_fast(deposit_fast_kernel<5, MODE, 1>);
-                if (ppt == 2) return launch_fast(deposit_fast_kernel<5, MODE, 2>);
-                return launch_fast(deposit_fast_kernel<5, MODE, 4>);
+        if constexpr (SHARD) {
+            if (e.g == 32) return launch_fast(deposit_fast_kernel<5, MODE, 4, MODE == 1, true>);
+            if (e.g == 16) return launch_fast(deposit_fast_kernel<4, MODE, 4, false, true>);
+            return launch_fast(deposit_fast_kernel<3, MODE, 4, false, true>);
+        } else {
+            if (e.g == 32) {
+                if constexpr (MODE == 1) {
+                    if (ppt == 1) return launch_fast(deposit_fast_kernel<5, 1, 1, true>);
+                    if (ppt == 2) return launch_fast(deposit_fast_kernel<5, 1, 2, true>);
+                    return launch_fast(deposit_fast_kernel<5, 1, 4, true>);
+                } else {
+                    if (ppt == 1) return launch_fast(deposit_fast_kernel<5, MODE, 1>);
+                    if (ppt == 2) return launch_fast(deposit_fast_kernel<5, MODE, 2>);
+                    return launch_fast(deposit_fast_kernel<5, MODE, 4>);
+                }
             }
+            if (e.g == 16) {
+                if (ppt == 1) return launch_fast(deposit_fast_kernel<4, MODE, 1>);
+                if (ppt == 2) return launch_fast(deposit_fast_kernel<4, MODE, 2>);
+                return launch_fast(deposit_fast_kernel<4, MODE, 4>);
+            }
+            if (ppt == 1) return launch_fast(deposit_fast_kernel<3, MODE, 1>);
+            if (ppt == 2) return launch_fast(deposit_fast_kernel<3, MODE, 2>);
+            return launch_fast(deposit_fast_kernel<3, MODE, 4>);
         }
-        if (e.g == 16) {
-            if (ppt == 1) return launch_fast(deposit_fast_kernel<4, MODE, 1>);
-            if (ppt == 2) return launch_fast(deposit_fast_kernel<4, MODE, 2>);
-            return launch_fast(deposit_fast_kernel<4, MODE, 4>);
-        }
-        if (ppt == 1) return launch_fast(deposit_fast_kernel<3, MODE, 1>);
-        if (ppt == 2) return launch_fast(deposit_fast_kernel<3, MODE, 2>);
-        return launch_fast(deposit_fast_kernel<3, MODE, 4>);
     }
     auto launch = [&](auto kern) -> cudaError_t {
         cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -501,23 +553,36 @@ static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, const int
         kern<<<grid, sh.threads, smem, s>>>(pos, perm, n, chunk, e, gpc, slab_lg, mass);
         return cudaGetLastError();
     };
-    if (agg) {
-        if (ppt == 1) return launch(deposit_smem_kernel<MODE, IDX, 1, true>);
-        if (ppt == 4) return launch(deposit_smem_kernel<MODE, IDX, 4, true>);
-        return launch(deposit_smem_kernel<MODE, IDX, 2, true>);
+    if constexpr (SHARD) {
+        if (agg) return launch(deposit_smem_kernel<MODE, IDX, 4, true, true>);
+        return launch(deposit_smem_kernel<MODE, IDX, 4, false, true>);
+    } else {
+        if (agg) {
+            if (ppt == 1) return launch(deposit_smem_kernel<MODE, IDX, 1, true>);
+            if (ppt == 4) return launch(deposit_smem_kernel<MODE, IDX, 4, true>);
+            return launch(deposit_smem_kernel<MODE, IDX, 2, true>);
+        }
+        if (ppt == 1) return launch(deposit_smem_kernel<MODE, IDX, 1, false>);
+        if (ppt == 4) return launch(deposit_smem_kernel<MODE, IDX, 4, false>);
+        return launch(deposit_smem_kernel<MODE, IDX, 2, false>);
     }
-    if (ppt == 1) return launch(deposit_smem_kernel<MODE, IDX, 1, false>);
-    if (ppt == 4) return launch(deposit_smem_kernel<MODE, IDX, 4, false>);
-    return launch(deposit_smem_kernel<MODE, IDX, 2, false>);
 }
 
 cudaError_t launch_deposit(const Ensemble& e, const float4* pos, const int* perm, int64_t n,
-                           bool ordered, void* mass, const DepositShape& shape, cudaStream_t s) {
+                           bool ordered, void* mass, const DepositShape& shape, cudaStream_t s,
+                           bool shard) {
+    if (shard) {
+        if (e.mass_mode == 0)
+            return e.index_mode == 0 ? deposit_typed<1, 0, true>(e, pos, perm, n, ordered, mass, shape, s)
+                                     : deposit_typed<1, 1, true>(e, pos, perm, n, ordered, mass, shape, s);
+        return e.index_mode == 0 ? deposit_typed<0, 0, true>(e, pos, perm, n, ordered, mass, shape, s)
+                                 : deposit_typed<0, 1, true>(e, pos, perm, n, ordered, mass, shape, s);
+    }
     if (e.mass_mode == 0)
-        return e.index_mode == 0 ? deposit_typed<1, 0>(e, pos, perm, n, ordered, mass, shape, s)
-                                 : deposit_typed<1, 1>(e, pos, perm, n, ordered, mass, shape, s);
-    return e.index_mode == 0 ? deposit_typed<0, 0>(e, pos, perm, n, ordered, mass, shape, s)
-                             : deposit_typed<0, 1>(e, pos, perm, n, ordered, mass, shape, s);
+        return e.index_mode == 0 ? deposit_typed<1, 0, false>(e, pos, perm, n, ordered, mass, shape, s)
+                                 : deposit_typed<1, 1, false>(e, pos, perm, n, ordered, mass, shape, s);
+    return e.index_mode == 0 ? deposit_typed<0, 0, false>(e, pos, perm, n, ordered, mass, shape, s)
+                             : deposit_typed<0, 1, false>(e, pos, perm, n, ordered, mass, shape, s);
 }
 
 }  // namespace mog

@@ -150,6 +150,19 @@ struct mog_model {
     mog::ModelNorm norm{};
 };
 
+// A handle's part in a sharded step over peer memory (mog_shard_*).
+struct ShardState {
+    int rank = 0;
+    int world = 0;                   // 0: not sharded
+    void* d_accum = nullptr;         // this rank's accumulation buffer: 3 slots of k g^3 cells
+    uint64_t* d_flags = nullptr;     // this rank's flag words, one per rank
+    mog::ShardTargets* d_targets = nullptr;  // every rank's buffer for each of the 3 slots
+    mog::ShardView view;             // every rank's buffers (this rank's included)
+    bool ipc[mog::kMaxShardRanks] = {};  // rank q's buffers were opened from IPC handles
+    bool connected = false;
+    uint64_t epoch = 0;              // steps deposited (the flags' value)
+};
+
 struct mog_handle {
     mog_config cfg{};
     int device = 0;
@@ -183,6 +196,7 @@ struct mog_handle {
     int spread_cap = 0;               // CTAs d_spread has room for
     int spread_blocks = 0;
     int64_t spread_n = 0;
+    ShardState shard;
 };
 
 namespace {
@@ -366,7 +380,21 @@ size_t mass_bytes(const mog_handle* h) {
     return (size_t)h->e.cells() * (h->cfg.mass_mode == MOG_MASS_U64_FIXED ? 8 : 4);
 }
 
+void release_shard(mog_handle* h) {
+    ShardState& sh = h->shard;
+    for (int q = 0; q < mog::kMaxShardRanks; ++q)
+        if (sh.ipc[q]) {
+            if (sh.view.accum[q]) cudaIpcCloseMemHandle(sh.view.accum[q]);
+            if (sh.view.flags_peer[q]) cudaIpcCloseMemHandle(sh.view.flags_peer[q]);
+        }
+    if (sh.d_accum) cudaFree(sh.d_accum);
+    if (sh.d_flags) cudaFree(sh.d_flags);
+    if (sh.d_targets) cudaFree(sh.d_targets);
+    sh = ShardState();
+}
+
 void release(mog_handle* h) {
+    release_shard(h);
     for (auto& g : h->graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);
     h->graphs.clear();
@@ -790,6 +818,186 @@ int mog_get_status(mog_handle* h, uint32_t* flags, void* stream) {
     MOG_CUDA(cudaStreamSynchronize(s), "sync");
     *flags = v;
     return MOG_OK;
+}
+
+// The deposit's per-slot target tables, from the connected view.
+static int upload_targets(mog_handle* h) {
+    ShardState& sh = h->shard;
+    mog::ShardTargets t[3];
+    for (int slot = 0; slot < 3; ++slot) {
+        for (int q = 0; q < mog::kMaxShardRanks; ++q)
+            t[slot].base[q] = q < sh.world ? static_cast<char*>(sh.view.accum[q]) + (size_t)slot * mass_bytes(h)
+                                           : nullptr;
+        t[slot].world = sh.world;
+    }
+    MOG_CUDA(cudaMemcpy(sh.d_targets, t, sizeof t, cudaMemcpyHostToDevice), "shard targets upload");
+    sh.connected = true;
+    return MOG_OK;
+}
+
+int mog_shard_init(mog_handle* h, int32_t rank, int32_t world) {
+    if (!h) return fail(MOG_ERR_ARG, "null handle");
+    if (world < 1 || world > mog::kMaxShardRanks)
+        return fail(MOG_ERR_ARG, "world must be 1..8");
+    if (rank < 0 || rank >= world) return fail(MOG_ERR_ARG, "rank must be in [0, world)");
+    int rc = set_device(h);
+    if (rc) return rc;
+    release_shard(h);
+    ShardState& sh = h->shard;
+    const size_t bytes = 3 * mass_bytes(h);
+    MOG_CUDA(cudaMalloc(&sh.d_accum, bytes), "cudaMalloc shard accumulation");
+    MOG_CUDA(cudaMalloc((void**)&sh.d_flags, sizeof(uint64_t) * world), "cudaMalloc shard flags");
+    MOG_CUDA(cudaMalloc((void**)&sh.d_targets, sizeof(mog::ShardTargets) * 3), "cudaMalloc shard targets");
+    MOG_CUDA(cudaMemset(sh.d_accum, 0, bytes), "clear shard accumulation");
+    MOG_CUDA(cudaMemset(sh.d_flags, 0, sizeof(uint64_t) * world), "clear shard flags");
+    MOG_CUDA(cudaDeviceSynchronize(), "shard init");
+    sh.rank = rank;
+    sh.world = world;
+    return MOG_OK;
+}
+
+int mog_shard_export(const mog_handle* h, uint8_t* accum_ipc, uint8_t* flags_ipc) {
+    if (!h || !accum_ipc || !flags_ipc) return fail(MOG_ERR_ARG, "null argument");
+    if (!h->shard.world) return fail(MOG_ERR_ARG, "mog_shard_init first");
+    static_assert(sizeof(cudaIpcMemHandle_t) == 64, "IPC handles are 64 bytes");
+    cudaIpcMemHandle_t a, f;
+    MOG_CUDA(cudaIpcGetMemHandle(&a, h->shard.d_accum), "cudaIpcGetMemHandle");
+    MOG_CUDA(cudaIpcGetMemHandle(&f, h->shard.d_flags), "cudaIpcGetMemHandle");
+    std::memcpy(accum_ipc, &a, 64);
+    std::memcpy(flags_ipc, &f, 64);
+    return MOG_OK;
+}
+
+int mog_shard_connect(mog_handle* h, const uint8_t* accum_ipcs, const uint8_t* flags_ipcs) {
+    if (!h || !accum_ipcs || !flags_ipcs) return fail(MOG_ERR_ARG, "null argument");
+    ShardState& sh = h->shard;
+    if (!sh.world) return fail(MOG_ERR_ARG, "mog_shard_init first");
+    if (sh.connected) return fail(MOG_ERR_ARG, "already connected");
+    int rc = set_device(h);
+    if (rc) return rc;
+    for (int q = 0; q < sh.world; ++q) {
+        if (q == sh.rank) {
+            sh.view.accum[q] = sh.d_accum;
+            sh.view.flags_peer[q] = sh.d_flags;
+            continue;
+        }
+        cudaIpcMemHandle_t a, f;
+        std::memcpy(&a, accum_ipcs + 64 * q, 64);
+        std::memcpy(&f, flags_ipcs + 64 * q, 64);
+        void *pa = nullptr, *pf = nullptr;
+        cudaError_t err = cudaIpcOpenMemHandle(&pa, a, cudaIpcMemLazyEnablePeerAccess);
+        if (err == cudaSuccess) {
+            err = cudaIpcOpenMemHandle(&pf, f, cudaIpcMemLazyEnablePeerAccess);
+            if (err != cudaSuccess) cudaIpcCloseMemHandle(pa);
+        }
+        if (err != cudaSuccess) {
+            release_shard(h);
+            return cuda_fail(err, "cudaIpcOpenMemHandle (peer buffers)");
+        }
+        sh.view.accum[q] = pa;
+        sh.view.flags_peer[q] = static_cast<uint64_t*>(pf);
+        sh.ipc[q] = true;
+    }
+    sh.view.flags_local = sh.d_flags;
+    sh.view.rank = sh.rank;
+    sh.view.world = sh.world;
+    return upload_targets(h);
+}
+
+int mog_shard_connect_local(mog_handle* h, mog_handle* const* peers) {
+    if (!h || !peers) return fail(MOG_ERR_ARG, "null argument");
+    ShardState& sh = h->shard;
+    if (!sh.world) return fail(MOG_ERR_ARG, "mog_shard_init first");
+    if (sh.connected) return fail(MOG_ERR_ARG, "already connected");
+    int rc = set_device(h);
+    if (rc) return rc;
+    for (int q = 0; q < sh.world; ++q) {
+        const mog_handle* p = peers[q];
+        if (!p || p->shard.world != sh.world || p->shard.rank != q)
+            return fail(MOG_ERR_ARG, "peers[q] must be rank q of the same world (mog_shard_init)");
+        if (p->cfg.n_grids != h->cfg.n_grids || p->cfg.grid_size != h->cfg.grid_size ||
+            p->cfg.mass_mode != h->cfg.mass_mode)
+            return fail(MOG_ERR_ARG, "every rank needs the same n_grids, grid_size and mass_mode");
+        if (q == sh.rank && p != h) return fail(MOG_ERR_ARG, "peers[rank] must be this handle");
+        if (p->device != h->device) {
+            int can = 0;
+            MOG_CUDA(cudaDeviceCanAccessPeer(&can, h->device, p->device), "cudaDeviceCanAccessPeer");
+            if (!can) return fail(MOG_ERR_UNSUPPORTED, "no peer access between the ranks' devices");
+            cudaError_t err = cudaDeviceEnablePeerAccess(p->device, 0);
+            if (err == cudaErrorPeerAccessAlreadyEnabled)
+                cudaGetLastError();
+            else if (err != cudaSuccess)
+                return cuda_fail(err, "cudaDeviceEnablePeerAccess");
+        }
+        sh.view.accum[q] = p->shard.d_accum;
+        sh.view.flags_peer[q] = p->shard.d_flags;
+    }
+    sh.view.flags_local = sh.d_flags;
+    sh.view.rank = sh.rank;
+    sh.view.world = sh.world;
+    return upload_targets(h);
+}
+
+int mog_shard_deposit(mog_handle* h, const float* pos4, int64_t n, void* stream) {
+    if (!h) return fail(MOG_ERR_ARG, "null handle");
+    ShardState& sh = h->shard;
+    if (!sh.connected) return fail(MOG_ERR_ARG, "connect the shard first");
+    int rc = check_particles(h, pos4, nullptr, n, false);
+    if (rc) return rc;
+    if ((rc = set_device(h))) return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const uint64_t epoch = sh.epoch + 1;
+    const int slot = (int)(epoch % 3);
+    MOG_CUDA(mog::launch_deposit(h->e, reinterpret_cast<const float4*>(pos4), nullptr, n, false,
+                                 sh.d_targets + slot, h->dshape, s, true),
+             "sharded deposit");
+    MOG_CUDA(mog::launch_shard_signal(sh.view, epoch, s), "shard signal");
+    sh.epoch = epoch;
+    return MOG_OK;
+}
+
+int mog_shard_exchange(mog_handle* h, void* stream) {
+    if (!h) return fail(MOG_ERR_ARG, "null handle");
+    ShardState& sh = h->shard;
+    if (!sh.connected || sh.epoch == 0) return fail(MOG_ERR_ARG, "mog_shard_deposit first");
+    int rc = set_device(h);
+    if (rc) return rc;
+    MOG_CUDA(mog::launch_shard_exchange(h->e, sh.view, sh.epoch, (int)(sh.epoch % 3), h->d_mass,
+                                        static_cast<cudaStream_t>(stream)),
+             "shard exchange");
+    return MOG_OK;
+}
+
+int mog_shard_finish(mog_handle* h, float* pos4, float* vel4, int64_t n, float dt_eff,
+                     void* stream) {
+    if (!h) return fail(MOG_ERR_ARG, "null handle");
+    if (!h->shard.connected) return fail(MOG_ERR_ARG, "connect the shard first");
+    int rc = check_particles(h, pos4, vel4, n, true);
+    if (rc) return rc;
+    if (!std::isfinite(dt_eff)) return fail(MOG_ERR_ARG, "dt_eff must be finite");
+    if ((rc = set_device(h))) return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    float4* pos = reinterpret_cast<float4*>(pos4);
+    const int* perm = nullptr;
+    const float4* pos_s = nullptr;
+    if ((rc = order_particles(h, pos, n, wants_sort(h, n), s, &perm, &pos_s))) return rc;
+    const mog::Ensemble& e = h->e;
+    cudaError_t err = h->cfg.solver == MOG_SOLVER_FFT
+                          ? mog::launch_spectral(e, h->d_mass, h->d_force, true, true, h->d_scratch, s)
+                          : mog::launch_convolution(e, h->d_mass, h->d_force, true, true, s);
+    if (err != cudaSuccess) return cuda_fail(err, "solve");
+    err = mog::launch_update(e, pos, reinterpret_cast<float4*>(vel4), pos_s, perm, n, h->d_force,
+                             dt_eff, h->cfg.damping, nullptr, h->ushape, s);
+    if (err != cudaSuccess) return cuda_fail(err, "update");
+    ++h->step_count;
+    return MOG_OK;
+}
+
+int mog_shard_step(mog_handle* h, float* pos4, float* vel4, int64_t n, float dt_eff, void* stream) {
+    int rc = mog_shard_deposit(h, pos4, n, stream);
+    if (!rc) rc = mog_shard_exchange(h, stream);
+    if (!rc) rc = mog_shard_finish(h, pos4, vel4, n, dt_eff, stream);
+    return rc;
 }
 
 int mog_selftest_wait_timeout(mog_handle* h, void* stream) {

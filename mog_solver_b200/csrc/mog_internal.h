@@ -2,6 +2,7 @@
 // (mog_api.cu) and the kernel translation units.
 #pragma once
 
+#include <algorithm>
 #include <cstdint>
 #include <vector>
 #include <cuda_runtime.h>
@@ -9,6 +10,28 @@
 #include "mog_device.cuh"
 
 namespace mog {
+
+// Ranks of a sharded step over peer memory (at most this many).
+constexpr int kMaxShardRanks = 8;
+
+// Grid ownership of a sharded step: grid i belongs to rank
+// floor(i * world / k), so rank r owns the grids
+// [ceil(r k / world), ceil((r + 1) k / world)) (none when world > k and the
+// range is empty).  The owner accumulates the grid's cells from every rank.
+__host__ __device__ inline int shard_owner(int grid, int k, int world) {
+    return (int)(((int64_t)grid * world) / k);
+}
+__host__ __device__ inline int shard_first_grid(int rank, int k, int world) {
+    return (int)(((int64_t)rank * k + world - 1) / world);
+}
+
+// Where a sharded deposit sends each grid's cells (device memory, one per
+// slot): base[q] is rank q's accumulation buffer for the slot, in the full
+// k g^3 layout (only the grids q owns are written).
+struct ShardTargets {
+    void* base[kMaxShardRanks];
+    int world;
+};
 
 // Everything about one grid ensemble that the kernels read.  All pointers
 // are device memory owned by the handle.
@@ -66,12 +89,14 @@ struct UpdateShape {
 int num_sms();
 
 // mass grid (u64 or u32 per mode) <- particles.  Zeroes nothing: the
-// caller provides a zeroed grid.
+// caller provides a zeroed grid.  shard: `mass` is instead a device
+// ShardTargets, and each cell goes to its owning rank's buffer.
 // perm (nullable): slot s processes particle perm[s].  ordered: the
 // particles arrive in spatial order (pos already permuted, or perm set), so
 // warp merging of equal cells pays off.
 cudaError_t launch_deposit(const Ensemble& e, const float4* pos, const int* perm, int64_t n,
-                           bool ordered, void* mass, const DepositShape& shape, cudaStream_t s);
+                           bool ordered, void* mass, const DepositShape& shape, cudaStream_t s,
+                           bool shard = false);
 
 // force grid (float4 per cell) <- mass grid.  world_frame: rotate each
 // cell's force by M_i and store (x, y, z, 0) — what the production gather
@@ -112,6 +137,26 @@ size_t sort_scratch_bytes();
 // One bounded device wait that nothing satisfies (update.cu); raises
 // MOG_FLAG_TIMEOUT in *flags after about a second.
 cudaError_t launch_wait_timeout_selftest(unsigned* flags, cudaStream_t s);
+
+// Sharded step over peer memory (shard.cu).  accum[q]: rank q's
+// accumulation buffer (3 slots of k g^3 cells), flags_local: this rank's
+// world epoch words, flags_peer[q]: rank q's.
+struct ShardView {
+    void* accum[kMaxShardRanks] = {};
+    uint64_t* flags_peer[kMaxShardRanks] = {};
+    uint64_t* flags_local = nullptr;
+    int rank = 0;
+    int world = 0;
+};
+// This rank's deposit for `epoch` is complete: store epoch into word
+// `rank` of every rank's flags (system-scope release).
+cudaError_t launch_shard_signal(const ShardView& v, uint64_t epoch, cudaStream_t s);
+// Wait (bounded) until every rank has signalled `epoch`, copy every
+// owner's slice of slot `slot` into the local grid `local` (k g^3 cells),
+// then clear this rank's slice of the previous step's slot.  A wait that
+// runs out raises MOG_FLAG_TIMEOUT in e.flags and copies nothing.
+cudaError_t launch_shard_exchange(const Ensemble& e, const ShardView& v, uint64_t epoch, int slot,
+                                  void* local, cudaStream_t s);
 
 // Sets the calling thread's mog_last_error() text (mog_api.cu); returns code.
 int report_error(int code, const char* msg);
