@@ -17,8 +17,9 @@
 //                 within a tile the particles stay in index order;
 //   5. bounds:    first and one-past-last pair of every tile;
 //   6. composite: one CTA per tile, one thread per pixel: the tile's
-//                 particles are staged in shared memory 256 at a time and
-//                 every thread blends its pixel through them in order.
+//                 particles are staged in shared memory 256 at a time with
+//                 their pixel boxes, and every thread blends its pixel
+//                 through the ones whose box holds it, in order.
 // The result is the sequential GL blend, bit for bit (the host twin is
 // that sequential loop).
 #include <algorithm>
@@ -258,6 +259,7 @@ __global__ void __launch_bounds__(kTile* kTile) render_composite_kernel(
     const uint32_t* __restrict__ start, const uint32_t* __restrict__ end, Params R, int tiles_x,
     void* __restrict__ image) {
     __shared__ Splat stage[kTile * kTile];
+    __shared__ int4 box[kTile * kTile];  // pixel_range of each staged splat (a superset of its pixels)
     const int tile = blockIdx.x;
     const int px = (tile % tiles_x) * kTile + (threadIdx.x % kTile);
     const int py = (tile / tiles_x) * kTile + (threadIdx.x / kTile);
@@ -268,10 +270,20 @@ __global__ void __launch_bounds__(kTile* kTile) render_composite_kernel(
     const uint32_t lo = start[tile], hi = end[tile];
     for (uint32_t b = lo; b < hi; b += kTile * kTile) {
         const uint32_t cnt = min((uint32_t)(kTile * kTile), hi - b);
-        if (threadIdx.x < cnt) stage[threadIdx.x] = splats[vals[b + threadIdx.x]];
+        if (threadIdx.x < cnt) {
+            const Splat sp = splats[vals[b + threadIdx.x]];
+            int i0, i1, j0, j1;
+            rnd::pixel_range(sp, R, i0, i1, j0, j1);
+            stage[threadIdx.x] = sp;
+            box[threadIdx.x] = make_int4(i0, i1, j0, j1);
+        }
         __syncthreads();
         if (inside) {
             for (uint32_t j = 0; j < cnt; ++j) {
+                // most splats miss most pixels: reject on the integer box
+                // before the exact test
+                const int4 bx = box[j];
+                if (px < bx.x || px > bx.y || py < bx.z || py > bx.w) continue;
                 float a;
                 if (rnd::fragment(stage[j], xc, yc, a)) rnd::blend_pixel(R, stage[j], a, pix);
             }
