@@ -4,7 +4,7 @@ Run in a container that has the reference checkout (default /root/reference,
 or $MOG_REFERENCE) and the built oracle/_ref (python -m oracle.ref_build):
 
     python tests/golden/make_golden.py [transforms greens_kernel shaders two_galaxies init_particles camera
-                                        point_shaders]
+                                        point_shaders config]
 
 * transforms.npz   — Simulation.compute_transforms (main.py:157-172) with
                      the reference's own RandomSE3Sampler (main.py:9-62),
@@ -22,6 +22,9 @@ or $MOG_REFERENCE) and the built oracle/_ref (python -m oracle.ref_build):
                      (main.py:359-410, compiled as C++ by oracle/_ref) on
                      seeded vertices for three cameras and two speed
                      scales, and on seeded gl_PointCoord values.
+* config.json      — Simulation.load_config (main.py:174-189) run by the
+                     reference: the mapping it reads from its own config.yaml,
+                     and its in-code defaults (the file made to look absent).
 * shaders_g{8,16}.npz — the reference's compute shaders (compiled as C++ by
                      oracle/_ref) on small seeded particle sets: the mass
                      grid of mass.glsl, the gradient texture of the
@@ -240,9 +243,22 @@ def point_shaders(ref_main=None):
     np.savez_compressed(HERE / "point_shaders.npz", **out)
 
 
+def config(ref_main):
+    """The reference's load_config output, with and without its config.yaml."""
+    import json
+    from unittest import mock
+
+    fake = types.SimpleNamespace()
+    with_file = ref_main.Simulation.load_config(fake)
+    with mock.patch.object(ref_main.Path, "exists", lambda self: False):
+        defaults = ref_main.Simulation.load_config(fake)
+    (HERE / "config.json").write_text(json.dumps({"config_yaml": with_file, "defaults": defaults},
+                                                 indent=1, sort_keys=True) + "\n")
+
+
 PARTS = {"transforms": transforms, "greens_kernel": greens_kernel, "shaders": None,
          "two_galaxies": initial_conditions, "init_particles": perlin_sampler, "camera": camera,
-         "point_shaders": point_shaders}
+         "point_shaders": point_shaders, "config": config}
 
 
 def main():
