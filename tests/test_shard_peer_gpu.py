@@ -102,3 +102,29 @@ def test_a_rank_that_never_deposits_times_out():
         assert torch.isfinite(s0.pos).all()
     finally:
         grp.close()
+
+
+def test_peer_sharded_full_size():
+    """The benchmark's size (N = 2^20 colliding disks, k = 240, g = 16) over
+    4 ranks: bit-identical to one handle."""
+    from mog_solver_b200 import Simulation, ics
+    from mog_solver_b200.sharded import LocalPeerGroup, shard_bounds
+
+    n, world, steps = 1 << 20, 4, 4
+    cfg = dict(_cfg(240, 16, "u64", n), scale_bits=None)
+    ref = Simulation(cfg)
+    pos, vel = ics.two_disks(n, 100.0, seed=1, g_eff=ref.effective_g())
+    ref.set_particles(pos, vel)
+    cfg["scale_bits"] = ref.scale_bits
+    ref.step(steps)
+    bounds = [shard_bounds(n, r, world) for r in range(world)]
+    grp = LocalPeerGroup(cfg, [pos[lo:hi] for lo, hi in bounds], [vel[lo:hi] for lo, hi in bounds])
+    try:
+        grp.step(steps)
+        P, V = grp.gather()
+        torch.cuda.synchronize()
+        assert grp.status() == [0] * world
+        assert torch.equal(P, ref.pos) and torch.equal(V, ref.vel)
+    finally:
+        grp.close()
+        ref.close()
