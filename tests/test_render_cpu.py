@@ -249,3 +249,14 @@ def test_write_png_round_trip(tmp_path):
     rows = np.frombuffer(raw, np.uint8).reshape(30, 1 + 40 * 4)
     assert (rows[:, 0] == 0).all()
     assert np.array_equal(rows[:, 1:].reshape(30, 40, 4), img)
+
+
+def test_write_png_rejects_other_images(tmp_path):
+    from mog_solver_b200 import render as R
+
+    with pytest.raises(ValueError):
+        R.write_png(tmp_path / "f.png", np.zeros((4, 4, 4), np.float32))
+    with pytest.raises(ValueError):
+        R.write_png(tmp_path / "f.png", np.zeros((4, 4, 3), np.uint8))
+    with pytest.raises(ValueError):
+        R.params(8, 8, fmt="rgb565")

@@ -53,7 +53,6 @@ class Rank:
             if not self.pending:
                 self.pending = [("add", c) for c in range(self.cells) if self.contrib[self.step][c]]
                 self.pending += [("signal", q) for q in range(self.world)]
-                self.pending_order = "deposit"
             return self.pending
         if self.phase == "wait":
             if all(f >= epoch for f in self.flags):
@@ -136,8 +135,8 @@ def test_two_slots_are_not_enough():
 
 
 def test_ownership_partitions_the_grids():
-    from mog_solver_b200.sharded import shard_bounds  # noqa: F401  (same module family)
-
+    """floor(i * world / k) and ceil(r * k / world) describe the same split:
+    each grid has one owner and the owners' ranges tile [0, k)."""
     for k in (1, 2, 5, 16, 240):
         for world in range(1, 9):
             owned = []
@@ -184,3 +183,24 @@ def test_ipc_handles_are_exchanged_in_rank_order():
     want_f = b"".join(bytes([100 + r]) * 64 for r in range(world))
     for _, a, f in got:
         assert a == want_a and f == want_f
+
+
+def test_exchange_handles_checks_sizes():
+    from mog_solver_b200.sharded import exchange_handles
+
+    with pytest.raises(ValueError):
+        exchange_handles(b"\0" * 63, b"\0" * 64)
+
+
+def test_shard_entry_points_reject_bad_arguments_without_a_gpu():
+    """Argument checks come before any CUDA call."""
+    from mog_solver_b200 import _lib
+
+    lib = _lib.lib()
+    assert lib.mog_shard_init(None, 0, 2) == _lib.MOG_ERR_ARG
+    assert lib.mog_shard_deposit(None, None, 0, None) == _lib.MOG_ERR_ARG
+    assert lib.mog_shard_exchange(None, None) == _lib.MOG_ERR_ARG
+    assert lib.mog_shard_finish(None, None, None, 0, 0.0, None) == _lib.MOG_ERR_ARG
+    assert lib.mog_shard_connect(None, None, None) == _lib.MOG_ERR_ARG
+    assert lib.mog_shard_connect_local(None, None) == _lib.MOG_ERR_ARG
+    assert lib.mog_shard_export(None, None, None) == _lib.MOG_ERR_ARG
