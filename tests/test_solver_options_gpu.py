@@ -1,0 +1,105 @@
+"""Solver options and auxiliary subsystems on the GPU, beyond the core
+parity suite (test_gpu_parity.py):
+
+* the softened Green's function (softening > 0, the variant commented out
+  in greens.glsl:63-115) against the FP64 pipeline;
+* checkpoint / resume: save, load into a new Simulation and continue,
+  bit-identical to an uninterrupted run;
+* failure detection: a bounded device wait that nothing satisfies gives up,
+  raises MOG_FLAG_TIMEOUT and leaves the context usable.
+"""
+import numpy as np
+import pytest
+
+from oracle import pipeline as pl
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+FORCE_TOL = 1e-5  # relative L2 against the FP64 oracle (FP32 path)
+
+
+def make_sim(k=4, g=16, L=100.0, G=100.0, n=1000, seed=0, dt=1e-5, damping=0.999):
+    from mog_solver_b200 import Simulation
+
+    return Simulation({"n_grids": k, "grid_size": g, "world_size": L, "num_particles": n, "G": G,
+                       "dt": dt, "damping": damping, "seed": seed})
+
+
+def particles(n, L=100.0, seed=0):
+    rng = np.random.default_rng(seed)
+    pos = np.zeros((n, 4), dtype=np.float32)
+    nc = n // 2
+    pos[:nc, :3] = rng.normal(L / 2, L / 12, (nc, 3))
+    pos[nc:, :3] = rng.uniform(0, L, (n - nc, 3))
+    pos[:, :3] = np.mod(pos[:, :3], np.float32(L))
+    pos[:, 3] = 1.0 / max(n, 1)
+    vel = np.zeros_like(pos)
+    vel[:, :3] = rng.normal(0, 1, (n, 3))
+    return pos, vel
+
+
+@pytest.mark.parametrize("g", [16, 32])
+def test_softened_solve_matches_fp64(g):
+    """softening > 0: the variant commented out in greens.glsl:63-115."""
+    from mog_solver_b200 import Simulation
+
+    L, G, n, k, a = 100.0, 100.0, 20000, 3, 0.5
+    sim = Simulation({"n_grids": k, "grid_size": g, "world_size": L, "num_particles": n, "G": G,
+                      "dt": 1e-5, "seed": 1, "softening": a})
+    pos, vel = particles(n, L, seed=g + 1)
+    sim.set_particles(pos, vel)
+    m = sim.mass_grid()
+    F = sim.solve_grid(m).cpu().numpy()[..., :3]
+    rho = m.cpu().numpy().view(np.uint64).astype(np.float64) * 2.0 ** -sim.scale_bits
+    ref = pl.forces_grid_fp64(rho, G, L, softening=a)
+    assert pl.relative_l2(F, ref) <= FORCE_TOL
+    plain = pl.forces_grid_fp64(rho, G, L)
+    assert pl.relative_l2(ref, plain) > 0.05   # the softening changes the field
+
+
+def test_checkpoint_resume_is_bit_identical(tmp_path):
+    """save after 4 steps, load into a new Simulation, 4 more steps == 8
+    uninterrupted steps, bit for bit (the deposit is deterministic)."""
+    from mog_solver_b200 import Simulation
+
+    n = 20000
+    a = make_sim(k=6, g=16, n=n, dt=1e-3, damping=0.999, seed=3)
+    pos, vel = particles(n, seed=12)
+    a.set_particles(pos, vel)
+    a.step(4)
+    a.save(tmp_path / "ck.npz")
+    a.step(4)
+    b = Simulation.load(tmp_path / "ck.npz")
+    assert b.steps_taken == 4
+    b.step(4)
+    torch.cuda.synchronize()
+    assert torch.equal(a.pos, b.pos) and torch.equal(a.vel, b.vel)
+
+
+def test_bounded_wait_times_out_and_the_context_survives():
+    """A device wait that nothing satisfies gives up within its budget,
+    raises MOG_FLAG_TIMEOUT, and the next step still runs and matches a
+    fresh handle's."""
+    import time
+
+    from mog_solver_b200 import FLAG_TIMEOUT, _lib
+
+    n = 4096
+    a = make_sim(k=4, g=16, n=n, dt=1e-3)
+    b = make_sim(k=4, g=16, n=n, dt=1e-3)
+    pos, vel = particles(n, seed=21)
+    a.set_particles(pos, vel)
+    b.set_particles(pos, vel)
+    assert a.status() == 0
+    t0 = time.time()
+    _lib.check(_lib.lib().mog_selftest_wait_timeout(a.handle, None), "selftest")
+    assert a.status() == FLAG_TIMEOUT
+    assert time.time() - t0 < 30.0
+    assert a.status() == 0  # read and cleared
+    a.step(2)
+    b.step(2)
+    torch.cuda.synchronize()
+    assert torch.equal(a.pos, b.pos) and torch.equal(a.vel, b.vel)
+    assert a.status() == 0
