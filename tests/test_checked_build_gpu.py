@@ -9,7 +9,6 @@ import subprocess
 import sys
 from pathlib import Path
 
-import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
@@ -33,7 +32,6 @@ CASES = [
 
 CHILD = r"""
 import hashlib, json, sys
-import numpy as np
 import torch
 from mog_solver_b200 import Simulation, _lib
 
