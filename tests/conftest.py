@@ -3,7 +3,6 @@
 Tests marked ``gpu`` run the CUDA path (libmog.so) on a B200 and compare it
 with the oracle; everything else runs on the CPU.
 """
-import os
 import sys
 from pathlib import Path
 

@@ -5,7 +5,6 @@ must match exactly; a position differs only where the accept test of a
 candidate flips with the last-bit differences between CUDA's and the host
 library's cos, sin, acos and pow, so at least 99% of the records must be
 bit-identical and the rest inside the spawn region."""
-import ctypes
 from pathlib import Path
 
 import numpy as np
