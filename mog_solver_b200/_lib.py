@@ -106,6 +106,7 @@ class MogTuningC(ctypes.Structure):
         ("deposit_generic", ctypes.c_int32),
         ("deposit_sorted", ctypes.c_int32),
         ("update_threads", ctypes.c_int32),
+        ("deposit_split", ctypes.c_int32),
     ]
 
 

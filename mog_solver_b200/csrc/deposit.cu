@@ -493,11 +493,29 @@ static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, const int
     // the sharded deposit is built for 4 particles per thread only
     const int ppt = SHARD ? 4 : (sh.ppt == 1 || sh.ppt == 2 || sh.ppt == 4 ? sh.ppt : 4);
     const bool agg = sh.aggregate < 0 ? ordered : sh.aggregate != 0;
-    // g = 32 in u64 mode: the split histogram (high words only) fits one
-    // grid per CTA where the two-word one needs two slabs
-    const bool split = MODE == 1 && e.g == 32 && sh.grids_per_cta <= 1;
+    // The split histogram (u64, high words only, 4 bytes a cell; low halves
+    // go to the global cells, and equal power-of-two masses have none).  At
+    // g = 32 it fits one grid per CTA where the two-word one needs two
+    // slabs (the default); at g = 8 and 16 (tuning deposit_split = 1) it
+    // fits twice the grids per CTA.
+    const bool split32 = MODE == 1 && e.g == 32 && sh.grids_per_cta <= 1 && sh.split >= 0;
+    const bool split_small = !SHARD && MODE == 1 && (e.g == 8 || e.g == 16) && sh.split == 1;
+    const bool split = split32 || split_small;
     if (split && IDX == 0 && !agg && !perm && sh.fast != 0) {
-        gpc = 1;
+        const int fit = (int)std::max<size_t>(1, budget / ((size_t)4 << cells_lg));
+        if (split32) {
+            gpc = 1;
+        } else if (sh.grids_per_cta > 0) {
+            gpc = std::min(sh.grids_per_cta, fit);
+        } else {
+            const int most = std::min(e.k, fit);
+            gpc = most;
+            for (int d = most; d * 2 >= most && d >= 1; --d)
+                if (e.k % d == 0) {
+                    gpc = d;
+                    break;
+                }
+        }
         slab_lg = cells_lg;
     }
     if (IDX == 0 && !agg && !perm && slab_lg == cells_lg && (e.g == 8 || e.g == 16 || e.g == 32) &&
@@ -529,6 +547,10 @@ static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, const int
                     if (ppt == 2) return launch_fast(deposit_fast_kernel<5, MODE, 2>);
                     return launch_fast(deposit_fast_kernel<5, MODE, 4>);
                 }
+            }
+            if constexpr (MODE == 1) {
+                if (split_small && e.g == 16) return launch_fast(deposit_fast_kernel<4, 1, 4, true>);
+                if (split_small) return launch_fast(deposit_fast_kernel<3, 1, 4, true>);
             }
             if (e.g == 16) {
                 if (ppt == 1) return launch_fast(deposit_fast_kernel<4, MODE, 1>);

@@ -772,6 +772,7 @@ int mog_get_tuning(const mog_handle* h, mog_tuning* out) {
     out->deposit_sorted = h->dshape.sorted_input;
     out->update_threads = h->ushape.threads;
     out->update_direct_ppt = h->ushape.direct_ppt;
+    out->deposit_split = h->dshape.split;
     return MOG_OK;
 }
 
@@ -787,12 +788,13 @@ int mog_set_tuning(mog_handle* h, const mog_tuning* t) {
         (t->update_threads != 0 && t->update_threads != 512 && t->update_threads != 768 &&
          t->update_threads != 1024) ||
         (t->update_direct_ppt != 0 && t->update_direct_ppt != 1 && t->update_direct_ppt != 2 &&
-         t->update_direct_ppt != 4))
+         t->update_direct_ppt != 4) ||
+        t->deposit_split < -1 || t->deposit_split > 1)
         return fail(MOG_ERR_ARG, "tuning value out of range");
     h->dshape.threads = t->deposit_threads ? t->deposit_threads : 1024;
     h->dshape.grids_per_cta = t->deposit_grids_per_cta;
     h->dshape.chunks = t->deposit_chunks;
-    h->dshape.ppt = t->deposit_ppt ? t->deposit_ppt : 2;
+    h->dshape.ppt = t->deposit_ppt ? t->deposit_ppt : 4;
     h->ushape.staged = t->update_staged;
     h->ushape.ctas = t->update_ctas;
     h->ushape.direct_ppt = t->update_direct_ppt ? t->update_direct_ppt : 4;
@@ -801,6 +803,7 @@ int mog_set_tuning(mog_handle* h, const mog_tuning* t) {
     h->dshape.fast = t->deposit_generic ? 0 : 1;
     h->dshape.sorted_input = t->deposit_sorted ? 1 : 0;
     h->ushape.threads = t->update_threads ? t->update_threads : 512;
+    h->dshape.split = t->deposit_split;
     for (auto& g : h->graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);
     h->graphs.clear();

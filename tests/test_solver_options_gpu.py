@@ -103,3 +103,24 @@ def test_bounded_wait_times_out_and_the_context_survives():
     torch.cuda.synchronize()
     assert torch.equal(a.pos, b.pos) and torch.equal(a.vel, b.vel)
     assert a.status() == 0
+
+
+@pytest.mark.parametrize("g,k", [(16, 32), (16, 13), (8, 40)])
+@pytest.mark.parametrize("equal", [True, False])
+def test_split_histogram_at_small_grids_is_bit_exact(g, k, equal):
+    """Tuning deposit_split = 1: the high-word-only shared histogram at g = 8
+    and 16 (low halves as global atomics) gives the integer oracle's grid,
+    for power-of-two masses (no low halves) and for unequal ones."""
+    import oracle
+
+    n, L = 1 << 18, 100.0  # equal masses 1/n are a power of two: no low halves
+    sim = make_sim(k=k, g=g, n=n)
+    sim.tune(deposit_split=1)
+    pos, vel = particles(n, L, seed=g + k)
+    if not equal:
+        pos[:, 3] = np.random.default_rng(5).uniform(0.5, 2.0, n).astype(np.float32) / n
+    sim.set_particles(pos, vel)
+    got = sim.mass_grid().cpu().numpy().view(np.uint64)
+    ref = oracle.deposit(pos, sim.rotations, sim.offsets, g, L, oracle.MASS_U64, sim.scale_bits)
+    assert sim.tuning()["deposit_split"] == 1
+    assert np.array_equal(got, ref)
