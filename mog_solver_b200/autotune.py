@@ -57,6 +57,10 @@ def _candidates(sim: Simulation) -> dict[str, list[dict]]:
            for gpc, ppt, thr in itertools.product([0, 3, 6] if g <= 16 else [0],
                                                   [2, 4], [512, 1024])]
     dep.append(dict(deposit_grids_per_cta=-1))
+    if g in (8, 16) and sim.cfg.mass_mode == "u64":
+        # high-word-only histograms: more grids per CTA, low halves as global atomics
+        dep += [dict(deposit_split=1, deposit_grids_per_cta=0, deposit_ppt=4, deposit_threads=thr,
+                     deposit_chunks=0) for thr in (512, 1024)]
     upd = [dict(update_staged=0, update_direct_ppt=1), dict(update_staged=0, update_direct_ppt=4)]
     if g <= 16:
         upd += [dict(update_staged=1, update_threads=t) for t in (512, 768, 1024)]
