@@ -53,10 +53,12 @@ def _measure(sim: Simulation, reps: int) -> np.ndarray:
 
 def _candidates(sim: Simulation) -> dict[str, list[dict]]:
     g = sim.cfg.grid_size
-    dep = [dict(deposit_grids_per_cta=gpc, deposit_ppt=ppt, deposit_threads=thr, deposit_chunks=0)
+    # every candidate sets every deposit knob it could inherit from an earlier trial
+    dep = [dict(deposit_grids_per_cta=gpc, deposit_ppt=ppt, deposit_threads=thr, deposit_chunks=0,
+                deposit_split=0)
            for gpc, ppt, thr in itertools.product([0, 3, 6] if g <= 16 else [0],
                                                   [2, 4], [512, 1024])]
-    dep.append(dict(deposit_grids_per_cta=-1))
+    dep.append(dict(deposit_grids_per_cta=-1, deposit_split=0))
     if g in (8, 16) and sim.cfg.mass_mode == "u64":
         # high-word-only histograms: more grids per CTA, low halves as global atomics
         dep += [dict(deposit_split=1, deposit_grids_per_cta=0, deposit_ppt=4, deposit_threads=thr,
