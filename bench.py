@@ -456,6 +456,10 @@ def run_learned(args, w: dict) -> None:
     pos, vel = ics.two_disks(w["n"], w["L"], seed=w["seed"] + rank, g_eff=big.effective_g())
     cheap.set_particles(pos, vel)
     big.set_particles(pos, vel)
+    tuning = json.loads(args.tuning) if args.tuning else {}
+    if tuning:  # launch shapes for both ensembles (results never depend on them)
+        cheap.tune(**tuning)
+        big.tune(**{k: v for k, v in tuning.items() if k != "learned_fold"})
     model, model_src = learned_model()
     n = cheap.n_particles
     lib = _lib.lib()
@@ -596,6 +600,7 @@ def run_learned(args, w: dict) -> None:
                        "g": w["g"], "G": w["G"], "dt": w["dt"], "damping": w["damping"],
                        "network": "12-64-64-3 GELU, FP16 tensor-core inference, FP32 features",
                        "model": model_src, "index_mode": "fast", "mass_mode": "u64 fixed point",
+                       "tuning": tuning or "library defaults",
                        "parallelism": "single GPU" if world == 1 else f"{world} independent replicas",
                        "l2": "flushed between timed steps (256 MiB write)"},
             "accuracy": {"yardstick": "relative RMS force error vs FP64 periodic direct sum, 16,384 "

@@ -107,6 +107,7 @@ class MogTuningC(ctypes.Structure):
         ("deposit_sorted", ctypes.c_int32),
         ("update_threads", ctypes.c_int32),
         ("deposit_split", ctypes.c_int32),
+        ("learned_fold", ctypes.c_int32),
     ]
 
 

@@ -189,6 +189,7 @@ struct mog_handle {
     int64_t perm_cap = 0;        // capacity of d_perm
     int64_t perm_n = -1;         // n the permutation was built for
     int sort_every = 0;          // re-order every this many steps (0 = never)
+    int learned_fold = 0;        // learned step: cell masses written by the solve's epilogue
     uint64_t step_count = 0;     // steps issued (decides when to re-order)
     std::vector<GraphEntry> graphs;
     std::vector<mog::GridRows> rows;  // learned-gather rows of the k grids (host)
@@ -773,6 +774,7 @@ int mog_get_tuning(const mog_handle* h, mog_tuning* out) {
     out->update_threads = h->ushape.threads;
     out->update_direct_ppt = h->ushape.direct_ppt;
     out->deposit_split = h->dshape.split;
+    out->learned_fold = h->learned_fold;
     return MOG_OK;
 }
 
@@ -789,7 +791,8 @@ int mog_set_tuning(mog_handle* h, const mog_tuning* t) {
          t->update_threads != 1024) ||
         (t->update_direct_ppt != 0 && t->update_direct_ppt != 1 && t->update_direct_ppt != 2 &&
          t->update_direct_ppt != 4) ||
-        t->deposit_split < -1 || t->deposit_split > 1)
+        t->deposit_split < -1 || t->deposit_split > 1 || t->learned_fold < 0 ||
+        t->learned_fold > 1)
         return fail(MOG_ERR_ARG, "tuning value out of range");
     h->dshape.threads = t->deposit_threads ? t->deposit_threads : 1024;
     h->dshape.grids_per_cta = t->deposit_grids_per_cta;
@@ -804,6 +807,7 @@ int mog_set_tuning(mog_handle* h, const mog_tuning* t) {
     h->dshape.sorted_input = t->deposit_sorted ? 1 : 0;
     h->ushape.threads = t->update_threads ? t->update_threads : 512;
     h->dshape.split = t->deposit_split;
+    h->learned_fold = t->learned_fold;
     for (auto& g : h->graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);
     h->graphs.clear();
@@ -1121,14 +1125,22 @@ static int run_learned(mog_handle* h, const mog_model* m, int out_mode, float* p
     if (!err) err = mog::launch_deposit(e, pos, nullptr, n, false, h->d_mass, h->dshape, s);
     if (err != cudaSuccess) return cuda_fail(err, "deposit");
     if (ev && (err = cudaEventRecord(ev[1], s))) return cuda_fail(err, "event");
-    if (h->cfg.solver == MOG_SOLVER_FFT)
-        err = mog::launch_spectral(e, h->d_mass, h->d_force, true, false, h->d_scratch, s);
-    else
-        err = mog::launch_convolution(e, h->d_mass, h->d_force, true, false, s);
-    if (err != cudaSuccess) return cuda_fail(err, "solve");
-    if (ev && (err = cudaEventRecord(ev[2], s))) return cuda_fail(err, "event");
-    err = mog::launch_density_w(e, h->d_mass, h->d_force, s);
-    if (err != cudaSuccess) return cuda_fail(err, "cell masses");
+    if (h->cfg.solver == MOG_SOLVER_FFT && h->learned_fold) {
+        // the solve's epilogue leaves the cell masses in the force grid's .w
+        // (a separate pass where the fused kernel does not apply)
+        err = mog::launch_spectral_density(e, h->d_mass, h->d_force, h->d_scratch, s);
+        if (err != cudaSuccess) return cuda_fail(err, "solve");
+        if (ev && (err = cudaEventRecord(ev[2], s))) return cuda_fail(err, "event");
+    } else {
+        if (h->cfg.solver == MOG_SOLVER_FFT)
+            err = mog::launch_spectral(e, h->d_mass, h->d_force, true, false, h->d_scratch, s);
+        else
+            err = mog::launch_convolution(e, h->d_mass, h->d_force, true, false, s);
+        if (err != cudaSuccess) return cuda_fail(err, "solve");
+        if (ev && (err = cudaEventRecord(ev[2], s))) return cuda_fail(err, "event");
+        err = mog::launch_density_w(e, h->d_mass, h->d_force, s);
+        if (err != cudaSuccess) return cuda_fail(err, "cell masses");
+    }
     if (ev && (err = cudaEventRecord(ev[3], s))) return cuda_fail(err, "event");
     mog::LearnedOut out;
     out.out4 = out4;

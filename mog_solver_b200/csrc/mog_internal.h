@@ -118,6 +118,10 @@ cudaError_t launch_convolution(const Ensemble& e, void* mass, float4* force, boo
 std::vector<uint16_t> dft_tc_tables(int g);
 cudaError_t launch_dft_tc(int g, float2* f0, float2* f1, float2* f2, int nf, int axis, int pairs,
                           bool inverse, const void* tables, unsigned* flags, cudaStream_t s);
+// World-frame spectral solve that also leaves each cell's mass in the
+// force grid's .w lane and clears the mass grid (the learned path).
+cudaError_t launch_spectral_density(const Ensemble& e, void* mass, float4* force, void* scratch,
+                                    cudaStream_t s);
 cudaError_t launch_prerotate(const Ensemble& e, const float4* force_grid, float4* force_world,
                              cudaStream_t s);
 

@@ -237,9 +237,13 @@ __global__ void __launch_bounds__(G * G, (G == 16 ? 2 : 1))
 // multiply and the inverse transforms run one gradient field per third of
 // the threads; the epilogue stores with consecutive threads on consecutive
 // cells.  The arithmetic of every line is that of spectral_fused_kernel.
-template <int G, typename Acc, bool WORLD, bool ZERO>
+// DENS (with WORLD, without ZERO): the epilogue also puts each cell's mass
+// into the .w lane of its world-frame force and clears the mass grid (the
+// learned path's gather reads both from one float4).
+template <int G, typename Acc, bool WORLD, bool ZERO, bool DENS = false>
 __global__ void __launch_bounds__(3 * G * G, (G == 16 ? 1 : 4))
     spectral_fused3_kernel(Acc* __restrict__ mass, float4* __restrict__ force, Ensemble e) {
+    static_assert(!DENS || (WORLD && !ZERO), "cell masses go with world-frame forces");
     constexpr int P = G + 1, BUF = G * G * P, G3 = G * G * G, L = G * G;
     extern __shared__ float2 sm[];
     __shared__ float Rs[2][12];
@@ -249,7 +253,7 @@ __global__ void __launch_bounds__(3 * G * G, (G == 16 ? 1 : 4))
     const int l = t % L;  // line within a pass
     const int ga = 2 * blockIdx.x, gb = ga + 1;
     const bool hasb = gb < e.k;
-    if (blockIdx.x == 0 && t == 0 && ZERO) check_mass_total(e);
+    if (blockIdx.x == 0 && t == 0 && (ZERO || DENS)) check_mass_total(e);
     if (WORLD && t < 24) Rs[t / 12][t % 12] = (t < 12 || hasb) ? __ldg(e.rot12 + 12 * ga + t) : 0.f;
 
     // forward, x axis: line = row (y, z)
@@ -364,7 +368,13 @@ __global__ void __launch_bounds__(3 * G * G, (G == 16 ? 1 : 4))
             fy = z3.y * invn;
             fz = z2.y * invn;
         }
-        force[(size_t)(ga + gsel) * G3 + c] = make_out(WORLD, Rs[gsel], fx, fy, fz);
+        float4 o = make_out(WORLD, Rs[gsel], fx, fy, fz);
+        if (DENS) {
+            Acc* mc = mass + (size_t)(ga + gsel) * G3 + c;
+            o.w = mass_value(*mc, e.inv_scale);
+            *mc = 0;
+        }
+        force[(size_t)(ga + gsel) * G3 + c] = o;
     }
 }
 
@@ -613,6 +623,37 @@ __global__ void prerotate_kernel(const float4* __restrict__ in, float4* __restri
 }
 
 }  // namespace
+
+// World-frame solve that also leaves each cell's mass in the force grid's
+// .w lane and clears the mass grid: in the g = 8/16 fused kernel's epilogue,
+// else the general solve followed by the cell-mass pass.
+template <typename Acc>
+static cudaError_t spectral_density_typed(const Ensemble& e, Acc* mass, float4* force,
+                                          void* scratch, cudaStream_t s) {
+    if (!e.dft_tc && (e.g == 8 || e.g == 16)) {
+        const int pairs = (e.k + 1) / 2;
+        auto go = [&](auto kern, int G) -> cudaError_t {
+            const size_t smem = (size_t)3 * G * G * (G + 1) * sizeof(float2);
+            cudaError_t err =
+                cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (err != cudaSuccess) return err;
+            kern<<<pairs, 3 * G * G, smem, s>>>(mass, force, e);
+            return cudaGetLastError();
+        };
+        if (e.g == 16) return go(spectral_fused3_kernel<16, Acc, true, false, true>, 16);
+        return go(spectral_fused3_kernel<8, Acc, true, false, true>, 8);
+    }
+    cudaError_t err = spectral_typed(e, mass, force, true, false, scratch, s);
+    if (err != cudaSuccess) return err;
+    return launch_density_w(e, mass, force, s);
+}
+
+cudaError_t launch_spectral_density(const Ensemble& e, void* mass, float4* force, void* scratch,
+                                    cudaStream_t s) {
+    if (e.mass_mode == 0)
+        return spectral_density_typed(e, static_cast<unsigned long long*>(mass), force, scratch, s);
+    return spectral_density_typed(e, static_cast<unsigned*>(mass), force, scratch, s);
+}
 
 size_t spectral_scratch_bytes(const Ensemble& e) {
     if (e.g <= 16 && !e.dft_tc) return 0;

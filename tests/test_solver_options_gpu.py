@@ -124,3 +124,41 @@ def test_split_histogram_at_small_grids_is_bit_exact(g, k, equal):
     ref = oracle.deposit(pos, sim.rotations, sim.offsets, g, L, oracle.MASS_U64, sim.scale_bits)
     assert sim.tuning()["deposit_split"] == 1
     assert np.array_equal(got, ref)
+
+
+@pytest.mark.parametrize("g", [8, 16, 32])
+def test_learned_fold_is_bit_identical(g):
+    """Tuning learned_fold = 1: the solve's epilogue writes the cell masses
+    (g = 8, 16; a separate pass at g = 32): the learned step's particles and
+    its variance-gate statistics are those of the separate pass, bit for bit."""
+    import ctypes
+
+    from mog_solver_b200 import _lib
+    from mog_solver_b200.learned import Model
+    from mog_solver_b200.train_learned import DEFAULT_MODEL
+
+    n = 50000
+    model = Model.load(DEFAULT_MODEL)
+    a = make_sim(k=32, g=g, n=n, dt=1e-3)
+    b = make_sim(k=32, g=g, n=n, dt=1e-3)
+    b.tune(learned_fold=1)
+    pos, vel = particles(n, seed=31)
+    a.set_particles(pos, vel)
+    b.set_particles(pos, vel)
+    lib = _lib.lib()
+    try:
+        for _ in range(3):
+            for s in (a, b):
+                _lib.check(lib.mog_learned_step(s.handle, model.handle, s.pos.data_ptr(),
+                                                s.vel.data_ptr(), n, 1e-3, None), "learned step")
+        torch.cuda.synchronize()
+        assert torch.equal(a.pos, b.pos) and torch.equal(a.vel, b.vel)
+        sa, sb = (ctypes.c_double * 2)(), (ctypes.c_double * 2)()
+        _lib.check(lib.mog_learned_spread(a.handle, sa, None), "spread")
+        _lib.check(lib.mog_learned_spread(b.handle, sb, None), "spread")
+        assert list(sa) == list(sb)
+        assert a.status() == 0 and b.status() == 0
+    finally:
+        a.close()
+        b.close()
+        model.close()
