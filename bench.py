@@ -627,7 +627,7 @@ def run_learned(args, w: dict) -> None:
                     "d2h_bytes_per_step": 2 * 16 * n, "ms_per_step": t_e2e / args.steps,
                     "gate": f"variance gate every 10 steps, {ls.fallback_steps} fallback steps, "
                             f"last relative spread {ls.last_ratio} vs training {ls.train_ratio}"},
-            "gpu_launches": 4 * args.steps,
+            "gpu_launches": (3 if tuning.get("learned_fold") and w["g"] in (8, 16) else 4) * args.steps,
             "clocks": clk,
         }
         if base is not None:
