@@ -32,6 +32,7 @@ CASES = [
 
 CHILD = r"""
 import hashlib, json, sys
+import numpy as np
 import torch
 from mog_solver_b200 import Simulation, _lib
 
