@@ -210,27 +210,30 @@ def make_particles(w: dict, sim, seed_offset: int = 0):
     return ics.uniform_cube(n, L, seed=w["seed"] + seed_offset)
 
 
-def cpu_baseline(w: dict, budget_s: float = 20.0, steps: int | None = None) -> dict:
+def cpu_baseline(w: dict, budget_s: float = 20.0, steps: int = 3, warmup: int = 0) -> dict:
     """Time the reference's CPU path on a bounded sample of the workload."""
     import oracle.baseline as ob
 
-    return ob.time_reference(w, budget_s=budget_s, steps=steps)
+    return ob.time_reference(w, budget_s=budget_s, steps=steps, warmup=warmup)
 
 
 def run_reference(args, w: dict) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    res = cpu_baseline(w, budget_s=max(30.0, 3.0 * (args.steps + args.warmup)),
-                       steps=args.steps + args.warmup)
+    # every declared step runs (warm-up untimed, then exactly --steps timed),
+    # each on one particle sample sized so the whole run stays within ~2 min
+    res = cpu_baseline(w, budget_s=min(120.0, max(30.0, 3.0 * (args.steps + args.warmup))),
+                       steps=args.steps, warmup=args.warmup)
     line = {
         "impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT,
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "n_gpus": args.gpus, "steps": res["steps_timed"], "warmup": res["warmup_run"],
         "ms_per_step": res["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
         "config": {"workload": w["desc"] + ("; the reference's plain k=240 step (it has no learned "
                                             "path)" if "k_small" in w else ""),
-                   "n": w["n"], "k": w["k"], "g": w["g"], "sample_particles": res["sample_n"]},
+                   "n": w["n"], "k": w["k"], "g": w["g"], "sample_particles": res["sample_n"],
+                   "timed_seconds": round(res["timed_seconds"], 3)},
         "cpu_baseline": {"value": res["value"], "unit": UNIT, "cores": res["cores"],
                          "kind": res["kind"], "sample": res["sample"]},
         "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0,

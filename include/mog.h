@@ -298,7 +298,10 @@ int mog_direct_sum(const float* targets4, int64_t nt, const float* sources4, int
  * MOG_ERR_ARG with the limit in mog_last_error() and launch nothing.
  * The first call on each device does a one-time set-up (it looks up the
  * scratch's device address); make that first call before any stream
- * capture begins.  Nothing in the scratch needs to start at zero: every
+ * capture begins.  The looked-up address is kept for the life of the
+ * process, so the device's primary context must not be reset in between
+ * (cudaDeviceReset would unload the library's module and leave the kept
+ * address pointing at freed memory).  Nothing in the scratch needs to start at zero: every
  * partial sum a call reads was written earlier in the same call.  All
  * calls on one device share the one scratch, so calls that overlap in time
  * (other streams, other threads) race with one another and must be

@@ -67,7 +67,10 @@ def _time_ref(w: dict, sample_n: int, steps: int):
     return ref_harness.time_steps(pos, vel, off, rot, w, steps)
 
 
-def time_reference(w: dict, budget_s: float = 20.0, steps: int | None = None) -> dict:
+def time_reference(w: dict, budget_s: float = 20.0, steps: int = 3, warmup: int = 0) -> dict:
+    """Run ``warmup`` untimed steps, then time exactly ``steps`` steps, all on
+    one particle sample sized (from a one-step probe) so that the
+    ``warmup + steps`` steps take about ``budget_s`` seconds."""
     kind = "port"
     runner = _time_port
     try:
@@ -77,15 +80,19 @@ def time_reference(w: dict, budget_s: float = 20.0, steps: int | None = None) ->
             kind, runner = "reference", _time_ref
     except ImportError:
         pass
+    steps = max(1, int(steps))
+    warmup = max(0, int(warmup))
     sample_n = min(w["n"], 16384)
-    # one probe step to size the sample within the budget
     tp, tg, cores = runner(w, sample_n, 1)
-    n_steps = steps if steps else 3
     per_particle = tp / sample_n
-    room = budget_s / max(n_steps, 1) - tg
+    room = budget_s / (steps + warmup) - tg
     if room > 0 and per_particle > 0:
         sample_n = int(min(w["n"], max(4096, room / per_particle)))
-    tp, tg, cores = runner(w, sample_n, max(1, min(n_steps, 3)))
+    if warmup:
+        runner(w, sample_n, warmup)
+    t0 = time.perf_counter()
+    tp, tg, cores = runner(w, sample_n, steps)
+    timed_s = time.perf_counter() - t0
     t_step = tg + tp * (w["n"] / sample_n)
     return {
         "value": w["n"] / t_step,
@@ -93,8 +100,11 @@ def time_reference(w: dict, budget_s: float = 20.0, steps: int | None = None) ->
         "cores": cores,
         "kind": kind,
         "sample_n": sample_n,
-        "sample": (f"{sample_n} of {w['n']} particles of the workload with all {w['k']} grids of "
-                   f"{w['g']}^3 cells, uint x1000 masses; time per step = grid time + particle "
-                   f"time scaled by {w['n'] / sample_n:.1f}; host threads {cores} "
-                   f"of {os.cpu_count()}"),
+        "steps_timed": steps,
+        "warmup_run": warmup,
+        "timed_seconds": timed_s,
+        "sample": (f"{steps} timed steps (after {warmup} untimed) on {sample_n} of {w['n']} "
+                   f"particles of the workload with all {w['k']} grids of {w['g']}^3 cells, "
+                   f"uint x1000 masses; time per step = grid time + particle time scaled by "
+                   f"{w['n'] / sample_n:.1f}; host threads {cores} of {os.cpu_count()}"),
     }

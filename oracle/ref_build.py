@@ -3,7 +3,8 @@
 TEST AND CPU-BASELINE INFRASTRUCTURE ONLY.  Reads the seven hot-path shaders
 (shaders/{mass,complex,fft_batched,fourier,greens,pack,update}.glsl) and the
 initial-condition sampler (shaders/init_particles.glsl) from a
-reference checkout (default /root/reference, or $MOG_REFERENCE), and the
+reference checkout ($MOG_REFERENCE, else ``reference`` beside this
+repository's root), and the
 particle vertex and fragment shaders embedded in main.py's init_render
 (main.py:359-410), rewrites
 their GLSL-only declarations with a handful of regular expressions (SSBO
@@ -33,7 +34,9 @@ SHADERS = ["mass", "complex", "fft_batched", "fourier", "greens", "pack", "updat
 
 
 def reference_root() -> Path:
-    return Path(os.environ.get("MOG_REFERENCE", "/root/reference"))
+    """$MOG_REFERENCE, else a checkout named ``reference`` beside the repository."""
+    env = os.environ.get("MOG_REFERENCE")
+    return Path(env) if env else HERE.parent.parent / "reference"
 
 
 def translate(src: str, name: str) -> str:

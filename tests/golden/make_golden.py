@@ -1,7 +1,8 @@
 """Generate the golden fixtures in tests/golden from the reference itself.
 
-Run in a container that has the reference checkout (default /root/reference,
-or $MOG_REFERENCE) and the built oracle/_ref (python -m oracle.ref_build):
+Run in a container that has the reference checkout ($MOG_REFERENCE, else
+``reference`` beside this repository's root) and the built oracle/_ref
+(python -m oracle.ref_build):
 
     python tests/golden/make_golden.py [transforms greens_kernel shaders two_galaxies init_particles camera
                                         point_shaders config]
@@ -45,7 +46,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent.parent
 sys.path.insert(0, str(ROOT))
-REF = Path(os.environ.get("MOG_REFERENCE", "/root/reference"))
+REF = Path(os.environ.get("MOG_REFERENCE") or ROOT.parent / "reference")
 
 
 def import_reference_main():

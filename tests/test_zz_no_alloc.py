@@ -51,8 +51,31 @@ def test_noalloc_matches_allocating_entry_twice_in_a_row(nt, ns):
         rc_b, got = _call(lib.mog_direct_sum_noalloc, T, S, world, g_eff, soft)
         assert rc_a == L.MOG_OK and rc_b == L.MOG_OK, L.lib().mog_last_error()
         assert np.isfinite(got).all()
-        # same chunking and summation order: equal to rounding (tolerance 1e-12 relative)
-        np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
+        # same chunking and summation order: bit for bit
+        assert np.array_equal(got, ref)
+
+
+def test_noalloc_leaves_device_memory_unchanged():
+    """The point of the entry point: after the first call on a device (which
+    loads its kernels), further calls take no device memory at all."""
+    L, lib = _lib()
+    T, S = _sets(4096, 100000, 3)
+    out = torch.empty((T.shape[0], 3), dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def call():
+        rc = lib.mog_direct_sum_noalloc(T.data_ptr(), T.shape[0], S.data_ptr(), S.shape[0], 100.0,
+                                        1.0, 0.0, out.data_ptr(), ctypes.c_void_p(stream.cuda_stream))
+        assert rc == L.MOG_OK, lib.mog_last_error()
+
+    call()
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info()
+    for _ in range(3):
+        call()
+    torch.cuda.synchronize()
+    free_after, _ = torch.cuda.mem_get_info()
+    assert free_after == free_before
 
 
 def test_noalloc_rejects_requests_beyond_the_scratch():
