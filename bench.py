@@ -50,6 +50,14 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "particle-steps/s at fixed RMS force error vs FP64 direct sum: learned k=32 vs plain k=240"
+# the force the plain path computes at g = 16: the reference's step_fft hands
+# one scratch texture to both the x and the z inverse transform
+# (main.py:638-646), so its shaders store the z gradient as Fx at g = 4, 16,
+# 64; this library computes the intended x gradient unless
+# reference_texture_aliasing is set
+FFT_ALIASING = ("off: the intended x gradient (the reference's shaders store the z gradient as "
+                "Fx at g = 4, 16, 64 through a shared scratch texture, main.py:638-646; "
+                "config reference_texture_aliasing reproduces that)")
 UNIT = "particle-steps/s"
 
 WORKLOADS = {
@@ -367,7 +375,8 @@ def run_ours(args, w: dict) -> None:
             "config": {"workload": w["desc"] + " (plain path; learned k=32 not in this line)",
                        "n": w["n"], "k": w["k"], "g": w["g"], "G": w["G"], "dt": w["dt"],
                        "damping": w["damping"], "index_mode": args.index_mode,
-                       "mass_mode": "u64 fixed point", "parallelism":
+                       "mass_mode": "u64 fixed point", "texture_aliasing": FFT_ALIASING,
+                       "parallelism":
                        "single GPU" if world == 1 else f"{world} independent replicas",
                        "l2": "flushed between timed steps (256 MiB write)",
                        "tuning": sim.tuning()},
@@ -603,6 +612,7 @@ def run_learned(args, w: dict) -> None:
                        "g": w["g"], "G": w["G"], "dt": w["dt"], "damping": w["damping"],
                        "network": "12-64-64-3 GELU, FP16 tensor-core inference, FP32 features",
                        "model": model_src, "index_mode": "fast", "mass_mode": "u64 fixed point",
+                       "texture_aliasing": FFT_ALIASING,
                        "tuning": tuning or "library defaults",
                        "parallelism": "single GPU" if world == 1 else f"{world} independent replicas",
                        "l2": "flushed between timed steps (256 MiB write)"},
