@@ -429,6 +429,27 @@ int mog_init_particles_host(float* pos4, float* vel4, int64_t n, float world, fl
                             float contrast, uint32_t seed, float mass, float spawn_buffer,
                             int32_t shape);
 
+/*
+ * The reference's two-galaxy initialiser, Simulation.init_particles2
+ * (main.py:312-357), on the GPU.  Two spherical exponential blobs (scale
+ * 0.08 L) at L/2 -/+ 0.2 L along x with bulk velocities +/-(0.3, 0.1, 0),
+ * each spinning about its own axis with speed 0.3 sqrt(r / L + 0.01); the
+ * first n/2 records form galaxy 0, the next n/2 galaxy 1, an odd last
+ * record stays zero.  The reference draws from NumPy's sequential global
+ * generator; here particle i takes its three uniforms from a counter-based
+ * generator keyed by `seed` (SplitMix64), so the particle set has the
+ * reference's distribution but not its exact draws (for those, use the
+ * host routine ics.reference_two_galaxies).  Formulas in FP64, stored as
+ * FP32 records (x, y, z, mass) / (vx, vy, vz, 0).
+ * mog_init_two_galaxies: device buffers, on `stream`.
+ * mog_init_two_galaxies_host: host buffers, the same function on the host
+ * (the host math library's log, sin, cos, acos, sqrt).
+ */
+int mog_init_two_galaxies(float* pos4, float* vel4, int64_t n, float world, float mass,
+                          uint64_t seed, void* stream);
+int mog_init_two_galaxies_host(float* pos4, float* vel4, int64_t n, float world, float mass,
+                               uint64_t seed);
+
 /* ---- headless particle renderer ---------------------------------------
  * Replaces the reference's particle draw (vertex and fragment shaders,
  * main.py:359-423; on_render, main.py:678-703) with CUDA kernels writing

@@ -51,6 +51,7 @@ EXPORTS = (
     "mog_shard_step",
     "mog_get_tuning", "mog_set_tuning", "mog_diagnostics", "mog_direct_sum",
     "mog_direct_sum_noalloc", "mog_green_table", "mog_init_particles", "mog_init_particles_host",
+    "mog_init_two_galaxies", "mog_init_two_galaxies_host",
     "mog_batch_create", "mog_batch_step", "mog_batch_destroy",
     "mog_model_create", "mog_model_destroy", "mog_model_set", "mog_model_get",
     "mog_model_train_step", "mog_features", "mog_learned_forces", "mog_learned_step",
@@ -171,6 +172,8 @@ def _declare(lib: ctypes.CDLL) -> None:
     U32 = ctypes.c_uint32
     lib.mog_init_particles.argtypes = [P, P, I64, F, F, F, U32, F, F, ctypes.c_int32, P]
     lib.mog_init_particles_host.argtypes = [P, P, I64, F, F, F, U32, F, F, ctypes.c_int32]
+    lib.mog_init_two_galaxies.argtypes = [P, P, I64, F, F, ctypes.c_uint64, P]
+    lib.mog_init_two_galaxies_host.argtypes = [P, P, I64, F, F, ctypes.c_uint64]
     FP = ctypes.POINTER(ctypes.c_float)
     lib.mog_batch_create.argtypes = [P, ctypes.c_int32, ctypes.POINTER(P)]
     lib.mog_batch_step.argtypes = [P, P, P, P, P, ctypes.c_int32, P]

@@ -175,6 +175,43 @@ def reference_two_galaxies(n: int, world: float = 100.0, particle_mass: float = 
     return pos, vel
 
 
+def two_galaxies_host(n: int, world: float = 100.0, particle_mass: float = 1.0, seed: int = 0):
+    """The two-galaxy initialiser of mog_init_two_galaxies evaluated on the
+    host (mog_init_two_galaxies_host; no GPU needed): the reference's
+    formulas (main.py:312-357) with counter-based draws keyed by ``seed``."""
+    import ctypes
+
+    from . import _lib
+
+    pos = np.zeros((n, 4), dtype=np.float32)
+    vel = np.zeros((n, 4), dtype=np.float32)
+    _lib.check(_lib.lib().mog_init_two_galaxies_host(
+        pos.ctypes.data_as(ctypes.c_void_p), vel.ctypes.data_as(ctypes.c_void_p), int(n),
+        float(world), float(particle_mass), int(seed) & 0xFFFFFFFFFFFFFFFF),
+        "mog_init_two_galaxies_host")
+    return pos, vel
+
+
+def two_galaxies_uniforms(n: int, seed: int = 0) -> np.ndarray:
+    """The (n, 3) uniforms that mog_init_two_galaxies draws (SplitMix64 of a
+    seed-derived key plus 4 i + j, top 53 bits), in NumPy."""
+    M = np.uint64(0xFFFFFFFFFFFFFFFF)
+
+    def mix(z):
+        with np.errstate(over="ignore"):
+            z = (z + np.uint64(0x9E3779B97F4A7C15)) & M
+            z = ((z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)) & M
+            z = ((z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)) & M
+            return z ^ (z >> np.uint64(31))
+
+    key = mix(np.array([int(seed) & 0xFFFFFFFFFFFFFFFF], dtype=np.uint64))[0]
+    i = np.arange(n, dtype=np.uint64)[:, None]
+    j = np.arange(3, dtype=np.uint64)[None, :]
+    with np.errstate(over="ignore"):
+        ctr = (key + (i << np.uint64(2)) + j) & M
+    return (mix(ctr) >> np.uint64(11)).astype(np.float64) * 2.0 ** -53
+
+
 def perlin_args(n: int, world: float, mass: float, spawn_buffer: float = 0.1, seed: int = 12345,
                 noise_scale: float = 4.0, density_contrast: float = 2.0, shape: str = "sphere"):
     """Arguments of mog_init_particles after the buffers (stream excluded).

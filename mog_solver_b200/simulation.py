@@ -221,7 +221,9 @@ class Simulation:
     def init_particles(self, kind: str = "uniform", seed: int | None = None, **kw) -> None:
         """Replace the particles with a named initial set: uniform, disks,
         plummer, clumps (seed default 0), two_galaxies (the reference's
-        init_particles2) or perlin (the reference's GPU sampler,
+        init_particles2, its exact NumPy draws), two_galaxies_gpu (the same
+        initialiser as a CUDA kernel with counter-based draws) or perlin
+        (the reference's GPU sampler,
         init_particles.glsl, seed default 12345 as in main.py:281)."""
         from . import ics
 
@@ -239,6 +241,14 @@ class Simulation:
             pos, vel = ics.clumps(n, L, seed=seed, **kw)
         elif kind == "two_galaxies":  # the reference's init_particles2 (main.py:312-357)
             pos, vel = ics.reference_two_galaxies(n, L, self.cfg.particle_mass, seed=seed)
+        elif kind == "two_galaxies_gpu":  # the same distribution drawn on this GPU
+            torch = _torch()
+            pos = torch.empty((n, 4), dtype=torch.float32, device=self.device)
+            vel = torch.empty_like(pos)
+            with torch_device(self.device):
+                _lib.check(_lib.lib().mog_init_two_galaxies(
+                    pos.data_ptr(), vel.data_ptr(), n, float(L), float(self.cfg.particle_mass),
+                    int(seed) & 0xFFFFFFFFFFFFFFFF, self._stream()), "mog_init_two_galaxies")
         elif kind == "perlin":  # the reference's GPU sampler (main.py:280-310), on this GPU
             torch = _torch()
             pos = torch.empty((n, 4), dtype=torch.float32, device=self.device)
