@@ -329,6 +329,28 @@ int mog_batch_step(mog_batch* b, float* const* pos4, float* const* vel4, const i
 int mog_batch_destroy(mog_batch* b);
 
 /*
+ * Launch shapes of a batch.  work_queue = 1 (default): when every
+ * simulation uses the FFT solver, FAST cell indices, no spatial
+ * re-ordering, g = 8, 16 or 32 and one shared mass mode, an ensemble step
+ * is ONE persistent work-queue deposit over all simulations, each
+ * simulation's solve on its own graph branch, and ONE persistent
+ * work-queue gather + update over all simulations; every CTA pops tiles
+ * (simulation, grid group, particle chunk) / (simulation, particle chunk)
+ * from a largest-first list until it runs out.  Otherwise (or with
+ * work_queue = 0) each simulation's three kernels run on their own branch.
+ * deposit_chunk: particles per deposit tile (0 = 65536; else >= 1024).
+ * The result never depends on these.  mog_batch_get_tuning also reports
+ * whether the work-queue launches apply (active_work_queue, read only).
+ */
+typedef struct mog_batch_tuning {
+    int32_t work_queue;
+    int32_t deposit_chunk;
+    int32_t active_work_queue;
+} mog_batch_tuning;
+int mog_batch_set_tuning(mog_batch* b, const mog_batch_tuning* t);
+int mog_batch_get_tuning(const mog_batch* b, mog_batch_tuning* t);
+
+/*
  * Learned correction of a cheap ensemble (no counterpart in the reference,
  * whose force is always the plain k-grid average, update.glsl:67-81).
  * A model is a 12 -> 64 -> 64 -> 3 GELU network predicting, from per-particle

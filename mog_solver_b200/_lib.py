@@ -52,7 +52,8 @@ EXPORTS = (
     "mog_get_tuning", "mog_set_tuning", "mog_diagnostics", "mog_direct_sum",
     "mog_direct_sum_noalloc", "mog_green_table", "mog_init_particles", "mog_init_particles_host",
     "mog_init_two_galaxies", "mog_init_two_galaxies_host",
-    "mog_batch_create", "mog_batch_step", "mog_batch_destroy",
+    "mog_batch_create", "mog_batch_step", "mog_batch_destroy", "mog_batch_set_tuning",
+    "mog_batch_get_tuning",
     "mog_model_create", "mog_model_destroy", "mog_model_set", "mog_model_get",
     "mog_model_train_step", "mog_features", "mog_learned_forces", "mog_learned_step",
     "mog_learned_step_profiled", "mog_learned_spread",
@@ -109,6 +110,16 @@ class MogTuningC(ctypes.Structure):
         ("update_threads", ctypes.c_int32),
         ("deposit_split", ctypes.c_int32),
         ("learned_fold", ctypes.c_int32),
+    ]
+
+
+class MogBatchTuningC(ctypes.Structure):
+    """mog_batch_tuning (include/mog.h)."""
+
+    _fields_ = [
+        ("work_queue", ctypes.c_int32),
+        ("deposit_chunk", ctypes.c_int32),
+        ("active_work_queue", ctypes.c_int32),
     ]
 
 
@@ -178,6 +189,8 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.mog_batch_create.argtypes = [P, ctypes.c_int32, ctypes.POINTER(P)]
     lib.mog_batch_step.argtypes = [P, P, P, P, P, ctypes.c_int32, P]
     lib.mog_batch_destroy.argtypes = [P]
+    lib.mog_batch_set_tuning.argtypes = [P, ctypes.POINTER(MogBatchTuningC)]
+    lib.mog_batch_get_tuning.argtypes = [P, ctypes.POINTER(MogBatchTuningC)]
     lib.mog_model_create.argtypes = [ctypes.POINTER(P)]
     lib.mog_model_destroy.argtypes = [P]
     lib.mog_model_set.argtypes = [P, P, P]

@@ -1,10 +1,14 @@
 """Several independent simulations advanced together (one CUDA graph per
-ensemble step, one branch per simulation; mog_batch_* in include/mog.h).
+ensemble step; mog_batch_* in include/mog.h).
 
 The reference runs one simulation per window; this is the batched uneven
 ensemble of the benchmark configurations: simulations of different N, k and
-g step in a single graph launch so that small ones fill the GPU around
-large ones.
+g step in a single graph launch.  By default the graph holds one persistent
+work-queue deposit over every simulation, each simulation's solve on its
+own branch, and one persistent work-queue gather + update over every
+simulation (CTAs pop (simulation, grid group, particle chunk) tiles, largest
+first); ``tune(work_queue=0)`` runs each simulation's kernels on its own
+branch instead.
 """
 from __future__ import annotations
 
@@ -21,6 +25,7 @@ class Batch:
         self.sims = list(sims)
         self._h = ctypes.c_void_p()
         self._built_for = None
+        self._tuning = {"work_queue": 1, "deposit_chunk": 0}
 
     def _handles(self):
         hs = [s.handle for s in self.sims]  # creates / refreshes each handle
@@ -31,7 +36,31 @@ class Batch:
             _lib.check(_lib.lib().mog_batch_create(arr, len(hs), ctypes.byref(self._h)),
                        "mog_batch_create")
             self._built_for = key
+            self._apply_tuning()
         return self._h
+
+    def _apply_tuning(self) -> None:
+        t = _lib.MogBatchTuningC(int(self._tuning["work_queue"]), int(self._tuning["deposit_chunk"]), 0)
+        _lib.check(_lib.lib().mog_batch_set_tuning(self._h, ctypes.byref(t)), "mog_batch_set_tuning")
+
+    def tune(self, **kw) -> None:
+        """Set launch shapes: work_queue (1 persistent work-queue launches,
+        0 one branch per simulation), deposit_chunk (particles per deposit
+        tile, 0 = library default)."""
+        unknown = set(kw) - set(self._tuning)
+        if unknown:
+            raise ValueError(f"unknown batch tuning fields {sorted(unknown)}")
+        self._tuning.update(kw)
+        if self._h:
+            self._apply_tuning()
+
+    def tuning(self) -> dict:
+        """The batch's launch shapes, plus whether the work queue applies
+        to these simulations (active_work_queue)."""
+        t = _lib.MogBatchTuningC()
+        _lib.check(_lib.lib().mog_batch_get_tuning(self._handles(), ctypes.byref(t)),
+                   "mog_batch_get_tuning")
+        return {name: int(getattr(t, name)) for name, _ in t._fields_}
 
     def step(self, n_steps: int = 1) -> None:
         import torch

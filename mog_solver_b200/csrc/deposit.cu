@@ -12,6 +12,7 @@
 // bit-identical whatever the schedule.
 #include <algorithm>
 
+#include "../../include/mog.h"
 #include "mog_internal.h"
 
 namespace mog {
@@ -289,18 +290,22 @@ __device__ __forceinline__ uint32_t cell_byte_offset(const float4& r0, const flo
 // memory, g = 32): only the high words live in shared memory; a non-zero
 // low half goes straight to the global 64-bit cell with one global atomic
 // (equal power-of-two masses have none).
-template <int LG, int MODE, int PPT, bool SPLIT = false, bool SHARD = false>
-__global__ void __launch_bounds__(1024) deposit_fast_kernel(const float4* __restrict__ pos,
-                                                            int64_t n, int64_t chunk, Ensemble e,
-                                                            int gpc,
-                                                            typename SmemHist<MODE>::Acc* __restrict__ mass) {
+//
+// One tile: every thread of the CTA deposits particles [lo, hi) into grids
+// [g0, g0 + ng) through the shared histogram at smem_raw (gpc * 3 float4
+// rows, then the words).  count_total: add the tile's q to e.mass_total
+// (done by the tiles of the first grid group, which see every particle
+// once).  Returns after the flush, without a closing barrier.
+template <int LG, int MODE, int PPT, bool SPLIT, bool SHARD>
+__device__ __forceinline__ void deposit_fast_tile(const float4* __restrict__ pos, int64_t lo,
+                                                  int64_t hi, const Ensemble& e, int gpc, int g0,
+                                                  int ng, bool count_total,
+                                                  typename SmemHist<MODE>::Acc* __restrict__ mass,
+                                                  unsigned char* smem_raw) {
     using H = SmemHist<MODE>;
     using Acc = typename H::Acc;
     static_assert(!SPLIT || MODE == 1, "the split histogram is for u64 grids");
     constexpr int G3 = 1 << (3 * LG);
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int g0 = blockIdx.y * gpc;
-    const int ng = min(gpc, e.k - g0);
     const uint32_t words = (uint32_t)ng * G3;
     float4* rows = reinterpret_cast<float4*>(smem_raw);                       // gpc * 3 rows
     unsigned* lo_w = reinterpret_cast<unsigned*>(smem_raw + (size_t)gpc * 48);
@@ -316,8 +321,6 @@ __global__ void __launch_bounds__(1024) deposit_fast_kernel(const float4* __rest
     __syncthreads();
 
     const float half_l = e.world * 0.5f;
-    const int64_t lo = (int64_t)blockIdx.x * chunk;
-    const int64_t hi = min(n, lo + chunk);
     const int T = blockDim.x;
     unsigned bad = 0;
     double qsum = 0.0;
@@ -382,7 +385,7 @@ __global__ void __launch_bounds__(1024) deposit_fast_kernel(const float4* __rest
             }
         }
     }
-    if (MODE == 1 && blockIdx.y == 0) {
+    if (MODE == 1 && count_total) {
         for (int o = 16; o > 0; o >>= 1) qsum += __shfl_xor_sync(kFull, qsum, o);
         if ((threadIdx.x & 31) == 0 && qsum != 0.0) atomicAdd(e.mass_total, qsum);
     }
@@ -397,7 +400,57 @@ __global__ void __launch_bounds__(1024) deposit_fast_kernel(const float4* __rest
                 atomicAdd(mass + (size_t)g0 * G3 + i, v);
         }
     }
+}
+
+template <int LG, int MODE, int PPT, bool SPLIT = false, bool SHARD = false>
+__global__ void __launch_bounds__(1024) deposit_fast_kernel(const float4* __restrict__ pos,
+                                                            int64_t n, int64_t chunk, Ensemble e,
+                                                            int gpc,
+                                                            typename SmemHist<MODE>::Acc* __restrict__ mass) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int g0 = blockIdx.y * gpc;
+    const int64_t lo = (int64_t)blockIdx.x * chunk;
+    deposit_fast_tile<LG, MODE, PPT, SPLIT, SHARD>(pos, lo, min(n, lo + chunk), e, gpc, g0,
+                                                   min(gpc, e.k - g0), blockIdx.y == 0, mass,
+                                                   smem_raw);
     shard_release<SHARD>();
+}
+
+// Batched ensemble, one persistent launch for every simulation of a batch:
+// each CTA pops tiles (simulation, grid group, particle chunk) from the
+// host-built list with an atomic counter until it runs out, and deposits
+// each through the same tile body as deposit_fast_kernel.  The histogram
+// layout follows the tile's own grid count and grid size; at g = 32 in u64
+// mode it is the split (high-word) histogram, as in the single launch.
+template <int MODE>
+__global__ void __launch_bounds__(1024, 1) deposit_queue_kernel(const BatchSim* __restrict__ sims,
+                                                               const DepositTile* __restrict__ tiles,
+                                                               int ntiles, unsigned* __restrict__ counter) {
+    using Acc = typename SmemHist<MODE>::Acc;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int s_tile;
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = (int)atomicAdd(counter, 1u);
+        __syncthreads();
+        const int t = s_tile;
+        if (t >= ntiles) return;  // block-uniform
+        const DepositTile tile = tiles[t];
+        const BatchSim& S = sims[tile.sim];
+        const Ensemble e = S.e;
+        const float4* pos = S.pos;
+        Acc* mass = static_cast<Acc*>(S.mass);
+        const bool first = tile.g0 == 0;
+        if (e.lg == 3)
+            deposit_fast_tile<3, MODE, 4, false, false>(pos, tile.lo, tile.hi, e, tile.ng, tile.g0,
+                                                        tile.ng, first, mass, smem_raw);
+        else if (e.lg == 4)
+            deposit_fast_tile<4, MODE, 4, false, false>(pos, tile.lo, tile.hi, e, tile.ng, tile.g0,
+                                                        tile.ng, first, mass, smem_raw);
+        else
+            deposit_fast_tile<5, MODE, 4, MODE == 1, false>(pos, tile.lo, tile.hi, e, tile.ng,
+                                                            tile.g0, tile.ng, first, mass, smem_raw);
+        __syncthreads();  // the next tile reuses the histogram and s_tile
+    }
 }
 
 // Direct global-atomic deposit (any g): one thread per particle, all grids.
@@ -588,6 +641,38 @@ static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, const int
         if (ppt == 4) return launch(deposit_smem_kernel<MODE, IDX, 4, false>);
         return launch(deposit_smem_kernel<MODE, IDX, 2, false>);
     }
+}
+
+// Work-queue deposit tiles hold whole grids: two words a cell in u64 mode
+// at g <= 16, the split histogram's one word at g = 32, one word in u32
+// mode; as many grids as fit 200 KB, lowered to a divisor of k when one is
+// at least half of that (equal work per grid group).
+int queue_deposit_grids(int g, int mass_mode, int k) {
+    const size_t words = (mass_mode == MOG_MASS_U64_FIXED && g <= 16) ? 2 : 1;
+    const size_t grid_bytes = 4 * words * (size_t)g * g * g + 48;
+    const int most = (int)std::max<size_t>(1, std::min<size_t>((size_t)k, (200 * 1024) / grid_bytes));
+    for (int d = most; d * 2 >= most && d >= 1; --d)
+        if (k % d == 0) return d;
+    return most;
+}
+
+size_t queue_deposit_smem(int g, int mass_mode, int ng) {
+    const size_t words = (mass_mode == MOG_MASS_U64_FIXED && g <= 16) ? 2 : 1;
+    return (size_t)ng * 48 + 4 * words * (size_t)ng * g * g * g;
+}
+
+cudaError_t launch_deposit_queue(int mass_mode, const BatchSim* sims, const DepositTile* tiles,
+                                 int ntiles, unsigned* counter, size_t smem, cudaStream_t s) {
+    if (ntiles <= 0) return cudaSuccess;
+    auto go = [&](auto kern) -> cudaError_t {
+        cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)smem);
+        if (err != cudaSuccess) return err;
+        const int ctas = std::min(ntiles, num_sms() * (smem > 110 * 1024 ? 1 : 2));
+        kern<<<ctas, 1024, smem, s>>>(sims, tiles, ntiles, counter);
+        return cudaGetLastError();
+    };
+    return mass_mode == MOG_MASS_U64_FIXED ? go(deposit_queue_kernel<1>) : go(deposit_queue_kernel<0>);
 }
 
 cudaError_t launch_deposit(const Ensemble& e, const float4* pos, const int* perm, int64_t n,

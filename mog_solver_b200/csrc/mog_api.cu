@@ -1349,21 +1349,170 @@ struct mog_batch {
     std::vector<cudaStream_t> branch;
     std::vector<cudaEvent_t> done;
     cudaEvent_t fork = nullptr;
+    mog_batch_tuning tuning{1, 0, 0};
     struct Entry {
         std::vector<float*> pos, vel;
         std::vector<int64_t> n;
         std::vector<float> dt;
         cudaGraphExec_t exec = nullptr;
+        // work-queue mode: the simulation records, both tile lists and the
+        // two queue counters (device memory owned by the entry)
+        void* d_queue = nullptr;
+        int queue = 0;
     };
     std::vector<Entry> graphs;
 };
 
+namespace {
+
+void release_entry(mog_batch::Entry& g) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (g.d_queue) cudaFree(g.d_queue);
+    g.exec = nullptr;
+    g.d_queue = nullptr;
+}
+
+// Whether the batch can run as the two persistent work-queue launches:
+// every simulation uses the FFT solver, FAST cell indices, no spatial
+// re-ordering and g of 8, 16 or 32, and all share one mass mode.
+bool queue_eligible(const mog_batch* b) {
+    const int mm = b->sims[0]->cfg.mass_mode;
+    for (const mog_handle* h : b->sims) {
+        const int g = h->cfg.grid_size;
+        if (h->cfg.solver != MOG_SOLVER_FFT || h->cfg.index_mode != MOG_INDEX_FAST ||
+            h->sort_every != 0 || h->cfg.mass_mode != mm || (g != 8 && g != 16 && g != 32))
+            return false;
+    }
+    return true;
+}
+
+// Tile lists of one ensemble step, largest first (so the last tiles to
+// be popped are the short ones).  Deposit tiles: whole grid groups of
+// queue_deposit_grids grids over `chunk` particles; gather tiles:
+// kQueueGatherTile particles over all of a simulation's grids.  A g = 32
+// gather reads L2 instead of shared memory and counts double.
+void build_tiles(const mog_batch* b, const int64_t* n, int64_t chunk,
+                 std::vector<mog::DepositTile>& dep, std::vector<mog::GatherTile>& gat) {
+    std::vector<std::pair<double, mog::DepositTile>> d;
+    std::vector<std::pair<double, mog::GatherTile>> q;
+    for (int i = 0; i < (int)b->sims.size(); ++i) {
+        const mog_handle* h = b->sims[i];
+        const int k = h->cfg.n_grids, g = h->cfg.grid_size;
+        const int gpc = mog::queue_deposit_grids(g, h->cfg.mass_mode, k);
+        for (int g0 = 0; g0 < k; g0 += gpc)
+            for (int64_t lo = 0; lo < n[i]; lo += chunk) {
+                mog::DepositTile t{i, g0, std::min(gpc, k - g0), 0, lo, std::min(n[i], lo + chunk)};
+                d.push_back({(double)(t.hi - t.lo) * t.ng, t});
+            }
+        for (int64_t lo = 0; lo < n[i]; lo += mog::kQueueGatherTile) {
+            mog::GatherTile t{i, 0, lo, std::min(n[i], lo + mog::kQueueGatherTile)};
+            q.push_back({(double)(t.hi - t.lo) * k * (g > 16 ? 2.0 : 1.0), t});
+        }
+    }
+    auto by_cost = [](const auto& a, const auto& b2) { return a.first > b2.first; };
+    std::stable_sort(d.begin(), d.end(), by_cost);
+    std::stable_sort(q.begin(), q.end(), by_cost);
+    dep.clear();
+    gat.clear();
+    for (auto& x : d) dep.push_back(x.second);
+    for (auto& x : q) gat.push_back(x.second);
+}
+
+// Capture one ensemble step as: clear the two queue counters, the
+// work-queue deposit of every simulation, every simulation's solve on its
+// own branch, the work-queue gather + update of every simulation.
+int capture_queue_step(mog_batch* b, float* const* pos4, float* const* vel4, const int64_t* n,
+                       const float* dt_eff, mog_batch::Entry& entry, cudaGraph_t* graph) {
+    const int count = (int)b->sims.size();
+    const int64_t chunk = b->tuning.deposit_chunk > 0 ? b->tuning.deposit_chunk : 65536;
+    std::vector<mog::DepositTile> dep;
+    std::vector<mog::GatherTile> gat;
+    build_tiles(b, n, chunk, dep, gat);
+    std::vector<mog::BatchSim> recs(count);
+    size_t smem = 0;
+    int kmax = 1;
+    for (int i = 0; i < count; ++i) {
+        mog_handle* h = b->sims[i];
+        recs[i].e = h->e;
+        recs[i].pos = reinterpret_cast<float4*>(pos4[i]);
+        recs[i].vel = reinterpret_cast<float4*>(vel4[i]);
+        recs[i].n = n[i];
+        recs[i].mass = h->d_mass;
+        recs[i].force = h->d_force;
+        recs[i].dt = dt_eff[i];
+        recs[i].damping = h->cfg.damping;
+        const int g = h->cfg.grid_size;
+        smem = std::max(smem, mog::queue_deposit_smem(
+                                  g, h->cfg.mass_mode,
+                                  mog::queue_deposit_grids(g, h->cfg.mass_mode, h->cfg.n_grids)));
+        kmax = std::max(kmax, h->cfg.n_grids);
+    }
+    const size_t sims_b = sizeof(mog::BatchSim) * count;
+    const size_t dep_b = sizeof(mog::DepositTile) * dep.size();
+    const size_t gat_b = sizeof(mog::GatherTile) * gat.size();
+    auto up = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t total = up(sims_b) + up(dep_b) + up(gat_b) + 256;
+    char* base = nullptr;
+    MOG_CUDA(cudaMalloc((void**)&base, total), "batch queue buffers");
+    entry.d_queue = base;
+    auto* d_sims = reinterpret_cast<mog::BatchSim*>(base);
+    auto* d_dep = reinterpret_cast<mog::DepositTile*>(base + up(sims_b));
+    auto* d_gat = reinterpret_cast<mog::GatherTile*>(base + up(sims_b) + up(dep_b));
+    auto* d_cnt = reinterpret_cast<unsigned*>(base + up(sims_b) + up(dep_b) + up(gat_b));
+    MOG_CUDA(cudaMemcpy(d_sims, recs.data(), sims_b, cudaMemcpyHostToDevice), "batch records");
+    if (dep_b) MOG_CUDA(cudaMemcpy(d_dep, dep.data(), dep_b, cudaMemcpyHostToDevice), "deposit tiles");
+    if (gat_b) MOG_CUDA(cudaMemcpy(d_gat, gat.data(), gat_b, cudaMemcpyHostToDevice), "gather tiles");
+
+    int rc = MOG_OK;
+    MOG_CUDA(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal), "begin capture");
+    cudaError_t err = cudaMemsetAsync(d_cnt, 0, 2 * sizeof(unsigned), b->cap);
+    if (!err) err = mog::launch_deposit_queue(b->sims[0]->cfg.mass_mode, d_sims, d_dep, (int)dep.size(),
+                                              d_cnt, smem, b->cap);
+    if (!err) err = cudaEventRecord(b->fork, b->cap);
+    for (int i = 0; i < count && !err; ++i) {
+        mog_handle* h = b->sims[i];
+        err = cudaStreamWaitEvent(b->branch[i], b->fork, 0);
+        if (!err) err = mog::launch_spectral(h->e, h->d_mass, h->d_force, true, true, h->d_scratch,
+                                             b->branch[i]);
+        if (!err) err = cudaEventRecord(b->done[i], b->branch[i]);
+        if (!err) err = cudaStreamWaitEvent(b->cap, b->done[i], 0);
+    }
+    if (!err) err = mog::launch_gather_queue(d_sims, d_gat, (int)gat.size(), d_cnt + 1, kmax, b->cap);
+    cudaError_t end = cudaStreamEndCapture(b->cap, graph);
+    if (err || end) {
+        if (*graph) cudaGraphDestroy(*graph);
+        *graph = nullptr;
+        rc = cuda_fail(err ? err : end, "batch work-queue capture");
+    }
+    entry.queue = 1;
+    return rc;
+}
+
+}  // namespace
+
 extern "C" {
+
+int mog_batch_set_tuning(mog_batch* b, const mog_batch_tuning* t) {
+    if (!b || !t) return fail(MOG_ERR_ARG, "null argument");
+    if (t->work_queue < 0 || t->work_queue > 1 || t->deposit_chunk < 0 ||
+        (t->deposit_chunk > 0 && t->deposit_chunk < 1024))
+        return fail(MOG_ERR_ARG, "batch tuning value out of range");
+    b->tuning = *t;
+    for (auto& g : b->graphs) release_entry(g);
+    b->graphs.clear();
+    return MOG_OK;
+}
+
+int mog_batch_get_tuning(const mog_batch* b, mog_batch_tuning* t) {
+    if (!b || !t) return fail(MOG_ERR_ARG, "null argument");
+    *t = b->tuning;
+    t->active_work_queue = (b->tuning.work_queue && queue_eligible(b)) ? 1 : 0;
+    return MOG_OK;
+}
 
 int mog_batch_destroy(mog_batch* b) {
     if (!b) return MOG_OK;
-    for (auto& g : b->graphs)
-        if (g.exec) cudaGraphExecDestroy(g.exec);
+    for (auto& g : b->graphs) release_entry(g);
     for (auto s : b->branch)
         if (s) cudaStreamDestroy(s);
     for (auto e : b->done)
@@ -1432,6 +1581,27 @@ int mog_batch_step(mog_batch* b, float* const* pos4, float* const* vel4, const i
             same = g.pos[i] == pos4[i] && g.vel[i] == vel4[i] && g.n[i] == n[i] && g.dt[i] == dt_eff[i];
         if (same) ge = &g;
     }
+    if (!ge && b->tuning.work_queue && queue_eligible(b)) {
+        mog_batch::Entry entry;
+        cudaGraph_t graph = nullptr;
+        rc = capture_queue_step(b, pos4, vel4, n, dt_eff, entry, &graph);
+        cudaError_t err = rc ? cudaSuccess : cudaGraphInstantiate(&entry.exec, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        if (rc || err) {
+            release_entry(entry);
+            return rc ? rc : cuda_fail(err, "batch graph instantiate");
+        }
+        entry.pos.assign(pos4, pos4 + count);
+        entry.vel.assign(vel4, vel4 + count);
+        entry.n.assign(n, n + count);
+        entry.dt.assign(dt_eff, dt_eff + count);
+        if (b->graphs.size() >= 4) {
+            release_entry(b->graphs.front());
+            b->graphs.erase(b->graphs.begin());
+        }
+        b->graphs.push_back(std::move(entry));
+        ge = &b->graphs.back();
+    }
     if (!ge) {
         // buffers that a captured step cannot allocate
         for (int i = 0; i < count; ++i) {
@@ -1466,7 +1636,7 @@ int mog_batch_step(mog_batch* b, float* const* pos4, float* const* vel4, const i
         cudaGraphDestroy(graph);
         if (err) return cuda_fail(err, "batch graph instantiate");
         if (b->graphs.size() >= 4) {
-            cudaGraphExecDestroy(b->graphs.front().exec);
+            release_entry(b->graphs.front());
             b->graphs.erase(b->graphs.begin());
         }
         b->graphs.push_back(std::move(entry));

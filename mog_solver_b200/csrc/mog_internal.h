@@ -134,6 +134,46 @@ cudaError_t launch_update(const Ensemble& e, float4* pos, float4* vel, const flo
                           const int* perm, int64_t n, const float4* force_world, float dt,
                           float damping, float4* acc_out, const UpdateShape& shape, cudaStream_t s);
 
+// ---- batched ensemble work queue (deposit.cu, update.cu) -----------------
+// One simulation of a batch as the work-queue kernels read it (device
+// memory, one record per simulation).
+struct BatchSim {
+    Ensemble e;
+    float4* pos = nullptr;
+    float4* vel = nullptr;
+    int64_t n = 0;
+    void* mass = nullptr;           // its mass grid (zeroed by its previous solve)
+    const float4* force = nullptr;  // its world-frame force grid
+    float dt = 0.f;
+    float damping = 1.f;
+};
+// Deposit tile: particles [lo, hi) of simulation `sim` into its grids
+// [g0, g0 + ng).  Gather tile: particles [lo, hi) over all its grids.
+struct DepositTile {
+    int32_t sim, g0, ng, pad;
+    int64_t lo, hi;
+};
+struct GatherTile {
+    int32_t sim, pad;
+    int64_t lo, hi;
+};
+// Grids per deposit tile for a simulation (whole grids in shared memory),
+// the tile's shared-memory bytes, and the particles of one gather tile.
+int queue_deposit_grids(int g, int mass_mode, int k);
+size_t queue_deposit_smem(int g, int mass_mode, int ng);
+constexpr int kQueueGatherThreads = 512;
+constexpr int kQueueGatherPPT = 14;
+constexpr int64_t kQueueGatherTile = (int64_t)kQueueGatherThreads * kQueueGatherPPT;
+// Persistent launches over a host-built tile list (largest first): every
+// CTA pops tiles with an atomic counter (*counter must be 0 at launch)
+// until the list runs out.  All simulations use FAST cell indices and
+// share the mass mode; g is 8, 16 or 32.  kmax: the most grids of any
+// simulation (the gather stages their index rows in shared memory).
+cudaError_t launch_deposit_queue(int mass_mode, const BatchSim* sims, const DepositTile* tiles,
+                                 int ntiles, unsigned* counter, size_t smem, cudaStream_t s);
+cudaError_t launch_gather_queue(const BatchSim* sims, const GatherTile* tiles, int ntiles,
+                                unsigned* counter, int kmax, cudaStream_t s);
+
 // Spatial ordering: perm <- particles sorted by the Morton index of their
 // 32^3 world cell.  scratch: sort_scratch_bytes() bytes.
 size_t sort_scratch_bytes();

@@ -322,6 +322,137 @@ __global__ void __launch_bounds__(THREADS, 1)
     if (bad) raise_flags(e.flags, bad);
 }
 
+// Batched ensemble, one persistent launch for every simulation of a batch:
+// each CTA pops tiles (simulation, particle chunk of THREADS * PPT) from
+// the host-built list with an atomic counter.  A tile of a simulation with
+// g <= 16 stages its grids one by one in shared memory exactly as
+// update_staged_kernel does (bulk copies into `nstage` stages of 64 KB on
+// mbarriers); a tile with g = 32 (512 KB a grid) gathers from L2.  The
+// copy count runs on across tiles, so each stage's mbarrier parity is that
+// count's round.  Per particle the force is summed grid by grid in index
+// order, so every simulation's result is bit-identical to its own step.
+template <int PPT, int THREADS>
+__global__ void __launch_bounds__(THREADS, 1)
+    gather_queue_kernel(const BatchSim* __restrict__ sims, const GatherTile* __restrict__ tiles,
+                        int ntiles, unsigned* __restrict__ counter, int nstage) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    constexpr size_t kStageBytes = (size_t)16 << 12;  // one g = 16 grid of float4
+    float4* stage = reinterpret_cast<float4*>(smem);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + (size_t)nstage * kStageBytes);
+    float* xf = reinterpret_cast<float*>(full + 8);
+    __shared__ int s_tile;
+    __shared__ int abort_flag;
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        abort_flag = 0;
+        for (int q = 0; q < nstage; ++q) mbar_init(full + q, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    const float no_box[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    uint32_t issued = 0;  // bulk copies this CTA has issued (the same in every thread)
+    for (;;) {
+        if (tid == 0) s_tile = (int)atomicAdd(counter, 1u);
+        __syncthreads();
+        const int t = s_tile;
+        if (t >= ntiles) return;  // block-uniform
+        const GatherTile tile = tiles[t];
+        const BatchSim& S = sims[tile.sim];
+        const Ensemble e = S.e;
+        const float4* W = S.force;
+        float4* pos = S.pos;
+        const IndexParams ip = e.index_params();
+        const int G3 = 1 << (3 * e.lg);
+        const int64_t first = tile.lo + tid;
+        const int64_t mine = tile.hi - first;
+        const int cnt = mine <= 0 ? 0 : (int)((mine + THREADS - 1) / THREADS < PPT ? (mine + THREADS - 1) / THREADS : PPT);
+        float cx[PPT], cy[PPT], cz[PPT], ax[PPT], ay[PPT], az[PPT];
+#pragma unroll
+        for (int j = 0; j < PPT; ++j) {
+            const float4 P = j < cnt ? pos[first + (int64_t)j * THREADS] : make_float4(0.f, 0.f, 0.f, 0.f);
+            cx[j] = __fsub_rn(P.x, ip.half_l);
+            cy[j] = __fsub_rn(P.y, ip.half_l);
+            cz[j] = __fsub_rn(P.z, ip.half_l);
+            ax[j] = ay[j] = az[j] = 0.f;
+        }
+        if (e.lg <= 4) {
+            for (int i = tid; i < e.k * 16; i += THREADS) {
+                const int j = i >> 4, w = i & 15;
+                xf[i] = (w < 12) ? reinterpret_cast<const float*>(e.fast + j)[w] : 0.f;
+            }
+            __syncthreads();
+            if (tid == 0)
+                for (int q = 0; q < nstage && q < e.k; ++q)
+                    issue_grid(q, (int)((issued + q) % nstage), W, stage, full, e.lg, no_box, false,
+                               xf, 0, ip);
+            for (int i = 0; i < e.k; ++i) {
+                const uint32_t c = issued + (uint32_t)i;
+                const int q = (int)(c % nstage);
+                if (!mbar_wait_bounded(full + q, (c / nstage) & 1u)) abort_flag = 1;
+                const float4* F = stage + (size_t)q * G3;
+                const float* x = xf + i * 16;
+#pragma unroll
+                for (int j = 0; j < PPT; ++j) {
+                    if (j < cnt) {
+                        uint32_t cell = cell_of(0, x, cx[j], cy[j], cz[j], ip);
+                        if (!in_bounds(e.flags, cell, (uint64_t)G3)) cell = 0;
+                        const float4 f = F[cell];
+                        ax[j] = __fadd_rn(ax[j], f.x);
+                        ay[j] = __fadd_rn(ay[j], f.y);
+                        az[j] = __fadd_rn(az[j], f.z);
+                    }
+                }
+                __syncthreads();
+                if (abort_flag) {
+                    // let the copies still in flight land (bounded) before the
+                    // CTA's shared memory is released, then report and leave
+                    if (tid == 0) {
+                        atomicOr(e.flags, 4u);
+                        for (int j = i; j < i + nstage && j < e.k; ++j) {
+                            const uint32_t cj = issued + (uint32_t)j;
+                            (void)mbar_wait_bounded(full + cj % nstage, (cj / nstage) & 1u);
+                        }
+                    }
+                    return;
+                }
+                if (tid == 0 && i + nstage < e.k)
+                    issue_grid(i + nstage, q, W, stage, full, e.lg, no_box, false, xf, 0, ip);
+            }
+            issued += (uint32_t)e.k;
+        } else {
+            for (int i = 0; i < e.k; ++i) {
+                const FastXf xr = e.fast[i];
+                const float4* F = W + (size_t)i * G3;
+                uint32_t prev = 0xffffffffu;
+                float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+                for (int j = 0; j < PPT; ++j) {
+                    if (j < cnt) {
+                        uint32_t cell = cell_fast(xr.row[0], xr.row[1], xr.row[2], cx[j], cy[j], cz[j], ip.lg);
+                        if (!in_bounds(e.flags, cell, (uint64_t)G3)) cell = 0;
+                        if (cell != prev) f = __ldg(F + cell);
+                        prev = cell;
+                        ax[j] = __fadd_rn(ax[j], f.x);
+                        ay[j] = __fadd_rn(ay[j], f.y);
+                        az[j] = __fadd_rn(az[j], f.z);
+                    }
+                }
+            }
+        }
+        unsigned bad = 0;
+#pragma unroll
+        for (int j = 0; j < PPT; ++j) {
+            if (j < cnt) {
+                const int64_t p = first + (int64_t)j * THREADS;
+                finish_particle<false>(p, pos[p], ax[j], ay[j], az[j], pos, S.vel, nullptr,
+                                       (float)e.k, S.dt, S.damping, e.world, bad);
+            }
+        }
+        if (bad) raise_flags(e.flags, bad);
+        __syncthreads();  // the next tile reuses xf, the stages and s_tile
+    }
+}
+
 // Direct gather from L1/L2, any g: each thread owns DPPT consecutive slots
 // and reuses a force value when consecutive particles share a cell.
 template <int IDX, int DPPT, bool ACC_OUT>
@@ -477,6 +608,21 @@ __global__ void __launch_bounds__(32) wait_timeout_selftest_kernel(unsigned* fla
 
 cudaError_t launch_wait_timeout_selftest(unsigned* flags, cudaStream_t s) {
     wait_timeout_selftest_kernel<<<1, 32, 0, s>>>(flags);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gather_queue(const BatchSim* sims, const GatherTile* tiles, int ntiles,
+                                unsigned* counter, int kmax, cudaStream_t s) {
+    if (ntiles <= 0) return cudaSuccess;
+    constexpr int nstage = 3;
+    const size_t smem = nstage * ((size_t)16 << 12) + 8 * sizeof(uint64_t) +
+                        (size_t)std::max(kmax, 1) * 16 * sizeof(float);
+    if (smem > 227 * 1024) return cudaErrorInvalidValue;
+    auto kern = gather_queue_kernel<kQueueGatherPPT, kQueueGatherThreads>;
+    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return err;
+    kern<<<std::min(ntiles, num_sms()), kQueueGatherThreads, smem, s>>>(sims, tiles, ntiles, counter,
+                                                                        nstage);
     return cudaGetLastError();
 }
 
