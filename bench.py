@@ -415,14 +415,16 @@ def learned_bytes(n: int, k: int, g: int) -> dict:
     deposit: position read (16 N) + one 4-byte cell update per (particle,
     grid) (4 N k) + mass-grid write (4 k g^3); solve: mass read + force grid
     written (16 k g^3); cell masses: mass read + w lane written (8 k g^3);
-    learned kernel: position and velocity read and written (64 N) + the
-    force grid read once (16 k g^3) (its per-particle gathers are L1/L2
-    hits).
+    learned kernel: position and velocity read and written (64 N) + one
+    16-byte read per (particle, grid) (16 N k: the world-frame force and the
+    cell mass the features need), the same convention as the plain gather's
+    12 bytes of force per (particle, grid).  Whole step:
+    64 N + 20 N k + 28 k g^3 (the deposit's position read inside the 64 N).
     """
     g3 = g ** 3
     return {"deposit": 16 * n + 4 * n * k + 4 * k * g3, "solve": 16 * k * g3,
-            "cell_masses": 8 * k * g3, "learned": 64 * n + 16 * k * g3,
-            "step": 64 * n + 4 * n * k + 44 * k * g3}
+            "cell_masses": 8 * k * g3, "learned": 64 * n + 16 * n * k,
+            "step": 64 * n + 20 * n * k + 28 * k * g3}
 
 
 def learned_model():
@@ -634,8 +636,10 @@ def run_learned(args, w: dict) -> None:
                          "frac": l_ach / peaks["hbm_gbs"], "peak_source": peaks["source"],
                          "algorithmic_bytes": lb[lnames[ldom]],
                          "traffic": profiled_traffic(lnames[ldom], "learned"),
-                         "note": "the fused learned kernel is bound by FP32 instruction issue "
-                                 "(feature statistics over 32 gathered grids), not by HBM"},
+                         "note": "effective bytes: 64 N + 16 N k, one 16-byte (force, cell mass) "
+                                 "read per (particle, grid) served from L1/L2, like the plain "
+                                 "gather's 12 bytes; the kernel is bound by instruction issue "
+                                 "(feature statistics over 32 gathered grids)"},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 2 * 16 * n,
                     "d2h_bytes_per_step": 2 * 16 * n, "ms_per_step": t_e2e / args.steps,
                     "gate": f"variance gate every 10 steps, {ls.fallback_steps} fallback steps, "
@@ -677,13 +681,13 @@ def run_batch(args, w: dict) -> None:
         pos, vel = ics.plummer(n, w["L"], seed=w["seed"] + i + 1000 * rank)
         s.set_particles(pos, vel)
         sims.append(s)
-    if args.autotune:
-        from mog_solver_b200.autotune import autotune
-
-        for s in sims:
-            autotune(s, reps=2, cache=None)
     torch.cuda.synchronize()
     batch = Batch(sims)
+    tuned = None
+    if args.autotune:
+        from mog_solver_b200.autotune import autotune_batch
+
+        tuned = autotune_batch(batch, reps=2, cache=None)
     stream = torch.cuda.Stream(device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     n_tot = sum(s.n_particles for s in sims)
@@ -729,6 +733,7 @@ def run_batch(args, w: dict) -> None:
     total_ms, total_e2e = float(tot[0]), float(tot[1])
     for s in sims:
         s.check()
+    btune = batch.tuning()
     if rank == 0:
         peaks = measured_peaks()
         B = sum(step_bytes(n, k, g) for n, k, g in w["sims"])
@@ -742,14 +747,19 @@ def run_batch(args, w: dict) -> None:
             "config": {"workload": w["desc"], "sims": w["sims"], "particles": n_tot,
                        "parallelism": "single GPU" if world == 1 else f"{world} independent replicas",
                        "l2": "flushed between timed steps (256 MiB write)",
-                       "autotuned": bool(args.autotune)},
+                       "autotuned": bool(args.autotune), "batch_tuning": btune,
+                       **({"autotune_trials": tuned["trials"]} if tuned else {})},
             "roofline": {"bound": "hbm", "kernel": "whole ensemble step", "achieved": achieved,
                          "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
                          "peak_source": peaks["source"], "algorithmic_bytes": B, "traffic": None},
             "e2e": {"value": n_tot * world * args.steps / (total_e2e / 1e3), "unit": UNIT,
                     "h2d_bytes_per_step": 32 * n_tot, "d2h_bytes_per_step": 32 * n_tot,
                     "ms_per_step": total_e2e / args.steps},
-            "gpu_launches": sum(launches_per_step(g) for _, _, g in w["sims"]) * args.steps,
+            # work queue: one deposit and one gather launch for the whole
+            # batch, plus each simulation's solve
+            "gpu_launches": ((2 + sum(launches_per_step(g) - 2 for _, _, g in w["sims"]))
+                             if btune["active_work_queue"] else
+                             sum(launches_per_step(g) for _, _, g in w["sims"])) * args.steps,
             "clocks": clocks.summary(),
         }
         print(json.dumps(line), flush=True)

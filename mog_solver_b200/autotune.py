@@ -70,6 +70,69 @@ def _candidates(sim: Simulation) -> dict[str, list[dict]]:
     return {"deposit": dep, "update": upd, "order": order}
 
 
+def _batch_key(batch) -> str:
+    import torch
+
+    name = torch.cuda.get_device_name(batch.sims[0].device).replace(" ", "_")
+    parts = []
+    for s in batch.sims:
+        c = s.cfg
+        bucket = 1 << max(0, math.ceil(math.log2(max(1, s.n_particles))))
+        parts.append(f"n{bucket}k{c.n_grids}g{c.grid_size}{c.mass_mode}")
+    return "batch|" + name + "|" + ",".join(parts)
+
+
+def autotune_batch(batch, reps: int = 3, cache: Path | None = CACHE, force: bool = False) -> dict:
+    """Pick and apply the fastest launch shapes of a Batch (work queue on or
+    off, particles per deposit tile) by timing whole ensemble steps with
+    CUDA events; the particles every trial advanced are restored."""
+    import torch
+
+    key = _batch_key(batch)
+    table = {}
+    if cache is not None and cache.exists():
+        try:
+            table = json.loads(cache.read_text())
+        except (OSError, json.JSONDecodeError):
+            table = {}
+    if key in table and not force:
+        batch.tune(**table[key]["tuning"])
+        return table[key]
+    saved = [(s.pos.clone(), s.vel.clone()) for s in batch.sims]
+    cands = [dict(work_queue=1, deposit_chunk=c) for c in (32768, 65536, 131072, 262144)]
+    cands.append(dict(work_queue=0, deposit_chunk=0))
+    results = []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    try:
+        for cand in cands:
+            batch.tune(**cand)
+            batch.step(2)  # capture + warm-up
+            torch.cuda.synchronize()
+            e0.record()
+            batch.step(reps)
+            e1.record()
+            e1.synchronize()
+            results.append((e0.elapsed_time(e1) / reps, cand))
+            for s, (p, v) in zip(batch.sims, saved):
+                s.pos.copy_(p)
+                s.vel.copy_(v)
+    finally:
+        for s, (p, v) in zip(batch.sims, saved):
+            s.pos.copy_(p)
+            s.vel.copy_(v)
+    ms, best = min(results, key=lambda r: r[0])
+    batch.tune(**best)
+    entry = {"tuning": best, "step_ms": ms,
+             "trials": [{"tuning": c, "step_ms": t} for t, c in results]}
+    if cache is not None:
+        table[key] = entry
+        try:
+            cache.write_text(json.dumps(table, indent=1, sort_keys=True))
+        except OSError:
+            pass
+    return entry
+
+
 def autotune(sim: Simulation, reps: int = 4, cache: Path | None = CACHE, force: bool = False) -> dict:
     """Pick and apply the fastest launch shapes for sim's current particles."""
     key = _key(sim)
