@@ -775,6 +775,7 @@ int mog_get_tuning(const mog_handle* h, mog_tuning* out) {
     out->update_direct_ppt = h->ushape.direct_ppt;
     out->deposit_split = h->dshape.split;
     out->learned_fold = h->learned_fold;
+    out->deposit_dedup = h->dshape.dedup;
     return MOG_OK;
 }
 
@@ -792,7 +793,7 @@ int mog_set_tuning(mog_handle* h, const mog_tuning* t) {
         (t->update_direct_ppt != 0 && t->update_direct_ppt != 1 && t->update_direct_ppt != 2 &&
          t->update_direct_ppt != 4) ||
         t->deposit_split < -1 || t->deposit_split > 1 || t->learned_fold < 0 ||
-        t->learned_fold > 1)
+        t->learned_fold > 1 || t->deposit_dedup < 0 || t->deposit_dedup > 1)
         return fail(MOG_ERR_ARG, "tuning value out of range");
     h->dshape.threads = t->deposit_threads ? t->deposit_threads : 1024;
     h->dshape.grids_per_cta = t->deposit_grids_per_cta;
@@ -808,6 +809,7 @@ int mog_set_tuning(mog_handle* h, const mog_tuning* t) {
     h->ushape.threads = t->update_threads ? t->update_threads : 512;
     h->dshape.split = t->deposit_split;
     h->learned_fold = t->learned_fold;
+    h->dshape.dedup = t->deposit_dedup;
     for (auto& g : h->graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);
     h->graphs.clear();
