@@ -420,6 +420,30 @@ int mog_learned_step_profiled(mog_handle* h, const mog_model* m, float* pos4, fl
 int mog_learned_spread(mog_handle* h, double* out2, void* stream);
 
 /*
+ * mog_step / mog_learned_step over particles held in HOST memory, for a
+ * caller whose particle state lives on the host between steps (the
+ * reference's Simulation.step with its buffers read back every frame,
+ * main.py:592-676).  pos4_host / vel4_host: n float4 records in host
+ * memory, page-locked (cudaHostAlloc / cudaHostRegister) for the copies to
+ * run asynchronously; pageable memory works but serialises them.  The
+ * particles travel in `chunks` pieces (1..64; 4 to 8 overlap best): each
+ * chunk's positions are deposited as soon as they land, and after the
+ * solve each chunk is updated (the learned kernel; the plain gather runs
+ * as one launch) and copied back while later chunks still compute, so the
+ * copies in both directions overlap the kernels.  The handle keeps device
+ * copies of the records (2 n float4, allocated on the first call and when
+ * n grows) and two copy streams.  Everything is queued on `stream`; the
+ * host buffers hold the stepped particles once `stream` reaches the end of
+ * the call (synchronise it before reading them).  The result is bit-identical
+ * to copying the records to the device, stepping there and copying back.
+ * The variance-gate statistics of mog_learned_spread cover the whole step.
+ */
+int mog_step_host(mog_handle* h, float* pos4_host, float* vel4_host, int64_t n, float dt_eff,
+                  int32_t chunks, void* stream);
+int mog_learned_step_host(mog_handle* h, const mog_model* m, float* pos4_host, float* vel4_host,
+                          int64_t n, float dt_eff, int32_t chunks, void* stream);
+
+/*
  * The Green's factor table the spectral solve multiplies by, g^3 floats in
  * [kz][ky][kx] order, written to host memory `out`: -2 pi G / k^2
  * (softening 0) or -4 pi G exp(-k^2 a^2) / k^2 with a = softening * L / g,

@@ -56,7 +56,7 @@ EXPORTS = (
     "mog_batch_get_tuning",
     "mog_model_create", "mog_model_destroy", "mog_model_set", "mog_model_get",
     "mog_model_train_step", "mog_features", "mog_learned_forces", "mog_learned_step",
-    "mog_learned_step_profiled", "mog_learned_spread",
+    "mog_learned_step_profiled", "mog_learned_spread", "mog_step_host", "mog_learned_step_host",
     "mog_render_params_default", "mog_renderer_create", "mog_renderer_destroy", "mog_render",
     "mog_renderer_stats", "mog_render_host",
     "mog_strerror", "mog_last_error", "mog_version",
@@ -202,6 +202,8 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.mog_learned_step.argtypes = [P, P, P, P, I64, F, P]
     lib.mog_learned_step_profiled.argtypes = [P, P, P, P, I64, F, ctypes.POINTER(ctypes.c_float), P]
     lib.mog_learned_spread.argtypes = [P, ctypes.POINTER(ctypes.c_double), P]
+    lib.mog_step_host.argtypes = [P, P, P, I64, F, ctypes.c_int32, P]
+    lib.mog_learned_step_host.argtypes = [P, P, P, P, I64, F, ctypes.c_int32, P]
     RP = ctypes.POINTER(RenderParamsC)
     lib.mog_render_params_default.argtypes = [RP]
     lib.mog_render_params_default.restype = None

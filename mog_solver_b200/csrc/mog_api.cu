@@ -198,6 +198,17 @@ struct mog_handle {
     int spread_blocks = 0;
     int64_t spread_n = 0;
     ShardState shard;
+    // steps over host-memory particles (mog_step_host, mog_learned_step_host):
+    // device copies of the records, a copy-in and a copy-out stream, and the
+    // events that order each chunk's copies against its kernels
+    float4* d_hpos = nullptr;
+    float4* d_hvel = nullptr;
+    int64_t host_cap = 0;
+    cudaStream_t s_in = nullptr;
+    cudaStream_t s_out = nullptr;
+    cudaEvent_t ev_start = nullptr;
+    cudaEvent_t ev_out = nullptr;
+    std::vector<cudaEvent_t> ev_pos, ev_vel, ev_done;
 };
 
 namespace {
@@ -401,9 +412,17 @@ void release(mog_handle* h) {
     h->graphs.clear();
     void* ptrs[] = {h->d_rot12, h->d_off4, h->d_fast, h->d_green, h->d_ktab, h->d_conv,
                     h->d_flags, h->d_total, h->d_mass, h->d_force, h->d_force2, h->d_scratch,
-                    h->d_diag, h->d_perm, h->d_sort, h->d_pos_s, h->d_spread, h->d_dft};
+                    h->d_diag, h->d_perm, h->d_sort, h->d_pos_s, h->d_spread, h->d_dft,
+                    h->d_hpos, h->d_hvel};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    for (auto* evs : {&h->ev_pos, &h->ev_vel, &h->ev_done})
+        for (cudaEvent_t x : *evs)
+            if (x) cudaEventDestroy(x);
+    if (h->ev_start) cudaEventDestroy(h->ev_start);
+    if (h->ev_out) cudaEventDestroy(h->ev_out);
+    if (h->s_in) cudaStreamDestroy(h->s_in);
+    if (h->s_out) cudaStreamDestroy(h->s_out);
 }
 
 }  // namespace
@@ -518,7 +537,9 @@ int mog_create(const mog_config* cfg, const float* rot12, const float* off4, mog
         h->perm_cap = cfg->num_particles;
     }
     ALLOC(h->d_sort, mog::sort_scratch_bytes());
-    h->spread_cap = mog::num_sms() * 8;
+    // room for the CTAs of a whole learned step even when the host-buffer
+    // step launches its kernel once per chunk
+    h->spread_cap = mog::num_sms() * 32;
     ALLOC(h->d_spread, sizeof(float) * 2 * h->spread_cap);
 #undef ALLOC
     cudaError_t err;
@@ -1163,6 +1184,132 @@ static int run_learned(mog_handle* h, const mog_model* m, int out_mode, float* p
     return MOG_OK;
 }
 
+// Device copies, streams and per-chunk events of the host-buffer steps.
+static int ensure_host_step(mog_handle* h, int64_t n, int chunks) {
+    if (n > h->host_cap) {
+        if (h->d_hpos) cudaFree(h->d_hpos);
+        if (h->d_hvel) cudaFree(h->d_hvel);
+        h->d_hpos = h->d_hvel = nullptr;
+        h->host_cap = 0;
+        MOG_CUDA(cudaMalloc((void**)&h->d_hpos, sizeof(float4) * n), "host step buffers");
+        MOG_CUDA(cudaMalloc((void**)&h->d_hvel, sizeof(float4) * n), "host step buffers");
+        h->host_cap = n;
+    }
+    if (!h->s_in) {
+        MOG_CUDA(cudaStreamCreateWithFlags(&h->s_in, cudaStreamNonBlocking), "copy stream");
+        MOG_CUDA(cudaStreamCreateWithFlags(&h->s_out, cudaStreamNonBlocking), "copy stream");
+        MOG_CUDA(cudaEventCreateWithFlags(&h->ev_start, cudaEventDisableTiming), "event");
+        MOG_CUDA(cudaEventCreateWithFlags(&h->ev_out, cudaEventDisableTiming), "event");
+    }
+    while ((int)h->ev_done.size() < chunks) {
+        cudaEvent_t a, b, c;
+        MOG_CUDA(cudaEventCreateWithFlags(&a, cudaEventDisableTiming), "event");
+        MOG_CUDA(cudaEventCreateWithFlags(&b, cudaEventDisableTiming), "event");
+        MOG_CUDA(cudaEventCreateWithFlags(&c, cudaEventDisableTiming), "event");
+        h->ev_pos.push_back(a);
+        h->ev_vel.push_back(b);
+        h->ev_done.push_back(c);
+    }
+    return MOG_OK;
+}
+
+// One step over host-memory particles, in `chunks` pieces of whole 256-
+// particle blocks.  Copy-in stream: every position chunk, then every
+// velocity chunk.  Caller's stream: each chunk's deposit as soon as its
+// positions have landed; the solve; then each chunk's update (the learned
+// kernel, or the gather + leapfrog), each as soon as its velocities have
+// landed.  Copy-out stream: each chunk's records as soon as its update is
+// done.  The caller's stream finally waits for the last copy out.  The
+// plain update stages every grid once per launch, so it runs as one launch
+// (its copies out still go chunk by chunk).  Integer deposits and
+// per-particle updates make the result bit-identical to the device step.
+static int run_host_step(mog_handle* h, const mog_model* m, float* pos_host, float* vel_host,
+                         int64_t n, float dt, int chunks, cudaStream_t s) {
+    const mog::Ensemble& e = h->e;
+    int64_t per = (n + chunks - 1) / chunks;
+    per = std::max<int64_t>(256, (per + 255) / 256 * 256);
+    chunks = (int)((n + per - 1) / per);
+    int rc = ensure_host_step(h, n, chunks);
+    if (rc) return rc;
+    auto lo_of = [&](int c) { return (int64_t)c * per; };
+    auto n_of = [&](int c) { return std::min<int64_t>(n, lo_of(c) + per) - lo_of(c); };
+    const float4* hp = reinterpret_cast<const float4*>(pos_host);
+    const float4* hv = reinterpret_cast<const float4*>(vel_host);
+    MOG_CUDA(cudaEventRecord(h->ev_start, s), "event");
+    MOG_CUDA(cudaStreamWaitEvent(h->s_in, h->ev_start, 0), "wait");
+    for (int c = 0; c < chunks; ++c) {
+        MOG_CUDA(cudaMemcpyAsync(h->d_hpos + lo_of(c), hp + lo_of(c), sizeof(float4) * n_of(c),
+                                 cudaMemcpyHostToDevice, h->s_in), "positions in");
+        MOG_CUDA(cudaEventRecord(h->ev_pos[c], h->s_in), "event");
+    }
+    for (int c = 0; c < chunks; ++c) {
+        MOG_CUDA(cudaMemcpyAsync(h->d_hvel + lo_of(c), hv + lo_of(c), sizeof(float4) * n_of(c),
+                                 cudaMemcpyHostToDevice, h->s_in), "velocities in");
+        MOG_CUDA(cudaEventRecord(h->ev_vel[c], h->s_in), "event");
+    }
+    cudaError_t err = cudaSuccess;
+    for (int c = 0; c < chunks && !err; ++c) {
+        err = cudaStreamWaitEvent(s, h->ev_pos[c], 0);
+        if (!err)
+            err = mog::launch_deposit(e, h->d_hpos + lo_of(c), nullptr, n_of(c), false, h->d_mass,
+                                      h->dshape, s);
+    }
+    if (err) return cuda_fail(err, "deposit");
+    if (m) {
+        if (h->cfg.solver == MOG_SOLVER_FFT && h->learned_fold) {
+            err = mog::launch_spectral_density(e, h->d_mass, h->d_force, h->d_scratch, s);
+        } else {
+            err = h->cfg.solver == MOG_SOLVER_FFT
+                      ? mog::launch_spectral(e, h->d_mass, h->d_force, true, false, h->d_scratch, s)
+                      : mog::launch_convolution(e, h->d_mass, h->d_force, true, false, s);
+            if (!err) err = mog::launch_density_w(e, h->d_mass, h->d_force, s);
+        }
+    } else {
+        err = h->cfg.solver == MOG_SOLVER_FFT
+                  ? mog::launch_spectral(e, h->d_mass, h->d_force, true, true, h->d_scratch, s)
+                  : mog::launch_convolution(e, h->d_mass, h->d_force, true, true, s);
+    }
+    if (err) return cuda_fail(err, "solve");
+    int used = 0;  // spread partial sums written so far (one per learned CTA)
+    const int upd_chunks = m ? chunks : 1;
+    for (int c = 0; c < chunks && !err; ++c) {
+        if (c < upd_chunks) {
+            const int last = m ? c : chunks - 1;  // velocities this launch needs
+            for (int v = m ? c : 0; v <= last && !err; ++v) err = cudaStreamWaitEvent(s, h->ev_vel[v], 0);
+            const int64_t lo = m ? lo_of(c) : 0, cnt = m ? n_of(c) : n;
+            if (!err && m) {
+                mog::LearnedOut out;
+                out.spread = h->d_spread + 2 * used;
+                out.spread_cap = h->spread_cap - used;
+                err = mog::launch_learned(0, e, h->rows.data(), h->d_hpos + lo, h->d_hvel + lo, cnt,
+                                          h->d_force, m->norm, m->d_frags, m->d_params, dt,
+                                          h->cfg.damping, out, s);
+                used += out.blocks;
+            } else if (!err) {
+                err = mog::launch_update(e, h->d_hpos, h->d_hvel, nullptr, nullptr, n, h->d_force, dt,
+                                         h->cfg.damping, nullptr, h->ushape, s);
+            }
+            if (!err) err = cudaEventRecord(h->ev_done[c], s);
+        }
+        const int done_ev = std::min(c, upd_chunks - 1);
+        if (!err) err = cudaStreamWaitEvent(h->s_out, h->ev_done[done_ev], 0);
+        if (!err)
+            err = cudaMemcpyAsync(pos_host + 4 * lo_of(c), h->d_hpos + lo_of(c),
+                                  sizeof(float4) * n_of(c), cudaMemcpyDeviceToHost, h->s_out);
+        if (!err)
+            err = cudaMemcpyAsync(vel_host + 4 * lo_of(c), h->d_hvel + lo_of(c),
+                                  sizeof(float4) * n_of(c), cudaMemcpyDeviceToHost, h->s_out);
+    }
+    if (err) return cuda_fail(err, "host step");
+    MOG_CUDA(cudaEventRecord(h->ev_out, h->s_out), "event");
+    MOG_CUDA(cudaStreamWaitEvent(s, h->ev_out, 0), "wait");
+    if (m) {
+        h->spread_blocks = used;
+        h->spread_n = n;
+    }
+    return MOG_OK;
+}
+
 extern "C" {
 
 int mog_model_create(mog_model** out) {
@@ -1337,6 +1484,39 @@ int mog_learned_spread(mog_handle* h, double* out2, void* stream) {
     }
     out2[0] = a / (double)h->spread_n;
     out2[1] = b / (double)h->spread_n;
+    return MOG_OK;
+}
+
+static int host_step_args(mog_handle* h, float* pos4_host, float* vel4_host, int64_t n,
+                          float dt_eff, int32_t chunks) {
+    int rc = check_particles(h, pos4_host, vel4_host, n, true);
+    if (rc) return rc;
+    if (!std::isfinite(dt_eff)) return fail(MOG_ERR_ARG, "dt_eff must be finite");
+    if (chunks < 1 || chunks > 64) return fail(MOG_ERR_ARG, "chunks must be in [1, 64]");
+    return set_device(h);
+}
+
+int mog_step_host(mog_handle* h, float* pos4_host, float* vel4_host, int64_t n, float dt_eff,
+                  int32_t chunks, void* stream) {
+    if (!h) return fail(MOG_ERR_ARG, "handle is null");
+    int rc = host_step_args(h, pos4_host, vel4_host, n, dt_eff, chunks);
+    if (rc || n == 0) return rc;
+    if ((rc = run_host_step(h, nullptr, pos4_host, vel4_host, n, dt_eff, chunks,
+                            static_cast<cudaStream_t>(stream))))
+        return rc;
+    ++h->step_count;
+    return MOG_OK;
+}
+
+int mog_learned_step_host(mog_handle* h, const mog_model* m, float* pos4_host, float* vel4_host,
+                          int64_t n, float dt_eff, int32_t chunks, void* stream) {
+    if (!h || !m) return fail(MOG_ERR_ARG, "null argument");
+    int rc = host_step_args(h, pos4_host, vel4_host, n, dt_eff, chunks);
+    if (rc || n == 0) return rc;
+    if ((rc = run_host_step(h, m, pos4_host, vel4_host, n, dt_eff, chunks,
+                            static_cast<cudaStream_t>(stream))))
+        return rc;
+    ++h->step_count;
     return MOG_OK;
 }
 

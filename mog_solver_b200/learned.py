@@ -324,6 +324,42 @@ class LearnedSimulation:
                                                     c._stream()), "mog_learned_step")
             self.steps += 1
 
+    def step_host(self, pos_host, vel_host, n_steps: int = 1, chunks: int = 8) -> None:
+        """``step`` for particles held in host memory ((N, 4) float32 CPU
+        tensors, page-locked): each step copies the records in, steps them
+        and copies them back in overlapped chunks (mog_learned_step_host,
+        or mog_step_host on the fallback ensemble when the gate has fired).
+        The gate reads the last learned step's own statistics; after
+        fallback steps a feature pass over the current records decides.
+        Returns once the stepped records are in the host buffers."""
+        from .simulation import _check_host_records
+
+        torch = _torch()
+        _check_host_records(pos_host, vel_host)
+        lib = _lib.lib()
+        n = int(pos_host.shape[0])
+        c = self.cheap
+        for _ in range(n_steps):
+            if self.gate_every and self.steps % self.gate_every == 0 and self.steps > 0:
+                if self._use_fallback:
+                    c.pos.copy_(pos_host)
+                self._use_fallback = self.gate_fires()
+            with torch_device(c.device):
+                stream = c._stream()
+                if self._use_fallback:
+                    fb = self.fallback
+                    _lib.check(lib.mog_step_host(fb.handle, pos_host.data_ptr(), vel_host.data_ptr(),
+                                                 n, float(fb.cfg.dt * fb.timescale), int(chunks),
+                                                 stream), "mog_step_host")
+                    self.fallback_steps += 1
+                else:
+                    _lib.check(lib.mog_learned_step_host(c.handle, self.model.handle,
+                                                         pos_host.data_ptr(), vel_host.data_ptr(), n,
+                                                         float(c.cfg.dt * c.timescale), int(chunks),
+                                                         stream), "mog_learned_step_host")
+            self.steps += 1
+        torch.cuda.current_stream(c.device).synchronize()
+
 
 def rms_error(F, D) -> float:
     """Relative RMS error ||F - D|| / ||D|| over the target particles."""

@@ -43,6 +43,17 @@ def _torch():
     return torch
 
 
+def _check_host_records(pos_host, vel_host) -> None:
+    """Host-step buffers: (N, 4) contiguous float32 CPU tensors of one shape."""
+    torch = _torch()
+    for t in (pos_host, vel_host):
+        if not torch.is_tensor(t) or t.is_cuda or t.dtype != torch.float32 or t.dim() != 2 \
+                or t.shape[1] != 4 or not t.is_contiguous():
+            raise ValueError("host records must be contiguous (N, 4) float32 CPU tensors")
+    if pos_host.shape != vel_host.shape:
+        raise ValueError("pos and vel must have the same shape")
+
+
 def auto_scale_bits(total_mass: float) -> int:
     """u64 fixed-point scale 2^bits with bits = 52 - ceil(log2(total mass)).
 
@@ -276,6 +287,24 @@ class Simulation:
                 _lib.check(lib.mog_step_n(h, self.pos.data_ptr(), self.vel.data_ptr(),
                                           self.n_particles, dt_eff, int(n_steps), self._stream()),
                            "mog_step_n")
+        self.steps_taken += n_steps
+
+    def step_host(self, pos_host, vel_host, n_steps: int = 1, chunks: int = 8) -> None:
+        """Advance particles held in host memory (mog_step_host): (N, 4)
+        float32 CPU tensors, page-locked for the copies to overlap the
+        kernels.  The call returns once the stepped records are back in
+        the host buffers.  ``self.pos`` / ``self.vel`` are not touched."""
+        torch = _torch()
+        _check_host_records(pos_host, vel_host)
+        dt_eff = float(self.cfg.dt * self.timescale)
+        n = int(pos_host.shape[0])
+        lib = _lib.lib()
+        with torch_device(self.device):
+            stream = self._stream()
+            for _ in range(n_steps):
+                _lib.check(lib.mog_step_host(self.handle, pos_host.data_ptr(), vel_host.data_ptr(), n,
+                                             dt_eff, int(chunks), stream), "mog_step_host")
+            torch.cuda.current_stream(self.device).synchronize()
         self.steps_taken += n_steps
 
     def render(self, width: int = 2560, height: int = 1440, **kw):
