@@ -333,11 +333,9 @@ def run_ours(args, w: dict) -> None:
         for _ in range(args.steps):
             flush.zero_()
             e0.record(stream)
-            sim.pos.copy_(host_pos, non_blocking=True)
-            sim.vel.copy_(host_vel, non_blocking=True)
-            sim.step()
-            host_pos.copy_(sim.pos, non_blocking=True)
-            host_vel.copy_(sim.vel, non_blocking=True)
+            # copies in and out inside the call, overlapped with the deposit
+            # and the copy-out of finished chunks (mog_step_host)
+            sim.step_host(host_pos, host_vel, chunks=8)
             e1.record(stream)
             e1.synchronize()
             e2e_ms.append(e0.elapsed_time(e1))
@@ -568,11 +566,9 @@ def run_learned(args, w: dict) -> None:
         for _ in range(args.steps):
             flush.zero_()
             ev0.record(stream)
-            cheap.pos.copy_(host_pos, non_blocking=True)
-            cheap.vel.copy_(host_vel, non_blocking=True)
-            ls.step()
-            host_pos.copy_(cheap.pos, non_blocking=True)
-            host_vel.copy_(cheap.vel, non_blocking=True)
+            # the records travel host -> device -> host inside the call, in
+            # chunks overlapped with the kernels (mog_learned_step_host)
+            ls.step_host(host_pos, host_vel, chunks=8)
             ev1.record(stream)
             ev1.synchronize()
             e2e_ms.append(ev0.elapsed_time(ev1))
@@ -642,6 +638,8 @@ def run_learned(args, w: dict) -> None:
                                  "(feature statistics over 32 gathered grids)"},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 2 * 16 * n,
                     "d2h_bytes_per_step": 2 * 16 * n, "ms_per_step": t_e2e / args.steps,
+                    "api": "LearnedSimulation.step_host (mog_learned_step_host, 8 chunks, "
+                           "pinned host buffers)",
                     "gate": f"variance gate every 10 steps, {ls.fallback_steps} fallback steps, "
                             f"last relative spread {ls.last_ratio} vs training {ls.train_ratio}"},
             "gpu_launches": (3 if tuning.get("learned_fold") and w["g"] in (8, 16) else 4) * args.steps,
