@@ -146,9 +146,11 @@ __device__ __forceinline__ GridRows make_grid_rows_dev(const Ensemble& e, int i)
     const FastXf x = e.fast[i];
     const float* R = e.rot12 + 12 * i;
     GridRows g;
-    g.r[0] = x.row[0];
-    g.r[1] = x.row[1];
-    g.r[2] = x.row[2];
+    g.t01[0] = make_float2(x.row[0].x, x.row[1].x);
+    g.t01[1] = make_float2(x.row[0].y, x.row[1].y);
+    g.t01[2] = make_float2(x.row[0].z, x.row[1].z);
+    g.t01[3] = make_float2(x.row[0].w, x.row[1].w);
+    g.t2 = x.row[2];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
 #pragma unroll
@@ -158,76 +160,97 @@ __device__ __forceinline__ GridRows make_grid_rows_dev(const Ensemble& e, int i)
     return g;
 }
 
-// Running sums of one particle over the grids.
+// Running sums of one particle over the grids.  Pairs of sums that take
+// pairwise operands are float2, updated by one paired FP32 instruction
+// (add/fma .f32x2: two IEEE operations, each rounded as the scalar one).
 struct GatherAcc {
-    float sx = 0.f, sy = 0.f, sz = 0.f;  // plain sum, update.glsl order
-    float qx = 0.f, qy = 0.f, qz = 0.f;  // sum F^2 per component
-    float dx = 0.f, dy = 0.f, dz = 0.f;  // sum d
-    float dxx = 0.f, dxy = 0.f, dxz = 0.f, dyy = 0.f, dyz = 0.f, dzz = 0.f;
-    float fxdx = 0.f, fxdy = 0.f, fxdz = 0.f, fydx = 0.f, fydy = 0.f, fydz = 0.f,
-          fzdx = 0.f, fzdy = 0.f, fzdz = 0.f;  // sum F d^T
-    float rho = 0.f;
+    float2 s01 = make_float2(0.f, 0.f);   // plain sum (x, y), update.glsl order
+    float sz = 0.f;
+    float2 q01 = make_float2(0.f, 0.f);   // sum F^2 (x, y)
+    float qz = 0.f;
+    float2 d01 = make_float2(0.f, 0.f);   // sum d (x, y)
+    float dz = 0.f;
+    float2 dd01 = make_float2(0.f, 0.f);  // sum (dx dx, dy dy)
+    float dzz = 0.f, dxy = 0.f;
+    float2 dz01 = make_float2(0.f, 0.f);  // sum (dx dz, dy dz)
+    float2 fd_a = make_float2(0.f, 0.f);  // sum (Fx dx, Fy dy)
+    float2 fd_b = make_float2(0.f, 0.f);  // sum (Fx dy, Fy dx)
+    float2 fd_c = make_float2(0.f, 0.f);  // sum (Fx dz, Fy dz)
+    float2 fd_d = make_float2(0.f, 0.f);  // sum (Fz dx, Fz dy)
+    float fzdz = 0.f, rho = 0.f;
 };
 
 // Grid i's contribution.  IDX 0: FAST cells (LG = log2 g, or 0 for a
-// run-time g); IDX 1: EXACT cells.  In FAST mode the floor that picks the
-// cell also gives the offset: r = t + 1.5*2^23 rounded down holds floor(t)
-// in its low bits (the cell, as floor_mod_pow2) and r - 1.5*2^23 = floor(t)
-// exactly, for |t| < 2^22.
+// run-time g); IDX 1: EXACT cells.  cc: the centred position's components
+// each duplicated into a pair.  tx and ty come from paired FMAs in the
+// order cell_fast uses, so the cell is the deposit's.  In FAST mode the
+// floor that picks the cell also gives the offset: r = t + 1.5*2^23
+// rounded down holds floor(t) in its low bits (the cell, as
+// floor_mod_pow2) and r - 1.5*2^23 = floor(t) exactly, for |t| < 2^22.
 template <int IDX, int LG>
 __device__ __forceinline__ void gather_one(const GridRows& x, int i, const float4* __restrict__ W,
                                            const Ensemble& e, const IndexParams& ip, float cx,
-                                           float cy, float cz, GatherAcc& a) {
+                                           float cy, float cz, const float2 (&cc)[3],
+                                           GatherAcc& a) {
     const int lg = LG > 0 ? LG : e.lg;
     const int G3 = 1 << (3 * lg);
     const uint32_t mask = (1u << lg) - 1u;
     constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23
-    const float tx = __fmaf_rn(x.r[0].z, cz, __fmaf_rn(x.r[0].y, cy, __fmaf_rn(x.r[0].x, cx, x.r[0].w)));
-    const float ty = __fmaf_rn(x.r[1].z, cz, __fmaf_rn(x.r[1].y, cy, __fmaf_rn(x.r[1].x, cx, x.r[1].w)));
-    const float tz = __fmaf_rn(x.r[2].z, cz, __fmaf_rn(x.r[2].y, cy, __fmaf_rn(x.r[2].x, cx, x.r[2].w)));
+    const float2 txy = __ffma2_rn(x.t01[2], cc[2], __ffma2_rn(x.t01[1], cc[1],
+                                                              __ffma2_rn(x.t01[0], cc[0], x.t01[3])));
+    const float tz = __fmaf_rn(x.t2.z, cz, __fmaf_rn(x.t2.y, cy, __fmaf_rn(x.t2.x, cx, x.t2.w)));
     uint32_t c;
-    float gx, gy, gz;  // frac(t)
+    float2 gxy;  // frac(t) for x, y
+    float gz;
     if (IDX == 0) {
-        const float rx = __fadd_rd(tx, kMagic), ry = __fadd_rd(ty, kMagic), rz = __fadd_rd(tz, kMagic);
-        c = (__float_as_uint(rx) & mask) | ((__float_as_uint(ry) & mask) << lg) |
+        const float2 rxy = __fadd2_rd(txy, make_float2(kMagic, kMagic));
+        const float rz = __fadd_rd(tz, kMagic);
+        c = (__float_as_uint(rxy.x) & mask) | ((__float_as_uint(rxy.y) & mask) << lg) |
             ((__float_as_uint(rz) & mask) << (2 * lg));
-        gx = tx - (rx - kMagic);
-        gy = ty - (ry - kMagic);
+        // t - (r - 1.5*2^23): the inner difference is exact, the outer one a
+        // single rounding, as t - floor(t)
+        gxy = __ffma2_rn(__fadd2_rn(rxy, make_float2(-kMagic, -kMagic)), make_float2(-1.f, -1.f), txy);
         gz = tz - (rz - kMagic);
     } else {
         c = cell_exact(e.rot12 + 12 * i, e.off4 + 4 * i, cx, cy, cz, ip);
-        gx = tx - floorf(tx);
-        gy = ty - floorf(ty);
+        gxy = make_float2(txy.x - floorf(txy.x), txy.y - floorf(txy.y));
         gz = tz - floorf(tz);
     }
     if (!in_bounds(e.flags, c, (uint64_t)G3)) c = 0;
     const float4 f = __ldg(W + (size_t)i * G3 + c);
-    a.sx = __fadd_rn(a.sx, f.x);
-    a.sy = __fadd_rn(a.sy, f.y);
+    const float2 f01 = make_float2(f.x, f.y);
+    a.s01 = __fadd2_rn(a.s01, f01);
     a.sz = __fadd_rn(a.sz, f.z);
-    a.qx += f.x * f.x;
-    a.qy += f.y * f.y;
-    a.qz += f.z * f.z;
-    const float wx = x.m[0] * gx + x.m[1] * gy + x.m[2] * gz + x.o[0];
-    const float wy = x.m[3] * gx + x.m[4] * gy + x.m[5] * gz + x.o[1];
-    const float wz = x.m[6] * gx + x.m[7] * gy + x.m[8] * gz + x.o[2];
-    a.dx += wx; a.dy += wy; a.dz += wz;
-    a.dxx += wx * wx; a.dxy += wx * wy; a.dxz += wx * wz;
-    a.dyy += wy * wy; a.dyz += wy * wz; a.dzz += wz * wz;
-    a.fxdx += f.x * wx; a.fxdy += f.x * wy; a.fxdz += f.x * wz;
-    a.fydx += f.y * wx; a.fydy += f.y * wy; a.fydz += f.y * wz;
-    a.fzdx += f.z * wx; a.fzdy += f.z * wy; a.fzdz += f.z * wz;
-    a.rho += f.w;
+    a.q01 = __ffma2_rn(f01, f01, a.q01);
+    a.qz = __fmaf_rn(f.z, f.z, a.qz);
+    // world-frame offset from the cell centre: (h M) frac(t) + o
+    const float wx = __fmaf_rn(x.m[2], gz, __fmaf_rn(x.m[1], gxy.y, __fmaf_rn(x.m[0], gxy.x, x.o[0])));
+    const float wy = __fmaf_rn(x.m[5], gz, __fmaf_rn(x.m[4], gxy.y, __fmaf_rn(x.m[3], gxy.x, x.o[1])));
+    const float wz = __fmaf_rn(x.m[8], gz, __fmaf_rn(x.m[7], gxy.y, __fmaf_rn(x.m[6], gxy.x, x.o[2])));
+    const float2 w01 = make_float2(wx, wy), wzz = make_float2(wz, wz);
+    a.d01 = __fadd2_rn(a.d01, w01);
+    a.dz = __fadd_rn(a.dz, wz);
+    a.dd01 = __ffma2_rn(w01, w01, a.dd01);
+    a.dzz = __fmaf_rn(wz, wz, a.dzz);
+    a.dxy = __fmaf_rn(wx, wy, a.dxy);
+    a.dz01 = __ffma2_rn(w01, wzz, a.dz01);
+    a.fd_a = __ffma2_rn(f01, w01, a.fd_a);
+    a.fd_b = __ffma2_rn(f01, make_float2(wy, wx), a.fd_b);
+    a.fd_c = __ffma2_rn(f01, wzz, a.fd_c);
+    a.fd_d = __ffma2_rn(make_float2(f.z, f.z), w01, a.fd_d);
+    a.fzdz = __fmaf_rn(f.z, wz, a.fzdz);
+    a.rho = __fadd_rn(a.rho, f.w);
 }
 
 // Features from the sums over k grids of voxel size h.
 __device__ __forceinline__ void finish_features(const GatherAcc& a, int k, float h, float inv_fs,
                                                 float rho_ref, Features& out) {
-    const float sx = a.sx, sy = a.sy, sz = a.sz, qx = a.qx, qy = a.qy, qz = a.qz;
-    const float dx = a.dx, dy = a.dy, dz = a.dz, dxx = a.dxx, dxy = a.dxy, dxz = a.dxz,
-                dyy = a.dyy, dyz = a.dyz, dzz = a.dzz;
-    const float fxdx = a.fxdx, fxdy = a.fxdy, fxdz = a.fxdz, fydx = a.fydx, fydy = a.fydy,
-                fydz = a.fydz, fzdx = a.fzdx, fzdy = a.fzdy, fzdz = a.fzdz, rho = a.rho;
+    const float sx = a.s01.x, sy = a.s01.y, sz = a.sz, qx = a.q01.x, qy = a.q01.y, qz = a.qz;
+    const float dx = a.d01.x, dy = a.d01.y, dz = a.dz, dxx = a.dd01.x, dxy = a.dxy,
+                dxz = a.dz01.x, dyy = a.dd01.y, dyz = a.dz01.y, dzz = a.dzz;
+    const float fxdx = a.fd_a.x, fxdy = a.fd_b.x, fxdz = a.fd_c.x, fydx = a.fd_b.y,
+                fydy = a.fd_a.y, fydz = a.fd_c.y, fzdx = a.fd_d.x, fzdy = a.fd_d.y, fzdz = a.fzdz,
+                rho = a.rho;
     const float kf = (float)k, ik = 1.0f / kf;
     const float mx = __fdiv_rn(sx, kf), my = __fdiv_rn(sy, kf), mz = __fdiv_rn(sz, kf);
     const float ax_ = dx * ik, ay_ = dy * ik, az_ = dz * ik;  // dbar
@@ -382,12 +405,13 @@ __global__ void __launch_bounds__(kLT, 2) learned_kernel(
         const float cx = __fsub_rn(P.x, ip.half_l), cy = __fsub_rn(P.y, ip.half_l),
                     cz = __fsub_rn(P.z, ip.half_l);
         GatherAcc acc;
+        const float2 cc[3] = {make_float2(cx, cx), make_float2(cy, cy), make_float2(cz, cz)};
         if constexpr (K > 0) {
 #pragma unroll
-            for (int i = 0; i < K; ++i) gather_one<IDX, LG>(tab.r[i], i, W, e, ip, cx, cy, cz, acc);
+            for (int i = 0; i < K; ++i) gather_one<IDX, LG>(tab.r[i], i, W, e, ip, cx, cy, cz, cc, acc);
         } else {
 #pragma unroll 4
-            for (int i = 0; i < e.k; ++i) gather_one<IDX, LG>(xf[i], i, W, e, ip, cx, cy, cz, acc);
+            for (int i = 0; i < e.k; ++i) gather_one<IDX, LG>(xf[i], i, W, e, ip, cx, cy, cz, cc, acc);
         }
         Features F;
         finish_features(acc, e.k, e.voxel, inv_fs, norm.rho_ref, F);
@@ -645,9 +669,11 @@ cudaError_t launch_density_w(const Ensemble& e, void* mass, float4* W, cudaStrea
 
 GridRows make_grid_rows(const FastXf& fast, const float* R, float voxel) {
     GridRows g;
-    g.r[0] = fast.row[0];
-    g.r[1] = fast.row[1];
-    g.r[2] = fast.row[2];
+    g.t01[0] = make_float2(fast.row[0].x, fast.row[1].x);
+    g.t01[1] = make_float2(fast.row[0].y, fast.row[1].y);
+    g.t01[2] = make_float2(fast.row[0].z, fast.row[1].z);
+    g.t01[3] = make_float2(fast.row[0].w, fast.row[1].w);
+    g.t2 = fast.row[2];
     for (int a = 0; a < 3; ++a) {
         for (int b = 0; b < 3; ++b) g.m[3 * a + b] = R[4 * a + b] * voxel;
         g.o[a] = -0.5f * (g.m[3 * a] + g.m[3 * a + 1] + g.m[3 * a + 2]);

@@ -248,8 +248,11 @@ struct ModelNorm {
 // size and the cell-centre shift, so that the world-frame offset from the
 // cell centre is
 //     (h M) (t - floor(t) - 1/2) = (h M) frac(t) + o,  o = -(h M) (1/2, 1/2, 1/2).
+// The x and y index rows are stored interleaved, t01[j] = (row0[j], row1[j]),
+// so that tx and ty are computed together by paired FP32 FMAs (fma.rn.f32x2).
 struct GridRows {
-    float4 r[3];
+    float2 t01[4];  // (row 0, row 1) coefficients of c.x, c.y, c.z and the constant
+    float4 t2;      // row 2: coefficients of c.x, c.y, c.z and the constant
     float m[9];
     float o[3];
 };
