@@ -20,7 +20,9 @@ k = 240 step is timed the same way and reported under ``plain_k240``.
 ``e2e`` is the learned path through its public API
 (``LearnedSimulation.step_host``, with its variance gate) with the particles
 in pinned host memory: every step copies them in and back, in chunks
-overlapped with the kernels.
+overlapped with the kernels.  On one GPU the default run then times c1, c3,
+c4 and the render frame in short runs of their own and embeds their lines
+under ``other_workloads`` (``--no-extra`` skips them).
 
 ``c2`` times the plain k = 240 step alone, ``c1`` the small uniform-cube
 case, ``c3`` the batched uneven ensemble and ``c4`` the plain k = 240, g = 32
@@ -443,7 +445,7 @@ def learned_model():
     return model, "trained in this run (64 clump sets x 262,144, 2,000 Adam steps)"
 
 
-def run_learned(args, w: dict) -> None:
+def run_learned(args, w: dict) -> dict | None:
     import ctypes
 
     import torch
@@ -684,12 +686,34 @@ def run_learned(args, w: dict) -> None:
         }
         if base is not None:
             line["cpu_baseline"] = base
-        print(json.dumps(line), flush=True)
     model.close()
     cheap.close()
     big.close()
     if world > 1:
         dist.destroy_process_group()
+    return line if rank == 0 else None
+
+
+# The other configurations, timed after the headline in short runs of their
+# own (one process each, the GPU otherwise idle): c1 the small uniform cube,
+# c3 the batched uneven ensemble, c4 the tensor-core DFT at g = 32, and one
+# headless frame.  Their lines are embedded whole under "other_workloads".
+EXTRA_WORKLOADS = (("c1", 50), ("c3", 10), ("c4", 20), ("render", 10))
+
+
+def run_extra_workloads() -> dict:
+    out = {}
+    for name, steps in EXTRA_WORKLOADS:
+        cmd = [sys.executable, str(ROOT / "bench.py"), "--workload", name, "--steps", str(steps),
+               "--warmup", "3", "--no-cpu-baseline"]
+        try:
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=300, cwd=str(ROOT))
+            lines = [x for x in r.stdout.splitlines() if x.startswith("{")]
+            out[name] = json.loads(lines[-1]) if r.returncode == 0 and lines else \
+                {"error": f"exit {r.returncode}: {r.stderr[-300:]}"}
+        except subprocess.TimeoutExpired:
+            out[name] = {"error": "timed out after 300 s"}
+    return out
 
 
 def run_batch(args, w: dict) -> None:
@@ -938,6 +962,8 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tuning", default="", help="JSON object of mog_tuning fields to apply")
     ap.add_argument("--autotune", action="store_true", help="pick launch shapes before timing")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="default workload: skip the short c1 / c3 / c4 / render runs")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -958,7 +984,11 @@ def main() -> None:
     elif "sims" in w:
         run_batch(args, w)
     elif "k_small" in w:
-        run_learned(args, w)
+        line = run_learned(args, w)
+        if line is not None:
+            if int(os.environ.get("WORLD_SIZE", "1")) == 1 and not args.no_extra:
+                line["other_workloads"] = run_extra_workloads()
+            print(json.dumps(line), flush=True)
     else:
         run_ours(args, w)
 
