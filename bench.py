@@ -681,7 +681,8 @@ def run_learned(args, w: dict) -> dict | None:
                            "pinned host buffers)",
                     "gate": f"variance gate every 10 steps, {ls.fallback_steps} fallback steps, "
                             f"last relative spread {ls.last_ratio} vs training {ls.train_ratio}"},
-            "gpu_launches": (3 if tuning.get("learned_fold") and w["g"] in (8, 16) else 4) * args.steps,
+            "gpu_launches": (4 if tuning.get("learned_fold") == -1 or w["g"] not in (8, 16) else 3)
+                            * args.steps,
             "clocks": clk,
         }
         if base is not None:

@@ -130,10 +130,9 @@ typedef struct mog_tuning {
     int32_t deposit_split;          /* u64 shared histogram of high words only (low halves as
                                        global atomics; none for equal power-of-two masses):
                                        0 auto (g = 32), 1 also at g = 8 and 16, -1 never      */
-    int32_t learned_fold;           /* learned step: 1 = the fft solve's epilogue writes the cell
-                                       masses (one launch fewer at g = 8, 16), 0 = a separate pass */
-    int32_t deposit_dedup;          /* 1: lanes of a warp on one cell add once (count x value), for
-                                       warps whose particles carry equal masses; g = 8, 16      */
+    int32_t learned_fold;           /* learned step: 0 (default) or 1 = the fft solve's epilogue
+                                       writes the cell masses (one launch fewer at g = 8, 16),
+                                       -1 = a separate pass                                     */
 } mog_tuning;
 
 /* Fill a config with the reference's in-code defaults (main.py:179-189). */

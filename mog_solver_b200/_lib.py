@@ -110,7 +110,6 @@ class MogTuningC(ctypes.Structure):
         ("update_threads", ctypes.c_int32),
         ("deposit_split", ctypes.c_int32),
         ("learned_fold", ctypes.c_int32),
-        ("deposit_dedup", ctypes.c_int32),
     ]
 
 

@@ -296,12 +296,7 @@ __device__ __forceinline__ uint32_t cell_byte_offset(const float4& r0, const flo
 // rows, then the words).  count_total: add the tile's q to e.mass_total
 // (done by the tiles of the first grid group, which see every particle
 // once).  Returns after the flush, without a closing barrier.
-//
-// DEDUP: the lanes of a warp whose particles land in one cell add once, the
-// run's count times their common value (__match_any_sync groups them); used
-// for a batch whose particles all carry the same added word, so dense
-// regions cost one shared add per distinct cell instead of one per lane.
-template <int LG, int MODE, int PPT, bool SPLIT, bool SHARD, bool DEDUP = false>
+template <int LG, int MODE, int PPT, bool SPLIT, bool SHARD>
 __device__ __forceinline__ void deposit_fast_tile(const float4* __restrict__ pos, int64_t lo,
                                                   int64_t hi, const Ensemble& e, int gpc, int g0,
                                                   int ng, bool count_total,
@@ -360,31 +355,12 @@ __device__ __forceinline__ void deposit_fast_tile(const float4* __restrict__ pos
             for (int u = 0; u < PPT; ++u) any_lo |= ql[u];
             hi_only = __all_sync(kFull, any_lo == 0u);
         }
-        // DEDUP applies to a full batch whose added word (the u32 value, or
-        // the high word when no lane has a low word) is equal across the warp
-        unsigned dv[PPT];
-        bool dd[PPT];
-        if (DEDUP) {
-#pragma unroll
-            for (int u = 0; u < PPT; ++u) {
-                dv[u] = MODE == 0 ? ql[u] : qh[u];
-                dd[u] = __all_sync(kFull, full && (MODE == 0 || hi_only) &&
-                                              dv[u] == __shfl_sync(kFull, dv[u], 0));
-            }
-        }
         for (int j = 0; j < ng; ++j) {
             const float4 r0 = rows[3 * j], r1 = rows[3 * j + 1], r2 = rows[3 * j + 2];
             const uint32_t gbyte = (uint32_t)j * (G3 * 4u);
 #pragma unroll
             for (int u = 0; u < PPT; ++u) {
                 const uint32_t off = gbyte + cell_byte_offset<LG>(r0, r1, r2, cx[u], cy[u], cz[u]);
-                if (DEDUP && dd[u]) {  // warp-uniform
-                    const unsigned peers = __match_any_sync(kFull, off);
-                    if ((int)__ffs(peers) - 1 == (int)(threadIdx.x & 31) && dv[u] &&
-                        in_bounds(e.flags, off >> 2, words))
-                        red_shared((MODE == 0 ? lo_base : hi_base) + off, dv[u] * (unsigned)__popc(peers));
-                    continue;
-                }
                 if (!in_bounds(e.flags, off >> 2, words)) continue;
                 if (MODE == 0) {
                     if (ql[u]) red_shared(lo_base + off, ql[u]);   // zero for padding lanes
@@ -426,7 +402,7 @@ __device__ __forceinline__ void deposit_fast_tile(const float4* __restrict__ pos
     }
 }
 
-template <int LG, int MODE, int PPT, bool SPLIT = false, bool SHARD = false, bool DEDUP = false>
+template <int LG, int MODE, int PPT, bool SPLIT = false, bool SHARD = false>
 __global__ void __launch_bounds__(1024) deposit_fast_kernel(const float4* __restrict__ pos,
                                                             int64_t n, int64_t chunk, Ensemble e,
                                                             int gpc,
@@ -434,7 +410,7 @@ __global__ void __launch_bounds__(1024) deposit_fast_kernel(const float4* __rest
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int g0 = blockIdx.y * gpc;
     const int64_t lo = (int64_t)blockIdx.x * chunk;
-    deposit_fast_tile<LG, MODE, PPT, SPLIT, SHARD, DEDUP>(pos, lo, min(n, lo + chunk), e, gpc, g0,
+    deposit_fast_tile<LG, MODE, PPT, SPLIT, SHARD>(pos, lo, min(n, lo + chunk), e, gpc, g0,
                                                    min(gpc, e.k - g0), blockIdx.y == 0, mass,
                                                    smem_raw);
     shard_release<SHARD>();
@@ -624,15 +600,6 @@ static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, const int
                     if (ppt == 2) return launch_fast(deposit_fast_kernel<5, MODE, 2>);
                     return launch_fast(deposit_fast_kernel<5, MODE, 4>);
                 }
-            }
-            if (sh.dedup == 1 && ppt == 4) {
-                if constexpr (MODE == 1) {
-                    if (split_small && e.g == 16)
-                        return launch_fast(deposit_fast_kernel<4, 1, 4, true, false, true>);
-                    if (split_small) return launch_fast(deposit_fast_kernel<3, 1, 4, true, false, true>);
-                }
-                if (e.g == 16) return launch_fast(deposit_fast_kernel<4, MODE, 4, false, false, true>);
-                if (e.g == 8) return launch_fast(deposit_fast_kernel<3, MODE, 4, false, false, true>);
             }
             if constexpr (MODE == 1) {
                 if (split_small && e.g == 16) return launch_fast(deposit_fast_kernel<4, 1, 4, true>);

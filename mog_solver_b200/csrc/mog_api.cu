@@ -189,7 +189,7 @@ struct mog_handle {
     int64_t perm_cap = 0;        // capacity of d_perm
     int64_t perm_n = -1;         // n the permutation was built for
     int sort_every = 0;          // re-order every this many steps (0 = never)
-    int learned_fold = 0;        // learned step: cell masses written by the solve's epilogue
+    int learned_fold = 1;        // learned step: cell masses written by the solve's epilogue
     uint64_t step_count = 0;     // steps issued (decides when to re-order)
     std::vector<GraphEntry> graphs;
     std::vector<mog::GridRows> rows;  // learned-gather rows of the k grids (host)
@@ -795,8 +795,7 @@ int mog_get_tuning(const mog_handle* h, mog_tuning* out) {
     out->update_threads = h->ushape.threads;
     out->update_direct_ppt = h->ushape.direct_ppt;
     out->deposit_split = h->dshape.split;
-    out->learned_fold = h->learned_fold;
-    out->deposit_dedup = h->dshape.dedup;
+    out->learned_fold = h->learned_fold ? 1 : -1;
     return MOG_OK;
 }
 
@@ -813,8 +812,8 @@ int mog_set_tuning(mog_handle* h, const mog_tuning* t) {
          t->update_threads != 1024) ||
         (t->update_direct_ppt != 0 && t->update_direct_ppt != 1 && t->update_direct_ppt != 2 &&
          t->update_direct_ppt != 4) ||
-        t->deposit_split < -1 || t->deposit_split > 1 || t->learned_fold < 0 ||
-        t->learned_fold > 1 || t->deposit_dedup < 0 || t->deposit_dedup > 1)
+        t->deposit_split < -1 || t->deposit_split > 1 || t->learned_fold < -1 ||
+        t->learned_fold > 1)
         return fail(MOG_ERR_ARG, "tuning value out of range");
     h->dshape.threads = t->deposit_threads ? t->deposit_threads : 1024;
     h->dshape.grids_per_cta = t->deposit_grids_per_cta;
@@ -829,8 +828,7 @@ int mog_set_tuning(mog_handle* h, const mog_tuning* t) {
     h->dshape.sorted_input = t->deposit_sorted ? 1 : 0;
     h->ushape.threads = t->update_threads ? t->update_threads : 512;
     h->dshape.split = t->deposit_split;
-    h->learned_fold = t->learned_fold;
-    h->dshape.dedup = t->deposit_dedup;
+    h->learned_fold = t->learned_fold >= 0 ? 1 : 0;
     for (auto& g : h->graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);
     h->graphs.clear();

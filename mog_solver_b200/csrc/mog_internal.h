@@ -79,7 +79,6 @@ struct DepositShape {
     int fast = 1;           // use the specialised kernel where it applies
     int sorted_input = 0;   // read the spatially ordered copy (else the caller's order)
     int split = 0;          // u64 high-word-only histogram: 0 auto (g = 32), 1 also g = 8/16, -1 never
-    int dedup = 0;          // 1: one shared add per distinct cell of a warp (g = 8, 16)
 };
 struct UpdateShape {
     int threads = 512;      // staged gather block size: 512, 768 or 1024

@@ -126,41 +126,9 @@ def test_split_histogram_at_small_grids_is_bit_exact(g, k, equal):
     assert np.array_equal(got, ref)
 
 
-@pytest.mark.parametrize("g,k,mode,split", [(8, 5, "u64", 0), (16, 7, "u64", 0), (16, 7, "u64", 1),
-                                              (16, 3, "u32x1000", 0), (16, 7, "unequal", 0)])
-def test_warp_dedup_deposit_is_bit_exact(g, k, mode, split):
-    """Tuning deposit_dedup = 1: lanes of a warp on one cell add once (run
-    length times the common value); warps whose masses differ take the
-    per-lane adds.  Clumped particles so that warps do share cells."""
-    import oracle
-
-    from mog_solver_b200 import Simulation, ics
-
-    n, L = (1 << 18) + 77, 100.0  # a partial last batch
-    sim = Simulation({"n_grids": k, "grid_size": g, "world_size": L, "num_particles": n, "G": 100.0,
-                      "dt": 1e-5, "seed": 0,
-                      "mass_mode": "u32x1000" if mode == "u32x1000" else "u64"})
-    sim.tune(deposit_dedup=1, deposit_split=split)
-
-    pos, _ = ics.clumps(n, L, seed=g + k, sigma_range=(0.5, 3.0))
-    if mode == "u32x1000":
-        pos[:, 3] = 1.0
-    elif mode == "unequal":
-        pos[:, 3] = np.random.default_rng(5).uniform(0.5, 2.0, n).astype(np.float32) / n
-    sim.set_particles(pos)
-    assert sim.tuning()["deposit_dedup"] == 1
-    if mode == "u32x1000":
-        got = sim.mass_grid().cpu().numpy().view(np.uint32)
-        ref = oracle.deposit(pos, sim.rotations, sim.offsets, g, L, oracle.MASS_U32, 0)
-    else:
-        got = sim.mass_grid().cpu().numpy().view(np.uint64)
-        ref = oracle.deposit(pos, sim.rotations, sim.offsets, g, L, oracle.MASS_U64, sim.scale_bits)
-    assert np.array_equal(got, ref)
-
-
 @pytest.mark.parametrize("g", [8, 16, 32])
 def test_learned_fold_is_bit_identical(g):
-    """Tuning learned_fold = 1: the solve's epilogue writes the cell masses
+    """Tuning learned_fold = 1 (the default): the solve's epilogue writes the cell masses
     (g = 8, 16; a separate pass at g = 32): the learned step's particles and
     its variance-gate statistics are those of the separate pass, bit for bit."""
     import ctypes
@@ -173,6 +141,7 @@ def test_learned_fold_is_bit_identical(g):
     model = Model.load(DEFAULT_MODEL)
     a = make_sim(k=32, g=g, n=n, dt=1e-3)
     b = make_sim(k=32, g=g, n=n, dt=1e-3)
+    a.tune(learned_fold=-1)
     b.tune(learned_fold=1)
     pos, vel = particles(n, seed=31)
     a.set_particles(pos, vel)
