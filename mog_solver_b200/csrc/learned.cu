@@ -364,14 +364,10 @@ struct GridTable {
 };
 
 // K > 0: k == K and the rows come from `tab`; K == 0: any k, rows staged in
-// shared memory.  perm (nullable): slot s processes particle perm[s], whose
-// position pos_s[s] holds (the spatial order: the lanes of a warp are then
-// neighbours and their gathers hit the same cache lines); outputs go to the
-// particle's own index.
+// shared memory.
 template <int IDX, int LG, int OUT, int K>
 __global__ void __launch_bounds__(kLT, 2) learned_kernel(
-    float4* __restrict__ pos, float4* __restrict__ vel, int64_t n,
-    const float4* __restrict__ pos_s, const int* __restrict__ perm, const float4* __restrict__ W,
+    float4* __restrict__ pos, float4* __restrict__ vel, int64_t n, const float4* __restrict__ W,
     Ensemble e, ModelNorm norm, const uint2* __restrict__ frags, const float* __restrict__ params,
     float dt, float damp, float4* __restrict__ out4, float* __restrict__ feat_out,
     float* __restrict__ spread_part, const __grid_constant__ GridTable<K> tab) {
@@ -403,14 +399,9 @@ __global__ void __launch_bounds__(kLT, 2) learned_kernel(
     float fmag = 0.f;    // sum over this thread's particles of feature 10
     for (int64_t base = (int64_t)blockIdx.x * kLT; base < n; base += (int64_t)gridDim.x * kLT) {
         if (base + warp * 32 >= n) continue;  // whole warp past the end (warp-uniform)
-        const int64_t slot = base + threadIdx.x;
-        const bool live = slot < n;
-        int64_t p = slot;
-        if (live && perm) {
-            p = __ldg(perm + slot);
-            if (!in_bounds(e.flags, (uint64_t)p, (uint64_t)n)) p = slot;
-        }
-        const float4 P = !live ? make_float4(0.f, 0.f, 0.f, 0.f) : (perm ? pos_s[slot] : pos[p]);
+        const int64_t p = base + threadIdx.x;
+        const bool live = p < n;
+        const float4 P = live ? pos[p] : make_float4(0.f, 0.f, 0.f, 0.f);
         const float cx = __fsub_rn(P.x, ip.half_l), cy = __fsub_rn(P.y, ip.half_l),
                     cz = __fsub_rn(P.z, ip.half_l);
         GatherAcc acc;
@@ -709,8 +700,7 @@ cudaError_t launch_learned_t(const Ensemble& e, const GridRows* rows, float4* po
     int64_t blocks = std::min<int64_t>((n + kLT - 1) / kLT, (int64_t)num_sms() * std::max(per_sm, 1));
     if (out.spread && blocks > out.spread_cap) blocks = out.spread_cap;
     out.blocks = (int)blocks;
-    kern<<<(unsigned)blocks, kLT, smem, s>>>(pos, vel, n, out.pos_s, out.perm, W, e, norm,
-                                            static_cast<const uint2*>(frags),
+    kern<<<(unsigned)blocks, kLT, smem, s>>>(pos, vel, n, W, e, norm, static_cast<const uint2*>(frags),
                                             params, dt, damp, out.out4, out.feat, out.spread, tab);
     return cudaGetLastError();
 }

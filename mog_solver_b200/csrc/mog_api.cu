@@ -1170,12 +1170,6 @@ static int run_learned(mog_handle* h, const mog_model* m, int out_mode, float* p
         out.spread = h->d_spread;
         out.spread_cap = h->spread_cap;
     }
-    // with spatial ordering on, the learned kernel walks the particles in
-    // that order (its gathers then share cache lines); the deposit keeps the
-    // caller's order, where its shared adds collide less
-    int rc = order_particles(h, reinterpret_cast<const float4*>(pos4), n, wants_sort(h, n), s,
-                             &out.perm, &out.pos_s);
-    if (rc) return rc;
     err = mog::launch_learned(out_mode, e, h->rows.data(), reinterpret_cast<float4*>(pos4),
                               reinterpret_cast<float4*>(vel4), n, h->d_force, m->norm, m->d_frags,
                               m->d_params, dt, h->cfg.damping, out, s);

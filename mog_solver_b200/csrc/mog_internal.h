@@ -278,10 +278,6 @@ struct LearnedOut {
     float* spread = nullptr;
     int spread_cap = 0;
     int blocks = 0;
-    // optional spatial order the kernel walks: slot s is particle perm[s],
-    // whose position pos_s[s] holds (both null: the caller's order)
-    const float4* pos_s = nullptr;
-    const int* perm = nullptr;
 };
 // rows: the ensemble's k GridRows in host memory (they travel in the launch
 // parameters when k is one of the compiled ensemble sizes).

@@ -126,45 +126,6 @@ def test_split_histogram_at_small_grids_is_bit_exact(g, k, equal):
     assert np.array_equal(got, ref)
 
 
-@pytest.mark.parametrize("sort_every", [1, 3])
-def test_spatially_ordered_learned_step_is_bit_identical(sort_every):
-    """Tuning sort_every > 0 on the learned path: the learned kernel walks the
-    particles in spatial order (each particle's result is its own), so the
-    trajectory equals the caller's order bit for bit."""
-    import ctypes
-
-    from mog_solver_b200 import _lib
-    from mog_solver_b200.learned import Model
-    from mog_solver_b200.train_learned import DEFAULT_MODEL
-
-    n = 70001
-    model = Model.load(DEFAULT_MODEL)
-    a = make_sim(k=32, g=16, n=n, dt=1e-3)
-    b = make_sim(k=32, g=16, n=n, dt=1e-3)
-    b.tune(sort_every=sort_every)
-    pos, vel = particles(n, seed=33)
-    a.set_particles(pos, vel)
-    b.set_particles(pos, vel)
-    lib = _lib.lib()
-    try:
-        for _ in range(5):
-            for s in (a, b):
-                _lib.check(lib.mog_learned_step(s.handle, model.handle, s.pos.data_ptr(),
-                                                s.vel.data_ptr(), n, 1e-3, None), "learned step")
-        torch.cuda.synchronize()
-        assert torch.equal(a.pos, b.pos) and torch.equal(a.vel, b.vel)
-        sa, sb = (ctypes.c_double * 2)(), (ctypes.c_double * 2)()
-        _lib.check(lib.mog_learned_spread(a.handle, sa, None), "spread")
-        _lib.check(lib.mog_learned_spread(b.handle, sb, None), "spread")
-        # per-CTA float sums over differently ordered particles: equal to rounding
-        assert abs(sa[0] - sb[0]) <= 1e-5 * sa[0] and abs(sa[1] - sb[1]) <= 1e-5 * sa[1]
-        assert a.status() == 0 and b.status() == 0
-    finally:
-        a.close()
-        b.close()
-        model.close()
-
-
 @pytest.mark.parametrize("g", [8, 16, 32])
 def test_learned_fold_is_bit_identical(g):
     """Tuning learned_fold = 1 (the default): the solve's epilogue writes the cell masses
