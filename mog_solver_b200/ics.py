@@ -118,6 +118,27 @@ def plummer(n: int, world: float = 100.0, seed: int = 0, a: float = 5.0,
     return _records(xyz, total_mass / n)
 
 
+def rotated_disk_pair(n: int, world: float = 100.0, seed: int = 500):
+    """Two exponential disks (two_disks) with a scale radius drawn from
+    [5, 11], a sech^2 height log-uniform in [0.25, 1] and centres 25 to 55
+    apart, the whole set turned by a random rotation about the box centre
+    (periodic wrap).  Disk-like training data for the learned correction,
+    drawn around (never at) the benchmark's parameters."""
+    rng = np.random.default_rng(seed)
+    pos, vel = two_disks(n, world, seed=seed, r_d=float(rng.uniform(5.0, 11.0)),
+                         z0=float(np.exp(rng.uniform(np.log(0.25), np.log(1.0)))),
+                         sep=float(rng.uniform(25.0, 55.0)))
+    q = rng.normal(size=4)
+    w, x, y, z = q / np.linalg.norm(q)
+    R = np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
+                  [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
+                  [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)]])
+    c = pos[:, :3].astype(np.float64) - world / 2.0
+    pos[:, :3] = wrap(c @ R.T + world / 2.0, world)
+    vel[:, :3] = (vel[:, :3].astype(np.float64) @ R.T).astype(np.float32)
+    return pos, vel
+
+
 def clumps(n: int, world: float = 100.0, seed: int = 100, n_clumps: int = 20,
            sigma_range: tuple[float, float] = (1.0, 8.0), background: float = 0.1,
            total_mass: float = 1.0):

@@ -168,23 +168,34 @@ def _cfg(k: int, g: int, L: float, G: float, n: int, seed: int, dt: float = 1e-5
             "damping": damping, "seed": seed}
 
 
-def generate_dataset(n_sets: int = 64, n: int = 262144, k_small: int = 32, k_big: int = 240,
-                     g: int = 16, world: float = 100.0, G: float = 100.0, seed0: int = 100,
-                     small_seed: int = 1000, big_seed: int = 2000) -> Dataset:
-    """Training pairs the method generates itself: for seeded clump sets,
-    features of the k_small ensemble and the k_big force minus the k_small
-    base force (mean + least-squares correction, base_mode 1).  Returns
-    standardised tensors and the matching normalisation."""
+def training_sets(n_sets: int, n: int, world: float, seed0: int, disk_sets: int, disk_seed0: int):
+    """The particle sets of the training data: n_sets Gaussian-clump sets
+    (ics.clumps, seeds seed0...) and disk_sets randomly oriented disk pairs
+    (ics.rotated_disk_pair, seeds disk_seed0...)."""
     from . import ics
 
+    for i in range(n_sets):
+        yield ics.clumps(n, world, seed=seed0 + i)[0]
+    for i in range(disk_sets):
+        yield ics.rotated_disk_pair(n, world, seed=disk_seed0 + i)[0]
+
+
+def generate_dataset(n_sets: int = 64, n: int = 262144, k_small: int = 32, k_big: int = 240,
+                     g: int = 16, world: float = 100.0, G: float = 100.0, seed0: int = 100,
+                     small_seed: int = 1000, big_seed: int = 2000, disk_sets: int = 0,
+                     disk_seed0: int = 500) -> Dataset:
+    """Training pairs the method generates itself: for seeded clump sets
+    (and disk_sets randomly oriented disk pairs), features of the k_small
+    ensemble and the k_big force minus the k_small base force (mean +
+    least-squares correction, base_mode 1).  Returns standardised tensors
+    and the matching normalisation."""
     torch = _torch()
     small = Simulation(_cfg(k_small, g, world, G, n, small_seed))
     big = Simulation(_cfg(k_big, g, world, G, n, big_seed))
     rho_ref = 1.0 / g ** 3          # total mass 1 over g^3 cells
     raw = Model(norm=norm_vector(np.zeros(12), np.ones(12), 1.0, rho_ref, 1.0))
     feats, resid = [], []
-    for i in range(n_sets):
-        pos, _ = ics.clumps(n, world, seed=seed0 + i)
+    for pos in training_sets(n_sets, n, world, seed0, disk_sets, disk_seed0):
         small.set_particles(pos)
         big.set_particles(pos)
         mean, f = features(small, raw)
@@ -230,6 +241,56 @@ def train(model: Model, data: Dataset, steps: int = 2000, batch: int = 8192, lr:
         if want:
             history.append((step, loss))
     return history
+
+
+def residual_errors(model: Model, sets, k_small: int = 32, k_big: int = 240, g: int = 16,
+                    world: float = 100.0, G: float = 100.0, alphas=(1.0,), small_seed: int = 1000,
+                    big_seed: int = 2000) -> list[dict]:
+    """For each particle set: the relative RMS distance to the k_big force of
+    the k_small plain mean, of its least-squares correction alone ("ls") and
+    of the learned force with the network's output scaled by each alpha
+    (alpha 0 is the least-squares force)."""
+    n = max(int(p.shape[0]) for p in sets)
+    small = Simulation(_cfg(k_small, g, world, G, n, small_seed))
+    big = Simulation(_cfg(k_big, g, world, G, n, big_seed))
+    params, norm = model.get()
+    rows = []
+    try:
+        for pos in sets:
+            small.set_particles(pos)
+            big.set_particles(pos)
+            fb = big.forces()
+            mean, feat = features(small, model)
+            ls = mean.clone()
+            ls[:, :3] += feat[:, 12:15]
+            row = {"plain": rms_error(mean, fb), "ls": rms_error(ls, fb)}
+            for a in alphas:
+                scaled = norm.copy()
+                scaled[26] = norm[26] * a
+                model.set(params, scaled)
+                row[f"net_x{a:g}"] = rms_error(learned_forces(small, model), fb)
+            model.set(params, norm)
+            rows.append(row)
+    finally:
+        model.set(params, norm)
+        small.close()
+        big.close()
+    return rows
+
+
+def select_output_scale(model: Model, val_sets, alphas=(0.25, 0.5, 0.75, 1.0), **kw) -> dict:
+    """Scale the network's output (the norm's out_scale) by the alpha whose
+    learned force is closest to the k_big force on held-out validation
+    sets (mean relative RMS error); alpha 0, the least-squares force alone,
+    is kept when no alpha beats it.  Returns the table it chose from."""
+    rows = residual_errors(model, val_sets, alphas=alphas, **kw)
+    score = {a: float(np.mean([r[f"net_x{a:g}"] for r in rows])) for a in alphas}
+    score[0.0] = float(np.mean([r["ls"] for r in rows]))
+    best = min(score, key=score.get)
+    params, norm = model.get()
+    norm[26] = norm[26] * best
+    model.set(params, norm)
+    return {"alpha": best, "validation_mean_error": score, "validation": rows}
 
 
 def _gate_stats(feat, norm) -> tuple[float, float]:

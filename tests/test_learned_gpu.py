@@ -132,6 +132,27 @@ def test_features_match_fp64_oracle():
     m.close()
 
 
+def test_network_gains_over_least_squares_alone():
+    """The committed network against the method without it: the cheap
+    ensemble's mean plus its least-squares correction (the network's output
+    zeroed).  Against the k = 240 force, on a clump set held out of training
+    and on the evaluation disks (N = 2^20 each), the learned force must be
+    closer than least squares alone, which must be closer than the plain
+    k = 32 mean."""
+    from mog_solver_b200 import ics
+    from mog_solver_b200.learned import Model, residual_errors
+    from mog_solver_b200.train_learned import DEFAULT_MODEL
+
+    model = Model.load(DEFAULT_MODEL)
+    try:
+        sets = [ics.clumps(1 << 20, 100.0, seed=901)[0], ics.two_disks(1 << 20, 100.0, seed=1)[0]]
+        rows = residual_errors(model, sets, alphas=(1.0,))
+    finally:
+        model.close()
+    for name, r in zip(("held-out clumps", "disks"), rows):
+        assert r["net_x1"] < r["ls"] < r["plain"], (name, r)
+
+
 def test_training_gains_over_plain_cheap_ensemble():
     """Train briefly on clump sets; on held-out particles the corrected
     k=16 force is closer to the k=128 force than the plain k=16 mean is."""
