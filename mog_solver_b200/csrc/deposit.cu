@@ -296,13 +296,7 @@ __device__ __forceinline__ uint32_t cell_byte_offset(const float4& r0, const flo
 // rows, then the words).  count_total: add the tile's q to e.mass_total
 // (done by the tiles of the first grid group, which see every particle
 // once).  Returns after the flush, without a closing barrier.
-//
-// ORDERED (particles in spatial order, the lanes of a warp neighbours): when
-// every lane of a warp lands in one cell of a grid, lane 0 adds the warp's
-// summed word once (the u32 value, or the high word when no lane of the
-// batch has a low word); otherwise each lane adds its own.  Dense regions
-// then cost one shared add per warp and grid instead of 32 colliding ones.
-template <int LG, int MODE, int PPT, bool SPLIT, bool SHARD, bool ORDERED = false>
+template <int LG, int MODE, int PPT, bool SPLIT, bool SHARD>
 __device__ __forceinline__ void deposit_fast_tile(const float4* __restrict__ pos, int64_t lo,
                                                   int64_t hi, const Ensemble& e, int gpc, int g0,
                                                   int ng, bool count_total,
@@ -361,32 +355,12 @@ __device__ __forceinline__ void deposit_fast_tile(const float4* __restrict__ pos
             for (int u = 0; u < PPT; ++u) any_lo |= ql[u];
             hi_only = __all_sync(kFull, any_lo == 0u);
         }
-        // ORDERED: the warp's total of the word each lane adds (wrapping, as
-        // the adds themselves would), for the one-add-per-warp case
-        unsigned wsum[PPT];
-        const bool merge = ORDERED && (MODE == 0 || hi_only);  // warp-uniform
-        if (ORDERED) {
-#pragma unroll
-            for (int u = 0; u < PPT; ++u) {
-                unsigned v = MODE == 0 ? ql[u] : qh[u];
-                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
-                wsum[u] = v;
-            }
-        }
         for (int j = 0; j < ng; ++j) {
             const float4 r0 = rows[3 * j], r1 = rows[3 * j + 1], r2 = rows[3 * j + 2];
             const uint32_t gbyte = (uint32_t)j * (G3 * 4u);
 #pragma unroll
             for (int u = 0; u < PPT; ++u) {
                 const uint32_t off = gbyte + cell_byte_offset<LG>(r0, r1, r2, cx[u], cy[u], cz[u]);
-                if (ORDERED && merge) {
-                    const uint32_t off0 = __shfl_sync(kFull, off, 0);
-                    if (__all_sync(kFull, off == off0)) {  // the whole warp on one cell
-                        if ((threadIdx.x & 31) == 0 && wsum[u] && in_bounds(e.flags, off0 >> 2, words))
-                            red_shared((MODE == 0 ? lo_base : hi_base) + off0, wsum[u]);
-                        continue;
-                    }
-                }
                 if (!in_bounds(e.flags, off >> 2, words)) continue;
                 if (MODE == 0) {
                     if (ql[u]) red_shared(lo_base + off, ql[u]);   // zero for padding lanes
@@ -428,7 +402,7 @@ __device__ __forceinline__ void deposit_fast_tile(const float4* __restrict__ pos
     }
 }
 
-template <int LG, int MODE, int PPT, bool SPLIT = false, bool SHARD = false, bool ORDERED = false>
+template <int LG, int MODE, int PPT, bool SPLIT = false, bool SHARD = false>
 __global__ void __launch_bounds__(1024) deposit_fast_kernel(const float4* __restrict__ pos,
                                                             int64_t n, int64_t chunk, Ensemble e,
                                                             int gpc,
@@ -436,7 +410,7 @@ __global__ void __launch_bounds__(1024) deposit_fast_kernel(const float4* __rest
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int g0 = blockIdx.y * gpc;
     const int64_t lo = (int64_t)blockIdx.x * chunk;
-    deposit_fast_tile<LG, MODE, PPT, SPLIT, SHARD, ORDERED>(pos, lo, min(n, lo + chunk), e, gpc, g0,
+    deposit_fast_tile<LG, MODE, PPT, SPLIT, SHARD>(pos, lo, min(n, lo + chunk), e, gpc, g0,
                                                    min(gpc, e.k - g0), blockIdx.y == 0, mass,
                                                    smem_raw);
     shard_release<SHARD>();
@@ -571,12 +545,7 @@ static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, const int
     const size_t smem = (size_t)gpc * 16 * sizeof(float) + ((size_t)gpc * word_bytes << slab_lg);
     // the sharded deposit is built for 4 particles per thread only
     const int ppt = SHARD ? 4 : (sh.ppt == 1 || sh.ppt == 2 || sh.ppt == 4 ? sh.ppt : 4);
-    // Spatially ordered input: by default the specialised kernel with its
-    // one-add-per-warp merge (ORDERED); deposit_aggregate = 1 selects the
-    // generic kernel's merge of runs of equal cells, 0 no merging at all.
-    const bool fast_ordered = !SHARD && ordered && sh.aggregate < 0 && IDX == 0 && !perm &&
-                              (e.g == 8 || e.g == 16 || e.g == 32) && sh.fast != 0 && ppt == 4;
-    const bool agg = sh.aggregate < 0 ? ordered && !fast_ordered : sh.aggregate != 0;
+    const bool agg = sh.aggregate < 0 ? ordered : sh.aggregate != 0;
     // The split histogram (u64, high words only, 4 bytes a cell; low halves
     // go to the global cells, and equal power-of-two masses have none).  At
     // g = 32 it fits one grid per CTA where the two-word one needs two
@@ -621,16 +590,6 @@ static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, const int
             if (e.g == 16) return launch_fast(deposit_fast_kernel<4, MODE, 4, false, true>);
             return launch_fast(deposit_fast_kernel<3, MODE, 4, false, true>);
         } else {
-            if (fast_ordered) {
-                if (e.g == 32) return launch_fast(deposit_fast_kernel<5, MODE, 4, MODE == 1, false, true>);
-                if constexpr (MODE == 1) {
-                    if (split_small && e.g == 16)
-                        return launch_fast(deposit_fast_kernel<4, 1, 4, true, false, true>);
-                    if (split_small) return launch_fast(deposit_fast_kernel<3, 1, 4, true, false, true>);
-                }
-                if (e.g == 16) return launch_fast(deposit_fast_kernel<4, MODE, 4, false, false, true>);
-                return launch_fast(deposit_fast_kernel<3, MODE, 4, false, false, true>);
-            }
             if (e.g == 32) {
                 if constexpr (MODE == 1) {
                     if (ppt == 1) return launch_fast(deposit_fast_kernel<5, 1, 1, true>);

@@ -61,7 +61,6 @@ SHAPES = [(1, 1, 8), (7, 3, 16), (257, 16, 16), (65536, 16, 16), (5000, 5, 32), 
 # launch shapes that take different code paths; none may change a bit
 DEPOSIT_TUNINGS = {
     "sorted+merged": dict(sort_every=1, deposit_aggregate=-1, deposit_sorted=1),
-    "sorted+segmented": dict(sort_every=1, deposit_aggregate=1, deposit_sorted=1),
     "unsorted": dict(sort_every=0, deposit_aggregate=0),
     "sorted+plain": dict(sort_every=1, deposit_aggregate=0, deposit_ppt=1, deposit_sorted=1),
     "sorted-update-only": dict(sort_every=1),
