@@ -428,121 +428,6 @@ __global__ void __launch_bounds__(1024) deposit_fast_kernel(const float4* __rest
     shard_release<SHARD>();
 }
 
-// Deposit of spatially ordered particles (the sorted copy of the positions).
-// Each thread owns a contiguous segment of the CTA's slots and walks it four
-// particles at a time.  Consecutive particles of a segment are neighbours,
-// so within one grid they mostly share a cell: a run of them is summed in
-// registers and added once.  The 32 lanes of a warp own segments 1/32 of
-// the chunk apart, so their adds rarely meet on one cell.  Histogram layout,
-// swizzle and flush are deposit_fast_tile's; the u64 sums of a run are
-// split into words exactly as a single particle's q is.
-template <int LG, int MODE, bool SPLIT>
-__global__ void __launch_bounds__(1024) deposit_runs_kernel(const float4* __restrict__ pos_s,
-                                                            int64_t n, int64_t chunk, Ensemble e,
-                                                            int gpc,
-                                                            typename SmemHist<MODE>::Acc* __restrict__ mass) {
-    using H = SmemHist<MODE>;
-    using Acc = typename H::Acc;
-    constexpr int G3 = 1 << (3 * LG);
-    constexpr int R = 4;  // particles per step of a segment
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int g0 = blockIdx.y * gpc;
-    const int ng = min(gpc, e.k - g0);
-    const int64_t lo = (int64_t)blockIdx.x * chunk;
-    const int64_t hi = min(n, lo + chunk);
-    const uint32_t words = (uint32_t)ng * G3;
-    float4* rows = reinterpret_cast<float4*>(smem_raw);
-    unsigned* lo_w = reinterpret_cast<unsigned*>(smem_raw + (size_t)gpc * 48);
-    unsigned* hi_w = SPLIT ? lo_w : lo_w + (size_t)gpc * G3;
-    const uint32_t lo_base = (uint32_t)__cvta_generic_to_shared(lo_w);
-    const uint32_t hi_base = (uint32_t)__cvta_generic_to_shared(hi_w);
-    for (int i = threadIdx.x; i < ng * 3; i += blockDim.x) rows[i] = e.fast[g0 + i / 3].row[i % 3];
-    for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) {
-        lo_w[i] = 0u;
-        if (H::kWords == 2 && !SPLIT) hi_w[i] = 0u;
-    }
-    __syncthreads();
-
-    const int T = blockDim.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t seg = (hi - lo + T - 1) / T;
-    const int64_t my_lo = lo + (int64_t)(lane * (T >> 5) + warp) * seg;
-    const int64_t my_hi = min(hi, my_lo + seg);
-    const int steps = (int)((seg + R - 1) / R);
-    const float half_l = e.world * 0.5f;
-    unsigned bad = 0;
-    double qsum = 0.0;
-    // one shared add (MODE 0, or the two words of MODE 1) of a run's sum v
-    auto add = [&](uint32_t off, Acc v) {
-        const uint32_t soff = hist_swizzle(off >> 2) << 2;
-        if (MODE == 0) {
-            red_shared(lo_base + soff, (unsigned)v);
-        } else if (SPLIT) {
-            const unsigned vl = (unsigned)v, vh = (unsigned)((unsigned long long)v >> 32);
-            if (vl) atomicAdd(mass + (size_t)g0 * G3 + (off >> 2), (Acc)vl);
-            if (vh) red_shared(hi_base + soff, vh);
-        } else {
-            const unsigned vl = (unsigned)v;
-            unsigned vh = (unsigned)((unsigned long long)v >> 32);
-            if (vl) {
-                const unsigned old = atom_shared(lo_base + soff, vl);
-                vh += (old > ~vl) ? 1u : 0u;
-            }
-            if (vh) red_shared(hi_base + soff, vh);
-        }
-    };
-    for (int it = 0; it < steps; ++it) {
-        float cx[R], cy[R], cz[R];
-        Acc q[R];
-#pragma unroll
-        for (int u = 0; u < R; ++u) {
-            const int64_t slot = my_lo + (int64_t)it * R + u;
-            const bool valid = slot < my_hi;
-            const float4 P = valid ? __ldg(pos_s + slot) : make_float4(0.f, 0.f, 0.f, 0.f);
-            unsigned b = 0;
-            if (MODE == 1)
-                q[u] = valid ? quantize_u64(P.w, e.scale, b) : 0ull;
-            else
-                q[u] = valid ? quantize_u32(P.w, b) : 0u;
-            bad |= b;
-            qsum += (double)q[u];
-            cx[u] = __fsub_rn(P.x, half_l);
-            cy[u] = __fsub_rn(P.y, half_l);
-            cz[u] = __fsub_rn(P.z, half_l);
-        }
-        for (int j = 0; j < ng; ++j) {
-            const float4 r0 = rows[3 * j], r1 = rows[3 * j + 1], r2 = rows[3 * j + 2];
-            const uint32_t gbyte = (uint32_t)j * (G3 * 4u);
-            uint32_t run_off = 0u;
-            Acc run_q = 0;
-#pragma unroll
-            for (int u = 0; u < R; ++u) {
-                const uint32_t off = gbyte + cell_byte_offset<LG>(r0, r1, r2, cx[u], cy[u], cz[u]);
-                if (!q[u] || !in_bounds(e.flags, off >> 2, words)) continue;
-                if (run_q && off == run_off) {
-                    run_q += q[u];
-                    continue;
-                }
-                if (run_q) add(run_off, run_q);
-                run_off = off;
-                run_q = q[u];
-            }
-            if (run_q) add(run_off, run_q);
-        }
-    }
-    if (MODE == 1 && blockIdx.y == 0) {
-        for (int o = 16; o > 0; o >>= 1) qsum += __shfl_xor_sync(kFull, qsum, o);
-        if (lane == 0 && qsum != 0.0) atomicAdd(e.mass_total, qsum);
-    }
-    if (bad) raise_flags(e.flags, bad);
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) {
-        const Acc v = SPLIT ? (Acc)hi_w[i] << 32 : H::read(lo_w, hi_w, i);
-        const uint32_t w = hist_swizzle(i);
-        if (v && in_bounds(e.flags, (size_t)g0 * G3 + w, (uint64_t)e.cells()))
-            atomicAdd(mass + (size_t)g0 * G3 + w, v);
-    }
-}
-
 // Batched ensemble, one persistent launch for every simulation of a batch:
 // each CTA pops tiles (simulation, grid group, particle chunk) from the
 // host-built list with an atomic counter until it runs out, and deposits
@@ -672,13 +557,7 @@ static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, const int
     const size_t smem = (size_t)gpc * 16 * sizeof(float) + ((size_t)gpc * word_bytes << slab_lg);
     // the sharded deposit is built for 4 particles per thread only
     const int ppt = SHARD ? 4 : (sh.ppt == 1 || sh.ppt == 2 || sh.ppt == 4 ? sh.ppt : 4);
-    // Spatially ordered input: by default the run-summing kernel
-    // (deposit_runs_kernel) where the specialised shapes apply;
-    // deposit_aggregate = 1 selects the generic kernel's warp merge of runs
-    // of equal cells, 0 no merging at all.
-    const bool runs = !SHARD && ordered && sh.aggregate < 0 && IDX == 0 && !perm &&
-                      (e.g == 8 || e.g == 16 || e.g == 32) && sh.fast != 0;
-    const bool agg = sh.aggregate < 0 ? ordered && !runs : sh.aggregate != 0;
+    const bool agg = sh.aggregate < 0 ? ordered : sh.aggregate != 0;
     // The split histogram (u64, high words only, 4 bytes a cell; low halves
     // go to the global cells, and equal power-of-two masses have none).  At
     // g = 32 it fits one grid per CTA where the two-word one needs two
@@ -723,15 +602,6 @@ static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, const int
             if (e.g == 16) return launch_fast(deposit_fast_kernel<4, MODE, 4, false, true>);
             return launch_fast(deposit_fast_kernel<3, MODE, 4, false, true>);
         } else {
-            if (runs) {
-                if (e.g == 32) return launch_fast(deposit_runs_kernel<5, MODE, MODE == 1>);
-                if constexpr (MODE == 1) {
-                    if (split_small && e.g == 16) return launch_fast(deposit_runs_kernel<4, 1, true>);
-                    if (split_small) return launch_fast(deposit_runs_kernel<3, 1, true>);
-                }
-                if (e.g == 16) return launch_fast(deposit_runs_kernel<4, MODE, false>);
-                return launch_fast(deposit_runs_kernel<3, MODE, false>);
-            }
             if (e.g == 32) {
                 if constexpr (MODE == 1) {
                     if (ppt == 1) return launch_fast(deposit_fast_kernel<5, 1, 1, true>);
