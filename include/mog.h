@@ -133,6 +133,8 @@ typedef struct mog_tuning {
     int32_t learned_fold;           /* learned step: 0 (default) or 1 = the fft solve's epilogue
                                        writes the cell masses (one launch fewer at g = 8, 16),
                                        -1 = a separate pass                                     */
+    int32_t learned_ctas_per_sm;    /* learned kernel occupancy: 0 auto (2), 2 or 3 CTAs of 256
+                                       threads per SM (register budget 128, or 80 with spills) */
 } mog_tuning;
 
 /* Fill a config with the reference's in-code defaults (main.py:179-189). */

@@ -110,6 +110,7 @@ class MogTuningC(ctypes.Structure):
         ("update_threads", ctypes.c_int32),
         ("deposit_split", ctypes.c_int32),
         ("learned_fold", ctypes.c_int32),
+        ("learned_ctas_per_sm", ctypes.c_int32),
     ]
 
 

@@ -24,7 +24,7 @@ namespace {
 template <typename Acc>
 __global__ void __launch_bounds__(1024) conv_kernel(const Acc* __restrict__ mass,
                                                     float4* __restrict__ force, Ensemble e,
-                                                    float coef, int world_frame) {
+                                                    float coef, int frame) {
     extern __shared__ float msm[];
     const int lg = e.lg, g = 1 << lg;
     const int G3 = 1 << (3 * lg);
@@ -53,7 +53,7 @@ __global__ void __launch_bounds__(1024) conv_kernel(const Acc* __restrict__ mass
         fy *= coef;
         fz *= coef;
         float4 out;
-        if (world_frame) {
+        if (frame != kFrameGrid) {
             const float3 w = rotate_back(R, fx, fy, fz);
             out = make_float4(w.x, w.y, w.z, 0.f);
         } else {
@@ -61,7 +61,7 @@ __global__ void __launch_bounds__(1024) conv_kernel(const Acc* __restrict__ mass
                               __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, fx), __fmul_rn(fy, fy)),
                                                    __fmul_rn(fz, fz))));
         }
-        force[(size_t)i * G3 + t] = out;
+        force[(size_t)i * G3 + (frame == kFrameWorldSlot ? force_slot((uint32_t)t, lg) : (uint32_t)t)] = out;
     }
 }
 
@@ -74,8 +74,9 @@ __global__ void conv_check_total_kernel(Ensemble e) {
 
 }  // namespace
 
-cudaError_t launch_convolution(const Ensemble& e, void* mass, float4* force, bool world_frame,
+cudaError_t launch_convolution(const Ensemble& e, void* mass, float4* force, int frame,
                                bool zero_mass, cudaStream_t s) {
+    if (frame < kFrameGrid || frame > kFrameWorldSlot) return cudaErrorInvalidValue;
     const int G3 = 1 << (3 * e.lg);
     const size_t smem = (size_t)G3 * sizeof(float);
     if (smem > 200 * 1024) return cudaErrorInvalidValue;  // g <= 32
@@ -89,13 +90,13 @@ cudaError_t launch_convolution(const Ensemble& e, void* mass, float4* force, boo
         err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (err != cudaSuccess) return err;
         kern<<<e.k, threads, smem, s>>>(static_cast<unsigned long long*>(mass), force, e, coef,
-                                        world_frame ? 1 : 0);
+                                        frame);
     } else {
         auto kern = conv_kernel<unsigned>;
         err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (err != cudaSuccess) return err;
         kern<<<e.k, threads, smem, s>>>(static_cast<unsigned*>(mass), force, e, coef,
-                                        world_frame ? 1 : 0);
+                                        frame);
     }
     err = cudaGetLastError();
     if (err != cudaSuccess) return err;

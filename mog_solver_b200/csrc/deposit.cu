@@ -271,27 +271,45 @@ __device__ __forceinline__ unsigned atom_shared(uint32_t addr, unsigned v) {
 }
 
 // Shared-histogram word of a grid word w: the low 5 bits (the bank) XORed
-// with bits 5-9 and 10-14.  Cells of a compact region (a thin disk seen in
-// a rotated grid covers few distinct x) then spread over all 32 banks
-// instead of the few that their low x and y bits name.  An involution
-// (bits 5 and up are left alone), so the flush maps a word back to its
-// cell with the same function.
+// with bits 5-9.  Cells of a compact region (a thin disk seen in a rotated
+// grid covers few distinct x) then spread over all 32 banks instead of the
+// few that their low x and y bits name.  An involution (bits 5 and up are
+// left alone), so the flush maps a word back to its cell with the same
+// function.  hist_swizzle_bytes is the same map on byte offsets (4 w).
 __device__ __forceinline__ uint32_t hist_swizzle(uint32_t w) {
-    return w ^ (((w >> 5) ^ (w >> 10)) & 31u);
+    return w ^ ((w >> 5) & 31u);
+}
+__device__ __forceinline__ uint32_t hist_swizzle_bytes(uint32_t b) {
+    return b ^ ((b >> 5) & 124u);
 }
 
+// A grid's FAST index rows as the deposit keeps them in shared memory:
+// p0 = (r0.x, r1.x, r0.y, r1.y), p1 = (r0.z, r1.z, r0.w, r1.w), p2 = r2, so
+// that tx and ty come from paired FMAs (fma.rn.f32x2: two IEEE FMAs, each
+// rounded as the scalar one, in cell_fast's order).
+struct DepositRows {
+    float4 p0, p1, p2;
+};
+__device__ __forceinline__ DepositRows deposit_rows(const FastXf& f) {
+    const float4 r0 = f.row[0], r1 = f.row[1];
+    return {make_float4(r0.x, r1.x, r0.y, r1.y), make_float4(r0.z, r1.z, r0.w, r1.w), f.row[2]};
+}
+
+// 4 * (x | y << LG | z << 2 LG) of cell_fast's cell; cc[a] = the centred
+// coordinate a, duplicated into a pair.
 template <int LG>
-__device__ __forceinline__ uint32_t cell_byte_offset(const float4& r0, const float4& r1,
-                                                     const float4& r2, float cx, float cy,
-                                                     float cz) {
+__device__ __forceinline__ uint32_t cell_byte_offset(const DepositRows& r, const float2 (&cc)[3]) {
     constexpr uint32_t M = (1u << LG) - 1u;
-    const float tx = __fmaf_rn(r0.z, cz, __fmaf_rn(r0.y, cy, __fmaf_rn(r0.x, cx, r0.w)));
-    const float ty = __fmaf_rn(r1.z, cz, __fmaf_rn(r1.y, cy, __fmaf_rn(r1.x, cx, r1.w)));
-    const float tz = __fmaf_rn(r2.z, cz, __fmaf_rn(r2.y, cy, __fmaf_rn(r2.x, cx, r2.w)));
-    const uint32_t bx = __float_as_uint(__fadd_rd(tx, 12582912.0f));
-    const uint32_t by = __float_as_uint(__fadd_rd(ty, 12582912.0f));
-    const uint32_t bz = __float_as_uint(__fadd_rd(tz, 12582912.0f));
-    // 4 * (x | y << LG | z << 2 LG)
+    constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23, as floor_mod_pow2
+    const float2 txy =
+        __ffma2_rn(make_float2(r.p1.x, r.p1.y), cc[2],
+                   __ffma2_rn(make_float2(r.p0.z, r.p0.w), cc[1],
+                              __ffma2_rn(make_float2(r.p0.x, r.p0.y), cc[0], make_float2(r.p1.z, r.p1.w))));
+    const float tz =
+        __fmaf_rn(r.p2.z, cc[2].x, __fmaf_rn(r.p2.y, cc[1].x, __fmaf_rn(r.p2.x, cc[0].x, r.p2.w)));
+    const float2 bxy = __fadd2_rd(txy, make_float2(kMagic, kMagic));
+    const uint32_t bx = __float_as_uint(bxy.x), by = __float_as_uint(bxy.y);
+    const uint32_t bz = __float_as_uint(__fadd_rd(tz, kMagic));
     return ((bx & M) << 2) | ((by & M) << (LG + 2)) | ((bz & M) << (2 * LG + 2));
 }
 
@@ -316,14 +334,15 @@ __device__ __forceinline__ void deposit_fast_tile(const float4* __restrict__ pos
     using Acc = typename H::Acc;
     static_assert(!SPLIT || MODE == 1, "the split histogram is for u64 grids");
     constexpr int G3 = 1 << (3 * LG);
+    static_assert(sizeof(DepositRows) == 48, "DepositRows layout");
     const uint32_t words = (uint32_t)ng * G3;
-    float4* rows = reinterpret_cast<float4*>(smem_raw);                       // gpc * 3 rows
+    DepositRows* rows = reinterpret_cast<DepositRows*>(smem_raw);              // gpc rows
     unsigned* lo_w = reinterpret_cast<unsigned*>(smem_raw + (size_t)gpc * 48);
     unsigned* hi_w = SPLIT ? lo_w : lo_w + (size_t)gpc * G3;
     const uint32_t lo_base = (uint32_t)__cvta_generic_to_shared(lo_w);
     const uint32_t hi_base = (uint32_t)__cvta_generic_to_shared(hi_w);
 
-    for (int i = threadIdx.x; i < ng * 3; i += blockDim.x) rows[i] = e.fast[g0 + i / 3].row[i % 3];
+    for (int i = threadIdx.x; i < ng; i += blockDim.x) rows[i] = deposit_rows(e.fast[g0 + i]);
     for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) {
         lo_w[i] = 0u;
         if (H::kWords == 2 && !SPLIT) hi_w[i] = 0u;
@@ -336,7 +355,7 @@ __device__ __forceinline__ void deposit_fast_tile(const float4* __restrict__ pos
     double qsum = 0.0;
     for (int64_t base = lo; base < hi; base += (int64_t)T * PPT) {
         const bool full = base + (int64_t)T * PPT <= hi;  // block-uniform
-        float cx[PPT], cy[PPT], cz[PPT];
+        float2 cc[PPT][3];
         unsigned ql[PPT], qh[PPT];
 #pragma unroll
         for (int u = 0; u < PPT; ++u) {
@@ -353,9 +372,11 @@ __device__ __forceinline__ void deposit_fast_tile(const float4* __restrict__ pos
             qsum += (double)q;
             ql[u] = (unsigned)q;
             qh[u] = MODE == 1 ? (unsigned)((unsigned long long)q >> 32) : 0u;
-            cx[u] = __fsub_rn(P.x, half_l);
-            cy[u] = __fsub_rn(P.y, half_l);
-            cz[u] = __fsub_rn(P.z, half_l);
+            const float cx = __fsub_rn(P.x, half_l), cy = __fsub_rn(P.y, half_l),
+                        cz = __fsub_rn(P.z, half_l);
+            cc[u][0] = make_float2(cx, cx);
+            cc[u][1] = make_float2(cy, cy);
+            cc[u][2] = make_float2(cz, cz);
         }
         // one vote per batch: can the low words be skipped for the whole warp?
         bool hi_only = false;
@@ -365,14 +386,34 @@ __device__ __forceinline__ void deposit_fast_tile(const float4* __restrict__ pos
             for (int u = 0; u < PPT; ++u) any_lo |= ql[u];
             hi_only = __all_sync(kFull, any_lo == 0u);
         }
+        // the common case (equal power-of-two masses): one add of the high
+        // word per particle and grid, in a loop of its own
+        if (MODE == 1 && !SPLIT && hi_only) {
+            for (int j = 0; j < ng; ++j) {
+                const DepositRows r = rows[j];
+                const uint32_t gbyte = (uint32_t)j * (G3 * 4u);
+                const uint32_t base_j = hi_base + gbyte;
+#pragma unroll
+                for (int u = 0; u < PPT; ++u) {
+                    const uint32_t off = cell_byte_offset<LG>(r, cc[u]);
+                    if (!in_bounds(e.flags, (gbyte + off) >> 2, words)) continue;
+                    // for g >= 16 the grid's byte offset (bit 14 and up) lies
+                    // above the bits the swizzle reads and writes
+                    const uint32_t addr = LG >= 4 ? base_j + hist_swizzle_bytes(off)
+                                                  : hi_base + hist_swizzle_bytes(gbyte + off);
+                    if (qh[u]) red_shared(addr, qh[u]);
+                }
+            }
+            continue;
+        }
         for (int j = 0; j < ng; ++j) {
-            const float4 r0 = rows[3 * j], r1 = rows[3 * j + 1], r2 = rows[3 * j + 2];
+            const DepositRows r = rows[j];
             const uint32_t gbyte = (uint32_t)j * (G3 * 4u);
 #pragma unroll
             for (int u = 0; u < PPT; ++u) {
-                const uint32_t off = gbyte + cell_byte_offset<LG>(r0, r1, r2, cx[u], cy[u], cz[u]);
+                const uint32_t off = gbyte + cell_byte_offset<LG>(r, cc[u]);
                 if (!in_bounds(e.flags, off >> 2, words)) continue;
-                const uint32_t soff = hist_swizzle(off >> 2) << 2;  // the shared word's bytes
+                const uint32_t soff = hist_swizzle_bytes(off);  // the shared word's bytes
                 if (MODE == 0) {
                     if (ql[u]) red_shared(lo_base + soff, ql[u]);   // zero for padding lanes
                 } else if (SPLIT) {

@@ -59,6 +59,9 @@ __device__ __forceinline__ float gelu_grad(float x) {
 //   b0 = {W[n][k], W[n][k+1]} with n = nt*8 + l/4, k = ks*16 + 2*(l%4)
 //   b1 = the same at k + 8.
 // Stored as uint2 [ks][nt][32] so a warp reads 256 contiguous bytes.
+// Layer 1 carries its bias as input column 12 (the A tile holds a constant
+// 1 there); layers 2 and 3 are packed at half their weights, because the
+// activations they read are 2 gelu(x) (gelu2_h2).
 constexpr int kFrag1 = 1 * 8, kFrag2 = 4 * 8, kFrag3 = 4 * 1;  // (k-steps x n-tiles)
 constexpr int kFragTotal = (kFrag1 + kFrag2 + kFrag3) * 32;     // uint2 per model
 
@@ -67,19 +70,35 @@ __device__ __forceinline__ uint32_t pack_h2(float lo, float hi) {
     return *reinterpret_cast<const uint32_t*>(&v);
 }
 
-// GELU (tanh form) of two FP32 pre-activations, evaluated in packed FP16
-// (x * (c + c*0.044715*x^2), tanh.approx.f16x2, 0.5x + 0.5x*t): the result
-// is the FP16 A operand of the next layer either way.
-__device__ __forceinline__ uint32_t gelu_h2(float a, float b, uint32_t c1, uint32_t c2, uint32_t half) {
+// Twice the GELU (tanh form) of two FP32 pre-activations, evaluated in
+// packed FP16: u = x (c1 + c2 x^2), t = tanh.approx.f16x2(u), x + x t =
+// 2 gelu(x).  The result is the FP16 A operand of the next layer, whose
+// weights are packed at half their value; the factors of 2 are exact.
+__device__ __forceinline__ uint32_t gelu2_h2(float a, float b, uint32_t c1, uint32_t c2) {
     const uint32_t x = pack_h2(a, b);
-    uint32_t x2, p, u, t, hx, y;
+    uint32_t x2, p, u, t, y;
     asm("mul.rn.f16x2 %0, %1, %1;" : "=r"(x2) : "r"(x));
     asm("fma.rn.f16x2 %0, %1, %2, %3;" : "=r"(p) : "r"(x2), "r"(c2), "r"(c1));
     asm("mul.rn.f16x2 %0, %1, %2;" : "=r"(u) : "r"(x), "r"(p));
     asm("tanh.approx.f16x2 %0, %1;" : "=r"(t) : "r"(u));
-    asm("mul.rn.f16x2 %0, %1, %2;" : "=r"(hx) : "r"(x), "r"(half));
-    asm("fma.rn.f16x2 %0, %1, %2, %1;" : "=r"(y) : "r"(hx), "r"(t));
+    asm("fma.rn.f16x2 %0, %1, %2, %1;" : "=r"(y) : "r"(x), "r"(t));
     return y;
+}
+
+// (lo, hi) as FP16, values beyond the FP16 range clamped to its largest
+// finite value (cvt .satfinite).
+__device__ __forceinline__ uint32_t pack_h2_sat(float lo, float hi) {
+    uint32_t r;
+    asm("cvt.rn.satfinite.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+    return r;
+}
+
+// sqrt (sqrt.approx.f32, relative error about 2^-23) for the features,
+// which enter an FP16 network.
+__device__ __forceinline__ float sqrt_feature(float x) {
+    float r;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
 }
 
 __global__ void pack_fragments_kernel(const float* __restrict__ params, uint2* __restrict__ frags) {
@@ -100,7 +119,12 @@ __global__ void pack_fragments_kernel(const float* __restrict__ params, uint2* _
     nt = idx % ntiles;
     const int n = nt * 8 + (lane >> 2);
     const int k = ks * 16 + 2 * (lane & 3);
-    auto w = [&](int nn, int kk) { return (nn < out && kk < in) ? Wm[nn * in + kk] : 0.f; };
+    const float scale = Wm == params + kW1 ? 1.0f : 0.5f;
+    auto w = [&](int nn, int kk) {
+        if (nn >= out) return 0.f;
+        if (kk < in) return scale * Wm[nn * in + kk];
+        return (Wm == params + kW1 && kk == in) ? params[kB1 + nn] : 0.f;  // layer 1's bias column
+    };
     frags[t] = make_uint2(pack_h2(w(n, k), w(n, k + 1)), pack_h2(w(n, k + 8), w(n, k + 9)));
 }
 
@@ -242,7 +266,12 @@ __device__ __forceinline__ void gather_one(const GridRows& x, int i, const float
     a.rho = __fadd_rn(a.rho, f.w);
 }
 
-// Features from the sums over k grids of voxel size h.
+// Features from the sums over k grids of voxel size h.  EXACT_MEAN: the
+// mean force Fbar divides by k with IEEE division, bit-identical to the plain
+// gather's average (mog_features); otherwise it multiplies by 1/k (the same
+// value when k is a power of two).  Square roots, the logarithm and 1/det
+// use the approximate forms: the features enter an FP16 network.
+template <bool EXACT_MEAN>
 __device__ __forceinline__ void finish_features(const GatherAcc& a, int k, float h, float inv_fs,
                                                 float rho_ref, Features& out) {
     const float sx = a.s01.x, sy = a.s01.y, sz = a.sz, qx = a.q01.x, qy = a.q01.y, qz = a.qz;
@@ -252,7 +281,9 @@ __device__ __forceinline__ void finish_features(const GatherAcc& a, int k, float
                 fydy = a.fd_a.y, fydz = a.fd_c.y, fzdx = a.fd_d.x, fzdy = a.fd_d.y, fzdz = a.fzdz,
                 rho = a.rho;
     const float kf = (float)k, ik = 1.0f / kf;
-    const float mx = __fdiv_rn(sx, kf), my = __fdiv_rn(sy, kf), mz = __fdiv_rn(sz, kf);
+    const float mx = EXACT_MEAN ? __fdiv_rn(sx, kf) : sx * ik;
+    const float my = EXACT_MEAN ? __fdiv_rn(sy, kf) : sy * ik;
+    const float mz = EXACT_MEAN ? __fdiv_rn(sz, kf) : sz * ik;
     const float ax_ = dx * ik, ay_ = dy * ik, az_ = dz * ik;  // dbar
     const float ridge = 1e-3f * h * h;
     const float cxx = dxx * ik - ax_ * ax_ + ridge, cxy = dxy * ik - ax_ * ay_,
@@ -264,7 +295,7 @@ __device__ __forceinline__ void finish_features(const GatherAcc& a, int k, float
     const float det = cxx * A00 + cxy * A01 + cxz * A02;
     float wx = 0.f, wy = 0.f, wz = 0.f;
     if (det > 0.f) {
-        const float id = 1.0f / det;
+        const float id = __frcp_rn(det);
         wx = (A00 * ax_ + A01 * ay_ + A02 * az_) * id;
         wy = (A01 * ax_ + A11 * ay_ + A12 * az_) * id;
         wz = (A02 * ax_ + A12 * ay_ + A22 * az_) * id;
@@ -282,12 +313,12 @@ __device__ __forceinline__ void finish_features(const GatherAcc& a, int k, float
     out.f[3] = out.ex * inv_fs;
     out.f[4] = out.ey * inv_fs;
     out.f[5] = out.ez * inv_fs;
-    out.f[6] = sqrtf(fmaxf(qx * ik - mx * mx, 0.f)) * inv_fs;
-    out.f[7] = sqrtf(fmaxf(qy * ik - my * my, 0.f)) * inv_fs;
-    out.f[8] = sqrtf(fmaxf(qz * ik - mz * mz, 0.f)) * inv_fs;
-    out.f[9] = log1pf(rho * ik / rho_ref);
-    out.f[10] = sqrtf(mx * mx + my * my + mz * mz) * inv_fs;
-    out.f[11] = sqrtf(fmaxf(cxx + cyy + czz - 3.f * ridge, 0.f)) / h;
+    out.f[6] = sqrt_feature(fmaxf(qx * ik - mx * mx, 0.f)) * inv_fs;
+    out.f[7] = sqrt_feature(fmaxf(qy * ik - my * my, 0.f)) * inv_fs;
+    out.f[8] = sqrt_feature(fmaxf(qz * ik - mz * mz, 0.f)) * inv_fs;
+    out.f[9] = __logf(1.0f + rho * ik / rho_ref);
+    out.f[10] = sqrt_feature(mx * mx + my * my + mz * mz) * inv_fs;
+    out.f[11] = sqrt_feature(fmaxf(cxx + cyy + czz - 3.f * ridge, 0.f)) * (1.0f / h);
 }
 
 // The network on one m16 tile of a warp: A fragment (a0..a3) of the
@@ -299,22 +330,21 @@ __device__ __forceinline__ void mlp_tile(const uint2* __restrict__ sf, const flo
     const int tg = lane & 3;
     const uint32_t c1 = pack_h2(0.7978845608028654f, 0.7978845608028654f);
     const uint32_t c2 = pack_h2(0.7978845608028654f * 0.044715f, 0.7978845608028654f * 0.044715f);
-    const uint32_t hf = pack_h2(0.5f, 0.5f);
     float h[8][4];
 #pragma unroll
     for (int nt = 0; nt < 8; ++nt) {
-        const float b0 = sb[nt * 8 + 2 * tg], b1 = sb[nt * 8 + 2 * tg + 1];
-        h[nt][0] = b0; h[nt][1] = b1; h[nt][2] = b0; h[nt][3] = b1;
+        // layer 1's bias comes in through the constant input column
+        h[nt][0] = h[nt][1] = h[nt][2] = h[nt][3] = 0.f;
         const uint2 w = sf[(0 * 8 + nt) * 32 + lane];
         mma_f16(h[nt], a0, a1, a2, a3, w.x, w.y);
     }
     uint32_t A[4][4];
 #pragma unroll
     for (int ks = 0; ks < 4; ++ks) {
-        A[ks][0] = gelu_h2(h[2 * ks][0], h[2 * ks][1], c1, c2, hf);
-        A[ks][1] = gelu_h2(h[2 * ks][2], h[2 * ks][3], c1, c2, hf);
-        A[ks][2] = gelu_h2(h[2 * ks + 1][0], h[2 * ks + 1][1], c1, c2, hf);
-        A[ks][3] = gelu_h2(h[2 * ks + 1][2], h[2 * ks + 1][3], c1, c2, hf);
+        A[ks][0] = gelu2_h2(h[2 * ks][0], h[2 * ks][1], c1, c2);
+        A[ks][1] = gelu2_h2(h[2 * ks][2], h[2 * ks][3], c1, c2);
+        A[ks][2] = gelu2_h2(h[2 * ks + 1][0], h[2 * ks + 1][1], c1, c2);
+        A[ks][3] = gelu2_h2(h[2 * ks + 1][2], h[2 * ks + 1][3], c1, c2);
     }
 #pragma unroll
     for (int nt = 0; nt < 8; ++nt) {
@@ -328,10 +358,10 @@ __device__ __forceinline__ void mlp_tile(const uint2* __restrict__ sf, const flo
     }
 #pragma unroll
     for (int ks = 0; ks < 4; ++ks) {
-        A[ks][0] = gelu_h2(h[2 * ks][0], h[2 * ks][1], c1, c2, hf);
-        A[ks][1] = gelu_h2(h[2 * ks][2], h[2 * ks][3], c1, c2, hf);
-        A[ks][2] = gelu_h2(h[2 * ks + 1][0], h[2 * ks + 1][1], c1, c2, hf);
-        A[ks][3] = gelu_h2(h[2 * ks + 1][2], h[2 * ks + 1][3], c1, c2, hf);
+        A[ks][0] = gelu2_h2(h[2 * ks][0], h[2 * ks][1], c1, c2);
+        A[ks][1] = gelu2_h2(h[2 * ks][2], h[2 * ks][3], c1, c2);
+        A[ks][2] = gelu2_h2(h[2 * ks + 1][0], h[2 * ks + 1][1], c1, c2);
+        A[ks][3] = gelu2_h2(h[2 * ks + 1][2], h[2 * ks + 1][3], c1, c2);
     }
     y[0] = sb[2 * kH + 2 * tg];
     y[1] = sb[2 * kH + 2 * tg + 1];
@@ -365,8 +395,8 @@ struct GridTable {
 
 // K > 0: k == K and the rows come from `tab`; K == 0: any k, rows staged in
 // shared memory.
-template <int IDX, int LG, int OUT, int K>
-__global__ void __launch_bounds__(kLT, 2) learned_kernel(
+template <int IDX, int LG, int OUT, int K, int MINB = 2>
+__global__ void __launch_bounds__(kLT, MINB) learned_kernel(
     float4* __restrict__ pos, float4* __restrict__ vel, int64_t n, const float4* __restrict__ W,
     Ensemble e, ModelNorm norm, const uint2* __restrict__ frags, const float* __restrict__ params,
     float dt, float damp, float4* __restrict__ out4, float* __restrict__ feat_out,
@@ -414,7 +444,7 @@ __global__ void __launch_bounds__(kLT, 2) learned_kernel(
             for (int i = 0; i < e.k; ++i) gather_one<IDX, LG>(xf[i], i, W, e, ip, cx, cy, cz, cc, acc);
         }
         Features F;
-        finish_features(acc, e.k, e.voxel, inv_fs, norm.rho_ref, F);
+        finish_features<OUT == 2>(acc, e.k, e.voxel, inv_fs, norm.rho_ref, F);
         float z[kIn];
 #pragma unroll
         for (int j = 0; j < kIn; ++j) z[j] = (F.f[j] - norm.mu[j]) * norm.inv_sigma[j];
@@ -429,14 +459,11 @@ __global__ void __launch_bounds__(kLT, 2) learned_kernel(
             }
         } else {
             // this particle's row of the warp's A tile (FP16 pairs, clamped to the
-            // FP16 range; columns 12-15 zero)
-            float zc[kIn];
-#pragma unroll
-            for (int j = 0; j < kIn; ++j) zc[j] = fminf(fmaxf(z[j], -60000.f), 60000.f);
+            // FP16 range; column 12 the constant 1 of layer 1's bias, 13-15 zero)
             uint4* row = reinterpret_cast<uint4*>(A + lane * kARow);
-            row[0] = make_uint4(pack_h2(zc[0], zc[1]), pack_h2(zc[2], zc[3]), pack_h2(zc[4], zc[5]),
-                                pack_h2(zc[6], zc[7]));
-            row[1] = make_uint4(pack_h2(zc[8], zc[9]), pack_h2(zc[10], zc[11]), 0u, 0u);
+            row[0] = make_uint4(pack_h2_sat(z[0], z[1]), pack_h2_sat(z[2], z[3]),
+                                pack_h2_sat(z[4], z[5]), pack_h2_sat(z[6], z[7]));
+            row[1] = make_uint4(pack_h2_sat(z[8], z[9]), pack_h2_sat(z[10], z[11]), 0x3c00u, 0u);
             __syncwarp();
 #pragma unroll
             for (int m = 0; m < 2; ++m) {
@@ -686,8 +713,11 @@ template <int IDX, int LG, int OUT, int K>
 cudaError_t launch_learned_t(const Ensemble& e, const GridRows* rows, float4* pos, float4* vel,
                              int64_t n, const float4* W, const ModelNorm& norm, const void* frags,
                              const float* params, float dt, float damp, LearnedOut& out,
-                             cudaStream_t s) {
-    auto kern = learned_kernel<IDX, LG, OUT, K>;
+                             cudaStream_t s, int ctas_per_sm) {
+    // three CTAs per SM (80 registers, some spilled) on request, where the
+    // rows are launch parameters
+    auto kern = (K > 0 && ctas_per_sm == 3) ? learned_kernel<IDX, LG, OUT, K, 3>
+                                            : learned_kernel<IDX, LG, OUT, K, 2>;
     GridTable<K> tab{};
     if (K > 0)
         for (int i = 0; i < K; ++i) tab.r[i] = rows[i];
@@ -709,11 +739,11 @@ template <int IDX, int LG, int K>
 cudaError_t launch_learned_i(int out_mode, const Ensemble& e, const GridRows* rows, float4* pos,
                              float4* vel, int64_t n, const float4* W, const ModelNorm& norm,
                              const void* frags, const float* params, float dt, float damp,
-                             LearnedOut& out, cudaStream_t s) {
+                             LearnedOut& out, cudaStream_t s, int cps) {
     switch (out_mode) {
-        case 0: return launch_learned_t<IDX, LG, 0, K>(e, rows, pos, vel, n, W, norm, frags, params, dt, damp, out, s);
-        case 1: return launch_learned_t<IDX, LG, 1, K>(e, rows, pos, vel, n, W, norm, frags, params, dt, damp, out, s);
-        default: return launch_learned_t<IDX, LG, 2, K>(e, rows, pos, vel, n, W, norm, frags, params, dt, damp, out, s);
+        case 0: return launch_learned_t<IDX, LG, 0, K>(e, rows, pos, vel, n, W, norm, frags, params, dt, damp, out, s, cps);
+        case 1: return launch_learned_t<IDX, LG, 1, K>(e, rows, pos, vel, n, W, norm, frags, params, dt, damp, out, s, cps);
+        default: return launch_learned_t<IDX, LG, 2, K>(e, rows, pos, vel, n, W, norm, frags, params, dt, damp, out, s, cps);
     }
 }
 }  // namespace
@@ -721,11 +751,12 @@ cudaError_t launch_learned_i(int out_mode, const Ensemble& e, const GridRows* ro
 cudaError_t launch_learned(int out_mode, const Ensemble& e, const GridRows* rows, float4* pos,
                            float4* vel, int64_t n, const float4* W, const ModelNorm& norm,
                            const void* frags, const float* params, float dt, float damp,
-                           LearnedOut& out, cudaStream_t s) {
+                           LearnedOut& out, cudaStream_t s, int ctas_per_sm) {
     out.blocks = 0;
     if (n <= 0) return cudaSuccess;
 #define MOG_LEARNED(IDX, LG, K) \
-    return launch_learned_i<IDX, LG, K>(out_mode, e, rows, pos, vel, n, W, norm, frags, params, dt, damp, out, s)
+    return launch_learned_i<IDX, LG, K>(out_mode, e, rows, pos, vel, n, W, norm, frags, params, dt, damp, out, s, \
+                                        ctas_per_sm)
     // the k = 32, g = 16 FAST ensemble (the cheap ensemble the models are
     // trained for) gets its rows as launch parameters and an unrolled loop
     if (e.index_mode == 0 && e.lg == 4 && e.k == 32 && rows) MOG_LEARNED(0, 4, 32);

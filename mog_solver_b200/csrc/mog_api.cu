@@ -190,6 +190,7 @@ struct mog_handle {
     int64_t perm_n = -1;         // n the permutation was built for
     int sort_every = 0;          // re-order every this many steps (0 = never)
     int learned_fold = 1;        // learned step: cell masses written by the solve's epilogue
+    int learned_ctas = 2;        // learned kernel CTAs per SM (2 or 3)
     uint64_t step_count = 0;     // steps issued (decides when to re-order)
     std::vector<GraphEntry> graphs;
     std::vector<mog::GridRows> rows;  // learned-gather rows of the k grids (host)
@@ -378,9 +379,9 @@ int run_pipeline(mog_handle* h, float4* pos, float4* vel, int64_t n, float dt, f
                           : mog::launch_deposit(e, pos, nullptr, n, false, h->d_mass, h->dshape, s);
     if (err != cudaSuccess) return cuda_fail(err, "deposit");
     if (h->cfg.solver == MOG_SOLVER_FFT)
-        err = mog::launch_spectral(e, h->d_mass, h->d_force, true, true, h->d_scratch, s);
+        err = mog::launch_spectral(e, h->d_mass, h->d_force, mog::kFrameWorldSlot, true, h->d_scratch, s);
     else
-        err = mog::launch_convolution(e, h->d_mass, h->d_force, true, true, s);
+        err = mog::launch_convolution(e, h->d_mass, h->d_force, mog::kFrameWorldSlot, true, s);
     if (err != cudaSuccess) return cuda_fail(err, "solve");
     err = mog::launch_update(e, pos, vel, pos_s, perm, n, h->d_force, dt, h->cfg.damping, acc,
                              h->ushape, s);
@@ -689,8 +690,8 @@ int mog_step_profiled(mog_handle* h, float* pos4, float* vel4, int64_t n, float 
     if (!err) err = cudaEventRecord(ev[2], s);
     if (!err)
         err = h->cfg.solver == MOG_SOLVER_FFT
-                  ? mog::launch_spectral(e, h->d_mass, h->d_force, true, true, h->d_scratch, s)
-                  : mog::launch_convolution(e, h->d_mass, h->d_force, true, true, s);
+                  ? mog::launch_spectral(e, h->d_mass, h->d_force, mog::kFrameWorldSlot, true, h->d_scratch, s)
+                  : mog::launch_convolution(e, h->d_mass, h->d_force, mog::kFrameWorldSlot, true, s);
     if (!err) err = cudaEventRecord(ev[3], s);
     if (!err)
         err = mog::launch_update(e, pos, vel, pos_s, perm, n, h->d_force, dt_eff, h->cfg.damping,
@@ -748,11 +749,11 @@ int mog_solve(mog_handle* h, const void* mass_in, float* force4_out, void* strea
     cudaError_t err;
     if (h->cfg.solver == MOG_SOLVER_FFT)
         err = mog::launch_spectral(h->e, const_cast<void*>(mass_in),
-                                   reinterpret_cast<float4*>(force4_out), false, false,
+                                   reinterpret_cast<float4*>(force4_out), mog::kFrameGrid, false,
                                    h->d_scratch, s);
     else
         err = mog::launch_convolution(h->e, const_cast<void*>(mass_in),
-                                      reinterpret_cast<float4*>(force4_out), false, false, s);
+                                      reinterpret_cast<float4*>(force4_out), mog::kFrameGrid, false, s);
     if (err != cudaSuccess) return cuda_fail(err, "solve");
     return MOG_OK;
 }
@@ -796,6 +797,7 @@ int mog_get_tuning(const mog_handle* h, mog_tuning* out) {
     out->update_direct_ppt = h->ushape.direct_ppt;
     out->deposit_split = h->dshape.split;
     out->learned_fold = h->learned_fold ? 1 : -1;
+    out->learned_ctas_per_sm = h->learned_ctas;
     return MOG_OK;
 }
 
@@ -813,7 +815,8 @@ int mog_set_tuning(mog_handle* h, const mog_tuning* t) {
         (t->update_direct_ppt != 0 && t->update_direct_ppt != 1 && t->update_direct_ppt != 2 &&
          t->update_direct_ppt != 4) ||
         t->deposit_split < -1 || t->deposit_split > 1 || t->learned_fold < -1 ||
-        t->learned_fold > 1)
+        t->learned_fold > 1 ||
+        (t->learned_ctas_per_sm != 0 && t->learned_ctas_per_sm != 2 && t->learned_ctas_per_sm != 3))
         return fail(MOG_ERR_ARG, "tuning value out of range");
     h->dshape.threads = t->deposit_threads ? t->deposit_threads : 1024;
     h->dshape.grids_per_cta = t->deposit_grids_per_cta;
@@ -829,6 +832,7 @@ int mog_set_tuning(mog_handle* h, const mog_tuning* t) {
     h->ushape.threads = t->update_threads ? t->update_threads : 512;
     h->dshape.split = t->deposit_split;
     h->learned_fold = t->learned_fold >= 0 ? 1 : 0;
+    h->learned_ctas = t->learned_ctas_per_sm ? t->learned_ctas_per_sm : 2;
     for (auto& g : h->graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);
     h->graphs.clear();
@@ -1011,8 +1015,8 @@ int mog_shard_finish(mog_handle* h, float* pos4, float* vel4, int64_t n, float d
     if ((rc = order_particles(h, pos, n, wants_sort(h, n), s, &perm, &pos_s))) return rc;
     const mog::Ensemble& e = h->e;
     cudaError_t err = h->cfg.solver == MOG_SOLVER_FFT
-                          ? mog::launch_spectral(e, h->d_mass, h->d_force, true, true, h->d_scratch, s)
-                          : mog::launch_convolution(e, h->d_mass, h->d_force, true, true, s);
+                          ? mog::launch_spectral(e, h->d_mass, h->d_force, mog::kFrameWorldSlot, true, h->d_scratch, s)
+                          : mog::launch_convolution(e, h->d_mass, h->d_force, mog::kFrameWorldSlot, true, s);
     if (err != cudaSuccess) return cuda_fail(err, "solve");
     err = mog::launch_update(e, pos, reinterpret_cast<float4*>(vel4), pos_s, perm, n, h->d_force,
                              dt_eff, h->cfg.damping, nullptr, h->ushape, s);
@@ -1154,9 +1158,9 @@ static int run_learned(mog_handle* h, const mog_model* m, int out_mode, float* p
         if (ev && (err = cudaEventRecord(ev[2], s))) return cuda_fail(err, "event");
     } else {
         if (h->cfg.solver == MOG_SOLVER_FFT)
-            err = mog::launch_spectral(e, h->d_mass, h->d_force, true, false, h->d_scratch, s);
+            err = mog::launch_spectral(e, h->d_mass, h->d_force, mog::kFrameWorld, false, h->d_scratch, s);
         else
-            err = mog::launch_convolution(e, h->d_mass, h->d_force, true, false, s);
+            err = mog::launch_convolution(e, h->d_mass, h->d_force, mog::kFrameWorld, false, s);
         if (err != cudaSuccess) return cuda_fail(err, "solve");
         if (ev && (err = cudaEventRecord(ev[2], s))) return cuda_fail(err, "event");
         err = mog::launch_density_w(e, h->d_mass, h->d_force, s);
@@ -1172,7 +1176,7 @@ static int run_learned(mog_handle* h, const mog_model* m, int out_mode, float* p
     }
     err = mog::launch_learned(out_mode, e, h->rows.data(), reinterpret_cast<float4*>(pos4),
                               reinterpret_cast<float4*>(vel4), n, h->d_force, m->norm, m->d_frags,
-                              m->d_params, dt, h->cfg.damping, out, s);
+                              m->d_params, dt, h->cfg.damping, out, s, h->learned_ctas);
     if (err != cudaSuccess) return cuda_fail(err, "learned kernel");
     if (ev && (err = cudaEventRecord(ev[4], s))) return cuda_fail(err, "event");
     if (out_mode == 0) {
@@ -1258,14 +1262,14 @@ static int run_host_step(mog_handle* h, const mog_model* m, float* pos_host, flo
             err = mog::launch_spectral_density(e, h->d_mass, h->d_force, h->d_scratch, s);
         } else {
             err = h->cfg.solver == MOG_SOLVER_FFT
-                      ? mog::launch_spectral(e, h->d_mass, h->d_force, true, false, h->d_scratch, s)
-                      : mog::launch_convolution(e, h->d_mass, h->d_force, true, false, s);
+                      ? mog::launch_spectral(e, h->d_mass, h->d_force, mog::kFrameWorld, false, h->d_scratch, s)
+                      : mog::launch_convolution(e, h->d_mass, h->d_force, mog::kFrameWorld, false, s);
             if (!err) err = mog::launch_density_w(e, h->d_mass, h->d_force, s);
         }
     } else {
         err = h->cfg.solver == MOG_SOLVER_FFT
-                  ? mog::launch_spectral(e, h->d_mass, h->d_force, true, true, h->d_scratch, s)
-                  : mog::launch_convolution(e, h->d_mass, h->d_force, true, true, s);
+                  ? mog::launch_spectral(e, h->d_mass, h->d_force, mog::kFrameWorldSlot, true, h->d_scratch, s)
+                  : mog::launch_convolution(e, h->d_mass, h->d_force, mog::kFrameWorldSlot, true, s);
     }
     if (err) return cuda_fail(err, "solve");
     int used = 0;  // spread partial sums written so far (one per learned CTA)
@@ -1281,7 +1285,7 @@ static int run_host_step(mog_handle* h, const mog_model* m, float* pos_host, flo
                 out.spread_cap = h->spread_cap - used;
                 err = mog::launch_learned(0, e, h->rows.data(), h->d_hpos + lo, h->d_hvel + lo, cnt,
                                           h->d_force, m->norm, m->d_frags, m->d_params, dt,
-                                          h->cfg.damping, out, s);
+                                          h->cfg.damping, out, s, h->learned_ctas);
                 used += out.blocks;
             } else if (!err) {
                 err = mog::launch_update(e, h->d_hpos, h->d_hvel, nullptr, nullptr, n, h->d_force, dt,
@@ -1652,7 +1656,7 @@ int capture_queue_step(mog_batch* b, float* const* pos4, float* const* vel4, con
     for (int i = 0; i < count && !err; ++i) {
         mog_handle* h = b->sims[i];
         err = cudaStreamWaitEvent(b->branch[i], b->fork, 0);
-        if (!err) err = mog::launch_spectral(h->e, h->d_mass, h->d_force, true, true, h->d_scratch,
+        if (!err) err = mog::launch_spectral(h->e, h->d_mass, h->d_force, mog::kFrameWorldSlot, true, h->d_scratch,
                                              b->branch[i]);
         if (!err) err = cudaEventRecord(b->done[i], b->branch[i]);
         if (!err) err = cudaStreamWaitEvent(b->cap, b->done[i], 0);

@@ -60,6 +60,39 @@ __device__ __forceinline__ uint32_t cell_fast(const float4& r0, const float4& r1
     return ix | (iy << lg) | (iz << (2 * lg));
 }
 
+// Slot of cell c = x | y << lg | z << 2 lg in a kFrameWorldSlot force grid:
+// x XORed with (2y ^ 4z) mod 8 (and mod g).  A staged grid puts 8 cells
+// (128 bytes) across the 32 banks, so cell c and its y and z neighbours
+// (g and g^2 cells away, multiples of 8 for g >= 8) would share a 16-byte
+// bank quad; with the slot, the cells of any 2 x 2 x 2 block sit in 8
+// different quads.  x-rows and their aligned 8-cell blocks stay in place,
+// so slabs and 128-byte lines are copied as before.  Its own inverse.
+__host__ __device__ __forceinline__ uint32_t force_slot(uint32_t c, int lg) {
+    const uint32_t mask = (1u << lg) - 1u;
+    const uint32_t s = ((c >> (lg - 1)) & 6u) ^ ((c >> (2 * lg - 2)) & 4u);
+    return c ^ (s & mask);
+}
+
+// force_slot of the cell whose x, y, z are the low lg bits of bx, by, bz
+// (higher bits ignored).
+__device__ __forceinline__ uint32_t force_slot_xyz(uint32_t bx, uint32_t by, uint32_t bz, int lg) {
+    const uint32_t mask = (1u << lg) - 1u;
+    const uint32_t x = (bx ^ (((by << 1) ^ (bz << 2)) & 7u)) & mask;
+    return x | ((by & mask) << lg) | ((bz & mask) << (2 * lg));
+}
+
+// force_slot(cell_fast(...)).
+__device__ __forceinline__ uint32_t slot_fast(const float4& r0, const float4& r1,
+                                              const float4& r2, float cx, float cy,
+                                              float cz, int lg) {
+    const float tx = __fmaf_rn(r0.z, cz, __fmaf_rn(r0.y, cy, __fmaf_rn(r0.x, cx, r0.w)));
+    const float ty = __fmaf_rn(r1.z, cz, __fmaf_rn(r1.y, cy, __fmaf_rn(r1.x, cx, r1.w)));
+    const float tz = __fmaf_rn(r2.z, cz, __fmaf_rn(r2.y, cy, __fmaf_rn(r2.x, cx, r2.w)));
+    return force_slot_xyz(__float_as_uint(__fadd_rd(tx, 12582912.0f)),
+                          __float_as_uint(__fadd_rd(ty, 12582912.0f)),
+                          __float_as_uint(__fadd_rd(tz, 12582912.0f)), lg);
+}
+
 // EXACT mode cell index.  R is the packed rotation of one grid,
 // R[4j + r] = M[j][r]; the shader's mat3 has columns R[4j..4j+2], so
 // rotated_r = (R[r]*c.x + R[4+r]*c.y) + R[8+r]*c.z  (GLSL mat3 * vec3).

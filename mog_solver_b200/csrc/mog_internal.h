@@ -99,19 +99,27 @@ cudaError_t launch_deposit(const Ensemble& e, const float4* pos, const int* perm
                            bool ordered, void* mass, const DepositShape& shape, cudaStream_t s,
                            bool shard = false);
 
-// force grid (float4 per cell) <- mass grid.  world_frame: rotate each
-// cell's force by M_i and store (x, y, z, 0) — what the production gather
-// reads; otherwise store (fx, fy, fz, |f|) in the grid's own frame (the
-// reference's gradient texture).  zero_mass clears the input for the next
-// step.  scratch: device memory of spectral_scratch_bytes(e) bytes.
-cudaError_t launch_spectral(const Ensemble& e, void* mass, float4* force, bool world_frame,
+// Layout of a solve's force grid (float4 per cell).
+//   kFrameGrid      (fx, fy, fz, |f|) in each grid's own frame at cell c
+//                   (the reference's gradient texture, the stage entry points);
+//   kFrameWorld     M_i f as (x, y, z, 0) at cell c (the learned path's
+//                   gather, which reads it from L1/L2);
+//   kFrameWorldSlot M_i f as (x, y, z, 0) at force_slot(c) (the plain
+//                   gathers, which stage whole grids in shared memory).
+constexpr int kFrameGrid = 0;
+constexpr int kFrameWorld = 1;
+constexpr int kFrameWorldSlot = 2;
+
+// force grid <- mass grid in the layout `frame` names.  zero_mass clears
+// the input for the next step.  scratch: device memory of
+// spectral_scratch_bytes(e) bytes.
+cudaError_t launch_spectral(const Ensemble& e, void* mass, float4* force, int frame,
                             bool zero_mass, void* scratch, cudaStream_t s);
 size_t spectral_scratch_bytes(const Ensemble& e);
 
-cudaError_t launch_convolution(const Ensemble& e, void* mass, float4* force, bool world_frame,
+cudaError_t launch_convolution(const Ensemble& e, void* mass, float4* force, int frame,
                                bool zero_mass, cudaStream_t s);
 
-// Rotate a grid-frame force grid into the world frame (stage entry point).
 // Tensor-core DFT passes (dft_tc.cu), g = 16 or 32: host-built B tables
 // (forward hi, lo, inverse hi, lo; BF16 bits) and one in-place axis pass
 // over the lines of nf fields of pairs x g^3 complex values.
@@ -122,11 +130,14 @@ cudaError_t launch_dft_tc(int g, float2* f0, float2* f1, float2* f2, int nf, int
 // force grid's .w lane and clears the mass grid (the learned path).
 cudaError_t launch_spectral_density(const Ensemble& e, void* mass, float4* force, void* scratch,
                                     cudaStream_t s);
+// Rotate a grid-frame force grid (kFrameGrid) into the world frame, stored
+// as kFrameWorldSlot for launch_update (the stage entry point mog_update).
 cudaError_t launch_prerotate(const Ensemble& e, const float4* force_grid, float4* force_world,
                              cudaStream_t s);
 
-// Gather + average + (optionally) leapfrog.  When acc_out is non-null the
-// averaged force is written there and pos/vel are left untouched.
+// Gather + average + (optionally) leapfrog from a kFrameWorldSlot grid.
+// When acc_out is non-null the averaged force is written there and pos/vel
+// are left untouched.
 // pos_sorted (nullable): pos[perm[s]] for every slot s, from which the
 // cells are computed; the caller's pos/vel are read and written once per
 // particle through perm.
@@ -284,7 +295,7 @@ struct LearnedOut {
 cudaError_t launch_learned(int out_mode, const Ensemble& e, const GridRows* rows, float4* pos,
                            float4* vel, int64_t n, const float4* W, const ModelNorm& norm,
                            const void* frags, const float* params, float dt, float damp,
-                           LearnedOut& out, cudaStream_t s);
+                           LearnedOut& out, cudaStream_t s, int ctas_per_sm = 2);
 cudaError_t launch_pack_fragments(const float* params, void* frags, cudaStream_t s);
 cudaError_t launch_mlp_train_step(const float* feat, const float* target, const int* idx,
                                   int batch, float* params, float* partial, float* loss_partial,

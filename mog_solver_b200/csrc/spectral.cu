@@ -91,7 +91,7 @@ __device__ __forceinline__ Bins gradient_bins(float2 own, float2 mir, float gk, 
 // Shared layout: three complex fields [z][y][x] with rows padded to g+1
 // elements so that row-wise (x) and column-wise (y, z) passes are
 // bank-conflict free.
-template <int G, typename Acc, bool WORLD, bool ZERO>
+template <int G, typename Acc, bool WORLD, bool ZERO, bool SWZ = false>
 __global__ void __launch_bounds__(G * G, (G == 16 ? 2 : 1))
     spectral_fused_kernel(Acc* __restrict__ mass, float4* __restrict__ force, Ensemble e) {
     constexpr int P = G + 1, BUF = G * G * P, G3 = G * G * G;
@@ -209,10 +209,12 @@ __global__ void __launch_bounds__(G * G, (G == 16 ? 2 : 1))
 #pragma unroll
             for (int q = 0; q < 12; ++q) R[q] = __ldg(e.rot12 + 12 * ga + q);
         }
+        // SWZ: force_slot(row + x) = row + (x ^ sx)
+        const int sx = SWZ ? (((y << 1) ^ (z << 2)) & 7 & (G - 1)) : 0;
         float4* fa = force + (size_t)ga * G3 + row;
 #pragma unroll
         for (int x = 0; x < G; ++x)
-            fa[x] = make_out(WORLD, R, (e.alias_xz ? r2[x].x : r[x].x) * invn, r[x].y * invn,
+            fa[x ^ sx] = make_out(WORLD, R, (e.alias_xz ? r2[x].x : r[x].x) * invn, r[x].y * invn,
                              r2[x].x * invn);
         if (hasb) {
 #pragma unroll
@@ -225,7 +227,7 @@ __global__ void __launch_bounds__(G * G, (G == 16 ? 2 : 1))
             float4* fb = force + (size_t)gb * G3 + row;
 #pragma unroll
             for (int x = 0; x < G; ++x)
-                fb[x] = make_out(WORLD, R, (e.alias_xz ? r2[x].y : r[x].x) * invn, r[x].y * invn,
+                fb[x ^ sx] = make_out(WORLD, R, (e.alias_xz ? r2[x].y : r[x].x) * invn, r[x].y * invn,
                                  r2[x].y * invn);
         }
     }
@@ -240,10 +242,11 @@ __global__ void __launch_bounds__(G * G, (G == 16 ? 2 : 1))
 // DENS (with WORLD, without ZERO): the epilogue also puts each cell's mass
 // into the .w lane of its world-frame force and clears the mass grid (the
 // learned path's gather reads both from one float4).
-template <int G, typename Acc, bool WORLD, bool ZERO, bool DENS = false>
+template <int G, typename Acc, bool WORLD, bool ZERO, bool DENS = false, bool SWZ = false>
 __global__ void __launch_bounds__(3 * G * G, (G == 16 ? 1 : 4))
     spectral_fused3_kernel(Acc* __restrict__ mass, float4* __restrict__ force, Ensemble e) {
-    static_assert(!DENS || (WORLD && !ZERO), "cell masses go with world-frame forces");
+    static_assert(!DENS || (WORLD && !ZERO && !SWZ), "cell masses go with kFrameWorld forces");
+    static_assert(!SWZ || WORLD, "slots are a world-frame layout");
     constexpr int P = G + 1, BUF = G * G * P, G3 = G * G * G, L = G * G;
     extern __shared__ float2 sm[];
     __shared__ float Rs[2][12];
@@ -374,7 +377,7 @@ __global__ void __launch_bounds__(3 * G * G, (G == 16 ? 1 : 4))
             o.w = mass_value(*mc, e.inv_scale);
             *mc = 0;
         }
-        force[(size_t)(ga + gsel) * G3 + c] = o;
+        force[(size_t)(ga + gsel) * G3 + (SWZ ? force_slot((uint32_t)c, ilog2<G>()) : (uint32_t)c)] = o;
     }
 }
 
@@ -472,7 +475,7 @@ __global__ void __launch_bounds__(256) mp_green_kernel(const float2* __restrict_
     Z3[idx] = b.z3;
 }
 
-template <int G, bool WORLD>
+template <int G, bool WORLD, bool SWZ = false>
 __global__ void __launch_bounds__(256) mp_store_kernel(const float2* __restrict__ Z1,
                                                        const float2* __restrict__ Z2,
                                                        const float2* __restrict__ Z3,
@@ -482,7 +485,8 @@ __global__ void __launch_bounds__(256) mp_store_kernel(const float2* __restrict_
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (int64_t)pairs * G3) return;
     const int pair = (int)(idx / G3);
-    const int c = (int)(idx % G3);
+    const int c0 = (int)(idx % G3);
+    const int c = SWZ ? (int)force_slot((uint32_t)c0, ilog2<G>()) : c0;
     const int ga = 2 * pair, gb = ga + 1;
     const float invn = 1.0f / (float)G3;
     const float2 a = Z1[idx], z = Z2[idx];
@@ -501,8 +505,9 @@ __global__ void __launch_bounds__(256) mp_store_kernel(const float2* __restrict_
 }
 
 template <int G, typename Acc>
-cudaError_t run_fused(const Ensemble& e, Acc* mass, float4* force, bool world, bool zero,
+cudaError_t run_fused(const Ensemble& e, Acc* mass, float4* force, int frame, bool zero,
                       cudaStream_t s) {
+    const bool world = frame != kFrameGrid, swz = frame == kFrameWorldSlot;
     const int pairs = (e.k + 1) / 2;
     const size_t smem = (size_t)3 * G * G * (G + 1) * sizeof(float2);
     auto pick = [&](auto kern, int threads) -> cudaError_t {
@@ -514,12 +519,18 @@ cudaError_t run_fused(const Ensemble& e, Acc* mass, float4* force, bool world, b
     };
     if constexpr (G >= 8) {
         constexpr int T = 3 * G * G;
+        if (swz)
+            return zero ? pick(spectral_fused3_kernel<G, Acc, true, true, false, true>, T)
+                        : pick(spectral_fused3_kernel<G, Acc, true, false, false, true>, T);
         if (world)
             return zero ? pick(spectral_fused3_kernel<G, Acc, true, true>, T)
                         : pick(spectral_fused3_kernel<G, Acc, true, false>, T);
         return zero ? pick(spectral_fused3_kernel<G, Acc, false, true>, T)
                     : pick(spectral_fused3_kernel<G, Acc, false, false>, T);
     }
+    if (swz)
+        return zero ? pick(spectral_fused_kernel<G, Acc, true, true, true>, G * G)
+                    : pick(spectral_fused_kernel<G, Acc, true, false, true>, G * G);
     if (world)
         return zero ? pick(spectral_fused_kernel<G, Acc, true, true>, G * G)
                     : pick(spectral_fused_kernel<G, Acc, true, false>, G * G);
@@ -528,7 +539,7 @@ cudaError_t run_fused(const Ensemble& e, Acc* mass, float4* force, bool world, b
 }
 
 template <int G, typename Acc>
-cudaError_t run_multipass(const Ensemble& e, Acc* mass, float4* force, bool world, bool zero,
+cudaError_t run_multipass(const Ensemble& e, Acc* mass, float4* force, int frame, bool zero,
                           void* scratch, cudaStream_t s) {
     constexpr int G3 = G * G * G;
     const int pairs = (e.k + 1) / 2;
@@ -564,7 +575,9 @@ cudaError_t run_multipass(const Ensemble& e, Acc* mass, float4* force, bool worl
         mp_line_kernel<G, true><<<dim3(lb, 3), 128, 0, s>>>(Z1, Z2, Z3, 1, pairs);
         mp_line_kernel<G, true><<<dim3(lb, 3), 128, 0, s>>>(Z1, Z2, Z3, 0, pairs);
     }
-    if (world)
+    if (frame == kFrameWorldSlot)
+        mp_store_kernel<G, true, true><<<eb, 256, 0, s>>>(Z1, Z2, Z3, force, e, pairs);
+    else if (frame == kFrameWorld)
         mp_store_kernel<G, true><<<eb, 256, 0, s>>>(Z1, Z2, Z3, force, e, pairs);
     else
         mp_store_kernel<G, false><<<eb, 256, 0, s>>>(Z1, Z2, Z3, force, e, pairs);
@@ -572,16 +585,17 @@ cudaError_t run_multipass(const Ensemble& e, Acc* mass, float4* force, bool worl
 }
 
 template <typename Acc>
-cudaError_t spectral_typed(const Ensemble& e, Acc* mass, float4* force, bool world, bool zero,
+cudaError_t spectral_typed(const Ensemble& e, Acc* mass, float4* force, int frame, bool zero,
                            void* scratch, cudaStream_t s) {
-    if (e.dft_tc && e.g == 16) return run_multipass<16, Acc>(e, mass, force, world, zero, scratch, s);
+    if (frame < kFrameGrid || frame > kFrameWorldSlot) return cudaErrorInvalidValue;
+    if (e.dft_tc && e.g == 16) return run_multipass<16, Acc>(e, mass, force, frame, zero, scratch, s);
     switch (e.g) {
-        case 2: return run_fused<2, Acc>(e, mass, force, world, zero, s);
-        case 4: return run_fused<4, Acc>(e, mass, force, world, zero, s);
-        case 8: return run_fused<8, Acc>(e, mass, force, world, zero, s);
-        case 16: return run_fused<16, Acc>(e, mass, force, world, zero, s);
-        case 32: return run_multipass<32, Acc>(e, mass, force, world, zero, scratch, s);
-        case 64: return run_multipass<64, Acc>(e, mass, force, world, zero, scratch, s);
+        case 2: return run_fused<2, Acc>(e, mass, force, frame, zero, s);
+        case 4: return run_fused<4, Acc>(e, mass, force, frame, zero, s);
+        case 8: return run_fused<8, Acc>(e, mass, force, frame, zero, s);
+        case 16: return run_fused<16, Acc>(e, mass, force, frame, zero, s);
+        case 32: return run_multipass<32, Acc>(e, mass, force, frame, zero, scratch, s);
+        case 64: return run_multipass<64, Acc>(e, mass, force, frame, zero, scratch, s);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -619,7 +633,8 @@ __global__ void prerotate_kernel(const float4* __restrict__ in, float4* __restri
     for (int q = 0; q < 12; ++q) R[q] = __ldg(rot12 + 12 * i + q);
     const float4 f = in[c];
     const float3 w = rotate_back(R, f.x, f.y, f.z);
-    out[c] = make_float4(w.x, w.y, w.z, 0.f);
+    const int64_t G3 = (int64_t)1 << (3 * lg);
+    out[(int64_t)i * G3 + force_slot((uint32_t)(c - (int64_t)i * G3), lg)] = make_float4(w.x, w.y, w.z, 0.f);
 }
 
 }  // namespace
@@ -643,7 +658,7 @@ static cudaError_t spectral_density_typed(const Ensemble& e, Acc* mass, float4* 
         if (e.g == 16) return go(spectral_fused3_kernel<16, Acc, true, false, true>, 16);
         return go(spectral_fused3_kernel<8, Acc, true, false, true>, 8);
     }
-    cudaError_t err = spectral_typed(e, mass, force, true, false, scratch, s);
+    cudaError_t err = spectral_typed(e, mass, force, kFrameWorld, false, scratch, s);
     if (err != cudaSuccess) return err;
     return launch_density_w(e, mass, force, s);
 }
@@ -661,13 +676,12 @@ size_t spectral_scratch_bytes(const Ensemble& e) {
     return 4 * pairs * ((size_t)1 << (3 * e.lg)) * sizeof(float2);
 }
 
-cudaError_t launch_spectral(const Ensemble& e, void* mass, float4* force, bool world_frame,
+cudaError_t launch_spectral(const Ensemble& e, void* mass, float4* force, int frame,
                             bool zero_mass, void* scratch, cudaStream_t s) {
     if (e.mass_mode == 0)
-        return spectral_typed(e, static_cast<unsigned long long*>(mass), force, world_frame,
-                              zero_mass, scratch, s);
-    return spectral_typed(e, static_cast<unsigned*>(mass), force, world_frame, zero_mass, scratch,
-                          s);
+        return spectral_typed(e, static_cast<unsigned long long*>(mass), force, frame, zero_mass,
+                              scratch, s);
+    return spectral_typed(e, static_cast<unsigned*>(mass), force, frame, zero_mass, scratch, s);
 }
 
 cudaError_t launch_build_tables(int g, float world, float G, float* green, float* ktab,

@@ -6,7 +6,10 @@
 //  * the spectral epilogue already stored every grid's force rotated back
 //    into the world frame (M_i F_i(cell), the very product update.glsl:77
 //    forms, with the same FP32 operations), so a (particle, grid) touch is
-//    one cell index + one float4 load + three adds;
+//    one cell index + one float4 load + three adds; it stored cell c at
+//    force_slot(c) (x XORed with (2y ^ 4z) mod 8), so that the cells a
+//    warp's particles fall in, and their y and z neighbours, spread over
+//    the 16-byte bank quads of a staged grid instead of sharing one;
 //  * for large particle counts each CTA stages grid i's whole force field
 //    (g^3 float4, 64 KB at g = 16) in shared memory with one bulk async
 //    copy (cp.async.bulk + mbarrier), three stages deep, and every
@@ -95,13 +98,14 @@ __device__ __forceinline__ void finish_particle(int64_t p, float4 P, float ax, f
     vel[p] = make_float4(vx, vy, vz, 0.f);
 }
 
-__device__ __forceinline__ uint32_t cell_of(int idx_mode, const float* xf, float cx, float cy,
+// Slot (force_slot) of the particle's cell in a kFrameWorldSlot grid.
+__device__ __forceinline__ uint32_t slot_of(int idx_mode, const float* xf, float cx, float cy,
                                             float cz, const IndexParams& ip) {
     if (idx_mode == 0) {
         const float4* r = reinterpret_cast<const float4*>(xf);
-        return cell_fast(r[0], r[1], r[2], cx, cy, cz, ip.lg);
+        return slot_fast(r[0], r[1], r[2], cx, cy, cz, ip.lg);
     }
-    return cell_exact(xf, xf + 12, cx, cy, cz, ip);
+    return force_slot(cell_exact(xf, xf + 12, cx, cy, cz, ip), ip.lg);
 }
 
 // Particle in slot `slot` (slot < n).  A checked build redirects a
@@ -278,7 +282,7 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
         for (int j = 0; j < PPT; ++j) {
             if (j < cnt) {
-                uint32_t c = cell_of(IDX, x, cx[j], cy[j], cz[j], ip);
+                uint32_t c = slot_of(IDX, x, cx[j], cy[j], cz[j], ip);
                 if (!in_bounds(e.flags, c, (uint64_t)G3)) c = 0;
                 const float4 f = F[c];
                 ax[j] = __fadd_rn(ax[j], f.x);
@@ -394,7 +398,7 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
                 for (int j = 0; j < PPT; ++j) {
                     if (j < cnt) {
-                        uint32_t cell = cell_of(0, x, cx[j], cy[j], cz[j], ip);
+                        uint32_t cell = slot_of(0, x, cx[j], cy[j], cz[j], ip);
                         if (!in_bounds(e.flags, cell, (uint64_t)G3)) cell = 0;
                         const float4 f = F[cell];
                         ax[j] = __fadd_rn(ax[j], f.x);
@@ -428,7 +432,7 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
                 for (int j = 0; j < PPT; ++j) {
                     if (j < cnt) {
-                        uint32_t cell = cell_fast(xr.row[0], xr.row[1], xr.row[2], cx[j], cy[j], cz[j], ip.lg);
+                        uint32_t cell = slot_fast(xr.row[0], xr.row[1], xr.row[2], cx[j], cy[j], cz[j], ip.lg);
                         if (!in_bounds(e.flags, cell, (uint64_t)G3)) cell = 0;
                         if (cell != prev) f = __ldg(F + cell);
                         prev = cell;
@@ -489,9 +493,10 @@ __global__ void __launch_bounds__(256) update_direct_kernel(float4* __restrict__
                 uint32_t c;
                 if (IDX == 0) {
                     const FastXf x = e.fast[i];
-                    c = cell_fast(x.row[0], x.row[1], x.row[2], cx[j], cy[j], cz[j], ip.lg);
+                    c = slot_fast(x.row[0], x.row[1], x.row[2], cx[j], cy[j], cz[j], ip.lg);
                 } else {
-                    c = cell_exact(e.rot12 + 12 * i, e.off4 + 4 * i, cx[j], cy[j], cz[j], ip);
+                    c = force_slot(cell_exact(e.rot12 + 12 * i, e.off4 + 4 * i, cx[j], cy[j], cz[j], ip),
+                                   ip.lg);
                 }
                 if (!in_bounds(e.flags, c, (uint64_t)G3)) c = 0;
                 if (c != prev) f = __ldg(F + c);
