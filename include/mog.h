@@ -126,7 +126,7 @@ typedef struct mog_tuning {
     int32_t deposit_aggregate;      /* warp-merge runs of equal cells: -1 auto, 0 off, 1 on  */
     int32_t deposit_generic;        /* 1: never use the specialised g <= 16 deposit kernel    */
     int32_t deposit_sorted;         /* 1: deposit from the spatially ordered copy too         */
-    int32_t update_threads;         /* staged gather block: 512, 768 or 1024                  */
+    int32_t update_threads;         /* staged gather block: 512, 768 or 1024; 0 auto (512)   */
     int32_t deposit_split;          /* u64 shared histogram of high words only (low halves as
                                        global atomics; none for equal power-of-two masses):
                                        0 auto (g = 32), 1 also at g = 8 and 16, -1 never      */

@@ -387,8 +387,9 @@ __device__ __forceinline__ void deposit_fast_tile(const float4* __restrict__ pos
             hi_only = __all_sync(kFull, any_lo == 0u);
         }
         // the common case (equal power-of-two masses): one add of the high
-        // word per particle and grid, in a loop of its own
-        if (MODE == 1 && !SPLIT && hi_only) {
+        // word per particle and grid, in a loop of its own (in the split
+        // layout as well: there are no low halves to send to global memory)
+        if (MODE == 1 && hi_only) {
             for (int j = 0; j < ng; ++j) {
                 const DepositRows r = rows[j];
                 const uint32_t gbyte = (uint32_t)j * (G3 * 4u);

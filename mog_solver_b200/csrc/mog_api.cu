@@ -829,7 +829,7 @@ int mog_set_tuning(mog_handle* h, const mog_tuning* t) {
     h->dshape.aggregate = t->deposit_aggregate;
     h->dshape.fast = t->deposit_generic ? 0 : 1;
     h->dshape.sorted_input = t->deposit_sorted ? 1 : 0;
-    h->ushape.threads = t->update_threads ? t->update_threads : 512;
+    h->ushape.threads = t->update_threads;
     h->dshape.split = t->deposit_split;
     h->learned_fold = t->learned_fold >= 0 ? 1 : 0;
     h->learned_ctas = t->learned_ctas_per_sm ? t->learned_ctas_per_sm : 2;

@@ -81,7 +81,7 @@ struct DepositShape {
     int split = 0;          // u64 high-word-only histogram: 0 auto (g = 32), 1 also g = 8/16, -1 never
 };
 struct UpdateShape {
-    int threads = 512;      // staged gather block size: 512, 768 or 1024
+    int threads = 0;        // staged gather block size: 512, 768 or 1024; 0 auto
     int staged = -1;        // -1 auto, 0 global gathers, 1 smem-staged grids
     int ctas = 0;           // staged kernel CTAs; 0 = one per SM
     int direct_ppt = 4;     // particles per thread of the direct gather

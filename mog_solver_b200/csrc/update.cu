@@ -60,6 +60,22 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
         : "memory");
     return ok != 0;
 }
+// One 16-byte shared load (ld.shared.v4) at a shared-window address.  A
+// volatile asm is neither repeated nor moved across the mbarrier waits, so
+// the grid rows loaded with it stay in registers for the whole grid instead
+// of being reloaded for every particle.
+__device__ __forceinline__ float4 ld_shared_f4_at(uint32_t addr) {
+    float4 v;
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+                 : "r"(addr));
+    return v;
+}
+// Orders this thread's generic-proxy shared-memory accesses before its
+// later bulk (async-proxy) copies into the same memory.
+__device__ __forceinline__ void fence_proxy_async_shared() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
 // Bounded wait: gives up after ~2^31 SM cycles (about a second) and
 // reports false; the caller then abandons the launch with MOG_FLAG_TIMEOUT.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
@@ -98,14 +114,32 @@ __device__ __forceinline__ void finish_particle(int64_t p, float4 P, float ax, f
     vel[p] = make_float4(vx, vy, vz, 0.f);
 }
 
-// Slot (force_slot) of the particle's cell in a kFrameWorldSlot grid.
-__device__ __forceinline__ uint32_t slot_of(int idx_mode, const float* xf, float cx, float cy,
-                                            float cz, const IndexParams& ip) {
-    if (idx_mode == 0) {
-        const float4* r = reinterpret_cast<const float4*>(xf);
-        return slot_fast(r[0], r[1], r[2], cx, cy, cz, ip.lg);
+// One grid's gathers for a thread's PPT particles from the staged grid at
+// shared address F (xf: the grid's 16 transform floats there, r0..r2 its
+// FAST rows already in registers): slot, one 16-byte shared load, the
+// running force (x, y as a pair, one add.f32x2: two IEEE adds) in grid
+// order.  FULL: every slot is live (no per-particle test).  LG > 0: g = 2^LG
+// at compile time.
+template <int IDX, int PPT, int LG, bool FULL>
+__device__ __forceinline__ void gather_grid(uint32_t F, const float* x, const float4& r0,
+                                            const float4& r1, const float4& r2,
+                                            const float (&cx)[PPT], const float (&cy)[PPT],
+                                            const float (&cz)[PPT], float2 (&axy)[PPT],
+                                            float (&az)[PPT], int cnt, const IndexParams& ip,
+                                            unsigned* flags) {
+    const int lg = LG > 0 ? LG : ip.lg;
+    const uint32_t G3 = 1u << (3 * lg);
+#pragma unroll
+    for (int j = 0; j < PPT; ++j) {
+        if (FULL || j < cnt) {
+            uint32_t c = IDX == 0 ? slot_fast(r0, r1, r2, cx[j], cy[j], cz[j], lg)
+                                  : force_slot(cell_exact(x, x + 12, cx[j], cy[j], cz[j], ip), lg);
+            if (!in_bounds(flags, c, (uint64_t)G3)) c = 0;
+            const float4 f = ld_shared_f4_at(F + (c << 4));
+            axy[j] = __fadd2_rn(axy[j], make_float2(f.x, f.y));
+            az[j] = __fadd_rn(az[j], f.z);
+        }
     }
-    return force_slot(cell_exact(xf, xf + 12, cx, cy, cz, ip), ip.lg);
 }
 
 // Particle in slot `slot` (slot < n).  A checked build redirects a
@@ -180,7 +214,7 @@ __device__ __forceinline__ void issue_grid(int i, int s, const float4* __restric
 // ordering they fall in the same few cells and their shared-memory loads
 // broadcast instead of conflicting, and the CTA's particles occupy a small
 // box, so only the z-slabs of each grid that the box reaches are staged.
-template <int IDX, int PPT, bool ACC_OUT, int THREADS>
+template <int IDX, int PPT, bool ACC_OUT, int THREADS, int LG = 0, int FULLP = 0>
 __global__ void __launch_bounds__(THREADS, 1)
     update_staged_kernel(float4* __restrict__ pos, float4* __restrict__ vel,
                          const float4* __restrict__ pos_s, const int* __restrict__ perm,
@@ -196,12 +230,18 @@ __global__ void __launch_bounds__(THREADS, 1)
     __shared__ int abort_flag;
     __shared__ float box[6];        // min c.xyz, max c.xyz of the CTA's particles
     __shared__ float wbox[THREADS / 32][6];   // per-warp partial boxes
+    __shared__ unsigned stage_done[8];        // warps done with a stage's current grid
+    __shared__ int stage_grid[8];             // grid last copied into a stage
 
     const int tid = threadIdx.x;
     const int T = blockDim.x;
     if (tid == 0) {
         abort_flag = 0;
-        for (int s = 0; s < nstage; ++s) mbar_init(full + s, 1);
+        for (int s = 0; s < nstage; ++s) {
+            mbar_init(full + s, 1);
+            stage_done[s] = 0u;
+            stage_grid[s] = s < e.k ? s : -1;
+        }
         mbar_fence_init();
     }
     for (int i = tid; i < e.k * 16; i += T) {
@@ -221,7 +261,8 @@ __global__ void __launch_bounds__(THREADS, 1)
     const int64_t mine = hi - first;
     const int64_t slots = (mine + T - 1) / T;
     const int cnt = mine <= 0 ? 0 : (int)(slots < PPT ? slots : PPT);
-    float cx[PPT], cy[PPT], cz[PPT], ax[PPT], ay[PPT], az[PPT];
+    float cx[PPT], cy[PPT], cz[PPT], az[PPT];
+    float2 axy[PPT];
     float bmin[3] = {3.0e38f, 3.0e38f, 3.0e38f}, bmax[3] = {-3.0e38f, -3.0e38f, -3.0e38f};
 #pragma unroll
     for (int j = 0; j < PPT; ++j) {
@@ -233,7 +274,8 @@ __global__ void __launch_bounds__(THREADS, 1)
         cx[j] = __fsub_rn(P.x, ip.half_l);
         cy[j] = __fsub_rn(P.y, ip.half_l);
         cz[j] = __fsub_rn(P.z, ip.half_l);
-        ax[j] = ay[j] = az[j] = 0.f;
+        axy[j] = make_float2(0.f, 0.f);
+        az[j] = 0.f;
         if (j < cnt) {
             bmin[0] = fminf(bmin[0], cx[j]);
             bmin[1] = fminf(bmin[1], cy[j]);
@@ -272,41 +314,62 @@ __global__ void __launch_bounds__(THREADS, 1)
             issue_grid(s, s, W, stage, full, e.lg, box, sparse && box[0] <= box[3], xf, IDX, ip);
     }
 
-    int i_abort = -1;
+    // No block-wide barrier per grid: each warp waits for the grid's copy,
+    // gathers, and counts itself done with the stage; the last warp to finish
+    // grid i refills the stage with grid i + nstage.  Warps drift up to
+    // nstage grids apart instead of waiting for the slowest one every grid.
+    const unsigned nwarps = (unsigned)(T >> 5);
+    const uint32_t stage_s = smem_u32(stage);
+    bool aborted = false;
     for (int i = 0; i < e.k; ++i) {
         const int s = i % nstage;
         const unsigned parity = (unsigned)((i / nstage) & 1);
-        if (!mbar_wait_bounded(full + s, parity)) abort_flag = 1;
-        const float4* F = stage + (size_t)s * G3;
-        const float* x = xf + i * 16;
-#pragma unroll
-        for (int j = 0; j < PPT; ++j) {
-            if (j < cnt) {
-                uint32_t c = slot_of(IDX, x, cx[j], cy[j], cz[j], ip);
-                if (!in_bounds(e.flags, c, (uint64_t)G3)) c = 0;
-                const float4 f = F[c];
-                ax[j] = __fadd_rn(ax[j], f.x);
-                ay[j] = __fadd_rn(ay[j], f.y);
-                az[j] = __fadd_rn(az[j], f.z);
-            }
-        }
-        __syncthreads();
-        if (abort_flag) {
-            i_abort = i;
+        if (!__all_sync(kFull, mbar_wait_bounded(full + s, parity))) {
+            aborted = true;  // warp-uniform
             break;
         }
-        if (tid == 0 && i + nstage < e.k)
-            issue_grid(i + nstage, s, W, stage, full, e.lg, box, sparse && box[0] <= box[3], xf, IDX,
-                       ip);
+        const uint32_t F = stage_s + (uint32_t)s * (uint32_t)G3 * 16u;
+        const float* x = xf + i * 16;
+        float4 r0 = make_float4(0.f, 0.f, 0.f, 0.f), r1 = r0, r2 = r0;
+        if (IDX == 0) {  // the grid's FAST rows, once per grid
+            const uint32_t xa = smem_u32(x);
+            r0 = ld_shared_f4_at(xa);
+            r1 = ld_shared_f4_at(xa + 16);
+            r2 = ld_shared_f4_at(xa + 32);
+        }
+        if (FULLP && cnt == PPT)
+            gather_grid<IDX, PPT, LG, true>(F, x, r0, r1, r2, cx, cy, cz, axy, az, cnt, ip, e.flags);
+        else
+            gather_grid<IDX, PPT, LG, false>(F, x, r0, r1, r2, cx, cy, cz, axy, az, cnt, ip, e.flags);
+        // every lane's loads of the stage have returned (their values are
+        // summed) before the warp counts itself done
+        __syncwarp();
+        if ((tid & 31) == 0) {
+            __threadfence_block();
+            if (atomicAdd(&stage_done[s], 1u) == nwarps - 1) {
+                stage_done[s] = 0u;
+                __threadfence_block();
+                if (i + nstage < e.k) {
+                    stage_grid[s] = i + nstage;
+                    fence_proxy_async_shared();
+                    issue_grid(i + nstage, s, W, stage, full, e.lg, box, sparse && box[0] <= box[3],
+                               xf, IDX, ip);
+                }
+            }
+        }
     }
-    if (i_abort >= 0) {
-        // Copies for grids i_abort .. i_abort + nstage - 1 may still be in
-        // flight: let them land (bounded as well) before the CTA's shared
-        // memory is released, then report and leave.
+    if (aborted && (tid & 31) == 0) abort_flag = 1;
+    __syncthreads();
+    if (abort_flag) {
+        // A copy never landed.  The copy issued last into each stage may
+        // still be in flight: let it land (bounded as well) before the CTA's
+        // shared memory is released, then report and leave.
         if (tid == 0) {
             atomicOr(e.flags, 4u);
-            for (int j = i_abort; j < i_abort + nstage && j < e.k; ++j)
-                (void)mbar_wait_bounded(full + (j % nstage), (unsigned)((j / nstage) & 1));
+            for (int q = 0; q < nstage; ++q) {
+                const int j = stage_grid[q];
+                if (j >= 0) (void)mbar_wait_bounded(full + q, (unsigned)((j / nstage) & 1));
+            }
         }
         return;
     }
@@ -319,8 +382,8 @@ __global__ void __launch_bounds__(THREADS, 1)
             const int64_t slot = first + (int64_t)j * T;
             const int64_t p = particle_of(perm, slot, n, e.flags);
             const float4 P = pos_s ? pos_s[slot] : pos[p];
-            finish_particle<ACC_OUT>(p, P, ax[j], ay[j], az[j], pos, vel, acc_out, kf, dt, damp,
-                                     e.world, bad);
+            finish_particle<ACC_OUT>(p, P, axy[j].x, axy[j].y, az[j], pos, vel, acc_out, kf, dt,
+                                     damp, e.world, bad);
         }
     }
     if (bad) raise_flags(e.flags, bad);
@@ -370,14 +433,16 @@ __global__ void __launch_bounds__(THREADS, 1)
         const int64_t first = tile.lo + tid;
         const int64_t mine = tile.hi - first;
         const int cnt = mine <= 0 ? 0 : (int)((mine + THREADS - 1) / THREADS < PPT ? (mine + THREADS - 1) / THREADS : PPT);
-        float cx[PPT], cy[PPT], cz[PPT], ax[PPT], ay[PPT], az[PPT];
+        float cx[PPT], cy[PPT], cz[PPT], az[PPT];
+        float2 axy[PPT];
 #pragma unroll
         for (int j = 0; j < PPT; ++j) {
             const float4 P = j < cnt ? pos[first + (int64_t)j * THREADS] : make_float4(0.f, 0.f, 0.f, 0.f);
             cx[j] = __fsub_rn(P.x, ip.half_l);
             cy[j] = __fsub_rn(P.y, ip.half_l);
             cz[j] = __fsub_rn(P.z, ip.half_l);
-            ax[j] = ay[j] = az[j] = 0.f;
+            axy[j] = make_float2(0.f, 0.f);
+            az[j] = 0.f;
         }
         if (e.lg <= 4) {
             for (int i = tid; i < e.k * 16; i += THREADS) {
@@ -393,19 +458,12 @@ __global__ void __launch_bounds__(THREADS, 1)
                 const uint32_t c = issued + (uint32_t)i;
                 const int q = (int)(c % nstage);
                 if (!mbar_wait_bounded(full + q, (c / nstage) & 1u)) abort_flag = 1;
-                const float4* F = stage + (size_t)q * G3;
-                const float* x = xf + i * 16;
-#pragma unroll
-                for (int j = 0; j < PPT; ++j) {
-                    if (j < cnt) {
-                        uint32_t cell = slot_of(0, x, cx[j], cy[j], cz[j], ip);
-                        if (!in_bounds(e.flags, cell, (uint64_t)G3)) cell = 0;
-                        const float4 f = F[cell];
-                        ax[j] = __fadd_rn(ax[j], f.x);
-                        ay[j] = __fadd_rn(ay[j], f.y);
-                        az[j] = __fadd_rn(az[j], f.z);
-                    }
-                }
+                const uint32_t F = smem_u32(stage) + (uint32_t)q * (uint32_t)G3 * 16u;
+                const uint32_t xa = smem_u32(xf + i * 16);
+                const float4 r0 = ld_shared_f4_at(xa), r1 = ld_shared_f4_at(xa + 16),
+                             r2 = ld_shared_f4_at(xa + 32);
+                gather_grid<0, PPT, 0, false>(F, nullptr, r0, r1, r2, cx, cy, cz, axy, az, cnt, ip,
+                                              e.flags);
                 __syncthreads();
                 if (abort_flag) {
                     // let the copies still in flight land (bounded) before the
@@ -436,8 +494,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                         if (!in_bounds(e.flags, cell, (uint64_t)G3)) cell = 0;
                         if (cell != prev) f = __ldg(F + cell);
                         prev = cell;
-                        ax[j] = __fadd_rn(ax[j], f.x);
-                        ay[j] = __fadd_rn(ay[j], f.y);
+                        axy[j] = __fadd2_rn(axy[j], make_float2(f.x, f.y));
                         az[j] = __fadd_rn(az[j], f.z);
                     }
                 }
@@ -448,7 +505,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         for (int j = 0; j < PPT; ++j) {
             if (j < cnt) {
                 const int64_t p = first + (int64_t)j * THREADS;
-                finish_particle<false>(p, pos[p], ax[j], ay[j], az[j], pos, S.vel, nullptr,
+                finish_particle<false>(p, pos[p], axy[j].x, axy[j].y, az[j], pos, S.vel, nullptr,
                                        (float)e.k, S.dt, S.damping, e.world, bad);
             }
         }
@@ -524,7 +581,12 @@ cudaError_t launch_staged(const Ensemble& e, float4* pos, float4* vel, const flo
                           const int* perm, int64_t n, const float4* W, float dt, float damp,
                           float4* acc, int ctas, int nstage, size_t smem, int sparse,
                           cudaStream_t s) {
-    auto kern = update_staged_kernel<IDX, PPT, ACC, THREADS>;
+    // g = 16 (the staged grids are g <= 16) with compile-time shifts and
+    // masks; a check-free copy of the particle loop where the registers
+    // leave room for it (PPT <= 8)
+    auto kern = (IDX == 0 && e.lg == 4)
+                    ? update_staged_kernel<IDX, PPT, ACC, THREADS, 4, (PPT <= 8 ? 1 : 0)>
+                    : update_staged_kernel<IDX, PPT, ACC, THREADS, 0, 0>;
     const int threads = THREADS;
     cudaError_t err =
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -569,7 +631,9 @@ cudaError_t update_mode(const Ensemble& e, float4* pos, float4* vel, const float
     // Sparse staging only pays when the CTAs' particles are spatially compact.
     const int sparse = (pos_s || perm) ? 1 : 0;
     // Block size (occupancy) against particles per thread (registers): the
-    // launch bounds give 512 threads ~128 registers, 768 ~85, 1024 64.
+    // launch bounds give 512 threads ~128 registers, 768 ~85, 1024 64.  Auto
+    // (0) is 512: measured at c2 (N = 2^20, k = 240) 0.456 ms against 0.518
+    // ms for 1024 threads of 7 particles.
     const int T = sh.threads == 768 || sh.threads == 1024 ? sh.threads : 512;
     const int max_ppt = T == 512 ? 16 : (T == 768 ? 10 : 7);
     int ctas = sh.ctas > 0 ? sh.ctas : sms;
