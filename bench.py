@@ -803,6 +803,8 @@ def run_batch(args, w: dict) -> None:
         sims.append(s)
     torch.cuda.synchronize()
     batch = Batch(sims)
+    if args.tuning:
+        batch.tune(**json.loads(args.tuning))
     tuned = None
     if args.autotune:
         from mog_solver_b200.autotune import autotune_batch

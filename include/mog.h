@@ -341,7 +341,11 @@ int mog_batch_destroy(mog_batch* b);
  * (simulation, grid group, particle chunk) / (simulation, particle chunk)
  * from a largest-first list until it runs out.  Otherwise (or with
  * work_queue = 0) each simulation's three kernels run on their own branch.
- * deposit_chunk: particles per deposit tile (0 = 65536; else >= 1024).
+ * deposit_chunk: particles per deposit tile (0 = 262144; else >= 1024).
+ * deposit_split: 1 = u64 grids keep only their high words in the work-queue
+ * deposit's shared memory at g = 8 and 16 too (twice the grids per tile;
+ * pays when every mass has a zero fixed-point low half, which then needs no
+ * global atomic), 0 = only at g = 32.
  * The result never depends on these.  mog_batch_get_tuning also reports
  * whether the work-queue launches apply (active_work_queue, read only).
  */
@@ -349,6 +353,7 @@ typedef struct mog_batch_tuning {
     int32_t work_queue;
     int32_t deposit_chunk;
     int32_t active_work_queue;
+    int32_t deposit_split;
 } mog_batch_tuning;
 int mog_batch_set_tuning(mog_batch* b, const mog_batch_tuning* t);
 int mog_batch_get_tuning(const mog_batch* b, mog_batch_tuning* t);

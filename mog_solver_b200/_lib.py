@@ -121,6 +121,7 @@ class MogBatchTuningC(ctypes.Structure):
         ("work_queue", ctypes.c_int32),
         ("deposit_chunk", ctypes.c_int32),
         ("active_work_queue", ctypes.c_int32),
+        ("deposit_split", ctypes.c_int32),
     ]
 
 

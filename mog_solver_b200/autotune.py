@@ -99,8 +99,9 @@ def autotune_batch(batch, reps: int = 3, cache: Path | None = CACHE, force: bool
         batch.tune(**table[key]["tuning"])
         return table[key]
     saved = [(s.pos.clone(), s.vel.clone()) for s in batch.sims]
-    cands = [dict(work_queue=1, deposit_chunk=c) for c in (32768, 65536, 131072, 262144)]
-    cands.append(dict(work_queue=0, deposit_chunk=0))
+    cands = [dict(work_queue=1, deposit_chunk=c, deposit_split=sp)
+             for sp in (0, 1) for c in (65536, 131072, 262144)]
+    cands.append(dict(work_queue=0, deposit_chunk=0, deposit_split=0))
     results = []
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     try:

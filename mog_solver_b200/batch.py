@@ -25,7 +25,7 @@ class Batch:
         self.sims = list(sims)
         self._h = ctypes.c_void_p()
         self._built_for = None
-        self._tuning = {"work_queue": 1, "deposit_chunk": 0}
+        self._tuning = {"work_queue": 1, "deposit_chunk": 0, "deposit_split": 0}
 
     def _handles(self):
         hs = [s.handle for s in self.sims]  # creates / refreshes each handle
@@ -40,13 +40,16 @@ class Batch:
         return self._h
 
     def _apply_tuning(self) -> None:
-        t = _lib.MogBatchTuningC(int(self._tuning["work_queue"]), int(self._tuning["deposit_chunk"]), 0)
+        t = _lib.MogBatchTuningC(work_queue=int(self._tuning["work_queue"]),
+                                 deposit_chunk=int(self._tuning["deposit_chunk"]),
+                                 deposit_split=int(self._tuning["deposit_split"]))
         _lib.check(_lib.lib().mog_batch_set_tuning(self._h, ctypes.byref(t)), "mog_batch_set_tuning")
 
     def tune(self, **kw) -> None:
         """Set launch shapes: work_queue (1 persistent work-queue launches,
         0 one branch per simulation), deposit_chunk (particles per deposit
-        tile, 0 = library default)."""
+        tile, 0 = library default), deposit_split (1: high-word histograms
+        at every grid size, for masses whose fixed-point low halves are 0)."""
         unknown = set(kw) - set(self._tuning)
         if unknown:
             raise ValueError(f"unknown batch tuning fields {sorted(unknown)}")

@@ -475,8 +475,9 @@ __global__ void __launch_bounds__(1024) deposit_fast_kernel(const float4* __rest
 // host-built list with an atomic counter until it runs out, and deposits
 // each through the same tile body as deposit_fast_kernel.  The histogram
 // layout follows the tile's own grid count and grid size; at g = 32 in u64
-// mode it is the split (high-word) histogram, as in the single launch.
-template <int MODE>
+// mode it is the split (high-word) histogram, as in the single launch, and
+// with SPLIT16 at g = 8 and 16 as well.
+template <int MODE, bool SPLIT16>
 __global__ void __launch_bounds__(1024, 1) deposit_queue_kernel(const BatchSim* __restrict__ sims,
                                                                const DepositTile* __restrict__ tiles,
                                                                int ntiles, unsigned* __restrict__ counter) {
@@ -495,11 +496,13 @@ __global__ void __launch_bounds__(1024, 1) deposit_queue_kernel(const BatchSim* 
         Acc* mass = static_cast<Acc*>(S.mass);
         const bool first = tile.g0 == 0;
         if (e.lg == 3)
-            deposit_fast_tile<3, MODE, 4, false, false>(pos, tile.lo, tile.hi, e, tile.ng, tile.g0,
-                                                        tile.ng, first, mass, smem_raw);
+            deposit_fast_tile<3, MODE, 4, MODE == 1 && SPLIT16, false>(pos, tile.lo, tile.hi, e, tile.ng,
+                                                                       tile.g0, tile.ng, first, mass,
+                                                                       smem_raw);
         else if (e.lg == 4)
-            deposit_fast_tile<4, MODE, 4, false, false>(pos, tile.lo, tile.hi, e, tile.ng, tile.g0,
-                                                        tile.ng, first, mass, smem_raw);
+            deposit_fast_tile<4, MODE, 4, MODE == 1 && SPLIT16, false>(pos, tile.lo, tile.hi, e, tile.ng,
+                                                                       tile.g0, tile.ng, first, mass,
+                                                                       smem_raw);
         else
             deposit_fast_tile<5, MODE, 4, MODE == 1, false>(pos, tile.lo, tile.hi, e, tile.ng,
                                                             tile.g0, tile.ng, first, mass, smem_raw);
@@ -701,8 +704,8 @@ static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, const int
 // at g <= 16, the split histogram's one word at g = 32, one word in u32
 // mode; as many grids as fit 200 KB, lowered to a divisor of k when one is
 // at least half of that (equal work per grid group).
-int queue_deposit_grids(int g, int mass_mode, int k) {
-    const size_t words = (mass_mode == MOG_MASS_U64_FIXED && g <= 16) ? 2 : 1;
+int queue_deposit_grids(int g, int mass_mode, int k, bool split) {
+    const size_t words = (mass_mode == MOG_MASS_U64_FIXED && g <= 16 && !split) ? 2 : 1;
     const size_t grid_bytes = 4 * words * (size_t)g * g * g + 48;
     const int most = (int)std::max<size_t>(1, std::min<size_t>((size_t)k, (200 * 1024) / grid_bytes));
     for (int d = most; d * 2 >= most && d >= 1; --d)
@@ -710,13 +713,14 @@ int queue_deposit_grids(int g, int mass_mode, int k) {
     return most;
 }
 
-size_t queue_deposit_smem(int g, int mass_mode, int ng) {
-    const size_t words = (mass_mode == MOG_MASS_U64_FIXED && g <= 16) ? 2 : 1;
+size_t queue_deposit_smem(int g, int mass_mode, int ng, bool split) {
+    const size_t words = (mass_mode == MOG_MASS_U64_FIXED && g <= 16 && !split) ? 2 : 1;
     return (size_t)ng * 48 + 4 * words * (size_t)ng * g * g * g;
 }
 
-cudaError_t launch_deposit_queue(int mass_mode, const BatchSim* sims, const DepositTile* tiles,
-                                 int ntiles, unsigned* counter, size_t smem, cudaStream_t s) {
+cudaError_t launch_deposit_queue(int mass_mode, bool split, const BatchSim* sims,
+                                 const DepositTile* tiles, int ntiles, unsigned* counter, size_t smem,
+                                 cudaStream_t s) {
     if (ntiles <= 0) return cudaSuccess;
     auto go = [&](auto kern) -> cudaError_t {
         cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -726,7 +730,8 @@ cudaError_t launch_deposit_queue(int mass_mode, const BatchSim* sims, const Depo
         kern<<<ctas, 1024, smem, s>>>(sims, tiles, ntiles, counter);
         return cudaGetLastError();
     };
-    return mass_mode == MOG_MASS_U64_FIXED ? go(deposit_queue_kernel<1>) : go(deposit_queue_kernel<0>);
+    if (mass_mode != MOG_MASS_U64_FIXED) return go(deposit_queue_kernel<0, false>);
+    return split ? go(deposit_queue_kernel<1, true>) : go(deposit_queue_kernel<1, false>);
 }
 
 cudaError_t launch_deposit(const Ensemble& e, const float4* pos, const int* perm, int64_t n,

@@ -1533,7 +1533,7 @@ struct mog_batch {
     std::vector<cudaStream_t> branch;
     std::vector<cudaEvent_t> done;
     cudaEvent_t fork = nullptr;
-    mog_batch_tuning tuning{1, 0, 0};
+    mog_batch_tuning tuning{1, 0, 0, 0};
     struct Entry {
         std::vector<float*> pos, vel;
         std::vector<int64_t> n;
@@ -1582,7 +1582,7 @@ void build_tiles(const mog_batch* b, const int64_t* n, int64_t chunk,
     for (int i = 0; i < (int)b->sims.size(); ++i) {
         const mog_handle* h = b->sims[i];
         const int k = h->cfg.n_grids, g = h->cfg.grid_size;
-        const int gpc = mog::queue_deposit_grids(g, h->cfg.mass_mode, k);
+        const int gpc = mog::queue_deposit_grids(g, h->cfg.mass_mode, k, b->tuning.deposit_split > 0);
         for (int g0 = 0; g0 < k; g0 += gpc)
             for (int64_t lo = 0; lo < n[i]; lo += chunk) {
                 mog::DepositTile t{i, g0, std::min(gpc, k - g0), 0, lo, std::min(n[i], lo + chunk)};
@@ -1608,7 +1608,7 @@ void build_tiles(const mog_batch* b, const int64_t* n, int64_t chunk,
 int capture_queue_step(mog_batch* b, float* const* pos4, float* const* vel4, const int64_t* n,
                        const float* dt_eff, mog_batch::Entry& entry, cudaGraph_t* graph) {
     const int count = (int)b->sims.size();
-    const int64_t chunk = b->tuning.deposit_chunk > 0 ? b->tuning.deposit_chunk : 65536;
+    const int64_t chunk = b->tuning.deposit_chunk > 0 ? b->tuning.deposit_chunk : 262144;
     std::vector<mog::DepositTile> dep;
     std::vector<mog::GatherTile> gat;
     build_tiles(b, n, chunk, dep, gat);
@@ -1626,9 +1626,11 @@ int capture_queue_step(mog_batch* b, float* const* pos4, float* const* vel4, con
         recs[i].dt = dt_eff[i];
         recs[i].damping = h->cfg.damping;
         const int g = h->cfg.grid_size;
+        const bool split = b->tuning.deposit_split > 0;
         smem = std::max(smem, mog::queue_deposit_smem(
                                   g, h->cfg.mass_mode,
-                                  mog::queue_deposit_grids(g, h->cfg.mass_mode, h->cfg.n_grids)));
+                                  mog::queue_deposit_grids(g, h->cfg.mass_mode, h->cfg.n_grids, split),
+                                  split));
         kmax = std::max(kmax, h->cfg.n_grids);
     }
     const size_t sims_b = sizeof(mog::BatchSim) * count;
@@ -1650,8 +1652,8 @@ int capture_queue_step(mog_batch* b, float* const* pos4, float* const* vel4, con
     int rc = MOG_OK;
     MOG_CUDA(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal), "begin capture");
     cudaError_t err = cudaMemsetAsync(d_cnt, 0, 2 * sizeof(unsigned), b->cap);
-    if (!err) err = mog::launch_deposit_queue(b->sims[0]->cfg.mass_mode, d_sims, d_dep, (int)dep.size(),
-                                              d_cnt, smem, b->cap);
+    if (!err) err = mog::launch_deposit_queue(b->sims[0]->cfg.mass_mode, b->tuning.deposit_split > 0,
+                                              d_sims, d_dep, (int)dep.size(), d_cnt, smem, b->cap);
     if (!err) err = cudaEventRecord(b->fork, b->cap);
     for (int i = 0; i < count && !err; ++i) {
         mog_handle* h = b->sims[i];
@@ -1679,7 +1681,8 @@ extern "C" {
 int mog_batch_set_tuning(mog_batch* b, const mog_batch_tuning* t) {
     if (!b || !t) return fail(MOG_ERR_ARG, "null argument");
     if (t->work_queue < 0 || t->work_queue > 1 || t->deposit_chunk < 0 ||
-        (t->deposit_chunk > 0 && t->deposit_chunk < 1024))
+        (t->deposit_chunk > 0 && t->deposit_chunk < 1024) || t->deposit_split < 0 ||
+        t->deposit_split > 1)
         return fail(MOG_ERR_ARG, "batch tuning value out of range");
     b->tuning = *t;
     for (auto& g : b->graphs) release_entry(g);

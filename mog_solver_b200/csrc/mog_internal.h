@@ -170,8 +170,10 @@ struct GatherTile {
 };
 // Grids per deposit tile for a simulation (whole grids in shared memory),
 // the tile's shared-memory bytes, and the particles of one gather tile.
-int queue_deposit_grids(int g, int mass_mode, int k);
-size_t queue_deposit_smem(int g, int mass_mode, int ng);
+// split: u64 grids keep only high words in shared memory at every g (at
+// g = 32 they always do).
+int queue_deposit_grids(int g, int mass_mode, int k, bool split);
+size_t queue_deposit_smem(int g, int mass_mode, int ng, bool split);
 constexpr int kQueueGatherThreads = 512;
 constexpr int kQueueGatherPPT = 14;
 constexpr int64_t kQueueGatherTile = (int64_t)kQueueGatherThreads * kQueueGatherPPT;
@@ -180,8 +182,9 @@ constexpr int64_t kQueueGatherTile = (int64_t)kQueueGatherThreads * kQueueGather
 // until the list runs out.  All simulations use FAST cell indices and
 // share the mass mode; g is 8, 16 or 32.  kmax: the most grids of any
 // simulation (the gather stages their index rows in shared memory).
-cudaError_t launch_deposit_queue(int mass_mode, const BatchSim* sims, const DepositTile* tiles,
-                                 int ntiles, unsigned* counter, size_t smem, cudaStream_t s);
+cudaError_t launch_deposit_queue(int mass_mode, bool split, const BatchSim* sims,
+                                 const DepositTile* tiles, int ntiles, unsigned* counter, size_t smem,
+                                 cudaStream_t s);
 cudaError_t launch_gather_queue(const BatchSim* sims, const GatherTile* tiles, int ntiles,
                                 unsigned* counter, int kmax, cudaStream_t s);
 

@@ -75,10 +75,13 @@ def test_autotune_keeps_results_bit_exact(tmp_path):
     assert torch.equal(a.pos, b.pos) and torch.equal(a.vel, b.vel)
 
 
-@pytest.mark.parametrize("mass_mode,chunk", [("u64", 0), ("u64", 4096), ("u32x1000", 20000)])
-def test_work_queue_tiles_are_bit_exact(mass_mode, chunk):
+@pytest.mark.parametrize("mass_mode,chunk,split", [("u64", 0, 0), ("u64", 4096, 0), ("u32x1000", 20000, 0),
+                                                   ("u64", 0, 1), ("u64", 4096, 1)])
+def test_work_queue_tiles_are_bit_exact(mass_mode, chunk, split):
     """Tile sizes that split every simulation into many deposit tiles (and
-    a chunk that is not a multiple of the block), both mass modes."""
+    a chunk that is not a multiple of the block), both mass modes, and the
+    high-word histograms at every grid size (deposit_split; these masses
+    have non-zero low halves, which take the global atomics)."""
     from mog_solver_b200 import Simulation, ics
     from mog_solver_b200.batch import Batch
 
@@ -98,8 +101,8 @@ def test_work_queue_tiles_are_bit_exact(mass_mode, chunk):
 
     a, b = make(), make()
     batch = Batch(a)
-    batch.tune(deposit_chunk=chunk)
-    assert batch.tuning()["active_work_queue"] == 1
+    batch.tune(deposit_chunk=chunk, deposit_split=split)
+    assert batch.tuning()["active_work_queue"] == 1 and batch.tuning()["deposit_split"] == split
     batch.step(4)
     for s in b:
         s.step(4)
