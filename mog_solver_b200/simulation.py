@@ -155,11 +155,43 @@ class Simulation:
         self.handle
         return self._handle_bits
 
+    def _zero_low_halves(self, bits: int) -> bool:
+        """Every particle has the same mass m and its fixed-point value
+        q = m 2^bits is a non-zero multiple of 2^32 (N = 2^n particles of
+        mass total/N up to N = 2^20 with the automatic scale): the deposit's
+        low words would all stay zero."""
+        if self.cfg.mass_mode != "u64" or not self.n_particles:
+            return False
+        w = self.pos[:, 3]
+        lo, hi = float(w.min().item()), float(w.max().item())
+        if lo != hi or not (lo > 0 and math.isfinite(lo)):
+            return False
+        q = lo * 2.0 ** bits  # exact: a float32 times a power of two
+        return q < 2.0 ** 64 and q == math.floor(q) and q >= 2.0 ** 32 and math.fmod(q, 2.0 ** 32) == 0
+
+    def _apply_layout(self, h) -> None:
+        """Deposit histogram layout unless the caller chose one: high words
+        only (deposit_split = 1, twice the grids per CTA) when every low
+        half is zero, else the library's default.  Checked once per
+        particle set (one host read of the masses' range)."""
+        self._layout_checked = True
+        if "deposit_split" in (getattr(self, "_tuning", None) or {}):
+            return
+        want = 1 if self._zero_low_halves(self._handle_bits or 0) else 0
+        lib = _lib.lib()
+        t = _lib.MogTuningC()
+        _lib.check(lib.mog_get_tuning(h, ctypes.byref(t)), "mog_get_tuning")
+        if t.deposit_split != want:
+            t.deposit_split = want
+            _lib.check(lib.mog_set_tuning(h, ctypes.byref(t)), "mog_set_tuning")
+
     @property
     def handle(self):
         """The libmog handle; (re)created when the fixed-point scale changes."""
         bits = self._scale_bits() if self.cfg.mass_mode == "u64" else 0
         if self._handle is not None and bits == self._handle_bits:
+            if not getattr(self, "_layout_checked", False):
+                self._apply_layout(self._handle)
             return self._handle
         self.close()
         lib = _lib.lib()
@@ -177,6 +209,7 @@ class Simulation:
             for k, v in self._tuning.items():
                 setattr(t, k, int(v))
             _lib.check(lib.mog_set_tuning(h, ctypes.byref(t)), "mog_set_tuning")
+        self._apply_layout(h)
         return h
 
     def close(self) -> None:
@@ -207,7 +240,7 @@ class Simulation:
                 raise KeyError(f"unknown tuning field {k!r}")
             setattr(t, k, int(v))
         _lib.check(lib.mog_set_tuning(self.handle, ctypes.byref(t)), "mog_set_tuning")
-        self._tuning = dict(shapes)
+        self._tuning = {**(getattr(self, "_tuning", None) or {}), **shapes}
 
     # ------------------------------------------------------------------
     def set_particles(self, pos, vel=None) -> None:
@@ -228,6 +261,7 @@ class Simulation:
         self.pos = p
         self.vel = v
         self._auto_bits = None  # the fixed-point scale depends on the masses
+        self._layout_checked = False  # and so does the deposit's histogram layout
 
     def init_particles(self, kind: str = "uniform", seed: int | None = None, **kw) -> None:
         """Replace the particles with a named initial set: uniform, disks,

@@ -163,3 +163,33 @@ def test_learned_fold_is_bit_identical(g):
         a.close()
         b.close()
         model.close()
+
+
+def test_deposit_layout_follows_the_masses():
+    """Simulation picks the high-word deposit histogram (deposit_split = 1)
+    exactly when every fixed-point low half is zero, re-checks it when the
+    particles change, and leaves a caller's own choice alone; the steps are
+    bit-identical either way."""
+    n = 1 << 16
+    pos, vel = particles(n, seed=41)
+    pos[:, 3] = 1.0 / n  # q = 2^52 / 2^16 = 2^36: low halves zero
+    a = make_sim(k=8, g=16, n=n)
+    b = make_sim(k=8, g=16, n=n)
+    try:
+        a.set_particles(pos, vel)
+        b.set_particles(pos, vel)
+        b.tune(deposit_split=-1)
+        assert a.tuning()["deposit_split"] == 1 and b.tuning()["deposit_split"] == -1
+        a.step(3)
+        b.step(3)
+        torch.cuda.synchronize()
+        assert torch.equal(a.pos, b.pos) and torch.equal(a.vel, b.vel)
+        uneven = pos.copy()
+        uneven[:, 3] = np.linspace(0.5, 1.5, n, dtype=np.float32) / n
+        a.set_particles(uneven, vel)
+        assert a.tuning()["deposit_split"] == 0
+        a.set_particles(pos, vel)
+        assert a.tuning()["deposit_split"] == 1
+    finally:
+        a.close()
+        b.close()
