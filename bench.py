@@ -695,11 +695,12 @@ def run_learned(args, w: dict) -> dict | None:
                        "model": model_src, "index_mode": "fast", "mass_mode": "u64 fixed point",
                        "texture_aliasing": FFT_ALIASING,
                        "tuning": tuning or "library defaults",
-                       "deposit_layout": ("high words only (deposit_split 1), chosen by "
-                                          "Simulation: every mass is 1/N, N = 2^20, a fixed-point "
-                                          "value with a zero low half")
-                                         if cheap.tuning()["deposit_split"] == 1 else
-                                         "two words per cell",
+                       "deposit_layout": {1: "high words only (deposit_split 1), chosen by "
+                                             "Simulation: every mass is 1/N, N = 2^20, a "
+                                             "fixed-point value with a zero low half",
+                                          2: "counts of the equal masses (deposit_split 2), "
+                                             "chosen by Simulation"}.get(
+                                             cheap.tuning()["deposit_split"], "two words per cell"),
                        "parallelism": "single GPU" if world == 1 else f"{world} independent replicas",
                        "l2": "flushed between timed steps (256 MiB write)"},
             "accuracy": {"yardstick": "relative RMS force error vs FP64 periodic direct sum, 16,384 "

@@ -129,7 +129,10 @@ typedef struct mog_tuning {
     int32_t update_threads;         /* staged gather block: 512, 768 or 1024; 0 auto (512)   */
     int32_t deposit_split;          /* u64 shared histogram of high words only (low halves as
                                        global atomics; none for equal power-of-two masses):
-                                       0 auto (g = 32), 1 also at g = 8 and 16, -1 never      */
+                                       0 auto (g = 32), 1 also at g = 8 and 16, -1 never;
+                                       2 = one word per cell counting the particles of a CTA's
+                                       first mass (uniform masses of any value; any other mass
+                                       takes a global atomic), at g = 8, 16 and 32            */
     int32_t learned_fold;           /* learned step: 0 (default) or 1 = the fft solve's epilogue
                                        writes the cell masses (one launch fewer at g = 8, 16),
                                        -1 = a separate pass                                     */
@@ -345,7 +348,9 @@ int mog_batch_destroy(mog_batch* b);
  * deposit_split: 1 = u64 grids keep only their high words in the work-queue
  * deposit's shared memory at g = 8 and 16 too (twice the grids per tile;
  * pays when every mass has a zero fixed-point low half, which then needs no
- * global atomic), 0 = only at g = 32.
+ * global atomic), 0 = only at g = 32; 2 = one word per cell counting the
+ * particles of a tile's first mass at every g (uniform masses of any value;
+ * any other mass takes a global atomic).
  * The result never depends on these.  mog_batch_get_tuning also reports
  * whether the work-queue launches apply (active_work_queue, read only).
  */

@@ -26,6 +26,7 @@ class Batch:
         self._h = ctypes.c_void_p()
         self._built_for = None
         self._tuning = {"work_queue": 1, "deposit_chunk": 0, "deposit_split": 0}
+        self._split_chosen = False  # deposit_split set by the caller
 
     def _handles(self):
         hs = [s.handle for s in self.sims]  # creates / refreshes each handle
@@ -40,20 +41,31 @@ class Batch:
         return self._h
 
     def _apply_tuning(self) -> None:
+        split = int(self._tuning["deposit_split"])
+        if not self._split_chosen:
+            # one word per cell when every simulation's masses are equal:
+            # high words if every low half is zero, else counts (checked
+            # when the batch is built or retuned)
+            kinds = {s.deposit_layout(s.scale_bits) for s in self.sims}
+            split = 0 if 0 in kinds else (1 if kinds == {1} else 2)
         t = _lib.MogBatchTuningC(work_queue=int(self._tuning["work_queue"]),
                                  deposit_chunk=int(self._tuning["deposit_chunk"]),
-                                 deposit_split=int(self._tuning["deposit_split"]))
+                                 deposit_split=split)
         _lib.check(_lib.lib().mog_batch_set_tuning(self._h, ctypes.byref(t)), "mog_batch_set_tuning")
 
     def tune(self, **kw) -> None:
         """Set launch shapes: work_queue (1 persistent work-queue launches,
         0 one branch per simulation), deposit_chunk (particles per deposit
         tile, 0 = library default), deposit_split (1: high-word histograms
-        at every grid size, for masses whose fixed-point low halves are 0)."""
+        at every grid size, for masses whose fixed-point low halves are 0;
+        2: count histograms, for equal masses; chosen from the masses
+        unless set here)."""
         unknown = set(kw) - set(self._tuning)
         if unknown:
             raise ValueError(f"unknown batch tuning fields {sorted(unknown)}")
         self._tuning.update(kw)
+        if "deposit_split" in kw:
+            self._split_chosen = True
         if self._h:
             self._apply_tuning()
 

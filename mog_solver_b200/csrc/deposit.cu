@@ -324,7 +324,11 @@ __device__ __forceinline__ uint32_t cell_byte_offset(const DepositRows& r, const
 // rows, then the words).  count_total: add the tile's q to e.mass_total
 // (done by the tiles of the first grid group, which see every particle
 // once).  Returns after the flush, without a closing barrier.
-template <int LG, int MODE, int PPT, bool SPLIT, bool SHARD>
+// COUNT (u64, uniform masses): one word per cell counts the particles whose
+// fixed-point mass equals the tile's first particle's, q_ref; the flush adds
+// count * q_ref.  A particle with another mass (only when the masses are not
+// all equal) goes straight to its global cell with one 64-bit atomic.
+template <int LG, int MODE, int PPT, bool SPLIT, bool SHARD, bool COUNT = false>
 __device__ __forceinline__ void deposit_fast_tile(const float4* __restrict__ pos, int64_t lo,
                                                   int64_t hi, const Ensemble& e, int gpc, int g0,
                                                   int ng, bool count_total,
@@ -333,22 +337,30 @@ __device__ __forceinline__ void deposit_fast_tile(const float4* __restrict__ pos
     using H = SmemHist<MODE>;
     using Acc = typename H::Acc;
     static_assert(!SPLIT || MODE == 1, "the split histogram is for u64 grids");
+    static_assert(!COUNT || (MODE == 1 && !SPLIT && !SHARD), "the count histogram is for u64 grids");
+    constexpr bool ONE = SPLIT || COUNT;  // one shared word per cell
     constexpr int G3 = 1 << (3 * LG);
     static_assert(sizeof(DepositRows) == 48, "DepositRows layout");
     const uint32_t words = (uint32_t)ng * G3;
     DepositRows* rows = reinterpret_cast<DepositRows*>(smem_raw);              // gpc rows
     unsigned* lo_w = reinterpret_cast<unsigned*>(smem_raw + (size_t)gpc * 48);
-    unsigned* hi_w = SPLIT ? lo_w : lo_w + (size_t)gpc * G3;
+    unsigned* hi_w = ONE ? lo_w : lo_w + (size_t)gpc * G3;
     const uint32_t lo_base = (uint32_t)__cvta_generic_to_shared(lo_w);
     const uint32_t hi_base = (uint32_t)__cvta_generic_to_shared(hi_w);
 
     for (int i = threadIdx.x; i < ng; i += blockDim.x) rows[i] = deposit_rows(e.fast[g0 + i]);
     for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) {
         lo_w[i] = 0u;
-        if (H::kWords == 2 && !SPLIT) hi_w[i] = 0u;
+        if (H::kWords == 2 && !ONE) hi_w[i] = 0u;
     }
     __syncthreads();
 
+    Acc q_ref = 0;
+    if (COUNT && lo < hi) {
+        unsigned b = 0;
+        q_ref = (Acc)quantize_u64(__ldg(pos + lo).w, e.scale, b);
+    }
+    const unsigned rl = (unsigned)q_ref, rh = (unsigned)((unsigned long long)q_ref >> 32);
     const float half_l = e.world * 0.5f;
     const int T = blockDim.x;
     unsigned bad = 0;
@@ -357,10 +369,12 @@ __device__ __forceinline__ void deposit_fast_tile(const float4* __restrict__ pos
         const bool full = base + (int64_t)T * PPT <= hi;  // block-uniform
         float2 cc[PPT][3];
         unsigned ql[PPT], qh[PPT];
+        bool live[PPT];
 #pragma unroll
         for (int u = 0; u < PPT; ++u) {
             const int64_t slot = base + (int64_t)u * T + threadIdx.x;
             const bool valid = full || slot < hi;
+            live[u] = valid;
             const float4 P = valid ? __ldg(pos + slot) : make_float4(0.f, 0.f, 0.f, 0.f);
             unsigned b = 0;
             Acc q;
@@ -377,6 +391,45 @@ __device__ __forceinline__ void deposit_fast_tile(const float4* __restrict__ pos
             cc[u][0] = make_float2(cx, cx);
             cc[u][1] = make_float2(cy, cy);
             cc[u][2] = make_float2(cz, cz);
+        }
+        if constexpr (COUNT) {
+            // one vote per batch: does every particle of the warp have q_ref?
+            unsigned odd = 0;
+#pragma unroll
+            for (int u = 0; u < PPT; ++u) odd |= (live[u] && (ql[u] != rl || qh[u] != rh)) ? 1u : 0u;
+            if (__all_sync(kFull, odd == 0u)) {
+                // the whole warp counts: one add of 1 per particle and grid
+                // (full batches need no per-particle test)
+                for (int j = 0; j < ng; ++j) {
+                    const DepositRows r = rows[j];
+                    const uint32_t gbyte = (uint32_t)j * (G3 * 4u);
+                    const uint32_t base_j = hi_base + gbyte;
+#pragma unroll
+                    for (int u = 0; u < PPT; ++u) {
+                        const uint32_t off = cell_byte_offset<LG>(r, cc[u]);
+                        if (!in_bounds(e.flags, (gbyte + off) >> 2, words)) continue;
+                        const uint32_t addr = LG >= 4 ? base_j + hist_swizzle_bytes(off)
+                                                      : hi_base + hist_swizzle_bytes(gbyte + off);
+                        if (full || live[u]) red_shared(addr, 1u);
+                    }
+                }
+                continue;
+            }
+            for (int j = 0; j < ng; ++j) {
+                const DepositRows r = rows[j];
+                const uint32_t gbyte = (uint32_t)j * (G3 * 4u);
+#pragma unroll
+                for (int u = 0; u < PPT; ++u) {
+                    const uint32_t off = gbyte + cell_byte_offset<LG>(r, cc[u]);
+                    if (!in_bounds(e.flags, off >> 2, words)) continue;
+                    if (!live[u]) continue;
+                    if (ql[u] == rl && qh[u] == rh)
+                        red_shared(hi_base + hist_swizzle_bytes(off), 1u);
+                    else if (ql[u] | qh[u])
+                        atomicAdd(mass + (size_t)g0 * G3 + (off >> 2), ((Acc)qh[u] << 32) | (Acc)ql[u]);
+                }
+            }
+            continue;
         }
         // one vote per batch: can the low words be skipped for the whole warp?
         bool hi_only = false;
@@ -445,7 +498,7 @@ __device__ __forceinline__ void deposit_fast_tile(const float4* __restrict__ pos
     if (bad) raise_flags(e.flags, bad);
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) {
-        const Acc v = SPLIT ? (Acc)hi_w[i] << 32 : H::read(lo_w, hi_w, i);
+        const Acc v = COUNT ? (Acc)hi_w[i] * q_ref : (SPLIT ? (Acc)hi_w[i] << 32 : H::read(lo_w, hi_w, i));
         const uint32_t w = hist_swizzle(i);  // the grid word this shared word holds
         if (v && in_bounds(e.flags, (size_t)g0 * G3 + w, (uint64_t)e.cells())) {
             if constexpr (SHARD)
@@ -456,7 +509,7 @@ __device__ __forceinline__ void deposit_fast_tile(const float4* __restrict__ pos
     }
 }
 
-template <int LG, int MODE, int PPT, bool SPLIT = false, bool SHARD = false>
+template <int LG, int MODE, int PPT, bool SPLIT = false, bool SHARD = false, bool COUNT = false>
 __global__ void __launch_bounds__(1024) deposit_fast_kernel(const float4* __restrict__ pos,
                                                             int64_t n, int64_t chunk, Ensemble e,
                                                             int gpc,
@@ -464,7 +517,7 @@ __global__ void __launch_bounds__(1024) deposit_fast_kernel(const float4* __rest
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int g0 = blockIdx.y * gpc;
     const int64_t lo = (int64_t)blockIdx.x * chunk;
-    deposit_fast_tile<LG, MODE, PPT, SPLIT, SHARD>(pos, lo, min(n, lo + chunk), e, gpc, g0,
+    deposit_fast_tile<LG, MODE, PPT, SPLIT, SHARD, COUNT>(pos, lo, min(n, lo + chunk), e, gpc, g0,
                                                    min(gpc, e.k - g0), blockIdx.y == 0, mass,
                                                    smem_raw);
     shard_release<SHARD>();
@@ -475,9 +528,10 @@ __global__ void __launch_bounds__(1024) deposit_fast_kernel(const float4* __rest
 // host-built list with an atomic counter until it runs out, and deposits
 // each through the same tile body as deposit_fast_kernel.  The histogram
 // layout follows the tile's own grid count and grid size; at g = 32 in u64
-// mode it is the split (high-word) histogram, as in the single launch, and
-// with SPLIT16 at g = 8 and 16 as well.
-template <int MODE, bool SPLIT16>
+// mode it is the split (high-word) histogram, as in the single launch;
+// LAYOUT 1: the split histogram at g = 8 and 16 as well; LAYOUT 2: the count
+// histogram (uniform masses) at every grid size.
+template <int MODE, int LAYOUT>
 __global__ void __launch_bounds__(1024, 1) deposit_queue_kernel(const BatchSim* __restrict__ sims,
                                                                const DepositTile* __restrict__ tiles,
                                                                int ntiles, unsigned* __restrict__ counter) {
@@ -495,17 +549,18 @@ __global__ void __launch_bounds__(1024, 1) deposit_queue_kernel(const BatchSim* 
         const float4* pos = S.pos;
         Acc* mass = static_cast<Acc*>(S.mass);
         const bool first = tile.g0 == 0;
+        constexpr bool CNT = MODE == 1 && LAYOUT == 2;
+        constexpr bool SPL = MODE == 1 && LAYOUT == 1;
         if (e.lg == 3)
-            deposit_fast_tile<3, MODE, 4, MODE == 1 && SPLIT16, false>(pos, tile.lo, tile.hi, e, tile.ng,
-                                                                       tile.g0, tile.ng, first, mass,
-                                                                       smem_raw);
+            deposit_fast_tile<3, MODE, 4, SPL, false, CNT>(pos, tile.lo, tile.hi, e, tile.ng, tile.g0,
+                                                           tile.ng, first, mass, smem_raw);
         else if (e.lg == 4)
-            deposit_fast_tile<4, MODE, 4, MODE == 1 && SPLIT16, false>(pos, tile.lo, tile.hi, e, tile.ng,
-                                                                       tile.g0, tile.ng, first, mass,
-                                                                       smem_raw);
+            deposit_fast_tile<4, MODE, 4, SPL, false, CNT>(pos, tile.lo, tile.hi, e, tile.ng, tile.g0,
+                                                           tile.ng, first, mass, smem_raw);
         else
-            deposit_fast_tile<5, MODE, 4, MODE == 1, false>(pos, tile.lo, tile.hi, e, tile.ng,
-                                                            tile.g0, tile.ng, first, mass, smem_raw);
+            deposit_fast_tile<5, MODE, 4, MODE == 1 && !CNT, false, CNT>(pos, tile.lo, tile.hi, e,
+                                                                        tile.ng, tile.g0, tile.ng,
+                                                                        first, mass, smem_raw);
         __syncthreads();  // the next tile reuses the histogram and s_tile
     }
 }
@@ -608,12 +663,16 @@ static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, const int
     // g = 32 it fits one grid per CTA where the two-word one needs two
     // slabs (the default); at g = 8 and 16 (tuning deposit_split = 1) it
     // fits twice the grids per CTA.
-    const bool split32 = MODE == 1 && e.g == 32 && sh.grids_per_cta <= 1 && sh.split >= 0;
-    const bool split_small = !SHARD && MODE == 1 && (e.g == 8 || e.g == 16) && sh.split == 1;
-    const bool split = split32 || split_small;
+    // The count histogram (u64, tuning deposit_split = 2, for uniform masses):
+    // one word per cell at g = 8, 16 and 32 counting the particles of the
+    // tile's first mass, whatever that mass is.
+    const bool count = !SHARD && MODE == 1 && sh.split == 2 && (e.g == 8 || e.g == 16 || e.g == 32);
+    const bool split32 = !count && MODE == 1 && e.g == 32 && sh.grids_per_cta <= 1 && sh.split >= 0;
+    const bool split_small = !count && !SHARD && MODE == 1 && (e.g == 8 || e.g == 16) && sh.split == 1;
+    const bool split = split32 || split_small || count;
     if (split && IDX == 0 && !agg && !perm && sh.fast != 0) {
         const int fit = (int)std::max<size_t>(1, budget / ((size_t)4 << cells_lg));
-        if (split32) {
+        if (split32 || (count && e.g == 32 && sh.grids_per_cta <= 1)) {
             gpc = 1;
         } else if (sh.grids_per_cta > 0) {
             gpc = std::min(sh.grids_per_cta, fit);
@@ -647,6 +706,9 @@ static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, const int
             if (e.g == 16) return launch_fast(deposit_fast_kernel<4, MODE, 4, false, true>);
             return launch_fast(deposit_fast_kernel<3, MODE, 4, false, true>);
         } else {
+            if constexpr (MODE == 1) {
+                if (count && e.g == 32) return launch_fast(deposit_fast_kernel<5, 1, 4, false, false, true>);
+            }
             if (e.g == 32) {
                 if constexpr (MODE == 1) {
                     if (ppt == 1) return launch_fast(deposit_fast_kernel<5, 1, 1, true>);
@@ -659,6 +721,8 @@ static cudaError_t deposit_typed(const Ensemble& e, const float4* pos, const int
                 }
             }
             if constexpr (MODE == 1) {
+                if (count && e.g == 16) return launch_fast(deposit_fast_kernel<4, 1, 4, false, false, true>);
+                if (count) return launch_fast(deposit_fast_kernel<3, 1, 4, false, false, true>);
                 if (split_small && e.g == 16) return launch_fast(deposit_fast_kernel<4, 1, 4, true>);
                 if (split_small) return launch_fast(deposit_fast_kernel<3, 1, 4, true>);
             }
@@ -718,7 +782,7 @@ size_t queue_deposit_smem(int g, int mass_mode, int ng, bool split) {
     return (size_t)ng * 48 + 4 * words * (size_t)ng * g * g * g;
 }
 
-cudaError_t launch_deposit_queue(int mass_mode, bool split, const BatchSim* sims,
+cudaError_t launch_deposit_queue(int mass_mode, int layout, const BatchSim* sims,
                                  const DepositTile* tiles, int ntiles, unsigned* counter, size_t smem,
                                  cudaStream_t s) {
     if (ntiles <= 0) return cudaSuccess;
@@ -730,8 +794,9 @@ cudaError_t launch_deposit_queue(int mass_mode, bool split, const BatchSim* sims
         kern<<<ctas, 1024, smem, s>>>(sims, tiles, ntiles, counter);
         return cudaGetLastError();
     };
-    if (mass_mode != MOG_MASS_U64_FIXED) return go(deposit_queue_kernel<0, false>);
-    return split ? go(deposit_queue_kernel<1, true>) : go(deposit_queue_kernel<1, false>);
+    if (mass_mode != MOG_MASS_U64_FIXED) return go(deposit_queue_kernel<0, 0>);
+    if (layout == 2) return go(deposit_queue_kernel<1, 2>);
+    return layout == 1 ? go(deposit_queue_kernel<1, 1>) : go(deposit_queue_kernel<1, 0>);
 }
 
 cudaError_t launch_deposit(const Ensemble& e, const float4* pos, const int* perm, int64_t n,

@@ -814,7 +814,7 @@ int mog_set_tuning(mog_handle* h, const mog_tuning* t) {
          t->update_threads != 1024) ||
         (t->update_direct_ppt != 0 && t->update_direct_ppt != 1 && t->update_direct_ppt != 2 &&
          t->update_direct_ppt != 4) ||
-        t->deposit_split < -1 || t->deposit_split > 1 || t->learned_fold < -1 ||
+        t->deposit_split < -1 || t->deposit_split > 2 || t->learned_fold < -1 ||
         t->learned_fold > 1 ||
         (t->learned_ctas_per_sm != 0 && t->learned_ctas_per_sm != 2 && t->learned_ctas_per_sm != 3))
         return fail(MOG_ERR_ARG, "tuning value out of range");
@@ -1652,7 +1652,7 @@ int capture_queue_step(mog_batch* b, float* const* pos4, float* const* vel4, con
     int rc = MOG_OK;
     MOG_CUDA(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal), "begin capture");
     cudaError_t err = cudaMemsetAsync(d_cnt, 0, 2 * sizeof(unsigned), b->cap);
-    if (!err) err = mog::launch_deposit_queue(b->sims[0]->cfg.mass_mode, b->tuning.deposit_split > 0,
+    if (!err) err = mog::launch_deposit_queue(b->sims[0]->cfg.mass_mode, b->tuning.deposit_split,
                                               d_sims, d_dep, (int)dep.size(), d_cnt, smem, b->cap);
     if (!err) err = cudaEventRecord(b->fork, b->cap);
     for (int i = 0; i < count && !err; ++i) {
@@ -1682,7 +1682,7 @@ int mog_batch_set_tuning(mog_batch* b, const mog_batch_tuning* t) {
     if (!b || !t) return fail(MOG_ERR_ARG, "null argument");
     if (t->work_queue < 0 || t->work_queue > 1 || t->deposit_chunk < 0 ||
         (t->deposit_chunk > 0 && t->deposit_chunk < 1024) || t->deposit_split < 0 ||
-        t->deposit_split > 1)
+        t->deposit_split > 2)
         return fail(MOG_ERR_ARG, "batch tuning value out of range");
     b->tuning = *t;
     for (auto& g : b->graphs) release_entry(g);

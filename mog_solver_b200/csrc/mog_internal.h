@@ -78,7 +78,7 @@ struct DepositShape {
     int aggregate = -1;     // warp-merge runs of equal cells: -1 auto (when ordered), 0, 1
     int fast = 1;           // use the specialised kernel where it applies
     int sorted_input = 0;   // read the spatially ordered copy (else the caller's order)
-    int split = 0;          // u64 high-word-only histogram: 0 auto (g = 32), 1 also g = 8/16, -1 never
+    int split = 0;          // u64 one-word histogram: 0 auto (high words, g = 32), 1 high words also g = 8/16, 2 counts (uniform masses), -1 never
 };
 struct UpdateShape {
     int threads = 0;        // staged gather block size: 512, 768 or 1024; 0 auto
@@ -170,8 +170,8 @@ struct GatherTile {
 };
 // Grids per deposit tile for a simulation (whole grids in shared memory),
 // the tile's shared-memory bytes, and the particles of one gather tile.
-// split: u64 grids keep only high words in shared memory at every g (at
-// g = 32 they always do).
+// split: u64 grids keep one word per cell in shared memory at every g (high
+// words, or counts for uniform masses; at g = 32 they always do).
 int queue_deposit_grids(int g, int mass_mode, int k, bool split);
 size_t queue_deposit_smem(int g, int mass_mode, int ng, bool split);
 constexpr int kQueueGatherThreads = 512;
@@ -182,7 +182,7 @@ constexpr int64_t kQueueGatherTile = (int64_t)kQueueGatherThreads * kQueueGather
 // until the list runs out.  All simulations use FAST cell indices and
 // share the mass mode; g is 8, 16 or 32.  kmax: the most grids of any
 // simulation (the gather stages their index rows in shared memory).
-cudaError_t launch_deposit_queue(int mass_mode, bool split, const BatchSim* sims,
+cudaError_t launch_deposit_queue(int mass_mode, int layout, const BatchSim* sims,
                                  const DepositTile* tiles, int ntiles, unsigned* counter, size_t smem,
                                  cudaStream_t s);
 cudaError_t launch_gather_queue(const BatchSim* sims, const GatherTile* tiles, int ntiles,

@@ -155,29 +155,32 @@ class Simulation:
         self.handle
         return self._handle_bits
 
-    def _zero_low_halves(self, bits: int) -> bool:
-        """Every particle has the same mass m and its fixed-point value
-        q = m 2^bits is a non-zero multiple of 2^32 (N = 2^n particles of
-        mass total/N up to N = 2^20 with the automatic scale): the deposit's
-        low words would all stay zero."""
+    def deposit_layout(self, bits: int) -> int:
+        """The one-word deposit histogram that suits the masses at scale
+        2^bits (u64 fixed-point mode): 1 (high words) when every particle
+        has the same mass m and q = m 2^bits is a multiple of 2^32, 2
+        (counts) when the masses are equal otherwise, 0 (the two-word
+        histogram) for unequal masses."""
         if self.cfg.mass_mode != "u64" or not self.n_particles:
-            return False
+            return 0
         w = self.pos[:, 3]
         lo, hi = float(w.min().item()), float(w.max().item())
         if lo != hi or not (lo > 0 and math.isfinite(lo)):
-            return False
+            return 0
         q = lo * 2.0 ** bits  # exact: a float32 times a power of two
-        return q < 2.0 ** 64 and q == math.floor(q) and q >= 2.0 ** 32 and math.fmod(q, 2.0 ** 32) == 0
+        if q < 2.0 ** 64 and q >= 2.0 ** 32 and math.fmod(q, 2.0 ** 32) == 0:
+            return 1
+        return 2
 
     def _apply_layout(self, h) -> None:
-        """Deposit histogram layout unless the caller chose one: high words
-        only (deposit_split = 1, twice the grids per CTA) when every low
-        half is zero, else the library's default.  Checked once per
-        particle set (one host read of the masses' range)."""
+        """Deposit histogram layout unless the caller chose one (see
+        deposit_layout): one word per cell, twice the grids per CTA, when
+        the masses are equal.  Checked once per particle set (one host read
+        of the masses' range)."""
         self._layout_checked = True
         if "deposit_split" in (getattr(self, "_tuning", None) or {}):
             return
-        want = 1 if self._zero_low_halves(self._handle_bits or 0) else 0
+        want = self.deposit_layout(self._handle_bits or 0)
         lib = _lib.lib()
         t = _lib.MogTuningC()
         _lib.check(lib.mog_get_tuning(h, ctypes.byref(t)), "mog_get_tuning")

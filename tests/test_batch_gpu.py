@@ -76,12 +76,14 @@ def test_autotune_keeps_results_bit_exact(tmp_path):
 
 
 @pytest.mark.parametrize("mass_mode,chunk,split", [("u64", 0, 0), ("u64", 4096, 0), ("u32x1000", 20000, 0),
-                                                   ("u64", 0, 1), ("u64", 4096, 1)])
+                                                   ("u64", 0, 1), ("u64", 4096, 1), ("u64", 0, 2),
+                                                   ("u64", 4096, 2)])
 def test_work_queue_tiles_are_bit_exact(mass_mode, chunk, split):
     """Tile sizes that split every simulation into many deposit tiles (and
     a chunk that is not a multiple of the block), both mass modes, and the
-    high-word histograms at every grid size (deposit_split; these masses
-    have non-zero low halves, which take the global atomics)."""
+    one-word histograms at every grid size (deposit_split 1: high words, the
+    non-zero low halves of these masses as global atomics; 2: counts of each
+    tile's first mass, the other masses as global atomics)."""
     from mog_solver_b200 import Simulation, ics
     from mog_solver_b200.batch import Batch
 

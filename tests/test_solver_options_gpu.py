@@ -126,6 +126,34 @@ def test_split_histogram_at_small_grids_is_bit_exact(g, k, equal):
     assert np.array_equal(got, ref)
 
 
+@pytest.mark.parametrize("g,k", [(16, 32), (8, 40), (32, 6)])
+@pytest.mark.parametrize("masses", ["equal", "two", "random"])
+def test_count_histogram_is_bit_exact(g, k, masses):
+    """Tuning deposit_split = 2: the count histogram (one word per cell counting
+    the particles of a CTA's first mass, any other mass as a global atomic)
+    gives the integer oracle's grid for equal masses with non-zero low halves,
+    for two interleaved masses and for random ones."""
+    import oracle
+
+    n, L = 200003, 100.0
+    sim = make_sim(k=k, g=g, n=n)
+    sim.tune(deposit_split=2)
+    pos, vel = particles(n, L, seed=g + k + 1)
+    if masses == "equal":
+        pos[:, 3] = np.float32(1.0 / n)
+    elif masses == "two":
+        pos[:, 3] = np.where(np.arange(n) % 7 == 0, 2.0, 1.0).astype(np.float32) / n
+    else:
+        pos[:, 3] = np.random.default_rng(6).uniform(0.5, 2.0, n).astype(np.float32) / n
+    sim.set_particles(pos, vel)
+    got = sim.mass_grid().cpu().numpy().view(np.uint64)
+    ref = oracle.deposit(pos, sim.rotations, sim.offsets, g, L, oracle.MASS_U64, sim.scale_bits)
+    assert sim.tuning()["deposit_split"] == 2
+    assert np.array_equal(got, ref)
+    assert sim.status() == 0
+    sim.close()
+
+
 @pytest.mark.parametrize("g", [8, 16, 32])
 def test_learned_fold_is_bit_identical(g):
     """Tuning learned_fold = 1 (the default): the solve's epilogue writes the cell masses
@@ -166,9 +194,10 @@ def test_learned_fold_is_bit_identical(g):
 
 
 def test_deposit_layout_follows_the_masses():
-    """Simulation picks the high-word deposit histogram (deposit_split = 1)
-    exactly when every fixed-point low half is zero, re-checks it when the
-    particles change, and leaves a caller's own choice alone; the steps are
+    """Simulation picks a one-word deposit histogram exactly when every mass
+    is the same (deposit_split 1, high words, when every fixed-point low
+    half is zero; 2, counts, otherwise), re-checks it when the particles
+    change, and leaves a caller's own choice alone; the steps are
     bit-identical either way."""
     n = 1 << 16
     pos, vel = particles(n, seed=41)
@@ -180,6 +209,15 @@ def test_deposit_layout_follows_the_masses():
         b.set_particles(pos, vel)
         b.tune(deposit_split=-1)
         assert a.tuning()["deposit_split"] == 1 and b.tuning()["deposit_split"] == -1
+        a.step(3)
+        b.step(3)
+        torch.cuda.synchronize()
+        assert torch.equal(a.pos, b.pos) and torch.equal(a.vel, b.vel)
+        odd = pos.copy()
+        odd[:, 3] = np.float32(1.0 / 3.0) / n  # equal, with non-zero low halves
+        a.set_particles(odd, vel)
+        b.set_particles(odd, vel)
+        assert a.tuning()["deposit_split"] == 2
         a.step(3)
         b.step(3)
         torch.cuda.synchronize()
