@@ -462,8 +462,12 @@ __global__ void __launch_bounds__(THREADS, 1)
                 const uint32_t xa = smem_u32(xf + i * 16);
                 const float4 r0 = ld_shared_f4_at(xa), r1 = ld_shared_f4_at(xa + 16),
                              r2 = ld_shared_f4_at(xa + 32);
-                gather_grid<0, PPT, 0, false>(F, nullptr, r0, r1, r2, cx, cy, cz, axy, az, cnt, ip,
-                                              e.flags);
+                if (e.lg == 4)  // g = 16 with compile-time shifts and masks
+                    gather_grid<0, PPT, 4, false>(F, nullptr, r0, r1, r2, cx, cy, cz, axy, az, cnt,
+                                                  ip, e.flags);
+                else
+                    gather_grid<0, PPT, 0, false>(F, nullptr, r0, r1, r2, cx, cy, cz, axy, az, cnt,
+                                                  ip, e.flags);
                 __syncthreads();
                 if (abort_flag) {
                     // let the copies still in flight land (bounded) before the
