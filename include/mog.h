@@ -122,7 +122,8 @@ typedef struct mog_tuning {
     int32_t update_staged;          /* -1 auto, 0 gathers from L2, 1 shared-memory staged    */
     int32_t update_ctas;            /* CTAs of the staged gather (0 = one per SM)            */
     int32_t sort_every;             /* spatial re-ordering period in steps; 0 = never (default) */
-    int32_t update_direct_ppt;      /* particles per thread of the L2-gather update: 1, 2, 4 */
+    int32_t update_direct_ppt;      /* particles per thread of the L2-gather update: 1, 2, 4;
+                                       0 auto (4 from 8 x 256 threads per SM, else 1)       */
     int32_t deposit_aggregate;      /* warp-merge runs of equal cells: -1 auto, 0 off, 1 on  */
     int32_t deposit_generic;        /* 1: never use the specialised g <= 16 deposit kernel    */
     int32_t deposit_sorted;         /* 1: deposit from the spatially ordered copy too         */

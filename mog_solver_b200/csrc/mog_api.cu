@@ -824,7 +824,7 @@ int mog_set_tuning(mog_handle* h, const mog_tuning* t) {
     h->dshape.ppt = t->deposit_ppt ? t->deposit_ppt : 4;
     h->ushape.staged = t->update_staged;
     h->ushape.ctas = t->update_ctas;
-    h->ushape.direct_ppt = t->update_direct_ppt ? t->update_direct_ppt : 4;
+    h->ushape.direct_ppt = t->update_direct_ppt;
     h->sort_every = t->sort_every < 0 ? 0 : t->sort_every;
     h->dshape.aggregate = t->deposit_aggregate;
     h->dshape.fast = t->deposit_generic ? 0 : 1;

@@ -84,7 +84,7 @@ struct UpdateShape {
     int threads = 0;        // staged gather block size: 512, 768 or 1024; 0 auto
     int staged = -1;        // -1 auto, 0 global gathers, 1 smem-staged grids
     int ctas = 0;           // staged kernel CTAs; 0 = one per SM
-    int direct_ppt = 4;     // particles per thread of the direct gather
+    int direct_ppt = 0;     // particles per thread of the direct gather; 0 auto
 };
 
 int num_sms();

@@ -618,7 +618,11 @@ cudaError_t update_mode(const Ensemble& e, float4* pos, float4* vel, const float
         staged = e.g <= 16 && n >= (int64_t)sms * threads * 2 && smem <= 220 * 1024;
     if (staged && smem > 220 * 1024) staged = false;
     if (!staged) {
-        const int dppt = sh.direct_ppt == 1 ? 1 : (sh.direct_ppt == 2 ? 2 : 4);
+        // auto (0): 4 particles a thread (cell reuse, loads in flight) once
+        // there are enough threads to fill the SMs, else 1
+        const int dppt = sh.direct_ppt == 1 || sh.direct_ppt == 2 || sh.direct_ppt == 4
+                             ? sh.direct_ppt
+                             : (n >= (int64_t)sms * 256 * 8 ? 4 : 1);
         const int64_t threads_needed = (n + dppt - 1) / dppt;
         const unsigned blocks = (unsigned)((threads_needed + 255) / 256);
         if (dppt == 1)
