@@ -63,6 +63,11 @@ def _candidates(sim: Simulation) -> dict[str, list[dict]]:
         # high-word-only histograms: more grids per CTA, low halves as global atomics
         dep += [dict(deposit_split=1, deposit_grids_per_cta=0, deposit_ppt=4, deposit_threads=thr,
                      deposit_chunks=0) for thr in (512, 1024)]
+    if g in (8, 16, 32) and sim.cfg.mass_mode == "u64":
+        # count histograms: one word per cell, other masses than a CTA's
+        # first as global atomics
+        dep += [dict(deposit_split=2, deposit_grids_per_cta=0, deposit_ppt=4, deposit_threads=1024,
+                     deposit_chunks=0)]
     upd = [dict(update_staged=0, update_direct_ppt=1), dict(update_staged=0, update_direct_ppt=4)]
     if g <= 16:
         upd += [dict(update_staged=1, update_threads=t) for t in (512, 768, 1024)]
