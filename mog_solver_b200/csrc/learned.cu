@@ -419,6 +419,11 @@ __global__ void __launch_bounds__(kLT, MINB) learned_kernel(
         if (threadIdx.x < 8) sb[2 * kH + threadIdx.x] = threadIdx.x < kOut ? params[kB3 + threadIdx.x] : 0.f;
     }
     __syncthreads();
+    // Launched as a programmatic dependent of the solve (launch_learned), this
+    // grid may start while the solve still runs: the prologue above reads
+    // only the model and the transforms; the force grid, written by the
+    // solve, is read after this wait (a no-op without the dependency).
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     const IndexParams ip = e.index_params();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, tg = lane & 3;
     uint32_t* A = sA + warp * 32 * kARow;
@@ -730,9 +735,21 @@ cudaError_t launch_learned_t(const Ensemble& e, const GridRows* rows, float4* po
     int64_t blocks = std::min<int64_t>((n + kLT - 1) / kLT, (int64_t)num_sms() * std::max(per_sm, 1));
     if (out.spread && blocks > out.spread_cap) blocks = out.spread_cap;
     out.blocks = (int)blocks;
-    kern<<<(unsigned)blocks, kLT, smem, s>>>(pos, vel, n, W, e, norm, static_cast<const uint2*>(frags),
-                                            params, dt, damp, out.out4, out.feat, out.spread, tab);
-    return cudaGetLastError();
+    // programmatic dependent launch: the CTAs may be scheduled on the SMs the
+    // solve leaves idle (at k = 32 it runs 16 CTAs) and load the model while
+    // it finishes; the kernel waits for the solve before reading its grid
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)blocks);
+    cfg.blockDim = dim3(kLT);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, pos, vel, n, W, e, norm, static_cast<const uint2*>(frags),
+                              params, dt, damp, out.out4, out.feat, out.spread, tab);
 }
 
 template <int IDX, int LG, int K>

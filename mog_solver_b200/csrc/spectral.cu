@@ -256,6 +256,9 @@ __global__ void __launch_bounds__(3 * G * G, (G == 16 ? 1 : 4))
     const int l = t % L;  // line within a pass
     const int ga = 2 * blockIdx.x, gb = ga + 1;
     const bool hasb = gb < e.k;
+    // a grid launched after this one as its programmatic dependent (the
+    // learned kernel) may start once every CTA of this one has
+    asm volatile("griddepcontrol.launch_dependents;");
     if (blockIdx.x == 0 && t == 0 && (ZERO || DENS)) check_mass_total(e);
     if (WORLD && t < 24) Rs[t / 12][t % 12] = (t < 12 || hasb) ? __ldg(e.rot12 + 12 * ga + t) : 0.f;
 
