@@ -262,25 +262,37 @@ __global__ void __launch_bounds__(3 * G * G, (G == 16 ? 1 : 4))
     if (blockIdx.x == 0 && t == 0 && (ZERO || DENS)) check_mass_total(e);
     if (WORLD && t < 24) Rs[t / 12][t % 12] = (t < 12 || hasb) ? __ldg(e.rot12 + 12 * ga + t) : 0.f;
 
+    // the pair's masses into S0 (grid a in .x, grid b in .y), every thread
+    // of the CTA loading consecutive cells (coalesced); then the cells are
+    // cleared, in a loop of their own so that no store holds up the loads
+    constexpr int kPer = (G3 + 3 * L - 1) / (3 * L);
+    float2 mv[kPer];
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+        const int i = t + j * 3 * L;
+        if (i < G3) {
+            mv[j].x = load_mass(mass + (size_t)ga * G3 + i, e.inv_scale);
+            mv[j].y = hasb ? load_mass(mass + (size_t)gb * G3 + i, e.inv_scale) : 0.f;
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+        const int i = t + j * 3 * L;
+        if (i < G3) {
+            S0[(i / G) * P + (i % G)] = mv[j];
+            if (ZERO) {
+                mass[(size_t)ga * G3 + i] = 0;
+                if (hasb) mass[(size_t)gb * G3 + i] = 0;
+            }
+        }
+    }
+    __syncthreads();
     // forward, x axis: line = row (y, z)
     if (f == 0) {
         const int y = l % G, z = l / G;
-        const size_t row = (size_t)(z * G + y) * G;
-        Acc* ra = mass + (size_t)ga * G3 + row;
-        Acc* rb = mass + (size_t)gb * G3 + row;
         float2 v[G];
 #pragma unroll
-        for (int x = 0; x < G; ++x) {
-            v[x].x = load_mass(ra + x, e.inv_scale);
-            v[x].y = hasb ? load_mass(rb + x, e.inv_scale) : 0.f;
-        }
-        if (ZERO) {
-#pragma unroll
-            for (int x = 0; x < G; ++x) {
-                ra[x] = 0;
-                if (hasb) rb[x] = 0;
-            }
-        }
+        for (int x = 0; x < G; ++x) v[x] = S0[(z * G + y) * P + x];
         fft_reg<G, false>(v);
 #pragma unroll
         for (int x = 0; x < G; ++x) S0[(z * G + y) * P + x] = v[x];
