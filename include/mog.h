@@ -139,6 +139,9 @@ typedef struct mog_tuning {
                                        -1 = a separate pass                                     */
     int32_t learned_ctas_per_sm;    /* learned kernel occupancy: 0 auto (2), 2 or 3 CTAs of 256
                                        threads per SM (register budget 128, or 80 with spills) */
+    int32_t solve_split;            /* g = 8, 16 fft solve: 1 = a cluster of 3 CTAs per grid pair
+                                       (one gradient field each), -1 = one CTA per pair, 0 auto
+                                       (clusters while 3 x pairs <= SMs); same forces either way */
 } mog_tuning;
 
 /* Fill a config with the reference's in-code defaults (main.py:179-189). */

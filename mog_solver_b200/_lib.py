@@ -111,6 +111,7 @@ class MogTuningC(ctypes.Structure):
         ("deposit_split", ctypes.c_int32),
         ("learned_fold", ctypes.c_int32),
         ("learned_ctas_per_sm", ctypes.c_int32),
+        ("solve_split", ctypes.c_int32),
     ]
 
 

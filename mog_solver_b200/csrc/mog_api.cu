@@ -798,6 +798,7 @@ int mog_get_tuning(const mog_handle* h, mog_tuning* out) {
     out->deposit_split = h->dshape.split;
     out->learned_fold = h->learned_fold ? 1 : -1;
     out->learned_ctas_per_sm = h->learned_ctas;
+    out->solve_split = h->e.solve_split;
     return MOG_OK;
 }
 
@@ -816,7 +817,8 @@ int mog_set_tuning(mog_handle* h, const mog_tuning* t) {
          t->update_direct_ppt != 4) ||
         t->deposit_split < -1 || t->deposit_split > 2 || t->learned_fold < -1 ||
         t->learned_fold > 1 ||
-        (t->learned_ctas_per_sm != 0 && t->learned_ctas_per_sm != 2 && t->learned_ctas_per_sm != 3))
+        (t->learned_ctas_per_sm != 0 && t->learned_ctas_per_sm != 2 && t->learned_ctas_per_sm != 3) ||
+        t->solve_split < -1 || t->solve_split > 1)
         return fail(MOG_ERR_ARG, "tuning value out of range");
     h->dshape.threads = t->deposit_threads ? t->deposit_threads : 1024;
     h->dshape.grids_per_cta = t->deposit_grids_per_cta;
@@ -833,6 +835,7 @@ int mog_set_tuning(mog_handle* h, const mog_tuning* t) {
     h->dshape.split = t->deposit_split;
     h->learned_fold = t->learned_fold >= 0 ? 1 : 0;
     h->learned_ctas = t->learned_ctas_per_sm ? t->learned_ctas_per_sm : 2;
+    h->e.solve_split = t->solve_split;
     for (auto& g : h->graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);
     h->graphs.clear();

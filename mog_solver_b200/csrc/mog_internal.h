@@ -57,6 +57,7 @@ struct Ensemble {
     const void* dft_tables = nullptr;  // their DFT matrices (dft_tc_tables layout)
     unsigned* flags = nullptr;      // device status word
     double* mass_total = nullptr;   // running sum of q for the overflow check
+    int solve_split = 0;            // g = 8/16 fft solve on 3-CTA clusters: 0 auto, 1 always, -1 never
 
     __host__ __device__ int64_t cells() const { return (int64_t)k << (3 * lg); }
     __host__ __device__ IndexParams index_params() const {

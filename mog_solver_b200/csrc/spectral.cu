@@ -31,9 +31,13 @@
 // the result, and with physical masses (1/N) they would erase the field.
 #include <algorithm>
 
+#include <cooperative_groups.h>
+
 #include "mog_internal.h"
 
 namespace mog {
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -397,6 +401,153 @@ __global__ void __launch_bounds__(3 * G * G, (G == 16 ? 1 : 4))
 }
 
 // ---------------------------------------------------------------------
+// Split path, g = 8 and 16, for ensembles of few grid pairs: a cluster of
+// three CTAs of g^2 threads per pair, so that one pair's solve runs on
+// three SMs instead of one.  Every CTA of the cluster loads the pair and
+// runs the forward transform (one line per thread); CTA f then forms
+// gradient field f and runs its inverse transform in its own shared
+// memory; after a cluster barrier the three CTAs write the pair's cells,
+// reading the fields they lack from the other CTAs' shared memory
+// (distributed shared memory).  Per line and per cell the arithmetic is
+// that of spectral_fused3_kernel, so the forces are bit-identical to it;
+// the mass cells are cleared in the epilogue, once every CTA has read them.
+template <int G, typename Acc, bool WORLD, bool ZERO, bool DENS = false, bool SWZ = false>
+__global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(G * G)
+    spectral_split3_kernel(Acc* __restrict__ mass, float4* __restrict__ force, Ensemble e) {
+    static_assert(!DENS || (WORLD && !ZERO && !SWZ), "cell masses go with kFrameWorld forces");
+    static_assert(!SWZ || WORLD, "slots are a world-frame layout");
+    constexpr int P = G + 1, G3 = G * G * G, L = G * G;
+    extern __shared__ float2 sm[];  // this CTA's field, [z][y][x] with rows padded to P
+    __shared__ float Rs[2][12];
+    cg::cluster_group cluster = cg::this_cluster();
+    const int f = (int)cluster.block_rank();  // the gradient field of this CTA
+    const int t = threadIdx.x;                // the line of every pass
+    const int ga = 2 * (blockIdx.x / 3), gb = ga + 1;
+    const bool hasb = gb < e.k;
+    asm volatile("griddepcontrol.launch_dependents;");
+    if (blockIdx.x == 0 && t == 0 && (ZERO || DENS)) check_mass_total(e);
+    if (WORLD && t < 24) Rs[t / 12][t % 12] = (t < 12 || hasb) ? __ldg(e.rot12 + 12 * ga + t) : 0.f;
+
+    // the pair's masses (grid a in .x, grid b in .y), consecutive threads on
+    // consecutive cells; every load issued before the first store
+    float2 mv[G];
+#pragma unroll
+    for (int j = 0; j < G; ++j) {
+        const int i = t + j * L;
+        mv[j].x = load_mass(mass + (size_t)ga * G3 + i, e.inv_scale);
+        mv[j].y = hasb ? load_mass(mass + (size_t)gb * G3 + i, e.inv_scale) : 0.f;
+    }
+#pragma unroll
+    for (int j = 0; j < G; ++j) {
+        const int i = t + j * L;
+        sm[(i / G) * P + (i % G)] = mv[j];
+    }
+    __syncthreads();
+    {  // forward, x axis: line = row (y, z)
+        const int y = t % G, z = t / G;
+        float2 v[G];
+#pragma unroll
+        for (int x = 0; x < G; ++x) v[x] = sm[(z * G + y) * P + x];
+        fft_reg<G, false>(v);
+#pragma unroll
+        for (int x = 0; x < G; ++x) sm[(z * G + y) * P + x] = v[x];
+    }
+    __syncthreads();
+    {  // forward, y axis: line = column (x, z)
+        const int x = t % G, z = t / G;
+        float2 v[G];
+#pragma unroll
+        for (int y = 0; y < G; ++y) v[y] = sm[(z * G + y) * P + x];
+        fft_reg<G, false>(v);
+#pragma unroll
+        for (int y = 0; y < G; ++y) sm[(z * G + y) * P + x] = v[y];
+    }
+    __syncthreads();
+    const int kx = t % G, ky = t / G;
+    {  // forward, z axis: line = column (kx, ky)
+        float2 v[G];
+#pragma unroll
+        for (int z = 0; z < G; ++z) v[z] = sm[(z * G + ky) * P + kx];
+        fft_reg<G, false>(v);
+#pragma unroll
+        for (int z = 0; z < G; ++z) sm[(z * G + ky) * P + kx] = v[z];
+    }
+    __syncthreads();
+    {  // Green's factor and gradient of field f from X^(k) and X^(-k), inverse z
+        const float kxn = (kx == G / 2) ? 0.f : e.ktab[kx];
+        const float kyn = (ky == G / 2) ? 0.f : e.ktab[ky];
+        const int xm = (G - kx) & (G - 1), ym = (G - ky) & (G - 1);
+        float2 v[G];
+#pragma unroll
+        for (int kz = 0; kz < G; ++kz) {
+            const float2 own = sm[(kz * G + ky) * P + kx];
+            const float2 mir = sm[(((G - kz) & (G - 1)) * G + ym) * P + xm];
+            const float gk = __ldg(e.green + (kz * G + ky) * G + kx);
+            const float kzn = (kz == G / 2) ? 0.f : __ldg(e.ktab + kz);
+            const Bins b = gradient_bins(own, mir, gk, kxn, kyn, kzn);
+            v[kz] = f == 0 ? b.z1 : (f == 1 ? b.z2 : b.z3);
+        }
+        fft_reg<G, true>(v);
+        __syncthreads();  // every thread has read X^ before the field overwrites it
+#pragma unroll
+        for (int z = 0; z < G; ++z) sm[(z * G + ky) * P + kx] = v[z];
+    }
+    __syncthreads();
+    {  // inverse, y axis: line = column (x, z)
+        const int x = t % G, z = t / G;
+        float2 v[G];
+#pragma unroll
+        for (int y = 0; y < G; ++y) v[y] = sm[(z * G + y) * P + x];
+        fft_reg<G, true>(v);
+#pragma unroll
+        for (int y = 0; y < G; ++y) sm[(z * G + y) * P + x] = v[y];
+    }
+    __syncthreads();
+    {  // inverse, x axis: line = row (y, z)
+        const int y = t % G, z = t / G;
+        float2 v[G];
+#pragma unroll
+        for (int x = 0; x < G; ++x) v[x] = sm[(z * G + y) * P + x];
+        fft_reg<G, true>(v);
+#pragma unroll
+        for (int x = 0; x < G; ++x) sm[(z * G + y) * P + x] = v[x];
+    }
+    // the three fields complete and visible to the whole cluster
+    cluster.sync();
+    const float2* Z1 = cluster.map_shared_rank(sm, 0);
+    const float2* Z2 = cluster.map_shared_rank(sm, 1);
+    const float2* Z3 = cluster.map_shared_rank(sm, 2);
+    // epilogue (pack.glsl:20-29), the pair's cells dealt round the cluster's
+    // 3 g^2 threads as spectral_fused3_kernel deals them round its own
+    const float invn = 1.0f / (float)G3;
+    const int cells = (hasb ? 2 : 1) * G3;
+    for (int idx = f * L + t; idx < cells; idx += 3 * L) {
+        const int gsel = idx / G3, c = idx % G3;
+        const int srow = (c / G) * P + (c % G);
+        const float2 z2 = Z2[srow];
+        float fx, fy, fz;
+        if (gsel == 0) {
+            const float2 z1 = Z1[srow];
+            fx = (e.alias_xz ? z2.x : z1.x) * invn;
+            fy = z1.y * invn;
+            fz = z2.x * invn;
+        } else {
+            const float2 z3 = Z3[srow];
+            fx = (e.alias_xz ? z2.y : z3.x) * invn;
+            fy = z3.y * invn;
+            fz = z2.y * invn;
+        }
+        float4 o = make_out(WORLD, Rs[gsel], fx, fy, fz);
+        Acc* mc = mass + (size_t)(ga + gsel) * G3 + c;
+        if (DENS) o.w = mass_value(*mc, e.inv_scale);
+        if (ZERO || DENS) *mc = 0;
+        force[(size_t)(ga + gsel) * G3 + (SWZ ? force_slot((uint32_t)c, ilog2<G>()) : (uint32_t)c)] = o;
+    }
+    // no CTA leaves while another may still read its field
+    cluster.sync();
+}
+
+// ---------------------------------------------------------------------
 // Multi-pass path (any g up to 64, used for g >= 32): the same algebra,
 // with each axis pass a separate launch over global (L2-resident) scratch.
 
@@ -519,6 +670,24 @@ __global__ void __launch_bounds__(256) mp_store_kernel(const float2* __restrict_
     }
 }
 
+// The split solve (a 3-CTA cluster per pair) when asked for, or by default
+// when the clusters fill no more than one wave of the SMs, i.e. when one
+// CTA per pair would leave most SMs idle.
+static bool use_split(const Ensemble& e) {
+    if (e.solve_split != 0) return e.solve_split > 0;
+    return 3 * ((e.k + 1) / 2) <= num_sms();
+}
+
+template <int G, typename Acc, bool WORLD, bool ZERO, bool DENS = false, bool SWZ = false>
+cudaError_t launch_split(const Ensemble& e, Acc* mass, float4* force, cudaStream_t s) {
+    auto kern = spectral_split3_kernel<G, Acc, WORLD, ZERO, DENS, SWZ>;
+    const size_t smem = (size_t)G * G * (G + 1) * sizeof(float2);
+    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return err;
+    kern<<<3 * ((e.k + 1) / 2), G * G, smem, s>>>(mass, force, e);
+    return cudaGetLastError();
+}
+
 template <int G, typename Acc>
 cudaError_t run_fused(const Ensemble& e, Acc* mass, float4* force, int frame, bool zero,
                       cudaStream_t s) {
@@ -533,6 +702,16 @@ cudaError_t run_fused(const Ensemble& e, Acc* mass, float4* force, int frame, bo
         return cudaGetLastError();
     };
     if constexpr (G >= 8) {
+        if (use_split(e)) {
+            if (swz)
+                return zero ? launch_split<G, Acc, true, true, false, true>(e, mass, force, s)
+                            : launch_split<G, Acc, true, false, false, true>(e, mass, force, s);
+            if (world)
+                return zero ? launch_split<G, Acc, true, true>(e, mass, force, s)
+                            : launch_split<G, Acc, true, false>(e, mass, force, s);
+            return zero ? launch_split<G, Acc, false, true>(e, mass, force, s)
+                        : launch_split<G, Acc, false, false>(e, mass, force, s);
+        }
         constexpr int T = 3 * G * G;
         if (swz)
             return zero ? pick(spectral_fused3_kernel<G, Acc, true, true, false, true>, T)
@@ -661,6 +840,9 @@ template <typename Acc>
 static cudaError_t spectral_density_typed(const Ensemble& e, Acc* mass, float4* force,
                                           void* scratch, cudaStream_t s) {
     if (!e.dft_tc && (e.g == 8 || e.g == 16)) {
+        if (use_split(e))
+            return e.g == 16 ? launch_split<16, Acc, true, false, true>(e, mass, force, s)
+                             : launch_split<8, Acc, true, false, true>(e, mass, force, s);
         const int pairs = (e.k + 1) / 2;
         auto go = [&](auto kern, int G) -> cudaError_t {
             const size_t smem = (size_t)3 * G * G * (G + 1) * sizeof(float2);

@@ -231,3 +231,74 @@ def test_deposit_layout_follows_the_masses():
     finally:
         a.close()
         b.close()
+
+
+@pytest.mark.parametrize("g,k,alias", [(16, 32, False), (16, 7, False), (8, 40, False),
+                                       (16, 240, False), (16, 32, True)])
+def test_split_solve_is_bit_identical(g, k, alias):
+    """Tuning solve_split = 1 (a cluster of three CTAs per grid pair, one
+    gradient field each, the fields read across the cluster's shared memory)
+    gives the forces of the one-CTA-per-pair solve (-1) bit for bit: in the
+    grid frame (mog_solve), at the particles, over plain steps (world-frame
+    slots, mass grid cleared by the solve) and over learned steps (cell masses
+    in the force grid); odd k leaves the last pair one grid."""
+    import ctypes
+
+    from mog_solver_b200 import Simulation, _lib
+    from mog_solver_b200.learned import Model
+    from mog_solver_b200.train_learned import DEFAULT_MODEL
+
+    n = 60000
+    pos, vel = particles(n, seed=g + k + 3)
+    cfg = {"n_grids": k, "grid_size": g, "world_size": 100.0, "num_particles": n, "G": 100.0,
+           "dt": 1e-3, "seed": 4, "reference_texture_aliasing": alias}
+    a, b = Simulation(dict(cfg)), Simulation(dict(cfg))
+    model = None
+    try:
+        a.tune(solve_split=-1)
+        b.tune(solve_split=1)
+        assert a.tuning()["solve_split"] == -1 and b.tuning()["solve_split"] == 1
+        a.set_particles(pos, vel)
+        b.set_particles(pos, vel)
+        m = a.mass_grid()
+        assert torch.equal(a.solve_grid(m.clone()), b.solve_grid(m.clone()))
+        assert torch.equal(a.forces(), b.forces())
+        a.step(3)
+        b.step(3)
+        torch.cuda.synchronize()
+        assert torch.equal(a.pos, b.pos) and torch.equal(a.vel, b.vel)
+        if k == 32 and not alias:
+            model = Model.load(DEFAULT_MODEL)
+            lib = _lib.lib()
+            for _ in range(2):
+                for s in (a, b):
+                    _lib.check(lib.mog_learned_step(s.handle, model.handle, s.pos.data_ptr(),
+                                                    s.vel.data_ptr(), n, 1e-3, None), "learned step")
+            torch.cuda.synchronize()
+            assert torch.equal(a.pos, b.pos) and torch.equal(a.vel, b.vel)
+            sa, sb = (ctypes.c_double * 2)(), (ctypes.c_double * 2)()
+            _lib.check(lib.mog_learned_spread(a.handle, sa, None), "spread")
+            _lib.check(lib.mog_learned_spread(b.handle, sb, None), "spread")
+            assert list(sa) == list(sb)
+        assert a.status() == 0 and b.status() == 0
+    finally:
+        a.close()
+        b.close()
+        if model is not None:
+            model.close()
+
+
+def test_solve_split_defaults_to_auto_and_checks_its_range():
+    """solve_split starts at 0 (auto: the clustered solve while three CTAs per
+    grid pair fit one wave of the SMs) and mog_set_tuning refuses values
+    outside -1..1."""
+    from mog_solver_b200._lib import MogError
+
+    a = make_sim(k=32, g=16, n=1000)
+    try:
+        assert a.tuning()["solve_split"] == 0
+        with pytest.raises(MogError):
+            a.tune(solve_split=2)
+        assert a.tuning()["solve_split"] == 0
+    finally:
+        a.close()
