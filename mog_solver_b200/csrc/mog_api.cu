@@ -191,6 +191,7 @@ struct mog_handle {
     int sort_every = 0;          // re-order every this many steps (0 = never)
     int learned_fold = 1;        // learned step: cell masses written by the solve's epilogue
     int learned_ctas = 2;        // learned kernel CTAs per SM (2 or 3)
+    int solve_split = 0;         // g = 8/16 fft solve on 3-CTA clusters: 0 auto, 1, -1
     uint64_t step_count = 0;     // steps issued (decides when to re-order)
     std::vector<GraphEntry> graphs;
     std::vector<mog::GridRows> rows;  // learned-gather rows of the k grids (host)
@@ -379,7 +380,7 @@ int run_pipeline(mog_handle* h, float4* pos, float4* vel, int64_t n, float dt, f
                           : mog::launch_deposit(e, pos, nullptr, n, false, h->d_mass, h->dshape, s);
     if (err != cudaSuccess) return cuda_fail(err, "deposit");
     if (h->cfg.solver == MOG_SOLVER_FFT)
-        err = mog::launch_spectral(e, h->d_mass, h->d_force, mog::kFrameWorldSlot, true, h->d_scratch, s);
+        err = mog::launch_spectral(e, h->d_mass, h->d_force, mog::kFrameWorldSlot, true, h->d_scratch, s, h->solve_split);
     else
         err = mog::launch_convolution(e, h->d_mass, h->d_force, mog::kFrameWorldSlot, true, s);
     if (err != cudaSuccess) return cuda_fail(err, "solve");
@@ -690,7 +691,7 @@ int mog_step_profiled(mog_handle* h, float* pos4, float* vel4, int64_t n, float 
     if (!err) err = cudaEventRecord(ev[2], s);
     if (!err)
         err = h->cfg.solver == MOG_SOLVER_FFT
-                  ? mog::launch_spectral(e, h->d_mass, h->d_force, mog::kFrameWorldSlot, true, h->d_scratch, s)
+                  ? mog::launch_spectral(e, h->d_mass, h->d_force, mog::kFrameWorldSlot, true, h->d_scratch, s, h->solve_split)
                   : mog::launch_convolution(e, h->d_mass, h->d_force, mog::kFrameWorldSlot, true, s);
     if (!err) err = cudaEventRecord(ev[3], s);
     if (!err)
@@ -750,7 +751,7 @@ int mog_solve(mog_handle* h, const void* mass_in, float* force4_out, void* strea
     if (h->cfg.solver == MOG_SOLVER_FFT)
         err = mog::launch_spectral(h->e, const_cast<void*>(mass_in),
                                    reinterpret_cast<float4*>(force4_out), mog::kFrameGrid, false,
-                                   h->d_scratch, s);
+                                   h->d_scratch, s, h->solve_split);
     else
         err = mog::launch_convolution(h->e, const_cast<void*>(mass_in),
                                       reinterpret_cast<float4*>(force4_out), mog::kFrameGrid, false, s);
@@ -798,7 +799,7 @@ int mog_get_tuning(const mog_handle* h, mog_tuning* out) {
     out->deposit_split = h->dshape.split;
     out->learned_fold = h->learned_fold ? 1 : -1;
     out->learned_ctas_per_sm = h->learned_ctas;
-    out->solve_split = h->e.solve_split;
+    out->solve_split = h->solve_split;
     return MOG_OK;
 }
 
@@ -835,7 +836,7 @@ int mog_set_tuning(mog_handle* h, const mog_tuning* t) {
     h->dshape.split = t->deposit_split;
     h->learned_fold = t->learned_fold >= 0 ? 1 : 0;
     h->learned_ctas = t->learned_ctas_per_sm ? t->learned_ctas_per_sm : 2;
-    h->e.solve_split = t->solve_split;
+    h->solve_split = t->solve_split;
     for (auto& g : h->graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);
     h->graphs.clear();
@@ -1018,7 +1019,7 @@ int mog_shard_finish(mog_handle* h, float* pos4, float* vel4, int64_t n, float d
     if ((rc = order_particles(h, pos, n, wants_sort(h, n), s, &perm, &pos_s))) return rc;
     const mog::Ensemble& e = h->e;
     cudaError_t err = h->cfg.solver == MOG_SOLVER_FFT
-                          ? mog::launch_spectral(e, h->d_mass, h->d_force, mog::kFrameWorldSlot, true, h->d_scratch, s)
+                          ? mog::launch_spectral(e, h->d_mass, h->d_force, mog::kFrameWorldSlot, true, h->d_scratch, s, h->solve_split)
                           : mog::launch_convolution(e, h->d_mass, h->d_force, mog::kFrameWorldSlot, true, s);
     if (err != cudaSuccess) return cuda_fail(err, "solve");
     err = mog::launch_update(e, pos, reinterpret_cast<float4*>(vel4), pos_s, perm, n, h->d_force,
@@ -1156,12 +1157,12 @@ static int run_learned(mog_handle* h, const mog_model* m, int out_mode, float* p
     if (h->cfg.solver == MOG_SOLVER_FFT && h->learned_fold) {
         // the solve's epilogue leaves the cell masses in the force grid's .w
         // (a separate pass where the fused kernel does not apply)
-        err = mog::launch_spectral_density(e, h->d_mass, h->d_force, h->d_scratch, s);
+        err = mog::launch_spectral_density(e, h->d_mass, h->d_force, h->d_scratch, s, h->solve_split);
         if (err != cudaSuccess) return cuda_fail(err, "solve");
         if (ev && (err = cudaEventRecord(ev[2], s))) return cuda_fail(err, "event");
     } else {
         if (h->cfg.solver == MOG_SOLVER_FFT)
-            err = mog::launch_spectral(e, h->d_mass, h->d_force, mog::kFrameWorld, false, h->d_scratch, s);
+            err = mog::launch_spectral(e, h->d_mass, h->d_force, mog::kFrameWorld, false, h->d_scratch, s, h->solve_split);
         else
             err = mog::launch_convolution(e, h->d_mass, h->d_force, mog::kFrameWorld, false, s);
         if (err != cudaSuccess) return cuda_fail(err, "solve");
@@ -1262,16 +1263,16 @@ static int run_host_step(mog_handle* h, const mog_model* m, float* pos_host, flo
     if (err) return cuda_fail(err, "deposit");
     if (m) {
         if (h->cfg.solver == MOG_SOLVER_FFT && h->learned_fold) {
-            err = mog::launch_spectral_density(e, h->d_mass, h->d_force, h->d_scratch, s);
+            err = mog::launch_spectral_density(e, h->d_mass, h->d_force, h->d_scratch, s, h->solve_split);
         } else {
             err = h->cfg.solver == MOG_SOLVER_FFT
-                      ? mog::launch_spectral(e, h->d_mass, h->d_force, mog::kFrameWorld, false, h->d_scratch, s)
+                      ? mog::launch_spectral(e, h->d_mass, h->d_force, mog::kFrameWorld, false, h->d_scratch, s, h->solve_split)
                       : mog::launch_convolution(e, h->d_mass, h->d_force, mog::kFrameWorld, false, s);
             if (!err) err = mog::launch_density_w(e, h->d_mass, h->d_force, s);
         }
     } else {
         err = h->cfg.solver == MOG_SOLVER_FFT
-                  ? mog::launch_spectral(e, h->d_mass, h->d_force, mog::kFrameWorldSlot, true, h->d_scratch, s)
+                  ? mog::launch_spectral(e, h->d_mass, h->d_force, mog::kFrameWorldSlot, true, h->d_scratch, s, h->solve_split)
                   : mog::launch_convolution(e, h->d_mass, h->d_force, mog::kFrameWorldSlot, true, s);
     }
     if (err) return cuda_fail(err, "solve");
@@ -1662,7 +1663,7 @@ int capture_queue_step(mog_batch* b, float* const* pos4, float* const* vel4, con
         mog_handle* h = b->sims[i];
         err = cudaStreamWaitEvent(b->branch[i], b->fork, 0);
         if (!err) err = mog::launch_spectral(h->e, h->d_mass, h->d_force, mog::kFrameWorldSlot, true, h->d_scratch,
-                                             b->branch[i]);
+                                             b->branch[i], h->solve_split);
         if (!err) err = cudaEventRecord(b->done[i], b->branch[i]);
         if (!err) err = cudaStreamWaitEvent(b->cap, b->done[i], 0);
     }

@@ -57,7 +57,6 @@ struct Ensemble {
     const void* dft_tables = nullptr;  // their DFT matrices (dft_tc_tables layout)
     unsigned* flags = nullptr;      // device status word
     double* mass_total = nullptr;   // running sum of q for the overflow check
-    int solve_split = 0;            // g = 8/16 fft solve on 3-CTA clusters: 0 auto, 1 always, -1 never
 
     __host__ __device__ int64_t cells() const { return (int64_t)k << (3 * lg); }
     __host__ __device__ IndexParams index_params() const {
@@ -113,9 +112,12 @@ constexpr int kFrameWorldSlot = 2;
 
 // force grid <- mass grid in the layout `frame` names.  zero_mass clears
 // the input for the next step.  scratch: device memory of
-// spectral_scratch_bytes(e) bytes.
+// spectral_scratch_bytes(e) bytes.  split: the g = 8/16 fft solve on
+// clusters of three CTAs per grid pair, 0 auto, 1 always, -1 never (same
+// forces; kept out of Ensemble, whose size shapes every kernel's
+// parameter block).
 cudaError_t launch_spectral(const Ensemble& e, void* mass, float4* force, int frame,
-                            bool zero_mass, void* scratch, cudaStream_t s);
+                            bool zero_mass, void* scratch, cudaStream_t s, int split = 0);
 size_t spectral_scratch_bytes(const Ensemble& e);
 
 cudaError_t launch_convolution(const Ensemble& e, void* mass, float4* force, int frame,
@@ -130,7 +132,7 @@ cudaError_t launch_dft_tc(int g, float2* f0, float2* f1, float2* f2, int nf, int
 // World-frame spectral solve that also leaves each cell's mass in the
 // force grid's .w lane and clears the mass grid (the learned path).
 cudaError_t launch_spectral_density(const Ensemble& e, void* mass, float4* force, void* scratch,
-                                    cudaStream_t s);
+                                    cudaStream_t s, int split = 0);
 // Rotate a grid-frame force grid (kFrameGrid) into the world frame, stored
 // as kFrameWorldSlot for launch_update (the stage entry point mog_update).
 cudaError_t launch_prerotate(const Ensemble& e, const float4* force_grid, float4* force_world,

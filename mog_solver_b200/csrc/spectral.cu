@@ -673,8 +673,8 @@ __global__ void __launch_bounds__(256) mp_store_kernel(const float2* __restrict_
 // The split solve (a 3-CTA cluster per pair) when asked for, or by default
 // when the clusters fill no more than one wave of the SMs, i.e. when one
 // CTA per pair would leave most SMs idle.
-static bool use_split(const Ensemble& e) {
-    if (e.solve_split != 0) return e.solve_split > 0;
+static bool use_split(const Ensemble& e, int split) {
+    if (split != 0) return split > 0;
     return 3 * ((e.k + 1) / 2) <= num_sms();
 }
 
@@ -690,7 +690,7 @@ cudaError_t launch_split(const Ensemble& e, Acc* mass, float4* force, cudaStream
 
 template <int G, typename Acc>
 cudaError_t run_fused(const Ensemble& e, Acc* mass, float4* force, int frame, bool zero,
-                      cudaStream_t s) {
+                      cudaStream_t s, int split) {
     const bool world = frame != kFrameGrid, swz = frame == kFrameWorldSlot;
     const int pairs = (e.k + 1) / 2;
     const size_t smem = (size_t)3 * G * G * (G + 1) * sizeof(float2);
@@ -702,7 +702,7 @@ cudaError_t run_fused(const Ensemble& e, Acc* mass, float4* force, int frame, bo
         return cudaGetLastError();
     };
     if constexpr (G >= 8) {
-        if (use_split(e)) {
+        if (use_split(e, split)) {
             if (swz)
                 return zero ? launch_split<G, Acc, true, true, false, true>(e, mass, force, s)
                             : launch_split<G, Acc, true, false, false, true>(e, mass, force, s);
@@ -780,14 +780,14 @@ cudaError_t run_multipass(const Ensemble& e, Acc* mass, float4* force, int frame
 
 template <typename Acc>
 cudaError_t spectral_typed(const Ensemble& e, Acc* mass, float4* force, int frame, bool zero,
-                           void* scratch, cudaStream_t s) {
+                           void* scratch, cudaStream_t s, int split) {
     if (frame < kFrameGrid || frame > kFrameWorldSlot) return cudaErrorInvalidValue;
     if (e.dft_tc && e.g == 16) return run_multipass<16, Acc>(e, mass, force, frame, zero, scratch, s);
     switch (e.g) {
-        case 2: return run_fused<2, Acc>(e, mass, force, frame, zero, s);
-        case 4: return run_fused<4, Acc>(e, mass, force, frame, zero, s);
-        case 8: return run_fused<8, Acc>(e, mass, force, frame, zero, s);
-        case 16: return run_fused<16, Acc>(e, mass, force, frame, zero, s);
+        case 2: return run_fused<2, Acc>(e, mass, force, frame, zero, s, split);
+        case 4: return run_fused<4, Acc>(e, mass, force, frame, zero, s, split);
+        case 8: return run_fused<8, Acc>(e, mass, force, frame, zero, s, split);
+        case 16: return run_fused<16, Acc>(e, mass, force, frame, zero, s, split);
         case 32: return run_multipass<32, Acc>(e, mass, force, frame, zero, scratch, s);
         case 64: return run_multipass<64, Acc>(e, mass, force, frame, zero, scratch, s);
         default: return cudaErrorInvalidValue;
@@ -838,9 +838,9 @@ __global__ void prerotate_kernel(const float4* __restrict__ in, float4* __restri
 // else the general solve followed by the cell-mass pass.
 template <typename Acc>
 static cudaError_t spectral_density_typed(const Ensemble& e, Acc* mass, float4* force,
-                                          void* scratch, cudaStream_t s) {
+                                          void* scratch, cudaStream_t s, int split) {
     if (!e.dft_tc && (e.g == 8 || e.g == 16)) {
-        if (use_split(e))
+        if (use_split(e, split))
             return e.g == 16 ? launch_split<16, Acc, true, false, true>(e, mass, force, s)
                              : launch_split<8, Acc, true, false, true>(e, mass, force, s);
         const int pairs = (e.k + 1) / 2;
@@ -855,16 +855,17 @@ static cudaError_t spectral_density_typed(const Ensemble& e, Acc* mass, float4* 
         if (e.g == 16) return go(spectral_fused3_kernel<16, Acc, true, false, true>, 16);
         return go(spectral_fused3_kernel<8, Acc, true, false, true>, 8);
     }
-    cudaError_t err = spectral_typed(e, mass, force, kFrameWorld, false, scratch, s);
+    cudaError_t err = spectral_typed(e, mass, force, kFrameWorld, false, scratch, s, split);
     if (err != cudaSuccess) return err;
     return launch_density_w(e, mass, force, s);
 }
 
 cudaError_t launch_spectral_density(const Ensemble& e, void* mass, float4* force, void* scratch,
-                                    cudaStream_t s) {
+                                    cudaStream_t s, int split) {
     if (e.mass_mode == 0)
-        return spectral_density_typed(e, static_cast<unsigned long long*>(mass), force, scratch, s);
-    return spectral_density_typed(e, static_cast<unsigned*>(mass), force, scratch, s);
+        return spectral_density_typed(e, static_cast<unsigned long long*>(mass), force, scratch, s,
+                                      split);
+    return spectral_density_typed(e, static_cast<unsigned*>(mass), force, scratch, s, split);
 }
 
 size_t spectral_scratch_bytes(const Ensemble& e) {
@@ -874,11 +875,12 @@ size_t spectral_scratch_bytes(const Ensemble& e) {
 }
 
 cudaError_t launch_spectral(const Ensemble& e, void* mass, float4* force, int frame,
-                            bool zero_mass, void* scratch, cudaStream_t s) {
+                            bool zero_mass, void* scratch, cudaStream_t s, int split) {
     if (e.mass_mode == 0)
         return spectral_typed(e, static_cast<unsigned long long*>(mass), force, frame, zero_mass,
-                              scratch, s);
-    return spectral_typed(e, static_cast<unsigned*>(mass), force, frame, zero_mass, scratch, s);
+                              scratch, s, split);
+    return spectral_typed(e, static_cast<unsigned*>(mass), force, frame, zero_mass, scratch, s,
+                          split);
 }
 
 cudaError_t launch_build_tables(int g, float world, float G, float* green, float* ktab,
