@@ -348,7 +348,7 @@ int mog_batch_destroy(mog_batch* b);
  * (simulation, grid group, particle chunk) / (simulation, particle chunk)
  * from a largest-first list until it runs out.  Otherwise (or with
  * work_queue = 0) each simulation's three kernels run on their own branch.
- * deposit_chunk: particles per deposit tile (0 = 262144; else >= 1024).
+ * deposit_chunk: particles per deposit tile (0 = 393216; else >= 1024).
  * deposit_split: 1 = u64 grids keep only their high words in the work-queue
  * deposit's shared memory at g = 8 and 16 too (twice the grids per tile;
  * pays when every mass has a zero fixed-point low half, which then needs no

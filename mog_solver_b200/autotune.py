@@ -105,7 +105,7 @@ def autotune_batch(batch, reps: int = 3, cache: Path | None = CACHE, force: bool
         return table[key]
     saved = [(s.pos.clone(), s.vel.clone()) for s in batch.sims]
     cands = [dict(work_queue=1, deposit_chunk=c, deposit_split=sp)
-             for sp in (0, 1) for c in (65536, 131072, 262144)]
+             for sp in (0, 1) for c in (131072, 262144, 393216)]
     cands.append(dict(work_queue=0, deposit_chunk=0, deposit_split=0))
     results = []
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -1612,7 +1612,7 @@ void build_tiles(const mog_batch* b, const int64_t* n, int64_t chunk,
 int capture_queue_step(mog_batch* b, float* const* pos4, float* const* vel4, const int64_t* n,
                        const float* dt_eff, mog_batch::Entry& entry, cudaGraph_t* graph) {
     const int count = (int)b->sims.size();
-    const int64_t chunk = b->tuning.deposit_chunk > 0 ? b->tuning.deposit_chunk : 262144;
+    const int64_t chunk = b->tuning.deposit_chunk > 0 ? b->tuning.deposit_chunk : 393216;
     std::vector<mog::DepositTile> dep;
     std::vector<mog::GatherTile> gat;
     build_tiles(b, n, chunk, dep, gat);
