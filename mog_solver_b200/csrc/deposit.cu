@@ -609,13 +609,15 @@ __global__ void __launch_bounds__(256) deposit_global_kernel(const float4* __res
 // Particle chunks per grid group.  Every chunk costs one histogram flush
 // (gpc * g^3 global atomics), so chunks stay few, but the CTAs (groups x
 // chunks, `per_sm` resident per SM) should fill whole waves: one wave for
-// up to 4 groups (each SM flushes once), 2 for up to 16, 3 for up to 64, 5
-// beyond (measured on k = 16 / 32 / 240, g = 16: k = 32 in 4 groups takes
-// 49 us in one wave against 53 in two; in 8 groups, 60 us in two against
-// 62 in one; k = 240 in 20 groups 264 us in three against 269 in five and
-// 273 in two).  At least 2048 particles per chunk.
+// up to 4 groups (each SM flushes once), 2 for up to 16, 3 for up to 64, 13
+// beyond (measured on k = 16 / 32 / 240, g = 16, and k = 240, g = 32: k = 32
+// in 4 groups takes 49 us in one wave against 53 in two; in 8 groups, 60 us
+// in two against 62 in one; k = 240 in 20 groups 264 us in three against
+// 269 in five and 273 in two; k = 240 at g = 32, one grid a group, 706 us in
+// 13 waves against 748 in five and 721 to 740 in 10 to 26).  At least 2048
+// particles per chunk.
 static int auto_chunks(int64_t n, int64_t groups, int per_sm) {
-    const int64_t waves = groups <= 4 ? 1 : (groups <= 16 ? 2 : (groups <= 64 ? 3 : 5));
+    const int64_t waves = groups <= 4 ? 1 : (groups <= 16 ? 2 : (groups <= 64 ? 3 : 13));
     const int64_t c = waves * num_sms() * per_sm / std::max<int64_t>(groups, 1);
     const int64_t max_c = (n + 2047) / 2048;
     return (int)std::max<int64_t>(1, std::min<int64_t>(c, max_c));
